@@ -1,0 +1,341 @@
+"""Benchmark: unsteady BDF2 dual-time cylinder (181x181 O-grid, Re=100,
+dt=0.2, rotational kick 0.5 until t=2, outflow far field, <=5 Newton
+iterations per step, GMRES(30) with 2x2 block Jacobi).
+
+One "step" is one BDF2 physical time step through the device solver.
+``value`` = whole-job BDF2 steps/s with the state resident in HBM (headline:
+FP32 Krylov inside FP64 Newton / defect correction); the FP64-Krylov form is
+measured beside it.  ``e2e`` is the same metric through the public Python API
+with the state copied host->device and device->host every step (pinned host
+buffers).  ``--impl reference`` times the CPU restatement of the reference
+path (C assembly + SuperLU direct solves) on the host cores.
+
+Multi-GPU (``torchrun --nproc-per-node N``): independent replicas, one per
+GPU, no collective on the data path; timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+IMAX = JMAX = 181
+WORKLOAD = dict(re=100.0, steady=False, dt_phys=0.2, rot_speed=0.5, rot_until=2.0,
+                farfield_bc="outflow")
+SOLVER = dict(ksp_restart=30, ksp_rtol=1e-10, krylov_max_it=3000, pseudo_tol=1e-10,
+              max_pseudo_iter=5, precond="bjacobi")
+METRIC = "BDF2 steps/s, 181x181 cylinder O-grid Re=100 dt=0.2 (<=5 Newton, GMRES(30)+block-Jacobi)"
+L2_FLUSH_BYTES = 256 << 20
+SPMV_BYTES_PER_NNZ = {"fp64": 8 + 4, "fp32": 4 + 4}
+
+
+# ------------------------------------------------------------------ ranks
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def init_dist(world, backend):
+    import torch.distributed as dist
+    if world > 1 and not dist.is_initialized():
+        import datetime
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed
+    region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return self.summary()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return float("nan")
+        sm = np.array([num(r[1]) for r in self.rows])
+        smax = np.nanmax([num(r[2]) for r in self.rows])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if r[5 + k].lower().startswith("active")})
+        load = sm[sm > 0.5 * smax] if np.isfinite(smax) else sm
+        med = float(np.median(load if load.size else sm))
+        return {"sm_mhz": med, "sm_max_mhz": float(smax), "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------- our arm
+def make_solver(v, xg, yg, precision):
+    cfg = v.Config(verbose=False, write_csv=False, write_xdmf=False, compute_forces=False,
+                   raise_on_linear_failure=False, precision=precision, **WORKLOAD, **SOLVER)
+    return v.Solver(cfg, mesh=(xg, yg))
+
+
+def flush_l2(torch, buf):
+    buf.add_(1.0)
+
+
+def timed_steps(torch, s, times, k0, K, flush_buf):
+    """K BDF2 steps on the solver's stream, each preceded by an L2 flush
+    (outside the events); returns (per-step ms list, Newton its, Krylov its)."""
+    import ctypes
+    from vorti2d_b200 import _lib
+    sp = ctypes.c_void_p()
+    _lib.check(_lib.lib().v2d_solver_stream(s.dev.h, ctypes.byref(sp)))
+    stream = torch.cuda.ExternalStream(sp.value)
+    ms, newton, krylov = [], 0, 0
+    for m in range(K):
+        flush_l2(torch, flush_buf)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, it, _ = s.advance(times[k0 + m])
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        newton += it
+        krylov += s.newton_log[-1][2]
+    return ms, newton, krylov
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import vorti2d_b200 as v
+    from vorti2d_b200 import _lib
+    torch.cuda.set_device(local_rank)
+    xg, yg = v.generate_cylinder(IMAX, JMAX)
+    flush_buf = torch.zeros(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    K, W = args.steps, args.warmup
+    results = {}
+    legs = ["mixed", "fp64"] if args.precision == "both" else [args.precision]
+    launches = {}
+    for prec in legs:
+        s = make_solver(v, xg, yg, prec)
+        times = s.times()
+        for m in range(W):
+            s.advance(times[m])
+        barrier(world)
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local_rank).start() if prec == legs[0] else None
+        c0 = _lib.lib().v2d_launch_count()
+        t0 = time.perf_counter()
+        ms, nit, kit = timed_steps(torch, s, times, W, K, flush_buf)
+        wall = time.perf_counter() - t0
+        c1 = _lib.lib().v2d_launch_count()
+        if clocks is not None:
+            results["clocks"] = clocks.stop()
+        torch.cuda.synchronize()
+        barrier(world)
+        tot_ms = max_over_ranks(sum(ms), world, "cuda")
+        fc = s.force_coeffs()
+        results[prec] = dict(ms_per_step=tot_ms / K, newton=nit / K, krylov=kit / K,
+                             cd=fc.cd, cl=fc.cl, wall_s=wall, t_end=times[W + K - 1])
+        launches[prec] = c1 - c0
+        if prec == legs[0]:
+            # dominant kernel (SpMV of the Krylov loop), timed alone after L2 flushes
+            ms_spmv = _spmv_time(_lib, s, fp32=(prec == "mixed"))
+            results["spmv_ms"] = ms_spmv
+            import ctypes
+            nnz = ctypes.c_longlong()
+            _lib.check(_lib.lib().v2d_solver_nnz(s.dev.h, ctypes.byref(nnz)))
+            results["nnz"] = nnz.value
+            # e2e: the public API with host state every step
+            results["e2e"] = _e2e(torch, v, s, times, W + K, min(K, 5))
+        s.close()
+    return results, launches
+
+
+def _spmv_time(_lib, s, fp32, reps=20):
+    import ctypes
+    out = ctypes.c_double()
+    _lib.check(_lib.lib().v2d_solver_time_spmv(s.dev.h, int(fp32), reps, L2_FLUSH_BYTES,
+                                               ctypes.byref(out)))
+    return out.value
+
+
+def _e2e(torch, v, s, times, k0, K):
+    """Steps through Solver.set_state / advance / state readback with pinned
+    host buffers; the copies are inside the timed region."""
+    N = s.ndof
+    host = [torch.empty(N, dtype=torch.float64, pin_memory=True) for _ in range(4)]
+    st = s.dev.get_state()
+    for h, a in zip(host, st):
+        h.numpy()[:] = a
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for m in range(K):
+        s.set_state(*[h.numpy() for h in host])
+        s.advance(times[k0 + m])
+        out = s.dev.get_state()
+        for h, a in zip(host, out):
+            h.numpy()[:] = a
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    return dict(steps_per_s=K / dt, h2d=4 * N * 8, d2h=4 * N * 8, steps=K)
+
+
+# ------------------------------------------------------------ CPU arm
+def run_cpu_reference(steps):
+    """CPU restatement of the reference path (C assembly restating
+    vorti2d_core.f90 + SuperLU direct solve standing in for MUMPS),
+    single-threaded like one reference rank."""
+    from oracle import oracle as O
+    xg, yg = O.generate_cylinder(IMAX, JMAX)
+    s = O.OracleSolver(xg, yg, pseudo_tol=SOLVER["pseudo_tol"],
+                       max_pseudo_iter=SOLVER["max_pseudo_iter"], **WORKLOAD)
+    times = s.times()
+    t0 = time.perf_counter()
+    for m in range(steps):
+        s.advance(times[m])
+    dt = time.perf_counter() - t0
+    return steps / dt, dt, steps
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    args = ap.parse_args()
+    rank, world, local_rank = dist_env()
+
+    if args.impl == "reference":
+        # CPU restatement on rank 0 only; other ranks exit without work
+        if rank != 0:
+            return
+        K = max(1, min(args.steps, 3))
+        for _ in range(min(args.warmup, 0)):
+            pass
+        val, dt, n = run_cpu_reference(K)
+        line = {
+            "metric": METRIC, "value": val, "unit": "steps/s", "n_gpus": args.gpus,
+            "steps": n, "warmup": 0, "ms_per_step": 1e3 * dt / n, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "unsteady BDF2 cylinder 181x181 Re=100 dt=0.2 kick 0.5<=2 outflow",
+                       "solver": "C restatement of vorti2d_core.f90 + scipy SuperLU (MUMPS stand-in)"},
+            "cpu_baseline": {"value": val, "unit": "steps/s", "cores": 1, "kind": "port",
+                             "sample": f"{n} BDF2 steps from t=0 (bounded sample)"},
+            "e2e": {"value": val, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return
+
+    init_dist(world, "nccl")
+    res, launches = run_ours(args, rank, world, local_rank)
+    head = "mixed" if "mixed" in res else args.precision
+    ms_head = res[head]["ms_per_step"]
+    value = world * 1000.0 / ms_head
+    if rank != 0:
+        return
+    cpu = None
+    if world == 1 and args.cpu_steps > 0:
+        cval, cdt, cn = run_cpu_reference(args.cpu_steps)
+        cpu = {"value": cval, "unit": "steps/s", "cores": 1, "kind": "port",
+               "sample": f"{cn} BDF2 steps from t=0 of the same workload (C assembly + SuperLU)"}
+    nnz = res["nnz"]
+    n = 2 * IMAX * JMAX
+    prec_key = "fp32" if head == "mixed" else "fp64"
+    bytes_spmv = nnz * SPMV_BYTES_PER_NNZ[prec_key] + (n + 1) * 4 + 2 * n * (4 if prec_key == "fp32" else 8)
+    with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+        peaks = json.load(fh)
+    achieved = bytes_spmv / (res["spmv_ms"] * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_head,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32-krylov/f64" if head == "mixed" else "f64", "data": "synthetic",
+        "config": {"workload": "unsteady BDF2 cylinder 181x181 Re=100 dt=0.2 kick 0.5<=2 outflow",
+                   "precision": head, "newton_max": 5, "krylov": "GMRES(30)+2x2 block Jacobi",
+                   "l2": "flushed (256 MiB write) before every timed step",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": world * res["e2e"]["steps_per_s"], "unit": "steps/s",
+                "h2d_bytes_per_step": res["e2e"]["h2d"], "d2h_bytes_per_step": res["e2e"]["d2h"]},
+        "roofline": {"bound": "hbm", "kernel": f"spmv_csr_{prec_key}",
+                     "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "bytes_per_launch": bytes_spmv, "ms_per_launch": res["spmv_ms"]},
+        "cpu_baseline": cpu,
+        "gpu_launches": int(launches.get(head, 0)),
+        "clocks": res.get("clocks"),
+        "legs": {p: res[p] for p in ("mixed", "fp64") if p in res},
+    }
+    if "mixed" in res and "fp64" in res:
+        line["mixed_vs_fp64_speedup"] = res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"]
+        line["dCd_mixed_vs_fp64"] = abs(res["mixed"]["cd"] - res["fp64"]["cd"])
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,249 @@
+/*
+ * vorti2d_b200 -- C ABI of the B200-native vorti2d hot path
+ * (libvorti2d_b200.so, sm_100a).
+ *
+ * Every entry point returns an int status (V2D_OK = 0, negative on error) and
+ * leaves a message for v2d_last_error().  No torch or C++ types cross this
+ * boundary: plain pointers, sizes and POD structs only.
+ *
+ * Three groups:
+ *  1. The kernel seam: drop-ins for the f2py module `vorti2d.core`
+ *     (reference src/fortran/vorti2d_core.f90).  Host pointers in and out;
+ *     the work runs on the current CUDA device.  `*_dev` variants take device
+ *     pointers and a cudaStream_t (passed as void*).
+ *  2. The linear-solver seam: drop-in for vorti2d.petsc_solver.MumpsSolver
+ *     (reference vorti2d/petsc_solver.py:37-132): COO in, canonical CSR on the
+ *     device, GMRES(m) solve, full solution out.
+ *  3. The device-resident Newton / BDF2 driver behind vorti2d.Config / run()
+ *     (reference vorti2d/solver.py:48-224): metrics, state, CSR, Krylov
+ *     workspace and forces all live in HBM behind an opaque handle.
+ *
+ * Threading: a handle is owned by one host thread at a time; different
+ * handles may be used concurrently from different threads.
+ */
+#ifndef VORTI2D_B200_H
+#define VORTI2D_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define V2D_OK 0
+#define V2D_EARG (-1)          /* bad argument (shape, range, null pointer) */
+#define V2D_ECAPACITY (-2)     /* caller buffer too small (e.g. maxnnz)      */
+#define V2D_ECUDA (-3)         /* CUDA runtime error                         */
+#define V2D_ENONFINITE (-4)    /* NaN/Inf detected in a result               */
+#define V2D_ENOTCONVERGED (-5) /* Krylov solve hit max iterations            */
+#define V2D_ETIMEOUT (-6)      /* a bounded device wait ran out              */
+#define V2D_EBREAKDOWN (-7)    /* singular 2x2 block / Krylov breakdown      */
+#define V2D_ENOMEM (-8)        /* device allocation failed                   */
+
+const char *v2d_last_error(void);
+int v2d_version(void);
+/* Number of kernels launched by this library so far (CUDA-graph replays
+ * count their kernel nodes).  Measurement aid; no reference counterpart. */
+long long v2d_launch_count(void);
+
+/* ------------------------------------------------- 1. kernel seam (_core) */
+
+/* Replaces vorti2d_core.node_neighbors (vorti2d_core.f90:33-61).
+ * 1-based (i, j) -> out[9] = k, e, w, n, s, ne, nw, se, sw (1-based). */
+int v2d_node_neighbors(int i, int j, int imax, int *out9);
+
+/* Replaces vorti2d_core.compute_metrics (vorti2d_core.f90:66-189; called at
+ * vorti2d/solver.py:72-74).  xg, yg: Fortran-ordered (imax, jmax) doubles, i.e.
+ * element (i, j) at [(i-1) + imax*(j-1)].  Each output has imax*jmax doubles in
+ * pointer order k = imax*(j-1)+i.  Outputs in f2py tuple order: jac, alfa,
+ * beta, gama, pmet, qmet, detadx, detady, xphys, yphys. */
+int v2d_compute_metrics(int imax, int jmax, double dksi, double deta,
+                        const double *xg, const double *yg,
+                        double *jac, double *alfa, double *beta, double *gama,
+                        double *pmet, double *qmet, double *detadx, double *detady,
+                        double *xphys, double *yphys);
+
+/* Replaces vorti2d_core.compute_metrics_local (vorti2d_core.f90:392-495;
+ * called at vorti2d/dist_solver.py:92-93).  Ghosted local block gxm x jmax
+ * (Fortran order), owned 1-based columns [il0, il1]; outputs gxm*jmax, zero
+ * outside the owned columns except xphys/yphys. */
+int v2d_compute_metrics_local(int gxm, int jmax, int il0, int il1, double dksi,
+                              double deta, const double *xgl, const double *ygl,
+                              double *jac, double *alfa, double *beta, double *gama,
+                              double *pmet, double *qmet, double *detadx,
+                              double *detady, double *xphys, double *yphys);
+
+/* Replaces vorti2d_core.assemble_coo (vorti2d_core.f90:219-383; called at
+ * vorti2d/solver.py:121-127).  Rows [r0, r1) of the field-blocked 2N system
+ * (psi rows [0,N), ome rows [N,2N)).  COO triplets are written in the
+ * reference's push order (0-based); *nnz receives the count; bvec has r1-r0
+ * entries.  Unlike the reference (whose push has no bound check), a maxnnz
+ * that is too small returns V2D_ECAPACITY and writes no triplet. */
+int v2d_assemble_coo(int imax, int jmax, double re, double invdtau, double inv2dt,
+                     double urot, double dksi, double deta, const double *jac,
+                     const double *alfa, const double *beta, const double *gama,
+                     const double *pmet, const double *qmet, const double *detadx,
+                     const double *detady, const double *xphys, const double *yphys,
+                     const double *psi, const double *ome, const double *omeold,
+                     const double *omeoldold, int r0, int r1, int maxnnz, int ff_bc,
+                     double ca, double sa, int *coo_i, int *coo_j, double *coo_v,
+                     int *nnz, double *bvec);
+
+/* Replaces vorti2d_core.assemble_coo_local (vorti2d_core.f90:510-661; called
+ * at vorti2d/dist_solver.py:310-317).  Local ghosted arrays of gxm*jmax
+ * doubles, lg[2*gxm*jmax] the 0-based global dof of (local node, component).
+ * Owned rows are [r0, r0+nloc); bvec has nloc entries. */
+int v2d_assemble_coo_local(int gxm, int jmax, int il0, int il1, double re,
+                           double invdtau, double inv2dt, double urot, double dksi,
+                           double deta, const double *jac, const double *alfa,
+                           const double *beta, const double *gama, const double *pmet,
+                           const double *qmet, const double *detadx, const double *detady,
+                           const double *xphys, const double *yphys, const double *psi,
+                           const double *ome, const double *omeold,
+                           const double *omeoldold, int r0, int nloc, const int *lg,
+                           int maxnnz, int ff_bc, double ca, double sa, int *coo_i,
+                           int *coo_j, double *coo_v, int *nnz, double *bvec);
+
+/* Device-pointer form of v2d_compute_metrics (same layouts; stream may be 0). */
+int v2d_compute_metrics_dev(int imax, int jmax, double dksi, double deta,
+                            const double *d_xg, const double *d_yg, double *const *d_out10,
+                            void *stream);
+
+/* Replaces vorti2d.forces.compute_force_coeffs (vorti2d/forces.py:82-194),
+ * computed on the device from host arrays of imax*jmax doubles.
+ * ref_length <= 0 selects the automatic body-diameter estimate.
+ * out10 = cd, cl, cm, cdp, cdf, clp, clf, cmp, cmf, ref_length. */
+int v2d_force_coeffs(int imax, int jmax, double re, double dksi, double deta,
+                     const double *beta, const double *gama, const double *detadx,
+                     const double *detady, const double *xphys, const double *yphys,
+                     const double *ome, double ref_length, double x0, double y0,
+                     double *out10);
+
+/* ------------------------------------------------ Krylov solver parameters */
+#define V2D_PC_NONE 0
+#define V2D_PC_BJACOBI 1   /* 2x2 (psi, ome) node blocks                     */
+#define V2D_PC_MG 2        /* aggregation multigrid, 2x2-block Jacobi smoothing */
+
+#define V2D_PREC_FP64 0    /* FP64 Krylov                                     */
+#define V2D_PREC_MIXED 1   /* FP32 SpMV/PC/Krylov vectors, FP64 Gram-Schmidt
+                              sums, FP64 outer defect correction              */
+
+typedef struct {
+    int restart;          /* GMRES(m) restart length                  (30)   */
+    int max_it;           /* max Krylov iterations per solve          (5000) */
+    double rtol;          /* relative residual tolerance              (1e-10)*/
+    double atol;          /* absolute residual tolerance              (1e-50)*/
+    int precond;          /* V2D_PC_*                                         */
+    int precision;        /* V2D_PREC_*                                       */
+    double inner_rtol;    /* mixed: FP32 GMRES tolerance per correction (1e-5)*/
+    int dc_max_it;        /* mixed: max defect-correction passes       (20)  */
+    int mg_levels;        /* multigrid: max levels (0 = auto)                 */
+    int mg_smooth;        /* multigrid: smoothing sweeps per side      (2)   */
+    double mg_omega;      /* multigrid: Jacobi damping                 (0.7) */
+} v2d_krylov_params;
+
+void v2d_krylov_defaults(v2d_krylov_params *p);
+
+typedef struct {
+    int iterations;       /* Krylov iterations (all restarts / corrections) */
+    int restarts;
+    int corrections;      /* mixed: outer defect-correction passes          */
+    int converged;        /* 1 if the tolerance was met                     */
+    double res0;          /* ||b||                                          */
+    double res;           /* final true residual ||b - A x|| (FP64)         */
+} v2d_lin_stats;
+
+/* ----------------------------------------- 2. linear-solver seam (MumpsSolver) */
+typedef struct v2d_linsys v2d_linsys;
+
+/* Replaces MumpsSolver(n) (vorti2d/petsc_solver.py:38-70).  block_layout:
+ * 0 point diagonal, 1 field-blocked 2x2 pairs (r, r+n/2), 2 interleaved
+ * 2x2 pairs (2q, 2q+1). */
+int v2d_linsys_create(int n, int block_layout, const v2d_krylov_params *p,
+                      v2d_linsys **out);
+/* Replaces MumpsSolver.assemble (vorti2d/petsc_solver.py:76-95): the first
+ * call fixes the canonical CSR pattern (rows sorted, columns sorted,
+ * duplicates summed); later calls must repeat the same (i, j) sequence and
+ * only refresh the values. */
+int v2d_linsys_assemble(v2d_linsys *s, const int *coo_i, const int *coo_j,
+                        const double *coo_v, long long nnz, const double *b);
+/* Replaces MumpsSolver.solve (vorti2d/petsc_solver.py:97-115). */
+int v2d_linsys_solve(v2d_linsys *s, double *x, v2d_lin_stats *st);
+/* Canonical CSR export (for parity checks): sizes n+1, nnz, nnz. */
+int v2d_linsys_nnz(const v2d_linsys *s, long long *nnz);
+int v2d_linsys_csr(const v2d_linsys *s, int *indptr, int *indices, double *data);
+int v2d_linsys_destroy(v2d_linsys *s);
+
+/* -------------------------------------------- 3. device-resident driver */
+typedef struct v2d_solver v2d_solver;
+
+typedef struct {
+    double re;            /* Reynolds number (vorti2d/config.py:15)          */
+    double invdtau;       /* 1/dtau, 0 for pure Newton (config.py:139-140)   */
+    double inv2dt;        /* 1/(2 dt), 0 when steady (config.py:142-144)     */
+    double ca, sa;        /* cos/sin of the angle of attack (config.py:146-150) */
+    int ff_bc;            /* 0 dirichlet, 1 outflow, 2 outflow_psi           */
+    v2d_krylov_params krylov;
+} v2d_solver_params;
+
+typedef struct {
+    int newton_iters;
+    int krylov_iters;     /* summed over the Newton iterations             */
+    int corrections;
+    double res;           /* reference measure ||dq||_2 / (2N)              */
+    double lin_res_max;   /* worst relative linear residual of the solves  */
+} v2d_newton_info;
+
+/* Uploads the mesh (Fortran-ordered (imax, jmax) like v2d_compute_metrics),
+ * evaluates the metrics on the device, builds the canonical CSR pattern and
+ * initialises the state as vorti2d/solver.py:103-114 does. */
+int v2d_solver_create(int imax, int jmax, const double *xg, const double *yg,
+                      const v2d_solver_params *p, v2d_solver **out);
+int v2d_solver_destroy(v2d_solver *s);
+int v2d_solver_set_params(v2d_solver *s, const v2d_solver_params *p);
+/* State transfer (host pointers, N = imax*jmax doubles each, pointer order). */
+int v2d_solver_set_state(v2d_solver *s, const double *psi, const double *ome,
+                         const double *omeold, const double *omeoldold);
+int v2d_solver_get_state(v2d_solver *s, double *psi, double *ome, double *omeold,
+                         double *omeoldold);
+/* The 10 metric arrays in f2py order (host pointers, N doubles each). */
+int v2d_solver_get_metrics(v2d_solver *s, double *const *out10);
+/* One Newton iteration (vorti2d/solver.py:117-134): assemble on the device,
+ * GMRES solve, q += dq; *res = ||dq||_2 / (2N). */
+int v2d_solver_newton(v2d_solver *s, double urot, double *res, v2d_lin_stats *st);
+/* Inner loop (vorti2d/solver.py:136-145): iterate while res > pseudo_tol and
+ * it < max_iter. */
+int v2d_solver_pseudo_solve(v2d_solver *s, double urot, double pseudo_tol, int max_iter,
+                            v2d_newton_info *info);
+/* BDF2 history shift omeoldold <- omeold <- ome (vorti2d/solver.py:186-188). */
+int v2d_solver_shift_history(v2d_solver *s);
+/* One physical step = pseudo_solve + (unsteady) history shift. */
+int v2d_solver_step(v2d_solver *s, double urot, double pseudo_tol, int max_iter,
+                    int unsteady, v2d_newton_info *info);
+/* Force coefficients (vorti2d/forces.py:82-194) of the current state on the
+ * device.  ref_length <= 0 selects the automatic body-diameter estimate.
+ * out10 = cd, cl, cm, cdp, cdf, clp, clf, cmp, cmf, ref_length. */
+int v2d_solver_forces(v2d_solver *s, double re, double ref_length, double x0, double y0,
+                      double *out10);
+/* Current system (after the last assembly): canonical CSR of the 2N system
+ * and its right-hand side.  Sizes: 2N+1, nnz, nnz, 2N. */
+int v2d_solver_nnz(const v2d_solver *s, long long *nnz);
+int v2d_solver_assemble(v2d_solver *s, double urot);
+int v2d_solver_export_system(v2d_solver *s, int *indptr, int *indices, double *data,
+                             double *b);
+/* Device pointers of the state (psi, ome, omeold, omeoldold) for zero-copy
+ * interop (e.g. torch tensors via __cuda_array_interface__). */
+int v2d_solver_state_ptrs(v2d_solver *s, double **psi, double **ome, double **omeold,
+                          double **omeoldold);
+/* Measurement aid (no reference counterpart): average duration in ms of
+ * `reps` launches of the Krylov SpMV kernel on the current system (FP32
+ * values if fp32 != 0), each preceded by a write of flush_bytes to evict L2;
+ * CUDA events on the handle's stream. */
+int v2d_solver_time_spmv(v2d_solver *s, int fp32, int reps, long long flush_bytes,
+                         double *ms_avg);
+/* The stream the handle's kernels run on (cudaStream_t as void*). */
+int v2d_solver_stream(v2d_solver *s, void **stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VORTI2D_B200_H */

@@ -1,0 +1,184 @@
+// Newton-system assembly into a fixed canonical CSR (built with -fmad=false).
+//
+// The reference assembles COO triplets every iteration and converts them to
+// CSR on the host (vorti2d/petsc_solver.py:76-95); here the pattern is built
+// once per mesh on the device and each Newton iteration writes values straight
+// into their canonical slots: one thread per node computes the psi row and
+// the ome row (vorti2d_core.f90:247-381), places each entry at
+// rowptr[row] + (rank of its column in the row), writes b, the optional FP32
+// copy and the 2x2 (psi_k, ome_k) block inverse used by block Jacobi.
+#include "v2d_internal.cuh"
+#include "v2d_stencil.cuh"
+
+namespace v2d {
+
+static Fields fields_of(const GridDev &g)
+{
+    Fields f;
+    f.jac = g.met[0]; f.alfa = g.met[1]; f.beta = g.met[2]; f.gama = g.met[3];
+    f.pmet = g.met[4]; f.qmet = g.met[5]; f.detadx = g.met[6]; f.detady = g.met[7];
+    f.xphys = g.met[8]; f.yphys = g.met[9];
+    f.psi = g.psi; f.ome = g.ome; f.omeold = g.omeold; f.omeoldold = g.omeoldold;
+    return f;
+}
+
+__global__ void metrics_grid_kernel(int imax, int jmax, double dksi, double deta,
+                                    const double *__restrict__ x, const double *__restrict__ y,
+                                    double *jac, double *alfa, double *beta, double *gama,
+                                    double *pmet, double *qmet, double *detadx, double *detady,
+                                    double *xp, double *yp)
+{
+    const int N = imax * jmax;
+    V2D_GRID_STRIDE(t, N)
+    {
+        int K = (int)t;
+        int j = K / imax, i = K - j * imax;
+        Nbr nb = wrap_neighbors(i, j, imax);
+        MetricOut m = metrics_at(x, y, K, nb.e, nb.w, j, jmax, imax, dksi, deta);
+        jac[K] = m.jac; alfa[K] = m.alfa; beta[K] = m.beta; gama[K] = m.gama;
+        pmet[K] = m.pmet; qmet[K] = m.qmet; detadx[K] = m.detadx; detady[K] = m.detady;
+        xp[K] = x[K]; yp[K] = y[K];
+    }
+}
+
+int launch_metrics(GridDev &g, cudaStream_t s)
+{
+    metrics_grid_kernel<<<grid_for(g.N, 256), 256, 0, s>>>(
+        g.imax, g.jmax, g.dksi, g.deta, g.x, g.y, g.met[0], g.met[1], g.met[2], g.met[3],
+        g.met[4], g.met[5], g.met[6], g.met[7], g.met[8], g.met[9]);
+    V2D_CUDA_TRY(cudaGetLastError());
+    return V2D_OK;
+}
+
+__global__ void pattern_count(GlobalTopo T, Coeffs c, Fields f, int *cnt)
+{
+    V2D_GRID_STRIDE(t, 2 * T.N)
+    {
+        int r = (int)t;
+        cnt[r] = r < T.N ? psi_row_count(T, c, f, r) : ome_row_count(T, c, f, r - T.N);
+    }
+}
+
+__global__ void pattern_fill(GlobalTopo T, Coeffs c, Fields f, const int *__restrict__ rowptr,
+                             int *colind)
+{
+    V2D_GRID_STRIDE(t, 2 * T.N)
+    {
+        int r = (int)t;
+        int col[kOmeMax];
+        int n = r < T.N ? psi_row<false>(T, c, f, r, col, nullptr, nullptr)
+                        : ome_row<false>(T, c, f, r - T.N, col, nullptr, nullptr);
+        int base = rowptr[r];
+        for (int e = 0; e < n; ++e) colind[base + col_rank<kOmeMax>(col, n, e)] = col[e];
+    }
+}
+
+int build_pattern(GridDev &g, const AsmParams &p, cudaStream_t s)
+{
+    GlobalTopo T{g.imax, g.jmax, g.N};
+    Coeffs c{p.re, p.invdtau, p.inv2dt, p.urot, g.dksi, g.deta, p.ca, p.sa, p.ff_bc};
+    Fields f = fields_of(g);
+    DevBuf<int> scratch;
+    V2D_TRY(scratch.alloc(scan_scratch_ints(g.n) + 1, s));
+    pattern_count<<<grid_for(g.n, 256), 256, 0, s>>>(T, c, f, g.rowptr);
+    V2D_CUDA_TRY(cudaGetLastError());
+    V2D_TRY(exclusive_scan_i32(g.rowptr, g.rowptr, g.n, g.rowptr + g.n, scratch.p, s));
+    int nnz = 0;
+    V2D_CUDA_TRY(cudaMemcpyAsync(&nnz, g.rowptr + g.n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(s));
+    g.nnz = nnz;
+    if (g.colind) cudaFree(g.colind);
+    if (g.val) cudaFree(g.val);
+    if (g.val32) cudaFree(g.val32);
+    g.colind = nullptr; g.val = nullptr; g.val32 = nullptr;
+    V2D_CUDA_TRY(cudaMalloc(&g.colind, (size_t)nnz * sizeof(int)));
+    V2D_CUDA_TRY(cudaMalloc(&g.val, (size_t)nnz * sizeof(double)));
+    V2D_CUDA_TRY(cudaMalloc(&g.val32, (size_t)nnz * sizeof(float)));
+    pattern_fill<<<grid_for(g.n, 256), 256, 0, s>>>(T, c, f, g.rowptr, g.colind);
+    V2D_CUDA_TRY(cudaGetLastError());
+    return V2D_OK;
+}
+
+// One thread per node: psi row K and ome row N+K.
+template <bool W32>
+__global__ void __launch_bounds__(128) assemble_newton(GlobalTopo T, Coeffs c, Fields f,
+                                                       const int *__restrict__ rowptr,
+                                                       double *__restrict__ val,
+                                                       float *__restrict__ val32,
+                                                       double *__restrict__ b,
+                                                       double *__restrict__ dinv,
+                                                       float *__restrict__ dinv32, int *flag)
+{
+    const int N = T.N;
+    V2D_GRID_STRIDE(t, N)
+    {
+        const int K = (int)t;
+        int col[kOmeMax];
+        double v[kOmeMax];
+        double bk;
+        double a00 = 0, a01 = 0, a10 = 0, a11 = 0;
+        // psi row
+        int n = psi_row<true>(T, c, f, K, col, v, &bk);
+        int base = rowptr[K];
+#pragma unroll
+        for (int e = 0; e < kPsiMax; ++e) {
+            if (e < n) {
+                int slot = base + col_rank<kPsiMax>(col, n, e);
+                val[slot] = v[e];
+                if (W32) val32[slot] = (float)v[e];
+                if (col[e] == K) a00 += v[e];
+                if (col[e] == N + K) a01 += v[e];
+            }
+        }
+        b[K] = bk;
+        // ome row
+        n = ome_row<true>(T, c, f, K, col, v, &bk);
+        base = rowptr[N + K];
+#pragma unroll
+        for (int e = 0; e < kOmeMax; ++e) {
+            if (e < n) {
+                int slot = base + col_rank<kOmeMax>(col, n, e);
+                val[slot] = v[e];
+                if (W32) val32[slot] = (float)v[e];
+                if (col[e] == K) a10 += v[e];
+                if (col[e] == N + K) a11 += v[e];
+            }
+        }
+        b[N + K] = bk;
+        // 2x2 block inverse for block Jacobi
+        double det = a00 * a11 - a01 * a10;
+        double i00, i01, i10, i11;
+        if (det != 0.0 && isfinite(det)) {
+            double r = 1.0 / det;
+            i00 = a11 * r; i01 = -a01 * r; i10 = -a10 * r; i11 = a00 * r;
+        } else {
+            i00 = i01 = i10 = i11 = 0.0;
+            atomicOr(flag, 1);
+        }
+        dinv[K] = i00; dinv[N + K] = i01; dinv[2 * N + K] = i10; dinv[3 * N + K] = i11;
+        if (W32) {
+            dinv32[K] = (float)i00; dinv32[N + K] = (float)i01;
+            dinv32[2 * N + K] = (float)i10; dinv32[3 * N + K] = (float)i11;
+        }
+        if (!isfinite(bk)) atomicOr(flag, 2);
+    }
+}
+
+int launch_assemble(GridDev &g, const AsmParams &p, bool want32, int *d_flag, cudaStream_t s)
+{
+    GlobalTopo T{g.imax, g.jmax, g.N};
+    Coeffs c{p.re, p.invdtau, p.inv2dt, p.urot, g.dksi, g.deta, p.ca, p.sa, p.ff_bc};
+    Fields f = fields_of(g);
+    int grid = grid_for(g.N, 128);
+    if (want32)
+        assemble_newton<true><<<grid, 128, 0, s>>>(T, c, f, g.rowptr, g.val, g.val32, g.b, g.dinv,
+                                                   g.dinv32, d_flag);
+    else
+        assemble_newton<false><<<grid, 128, 0, s>>>(T, c, f, g.rowptr, g.val, g.val32, g.b,
+                                                    g.dinv, g.dinv32, d_flag);
+    V2D_CUDA_TRY(cudaGetLastError());
+    count_launches(1);
+    return V2D_OK;
+}
+
+}  // namespace v2d

@@ -1,0 +1,445 @@
+// Device-resident Newton / BDF2 driver (reference vorti2d/solver.py:48-224).
+//
+// The whole replicated state -- mesh, metrics, psi/ome and their BDF2 history,
+// the canonical CSR Jacobian, right-hand side, block inverses and the Krylov
+// workspace -- lives in HBM behind one handle.  One Newton iteration is:
+// fused assembly kernel (values written into fixed CSR slots + b + 2x2 block
+// inverses), GMRES(m) on the device, and a fused update kernel
+// (q += dq and ||dq||_2 in one pass).  The host reads one scalar per Newton
+// iteration to decide whether to continue, as the reference's loop does.
+#include <cmath>
+#include <cstring>
+
+#include "v2d_internal.cuh"
+
+using namespace v2d;
+
+struct v2d_solver {
+    GridDev g;
+    v2d_solver_params prm{};
+    AsmParams ap{};
+    cudaStream_t s = nullptr;
+    KrylovWork *kw = nullptr;
+    double *delta = nullptr;      // Newton update (2N)
+    double *partial = nullptr;    // reduction partials
+    double *scal = nullptr;       // device scalars: [0] res, [1..10] forces
+    int *flag = nullptr;
+    unsigned int *counter = nullptr;
+    double *host = nullptr;       // pinned mirror of scal
+    int pattern_ff_bc = -1;
+    double pattern_ca = 0, pattern_sa = 0;
+    bool assembled = false;
+};
+
+namespace {
+
+constexpr int kUpdThreads = 256;
+constexpr int kUpdBlocks = 2 * kSMs;
+
+// q += dq (psi: dq[0,N), ome: dq[N,2N)); *res = ||dq||_2 / (2N)
+// (vorti2d/solver.py:132-134).  Deterministic two-stage sum.
+__global__ void __launch_bounds__(kUpdThreads) k_newton_update(int N, const double *__restrict__ dq,
+                                                               double *psi, double *ome,
+                                                               double *partial, unsigned int *counter,
+                                                               double *res)
+{
+    __shared__ double red[32];
+    __shared__ bool last;
+    double acc = 0.0;
+    V2D_GRID_STRIDE(t, N)
+    {
+        double a = dq[t], b = dq[N + t];
+        psi[t] += a;
+        ome[t] += b;
+        acc += a * a + b * b;
+    }
+    acc = block_sum(acc, red);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (last && threadIdx.x < 32) {
+        __threadfence();
+        double s = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) s += partial[b];
+        s = warp_sum(s);
+        if (threadIdx.x == 0) {
+            *res = sqrt(s) / (2.0 * (double)N);
+            *counter = 0;
+        }
+    }
+}
+
+// Far-field initial streamfunction (vorti2d/solver.py:103-112).
+__global__ void k_init_state(int imax, int jmax, double ca, double sa, const double *xp,
+                             const double *yp, double *psi, double *ome, double *omeold,
+                             double *omeoldold)
+{
+    const int N = imax * jmax;
+    V2D_GRID_STRIDE(t, N)
+    {
+        int K = (int)t;
+        psi[K] = K >= imax * (jmax - 1) ? ca * yp[K] - sa * xp[K] : 0.0;
+        ome[K] = 0.0;
+        omeold[K] = 0.0;
+        omeoldold[K] = 0.0;
+    }
+}
+
+int check_params(const v2d_solver_params *p)
+{
+    V2D_ARG_CHECK(p, "null params");
+    V2D_ARG_CHECK(p->re > 0.0 && std::isfinite(p->re), "re must be positive (got %g)", p->re);
+    V2D_ARG_CHECK(p->ff_bc >= 0 && p->ff_bc <= 2, "ff_bc must be 0, 1 or 2 (got %d)", p->ff_bc);
+    V2D_ARG_CHECK(p->krylov.restart >= 1 && p->krylov.restart <= 256,
+                  "krylov restart must be in [1, 256] (got %d)", p->krylov.restart);
+    V2D_ARG_CHECK(p->krylov.max_it >= 1, "krylov max_it must be >= 1");
+    V2D_ARG_CHECK(p->krylov.precond == V2D_PC_NONE || p->krylov.precond == V2D_PC_BJACOBI ||
+                      p->krylov.precond == V2D_PC_MG,
+                  "unknown preconditioner %d", p->krylov.precond);
+    V2D_ARG_CHECK(p->krylov.precision == V2D_PREC_FP64 || p->krylov.precision == V2D_PREC_MIXED,
+                  "unknown precision %d", p->krylov.precision);
+    return V2D_OK;
+}
+
+int ensure_pattern(v2d_solver *S)
+{
+    const v2d_solver_params &p = S->prm;
+    if (S->pattern_ff_bc == p.ff_bc && S->pattern_ca == p.ca && S->pattern_sa == p.sa) return V2D_OK;
+    AsmParams ap{p.re, p.invdtau, p.inv2dt, 0.0, p.ca, p.sa, p.ff_bc};
+    V2D_TRY(build_pattern(S->g, ap, S->s));
+    S->pattern_ff_bc = p.ff_bc;
+    S->pattern_ca = p.ca;
+    S->pattern_sa = p.sa;
+    S->assembled = false;
+    return V2D_OK;
+}
+
+int sync_flag(v2d_solver *S, const char *what)
+{
+    int f = 0;
+    V2D_CUDA_TRY(cudaMemcpyAsync(&f, S->flag, sizeof(int), cudaMemcpyDeviceToHost, S->s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    if (f & 2) {
+        set_error("%s: non-finite right-hand side (check the state / mesh)", what);
+        return V2D_ENONFINITE;
+    }
+    if (f & 1) {
+        set_error("%s: singular 2x2 (psi, ome) diagonal block", what);
+        return V2D_EBREAKDOWN;
+    }
+    return V2D_OK;
+}
+
+}  // namespace
+
+extern "C" void v2d_krylov_defaults(v2d_krylov_params *p)
+{
+    if (!p) return;
+    p->restart = 30;
+    p->max_it = 5000;
+    p->rtol = 1e-10;
+    p->atol = 1e-50;
+    p->precond = V2D_PC_BJACOBI;
+    p->precision = V2D_PREC_FP64;
+    p->inner_rtol = 1e-5;
+    p->dc_max_it = 20;
+    p->mg_levels = 0;
+    p->mg_smooth = 2;
+    p->mg_omega = 0.7;
+}
+
+extern "C" int v2d_solver_destroy(v2d_solver *S)
+{
+    if (!S) return V2D_OK;
+    if (S->s) cudaStreamSynchronize(S->s);
+    GridDev &g = S->g;
+    void *ptrs[] = {g.x, g.rowptr, g.colind, g.val, g.val32, g.b, g.dinv, g.dinv32,
+                    S->delta, S->partial, S->scal, S->flag, S->counter};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (S->host) cudaFreeHost(S->host);
+    krylov_destroy(S->kw);
+    if (S->s) cudaStreamDestroy(S->s);
+    delete S;
+    return V2D_OK;
+}
+
+extern "C" int v2d_solver_create(int imax, int jmax, const double *xg, const double *yg,
+                                 const v2d_solver_params *p, v2d_solver **out)
+{
+    V2D_ARG_CHECK(out && xg && yg, "solver_create: null pointer");
+    *out = nullptr;
+    V2D_ARG_CHECK(imax >= 4 && jmax >= 4, "mesh must be at least 4x4 (got %d x %d)", imax, jmax);
+    V2D_ARG_CHECK((long long)imax * jmax * 2 < (1LL << 31) / 16, "mesh too large for int32 CSR");
+    V2D_TRY(check_params(p));
+    v2d_solver *S = new v2d_solver();
+    S->prm = *p;
+    GridDev &g = S->g;
+    g.imax = imax; g.jmax = jmax; g.N = imax * jmax; g.n = 2 * g.N;
+    g.dksi = 1.0 / (imax - 1);
+    g.deta = 1.0 / (jmax - 1);
+    const size_t N = g.N;
+    cudaError_t e = cudaStreamCreateWithFlags(&S->s, cudaStreamNonBlocking);
+    // one slab: x, y, 10 metrics, 4 state arrays
+    if (e == cudaSuccess) e = cudaMalloc(&g.x, 16 * N * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&g.rowptr, (2 * N + 1) * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&g.b, 2 * N * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&g.dinv, 4 * N * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&g.dinv32, 4 * N * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&S->delta, 2 * N * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&S->partial, 4096 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&S->scal, 16 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&S->flag, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&S->counter, sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMallocHost(&S->host, 16 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemsetAsync(S->counter, 0, sizeof(unsigned int), S->s);
+    if (e != cudaSuccess) {
+        set_error("solver_create: allocation failed: %s", cudaGetErrorString(e));
+        v2d_solver_destroy(S);
+        return V2D_ENOMEM;
+    }
+    g.y = g.x + N;
+    for (int q = 0; q < 10; ++q) g.met[q] = g.x + (2 + q) * N;
+    g.psi = g.x + 12 * N; g.ome = g.x + 13 * N; g.omeold = g.x + 14 * N; g.omeoldold = g.x + 15 * N;
+    int st = V2D_OK;
+    // Fortran-ordered (imax, jmax) is already pointer order
+    if (cudaMemcpyAsync(g.x, xg, N * sizeof(double), cudaMemcpyHostToDevice, S->s) != cudaSuccess ||
+        cudaMemcpyAsync(g.y, yg, N * sizeof(double), cudaMemcpyHostToDevice, S->s) != cudaSuccess) {
+        set_error("solver_create: mesh upload failed");
+        st = V2D_ECUDA;
+    }
+    if (st == V2D_OK) st = launch_metrics(g, S->s);
+    if (st == V2D_OK) {
+        k_init_state<<<grid_for(g.N, 256), 256, 0, S->s>>>(imax, jmax, p->ca, p->sa, g.met[8],
+                                                            g.met[9], g.psi, g.ome, g.omeold,
+                                                            g.omeoldold);
+        if (cudaGetLastError() != cudaSuccess) st = V2D_ECUDA;
+    }
+    if (st == V2D_OK) st = ensure_pattern(S);
+    if (st == V2D_OK) st = krylov_create(&S->kw, g.n, p->krylov.restart, S->s);
+    if (st == V2D_OK && cudaStreamSynchronize(S->s) != cudaSuccess) {
+        set_error("solver_create: %s", cudaGetErrorString(cudaGetLastError()));
+        st = V2D_ECUDA;
+    }
+    if (st != V2D_OK) {
+        v2d_solver_destroy(S);
+        return st;
+    }
+    *out = S;
+    return V2D_OK;
+}
+
+extern "C" int v2d_solver_set_params(v2d_solver *S, const v2d_solver_params *p)
+{
+    V2D_ARG_CHECK(S, "null solver");
+    V2D_TRY(check_params(p));
+    const int old_m = S->prm.krylov.restart;
+    S->prm = *p;
+    V2D_TRY(ensure_pattern(S));
+    if (p->krylov.restart != old_m) {
+        V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+        krylov_destroy(S->kw);
+        S->kw = nullptr;
+        V2D_TRY(krylov_create(&S->kw, S->g.n, p->krylov.restart, S->s));
+    }
+    return V2D_OK;
+}
+
+extern "C" int v2d_solver_set_state(v2d_solver *S, const double *psi, const double *ome,
+                                    const double *omeold, const double *omeoldold)
+{
+    V2D_ARG_CHECK(S, "null solver");
+    const size_t bytes = (size_t)S->g.N * sizeof(double);
+    const double *src[4] = {psi, ome, omeold, omeoldold};
+    double *dst[4] = {S->g.psi, S->g.ome, S->g.omeold, S->g.omeoldold};
+    for (int q = 0; q < 4; ++q)
+        if (src[q]) V2D_CUDA_TRY(cudaMemcpyAsync(dst[q], src[q], bytes, cudaMemcpyHostToDevice, S->s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    S->assembled = false;
+    return V2D_OK;
+}
+
+extern "C" int v2d_solver_get_state(v2d_solver *S, double *psi, double *ome, double *omeold,
+                                    double *omeoldold)
+{
+    V2D_ARG_CHECK(S, "null solver");
+    const size_t bytes = (size_t)S->g.N * sizeof(double);
+    double *dst[4] = {psi, ome, omeold, omeoldold};
+    const double *src[4] = {S->g.psi, S->g.ome, S->g.omeold, S->g.omeoldold};
+    for (int q = 0; q < 4; ++q)
+        if (dst[q]) V2D_CUDA_TRY(cudaMemcpyAsync(dst[q], src[q], bytes, cudaMemcpyDeviceToHost, S->s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    return V2D_OK;
+}
+
+extern "C" int v2d_solver_get_metrics(v2d_solver *S, double *const *out10)
+{
+    V2D_ARG_CHECK(S && out10, "null pointer");
+    const size_t bytes = (size_t)S->g.N * sizeof(double);
+    for (int q = 0; q < 10; ++q) {
+        V2D_ARG_CHECK(out10[q], "get_metrics: null output %d", q);
+        V2D_CUDA_TRY(cudaMemcpyAsync(out10[q], S->g.met[q], bytes, cudaMemcpyDeviceToHost, S->s));
+    }
+    V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    return V2D_OK;
+}
+
+static int assemble_now(v2d_solver *S, double urot)
+{
+    V2D_TRY(ensure_pattern(S));
+    const v2d_solver_params &p = S->prm;
+    AsmParams ap{p.re, p.invdtau, p.inv2dt, urot, p.ca, p.sa, p.ff_bc};
+    V2D_CUDA_TRY(cudaMemsetAsync(S->flag, 0, sizeof(int), S->s));
+    V2D_TRY(launch_assemble(S->g, ap, p.krylov.precision == V2D_PREC_MIXED, S->flag, S->s));
+    S->assembled = true;
+    return V2D_OK;
+}
+
+extern "C" int v2d_solver_assemble(v2d_solver *S, double urot)
+{
+    V2D_ARG_CHECK(S, "null solver");
+    V2D_TRY(assemble_now(S, urot));
+    return sync_flag(S, "assemble");
+}
+
+extern "C" int v2d_solver_newton(v2d_solver *S, double urot, double *res, v2d_lin_stats *st)
+{
+    V2D_ARG_CHECK(S, "null solver");
+    GridDev &g = S->g;
+    V2D_TRY(assemble_now(S, urot));
+    V2D_TRY(sync_flag(S, "newton assembly"));
+    CsrOp A;
+    A.n = g.n; A.nnz = g.nnz; A.rowptr = g.rowptr; A.colind = g.colind; A.val = g.val;
+    A.val32 = g.val32; A.dinv = g.dinv; A.dinv32 = g.dinv32; A.layout = 1; A.nblk = g.N;
+    v2d_lin_stats ls{};
+    V2D_TRY(krylov_solve(S->kw, A, g.b, S->delta, S->prm.krylov, &ls, S->s));
+    if (st) *st = ls;
+    const int grid = std::max(1, std::min(kUpdBlocks, (g.N + kUpdThreads * 8 - 1) / (kUpdThreads * 8)));
+    k_newton_update<<<grid, kUpdThreads, 0, S->s>>>(g.N, S->delta, g.psi, g.ome, S->partial,
+                                                     S->counter, S->scal);
+    V2D_CUDA_TRY(cudaGetLastError());
+    count_launches(1);
+    V2D_CUDA_TRY(cudaMemcpyAsync(S->host, S->scal, sizeof(double), cudaMemcpyDeviceToHost, S->s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    S->assembled = false;
+    const double r = S->host[0];
+    if (res) *res = r;
+    if (!std::isfinite(r)) {
+        set_error("newton: non-finite update norm");
+        return V2D_ENONFINITE;
+    }
+    if (!ls.converged) {
+        set_error("newton: Krylov solve did not converge (%d iterations, |r|/|b| = %.3e)",
+                  ls.iterations, ls.res0 > 0 ? ls.res / ls.res0 : 0.0);
+        return V2D_ENOTCONVERGED;
+    }
+    return V2D_OK;
+}
+
+extern "C" int v2d_solver_pseudo_solve(v2d_solver *S, double urot, double pseudo_tol,
+                                       int max_iter, v2d_newton_info *info)
+{
+    V2D_ARG_CHECK(S, "null solver");
+    double res = 1.0e5;
+    int it = 0;
+    v2d_newton_info inf{};
+    int status = V2D_OK;
+    while (res > pseudo_tol && it < max_iter) {
+        v2d_lin_stats ls{};
+        status = v2d_solver_newton(S, urot, &res, &ls);
+        inf.krylov_iters += ls.iterations;
+        inf.corrections += ls.corrections;
+        double rel = ls.res0 > 0 ? ls.res / ls.res0 : 0.0;
+        if (rel > inf.lin_res_max) inf.lin_res_max = rel;
+        ++it;
+        if (status != V2D_OK) break;
+    }
+    inf.newton_iters = it;
+    inf.res = res;
+    if (info) *info = inf;
+    return status;
+}
+
+extern "C" int v2d_solver_shift_history(v2d_solver *S)
+{
+    V2D_ARG_CHECK(S, "null solver");
+    const size_t bytes = (size_t)S->g.N * sizeof(double);
+    V2D_CUDA_TRY(cudaMemcpyAsync(S->g.omeoldold, S->g.omeold, bytes, cudaMemcpyDeviceToDevice, S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(S->g.omeold, S->g.ome, bytes, cudaMemcpyDeviceToDevice, S->s));
+    return V2D_OK;
+}
+
+extern "C" int v2d_solver_step(v2d_solver *S, double urot, double pseudo_tol, int max_iter,
+                               int unsteady, v2d_newton_info *info)
+{
+    int st = v2d_solver_pseudo_solve(S, urot, pseudo_tol, max_iter, info);
+    if (st != V2D_OK) return st;
+    if (unsteady) V2D_TRY(v2d_solver_shift_history(S));
+    return V2D_OK;
+}
+
+extern "C" int v2d_solver_forces(v2d_solver *S, double re, double ref_length, double x0,
+                                 double y0, double *out10)
+{
+    V2D_ARG_CHECK(S && out10, "null pointer");
+    V2D_TRY(launch_forces(S->g, re, ref_length, x0, y0, S->scal + 1, S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(S->host + 1, S->scal + 1, 10 * sizeof(double),
+                                 cudaMemcpyDeviceToHost, S->s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    std::memcpy(out10, S->host + 1, 10 * sizeof(double));
+    return V2D_OK;
+}
+
+extern "C" int v2d_solver_nnz(const v2d_solver *S, long long *nnz)
+{
+    V2D_ARG_CHECK(S && nnz, "null pointer");
+    *nnz = S->g.nnz;
+    return V2D_OK;
+}
+
+extern "C" int v2d_solver_export_system(v2d_solver *S, int *indptr, int *indices, double *data,
+                                        double *b)
+{
+    V2D_ARG_CHECK(S, "null solver");
+    const GridDev &g = S->g;
+    if (indptr)
+        V2D_CUDA_TRY(cudaMemcpyAsync(indptr, g.rowptr, (g.n + 1) * sizeof(int), cudaMemcpyDeviceToHost, S->s));
+    if (indices)
+        V2D_CUDA_TRY(cudaMemcpyAsync(indices, g.colind, g.nnz * sizeof(int), cudaMemcpyDeviceToHost, S->s));
+    if (data)
+        V2D_CUDA_TRY(cudaMemcpyAsync(data, g.val, g.nnz * sizeof(double), cudaMemcpyDeviceToHost, S->s));
+    if (b) V2D_CUDA_TRY(cudaMemcpyAsync(b, g.b, g.n * sizeof(double), cudaMemcpyDeviceToHost, S->s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    return V2D_OK;
+}
+
+extern "C" int v2d_solver_state_ptrs(v2d_solver *S, double **psi, double **ome, double **omeold,
+                                     double **omeoldold)
+{
+    V2D_ARG_CHECK(S, "null solver");
+    if (psi) *psi = S->g.psi;
+    if (ome) *ome = S->g.ome;
+    if (omeold) *omeold = S->g.omeold;
+    if (omeoldold) *omeoldold = S->g.omeoldold;
+    return V2D_OK;
+}
+
+extern "C" int v2d_solver_time_spmv(v2d_solver *S, int fp32, int reps, long long flush_bytes,
+                                    double *ms_avg)
+{
+    V2D_ARG_CHECK(S && ms_avg && reps > 0 && flush_bytes >= 0, "time_spmv: bad arguments");
+    GridDev &g = S->g;
+    CsrOp A;
+    A.n = g.n; A.nnz = g.nnz; A.rowptr = g.rowptr; A.colind = g.colind; A.val = g.val;
+    A.val32 = g.val32; A.layout = 1; A.nblk = g.N;
+    return time_spmv(A, fp32 != 0, reps, (size_t)flush_bytes, S->s, ms_avg);
+}
+
+extern "C" int v2d_solver_stream(v2d_solver *S, void **stream)
+{
+    V2D_ARG_CHECK(S && stream, "null pointer");
+    *stream = (void *)S->s;
+    return V2D_OK;
+}
