@@ -1,0 +1,85 @@
+"""The C-ABI library without a GPU: it builds, loads, exports every entry
+point that include/vorti2d_b200.h declares, and its host-only paths (argument
+checks, defaults, neighbour indices) behave as documented.  No call here
+launches a kernel."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER_DIR = os.path.join(ROOT, "include")
+
+
+def declared_symbols():
+    names = set()
+    for fn in os.listdir(HEADER_DIR):
+        if fn.endswith(".h"):
+            text = open(os.path.join(HEADER_DIR, fn)).read()
+            text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+            names.update(re.findall(r"\b(v2d_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
+
+
+@pytest.fixture(scope="module")
+def lib(v2d):
+    from vorti2d_b200 import _lib
+    return ctypes.CDLL(_lib.LIB_PATH)
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = declared_symbols()
+    assert len(names) >= 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_the_header(v2d):
+    from vorti2d_b200 import _lib
+    bound = set(_lib._SIGS)
+    missing = [n for n in declared_symbols() if n not in bound]
+    assert not missing, missing
+
+
+def test_library_is_built_for_sm100a(v2d):
+    """The in-tree library carries sm_100a code (fatbin section present)."""
+    from vorti2d_b200 import _lib
+    data = open(_lib.LIB_PATH, "rb").read()
+    assert b".nv_fatbin" in data or b"__nv_relfatbin" in data
+    assert b"sm_100a" in data
+
+
+def test_host_only_entry_points(v2d):
+    from vorti2d_b200 import _lib
+    L = _lib.lib()
+    assert L.v2d_version() >= 10000
+    p = _lib.KrylovParams()
+    L.v2d_krylov_defaults(ctypes.byref(p))
+    assert p.restart == 30 and p.rtol == 1e-10 and p.precond == _lib.PC_BJACOBI
+    out = (ctypes.c_int * 9)()
+    assert L.v2d_node_neighbors(1, 2, 9, out) == 0
+    # i=1 wraps west to i=imax-1 (vorti2d_core.f90:39-52)
+    k = 9 * 1 + 1
+    assert list(out) == [k, k + 1, k + 7, k + 9, k - 9, k + 10, k + 16, k - 8, k - 2]
+    assert L.v2d_node_neighbors(0, 2, 9, out) == _lib.V2D_EARG
+    assert b"node_neighbors" in L.v2d_last_error()
+
+
+def test_argument_errors_before_any_device_work(v2d):
+    from vorti2d_b200 import _lib
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    prm = _lib.SolverParams()
+    assert L.v2d_solver_create(181, 181, None, None, ctypes.byref(prm), ctypes.byref(h)) \
+        == _lib.V2D_EARG
+    assert L.v2d_solver_destroy(None) == 0
+
+
+def test_no_cpu_fallback(v2d, monkeypatch, tmp_path):
+    """A missing library raises instead of falling back to another path."""
+    from vorti2d_b200 import _lib
+    monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "missing.so"))
+    monkeypatch.setattr(_lib, "_LIB", None, raising=False)
+    with pytest.raises((RuntimeError, OSError)):
+        _lib.lib()

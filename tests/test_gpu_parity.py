@@ -8,18 +8,11 @@ import numpy as np
 import pytest
 import scipy.sparse as sp
 
+from cases import local_layout, smooth_state, to_local
+
 pytestmark = pytest.mark.gpu
 
 SIZES = [(5, 4), (9, 7), (25, 17), (33, 21), (64, 48), (129, 129)]
-
-
-def smooth_state(x, y):
-    """Seam-consistent analytic state of the reference's local-assembly test
-    (tests/test_assemble_local.py:23-30)."""
-    r = np.sqrt(x ** 2 + y ** 2)
-    psi = np.sin(0.3 * x) * np.cos(0.2 * y) / (1.0 + 0.01 * r)
-    ome = np.cos(0.25 * x) * np.sin(0.15 * y) * np.exp(-0.02 * r)
-    return psi, ome, 0.9 * ome, 0.8 * ome
 
 
 @pytest.mark.parametrize("imax,jmax", SIZES)
@@ -93,28 +86,6 @@ def test_assemble_coo_capacity_error(v2d, oracle_mod):
     with pytest.raises(Exception):
         v2d.core.assemble_coo(imax, jmax, 40.0, 0, 0, 0, 1 / 8, 1 / 6, *M, z, z, z, z, 0,
                               2 * imax * jmax, 10, 0, 1.0, 0.0)
-
-
-def local_layout(imax, jmax):
-    """1-rank periodic DMDA layout (ni = imax-1 columns, one ghost column on
-    each side, dof=2 node-interleaved natural ordering), as
-    vorti2d/domain.py:41-63 sets up on one rank."""
-    ni = imax - 1
-    gxs, gxm = -1, ni + 2
-    il0, il1 = 2, gxm - 1
-    gc = (gxs + np.arange(gxm)) % ni
-    lg = np.empty(2 * gxm * jmax, dtype=np.intc)
-    for j in range(jmax):
-        for il in range(gxm):
-            K = j * gxm + il
-            lg[2 * K] = (j * ni + gc[il]) * 2
-            lg[2 * K + 1] = (j * ni + gc[il]) * 2 + 1
-    return ni, gxs, gxm, il0, il1, gc, lg
-
-
-def to_local(field, imax, jmax, gxm, gc):
-    g2 = field.reshape(jmax, imax)[:, :imax - 1]
-    return np.ascontiguousarray(g2[:, gc].ravel())
 
 
 @pytest.mark.parametrize("imax,jmax", [(25, 17), (33, 21)])
