@@ -121,7 +121,8 @@ int v2d_force_coeffs(int imax, int jmax, double re, double dksi, double deta,
 /* ------------------------------------------------ Krylov solver parameters */
 #define V2D_PC_NONE 0
 #define V2D_PC_BJACOBI 1   /* 2x2 (psi, ome) node blocks                     */
-#define V2D_PC_MG 2        /* aggregation multigrid, 2x2-block Jacobi smoothing */
+#define V2D_PC_LU 2        /* multifrontal LU of the current Jacobian (nested
+                              dissection of the O-grid); solver API only     */
 
 #define V2D_PREC_FP64 0    /* FP64 Krylov                                     */
 #define V2D_PREC_MIXED 1   /* FP32 SpMV/PC/Krylov vectors, FP64 Gram-Schmidt
@@ -136,9 +137,7 @@ typedef struct {
     int precision;        /* V2D_PREC_*                                       */
     double inner_rtol;    /* mixed: FP32 GMRES tolerance per correction (1e-5)*/
     int dc_max_it;        /* mixed: max defect-correction passes       (20)  */
-    int mg_levels;        /* multigrid: max levels (0 = auto)                 */
-    int mg_smooth;        /* multigrid: smoothing sweeps per side      (2)   */
-    double mg_omega;      /* multigrid: Jacobi damping                 (0.7) */
+    int lu_leaf;          /* LU: max nodes of a leaf subdomain         (64)  */
 } v2d_krylov_params;
 
 void v2d_krylov_defaults(v2d_krylov_params *p);
@@ -240,6 +239,15 @@ int v2d_solver_state_ptrs(v2d_solver *s, double **psi, double **ome, double **om
  * CUDA events on the handle's stream. */
 int v2d_solver_time_spmv(v2d_solver *s, int fp32, int reps, long long flush_bytes,
                          double *ms_avg);
+/* Planning aid (no reference counterpart): host-only symbolic analysis of the
+ * multifrontal LU preconditioner (V2D_PC_LU) for the canonical CSR pattern of
+ * an imax x jmax O-grid system (indptr: 2*imax*jmax+1, indices: nnz).  No
+ * device work.  out8 = fronts, levels, largest separator, largest front,
+ * factor entries, factorization flop bound, front variables, contribution
+ * entries. */
+int v2d_lu_plan_info(int imax, int jmax, const int *indptr, const int *indices, int leaf,
+                     long long *out8);
+
 /* The stream the handle's kernels run on (cudaStream_t as void*). */
 int v2d_solver_stream(v2d_solver *s, void **stream);
 

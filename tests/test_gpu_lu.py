@@ -1,0 +1,103 @@
+"""GMRES with the multifrontal LU preconditioner (the default) against the
+oracle's direct solves (SuperLU standing in for the reference's MUMPS,
+vorti2d/petsc_solver.py:55-61): one Newton update on several grid shapes,
+converged steady and unsteady runs at the benchmark sizes, and the FP32-factor
+mixed form against the FP64 form."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+from cases import smooth_state
+
+pytestmark = pytest.mark.gpu
+
+
+def _close(a, b, tol):
+    return np.max(np.abs(a - b)) <= tol * max(1.0, np.max(np.abs(b)))
+
+
+def cfg(v2d, **kw):
+    base = dict(verbose=False, write_csv=False, write_xdmf=False, compute_forces=False,
+                ksp_restart=30, ksp_rtol=1e-12, pseudo_tol=1e-12, max_pseudo_iter=30,
+                precond="lu")
+    base.update(kw)
+    return v2d.Config(**base)
+
+
+# odd / even imax, small grids whose separator tree degenerates, every far-field BC
+SHAPES = [(5, 4, 0), (9, 7, 1), (24, 13, 2), (33, 21, 1), (64, 48, 0), (129, 65, 2)]
+
+
+@pytest.mark.parametrize("imax,jmax,ff_bc", SHAPES)
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_one_newton_update_matches_direct_solve(v2d, oracle_mod, imax, jmax, ff_bc, precision):
+    """Newton update dq of the smooth analytic state (the reference's
+    tests/test_assemble_local.py:23-30 state) equals scipy's direct solve of
+    the oracle's system to 1e-9 relative, in a few Krylov iterations."""
+    bc = {0: "dirichlet", 1: "outflow", 2: "outflow_psi"}[ff_bc]
+    xg, yg = oracle_mod.generate_cylinder(imax, jmax)
+    s = v2d.Solver(cfg(v2d, re=80.0, steady=False, dt_phys=0.2, farfield_bc=bc,
+                       alpha_deg=4.0, precision=precision), mesh=(xg, yg))
+    M = oracle_mod.core().compute_metrics(1 / (imax - 1), 1 / (jmax - 1), xg, yg)
+    st = smooth_state(M[8], M[9])
+    s.set_state(*st)
+    N = imax * jmax
+    ci, cj, cv, nnz, b = oracle_mod.core().assemble_coo(
+        imax, jmax, 80.0, 0.0, 2.5, 0.3, 1 / (imax - 1), 1 / (jmax - 1), *M, *st, 0, 2 * N,
+        26 * N, ff_bc, np.cos(np.radians(4.0)), np.sin(np.radians(4.0)))
+    A = sp.csr_matrix((cv[:nnz], (ci[:nnz], cj[:nnz])), shape=(2 * N, 2 * N))
+    dq = spla.spsolve(A.tocsc(), b)
+    code, res, lin = s.dev.newton(0.3)
+    assert code == 0, v2d._lib.last_error()
+    got = np.concatenate(s.dev.get_state()[:2]) - np.concatenate(st[:2])
+    assert _close(got, dq, 1e-9), np.max(np.abs(got - dq))
+    assert lin.converged and lin.res <= 1e-12 * lin.res0 * 1.0001
+    assert lin.iterations <= (12 if precision == "mixed" else 6), lin.iterations
+    s.close()
+
+
+def test_config1_steady_129_matches_oracle(v2d, oracle_mod):
+    """Plain FP64 steady Newton, 129x129 cylinder, Re=40, Dirichlet far field,
+    pure Newton (dtau = inf) to ||dq||/(2N) < 1e-12: psi/omega within 1e-9,
+    Cl/Cd/Cm within 1e-8 of the oracle; the reference's BC and symmetry checks
+    (tests/test_smoke.py:44-56)."""
+    imax = jmax = 129
+    xg, yg = oracle_mod.generate_cylinder(imax, jmax)
+    ref = oracle_mod.OracleSolver(xg, yg, re=40.0, steady=True, pseudo_tol=1e-12,
+                                  max_pseudo_iter=40).run()
+    s = v2d.Solver(cfg(v2d, re=40.0, steady=True, max_pseudo_iter=40), mesh=(xg, yg))
+    s.advance(0.0)
+    assert s.newton_log[-1][3] <= 1e-12
+    assert _close(s.psi, ref.psi, 1e-9) and _close(s.ome, ref.ome, 1e-9)
+    fg, fo = s.force_coeffs(), ref.force_coeffs()
+    for k in ("cd", "cl", "cm"):
+        assert abs(getattr(fg, k) - getattr(fo, k)) <= 1e-8, k
+    assert abs(fg.cd - 1.52) < 0.05          # documented steady Cd at Re=40
+    ff = slice(imax * (jmax - 1), imax * jmax)
+    assert np.max(np.abs(s.psi[ff] - s.yphys[ff])) < 1e-10
+    assert np.max(np.abs(s.psi[:imax])) < 1e-10
+    assert np.max(np.abs(s.ome[ff])) < 1e-12
+    assert abs(s.psi.max() + s.psi.min()) < 1e-6
+    s.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_config2_unsteady_181_matches_oracle(v2d, oracle_mod, precision):
+    """The benchmark case (181x181, Re=100, dt=0.2, rotational kick 0.5 until
+    t=2, outflow far field, at most 5 Newton iterations per step): the first
+    three BDF2 steps equal the oracle's to 1e-9 with |dCd| < 1e-8."""
+    imax = jmax = 181
+    xg, yg = oracle_mod.generate_cylinder(imax, jmax)
+    kw = dict(re=100.0, steady=False, dt_phys=0.2, rot_speed=0.5, rot_until=2.0,
+              farfield_bc="outflow")
+    ref = oracle_mod.OracleSolver(xg, yg, pseudo_tol=1e-10, max_pseudo_iter=5, **kw)
+    s = v2d.Solver(cfg(v2d, ksp_rtol=1e-10, pseudo_tol=1e-10, max_pseudo_iter=5,
+                       precision=precision, **kw), mesh=(xg, yg))
+    for t in ref.times()[:3]:
+        _, it_ref = ref.advance(t)
+        _, it, _ = s.advance(t)
+        assert abs(it - it_ref) <= 1
+        assert _close(s.psi, ref.psi, 1e-9) and _close(s.ome, ref.ome, 1e-9)
+    assert abs(s.force_coeffs().cd - ref.force_coeffs().cd) < 1e-8
+    s.close()

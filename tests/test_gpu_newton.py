@@ -50,7 +50,8 @@ def test_steady_newton_matches_oracle(v2d, oracle_mod):
                                   max_pseudo_iter=50).run()
     assert ref.history[-1][2] < 1e-13
     s = v2d.Solver(gpu_cfg(v2d, re=20.0, steady=True, ksp_restart=256, krylov_max_it=100000,
-                           pseudo_tol=1e-13, max_pseudo_iter=50), mesh=(xg, yg))
+                           pseudo_tol=1e-13, max_pseudo_iter=50, precond="bjacobi"),
+                   mesh=(xg, yg))
     s.advance(0.0)
     dpsi = np.max(np.abs(s.psi - ref.psi))
     dome = np.max(np.abs(s.ome - ref.ome))

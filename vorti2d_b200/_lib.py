@@ -24,7 +24,7 @@ V2D_ETIMEOUT = -6
 V2D_EBREAKDOWN = -7
 V2D_ENOMEM = -8
 
-PC_NONE, PC_BJACOBI, PC_MG = 0, 1, 2
+PC_NONE, PC_BJACOBI, PC_LU = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -38,7 +38,7 @@ _ll = ctypes.c_longlong
 class KrylovParams(ctypes.Structure):
     _fields_ = [("restart", _i), ("max_it", _i), ("rtol", _d), ("atol", _d),
                 ("precond", _i), ("precision", _i), ("inner_rtol", _d), ("dc_max_it", _i),
-                ("mg_levels", _i), ("mg_smooth", _i), ("mg_omega", _d)]
+                ("lu_leaf", _i)]
 
 
 class LinStats(ctypes.Structure):
@@ -104,6 +104,7 @@ _SIGS = {
     "v2d_solver_state_ptrs": (_i, [_vp] + [ctypes.POINTER(_vp)] * 4),
     "v2d_solver_stream": (_i, [_vp, ctypes.POINTER(_vp)]),
     "v2d_solver_time_spmv": (_i, [_vp, _i, _i, _ll, _dp]),
+    "v2d_lu_plan_info": (_i, [_i, _i, _ip, _ip, _i, ctypes.POINTER(_ll)]),
 }
 
 _LIB = None

@@ -25,7 +25,7 @@ SOURCES = [
     ("v2d_seam.cu", ["-fmad=false"]),
     ("v2d_assemble.cu", ["-fmad=false"]),
     ("v2d_krylov.cu", []),
-    ("v2d_mg.cu", []),
+    ("v2d_mf.cu", []),
     ("v2d_solver.cu", []),
     ("v2d_forces.cu", []),
     ("v2d_linsys.cu", []),

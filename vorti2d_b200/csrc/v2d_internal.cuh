@@ -1,6 +1,8 @@
 // Internal interfaces between the translation units of libvorti2d_b200.
 #pragma once
 
+#include <vector>
+
 #include "v2d_util.cuh"
 
 namespace v2d {
@@ -37,6 +39,68 @@ int launch_assemble(GridDev &g, const AsmParams &p, bool want32, int *d_flag, cu
 int launch_forces(const GridDev &g, double re, double ref_length, double x0, double y0,
                   double *d_out10, cudaStream_t s);
 
+// ---------------------------------------------- multifrontal direct LU
+// Symbolic plan of the nested-dissection multifrontal factorization of the
+// field-blocked 2N system of one O-grid (v2d_mf.cu).  Fronts are numbered
+// level by level; front q holds f[q] local variables (its S[q] fully summed
+// ones first), stored densely (row-major f x f) at foff[q].
+struct MfPlan {
+    int N = 0, n = 0, nfront = 0, nlevel = 0, maxS = 0, maxf = 0;
+    long long ftotal = 0, nasm = 0;
+    int vtotal = 0, utotal = 0;
+    double flops = 0.0;   // 2 * sum S f^2 (upper bound of the factorization flops)
+    std::vector<int> S, f, voff, uoff, child0, child1, parent;
+    std::vector<long long> foff;
+    std::vector<int> lvl_off, lvl_maxS, lvl_maxf, lvl_maxm_child;
+    std::vector<long long> lvl_fbeg, lvl_fend, lvl_abeg, lvl_aend;
+    int *d_S = nullptr, *d_f = nullptr, *d_voff = nullptr, *d_uoff = nullptr;
+    int *d_child0 = nullptr, *d_child1 = nullptr;
+    long long *d_foff = nullptr;
+    int *d_vars = nullptr, *d_cbmap = nullptr, *d_asm_csr = nullptr, *d_asm_row = nullptr;
+    long long *d_asm_pos = nullptr;
+    // host copies, kept only between the build and the upload
+    std::vector<int> h_vars, h_cbmap, h_asm_csr, h_asm_row;
+    std::vector<long long> h_asm_pos;
+};
+
+// Numeric factors of one plan in one precision.
+struct MfFactor {
+    int fp32 = 0;
+    void *F = nullptr, *upd = nullptr, *z = nullptr;
+    double *rs = nullptr;       // row scaling 1 / max |a_r.|
+    int *ipiv = nullptr, *perm = nullptr, *flag = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    const double *graph_val = nullptr;
+    const int *graph_rowptr = nullptr;
+    long long launches_per_factor = 0;
+};
+
+// Kernel-side view of a plan + factor (passed by value).
+struct MfDev {
+    const int *S, *f, *voff, *uoff, *child0, *child1;
+    const long long *foff;
+    const int *vars, *cbmap, *perm;
+    int maxS, maxf;
+};
+
+// Host-only symbolic phase (validates every index it produces).
+int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_colind, int leaf,
+                  MfPlan **out);
+// mf_plan_build + upload of the index arrays.
+int mf_plan_create(int imax, int jmax, int n, const int *h_rowptr, const int *h_colind, int leaf,
+                   MfPlan **out);
+void mf_plan_destroy(MfPlan *p);
+int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out);
+void mf_factor_destroy(MfFactor *M);
+MfDev mf_dev(const MfPlan *P, const MfFactor *M);
+// Factor the CSR values (FP64, row-scaled and rounded to the factor's precision).
+int mf_factor(const MfPlan *P, MfFactor *M, const int *rowptr, const double *val, cudaStream_t s);
+// x = A^-1 b with the factors (vectors in the factor's precision).  The
+// kernels exit at once while *stop_a or *stop_b is non-zero (either may be null).
+int mf_apply(const MfPlan *P, const MfFactor *M, const void *b, void *x, const int *stop_a,
+             const int *stop_b, cudaStream_t s);
+int mf_flag(const MfFactor *M, int *flag, cudaStream_t s);
+
 // ------------------------------------------------------------- Krylov
 // A CSR operator with optional FP32 copy and 2x2 block inverse.
 // layout: 0 point (dinv holds 1/a_rr in slot 0), 1 field-blocked pairs (q, q+n/2),
@@ -51,6 +115,8 @@ struct CsrOp {
     const float *dinv32 = nullptr;
     int layout = 1;
     int nblk = 0;  // number of 2x2 blocks (or n for point layout)
+    const MfPlan *lu_plan = nullptr;   // V2D_PC_LU: factors of this operator
+    const MfFactor *lu = nullptr;
 };
 
 struct KrylovWork;  // defined in v2d_krylov.cu

@@ -14,6 +14,11 @@
 //    without the host; a device control block makes the remaining kernels of
 //    a cycle exit at once after convergence or breakdown.
 //  * Each cycle is captured once as a CUDA graph and replayed.
+//  * Preconditioners: 2x2 (psi, ome) block Jacobi applied inline, or the
+//    multifrontal LU of the current Jacobian (v2d_mf.cu) applied by its own
+//    per-level kernels; with LU the preconditioned vectors Z_j = M^-1 v_j are
+//    kept (m extra vectors) so the cycle's correction x += Z y needs no
+//    further solve.
 //  * Precision T = double (plain FP64) or float (FP32 SpMV, preconditioner
 //    and Krylov vectors, FP64 dot-product accumulation and Hessenberg).  The
 //    true residual b - A x is recomputed in FP64 at every restart, so the
@@ -68,8 +73,8 @@ struct KrylovWork {
     int n = 0, m = 0;
     cudaStream_t s = 0;
     // FP64 and FP32 Arnoldi bases (allocated on first use of each precision)
-    double *V64 = nullptr, *w64 = nullptr, *z64 = nullptr;
-    float *V32 = nullptr, *w32 = nullptr, *z32 = nullptr;
+    double *V64 = nullptr, *w64 = nullptr, *z64 = nullptr, *Z64 = nullptr;
+    float *V32 = nullptr, *w32 = nullptr, *z32 = nullptr, *Z32 = nullptr;
     double *r = nullptr;          // FP64 residual
     double *H = nullptr;          // (m+1) x m column-major
     double *g = nullptr, *cs = nullptr, *sn = nullptr, *y = nullptr, *hcur = nullptr;
@@ -79,6 +84,8 @@ struct KrylovWork {
     Desc *desc = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int graph_m[2] = {0, 0};
+    int graph_pc[2] = {-1, -1};
+    const void *graph_lu[2] = {nullptr, nullptr};
 };
 
 // ---------------------------------------------------------------- helpers
@@ -123,6 +130,7 @@ __device__ __forceinline__ void block_rows(int layout, int nblk, int q, int &r0,
 template <class T>
 __device__ __forceinline__ void precond_block(const Desc *d, int q, const T *v, T *z)
 {
+    if (d->precond == V2D_PC_LU) return;   // applied by the multifrontal kernels
     if (d->precond == V2D_PC_NONE) {
         z[q] = v[q];
         return;
@@ -142,7 +150,7 @@ __device__ __forceinline__ void precond_block(const Desc *d, int q, const T *v, 
 
 __device__ __forceinline__ int precond_units(const Desc *d)
 {
-    return (d->precond == V2D_PC_NONE || d->layout == 0) ? d->n : d->nblk;
+    return (d->precond != V2D_PC_BJACOBI || d->layout == 0) ? d->n : d->nblk;
 }
 
 // ----------------------------------------------------------------- kernels
@@ -160,7 +168,7 @@ __global__ void __launch_bounds__(256) k_scale_precond(const Desc *d, Ctl *ctl, 
     const int units = precond_units(d);
     V2D_GRID_STRIDE(q, units)
     {
-        if (d->precond == V2D_PC_NONE || d->layout == 0) {
+        if (d->precond != V2D_PC_BJACOBI || d->layout == 0) {
             int r0 = (int)q;
             vj[r0] = j == 0 ? (T)(r[r0] * inv) : (T)(w[r0] * inv);
         } else {
@@ -366,10 +374,19 @@ __global__ void k_backsolve(const Desc *d, Ctl *ctl, const double *H, const doub
 // x += M^-1 (V y), x in FP64.
 template <class T>
 __global__ void __launch_bounds__(256) k_correct(const Desc *d, Ctl *ctl, const T *V, const double *y,
-                                                 T *t_scratch, double *x)
+                                                 T *t_scratch, double *x, const T *Z)
 {
     if (ctl->conv) return;
     const int n = d->n, jj = ctl->jdone;
+    if (d->precond == V2D_PC_LU) {   // x += Z y
+        V2D_GRID_STRIDE(r, n)
+        {
+            double s = 0.0;
+            for (int i = 0; i < jj; ++i) s += y[i] * (double)Z[(size_t)i * n + r];
+            x[r] += s;
+        }
+        return;
+    }
     const int units = precond_units(d);
     V2D_GRID_STRIDE(q, units)
     {
@@ -493,22 +510,37 @@ static int tile_grid(long long n)
 }
 
 template <class T>
-static int run_cycles(KrylovWork *w, int which, T *V, T *wv, T *z, double *x, int ncycles,
-                      cudaStream_t s)
+static int run_cycles(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, double *x, int ncycles,
+                      const CsrOp &A, int precond, cudaStream_t s)
 {
     const int n = w->n;
     const int gp = grid_for(n, 256);
     const int gs = grid_for((long long)n * kTPR, kSpmvThreads);
     const int gr = red_grid(n);
     const int gt = tile_grid(n);
-    if (!w->graph[which] || w->graph_m[which] != w->m) {
+    const bool lu = precond == V2D_PC_LU;
+    long long per_cycle = 6LL * w->m + 3;
+    if (!w->graph[which] || w->graph_m[which] != w->m || w->graph_pc[which] != precond ||
+        w->graph_lu[which] != (lu ? (const void *)A.lu : nullptr)) {
         if (w->graph[which]) cudaGraphExecDestroy(w->graph[which]);
         w->graph[which] = nullptr;
         cudaGraph_t gph;
         V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         for (int j = 0; j < w->m; ++j) {
             k_scale_precond<T><<<gp, 256, 0, s>>>(w->desc, w->ctl, j, w->r, wv, V, w->H, z);
-            k_spmv<T><<<gs, kSpmvThreads, 0, s>>>(w->desc, w->ctl, z, wv);
+            T *zj = z;
+            if (lu) {
+                zj = Z + (size_t)j * n;
+                int st = mf_apply(A.lu_plan, A.lu, V + (size_t)j * n, zj, &w->ctl->conv,
+                                  &w->ctl->cyc_stop, s);
+                if (st != V2D_OK) {
+                    cudaGraph_t junk;
+                    cudaStreamEndCapture(s, &junk);
+                    if (junk) cudaGraphDestroy(junk);
+                    return st;
+                }
+            }
+            k_spmv<T><<<gs, kSpmvThreads, 0, s>>>(w->desc, w->ctl, zj, wv);
             const dim3 gdot(gt, (j + 1 + kDotChunk - 1) / kDotChunk);
             for (int pass = 0; pass < 2; ++pass) {
                 k_mdot<T><<<gdot, kRedThreads, 0, s>>>(w->desc, w->ctl, j, pass, V, wv, w->partial,
@@ -518,7 +550,7 @@ static int run_cycles(KrylovWork *w, int which, T *V, T *wv, T *z, double *x, in
             }
         }
         k_backsolve<<<1, 32, 0, s>>>(w->desc, w->ctl, w->H, w->g, w->y);
-        k_correct<T><<<gp, 256, 0, s>>>(w->desc, w->ctl, V, w->y, z, x);
+        k_correct<T><<<gp, 256, 0, s>>>(w->desc, w->ctl, V, w->y, z, x, Z);
         k_residual<<<gr, kSpmvThreads, 0, s>>>(w->desc, w->ctl, w->r, w->partial, w->g, 0);
         cudaError_t e = cudaStreamEndCapture(s, &gph);
         if (e != cudaSuccess) {
@@ -532,9 +564,12 @@ static int run_cycles(KrylovWork *w, int which, T *V, T *wv, T *z, double *x, in
             return V2D_ECUDA;
         }
         w->graph_m[which] = w->m;
+        w->graph_pc[which] = precond;
+        w->graph_lu[which] = lu ? (const void *)A.lu : nullptr;
     }
+    if (lu) per_cycle += 2LL * A.lu_plan->nlevel * w->m;
     for (int c = 0; c < ncycles; ++c) V2D_CUDA_TRY(cudaGraphLaunch(w->graph[which], s));
-    count_launches((long long)ncycles * (6LL * w->m + 3));
+    count_launches((long long)ncycles * per_cycle);
     return V2D_OK;
 }
 
@@ -577,7 +612,7 @@ void krylov_destroy(KrylovWork *w)
     if (!w) return;
     for (int q = 0; q < 2; ++q)
         if (w->graph[q]) cudaGraphExecDestroy(w->graph[q]);
-    void *ptrs[] = {w->V64, w->w64, w->z64, w->V32, w->w32, w->z32, w->r, w->H, w->g,
+    void *ptrs[] = {w->V64, w->w64, w->z64, w->Z64, w->V32, w->w32, w->z32, w->Z32, w->r, w->H, w->g,
                     w->cs, w->sn, w->y, w->hcur, w->partial, w->ctl, w->desc};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -585,9 +620,11 @@ void krylov_destroy(KrylovWork *w)
     delete w;
 }
 
-static int ensure_basis(KrylovWork *w, bool fp32)
+static int ensure_basis(KrylovWork *w, bool fp32, bool lu)
 {
     const size_t n = w->n, m = w->m;
+    if (lu && fp32 && !w->Z32) V2D_CUDA_TRY(cudaMalloc(&w->Z32, m * n * sizeof(float)));
+    if (lu && !fp32 && !w->Z64) V2D_CUDA_TRY(cudaMalloc(&w->Z64, m * n * sizeof(double)));
     if (fp32 && !w->V32) {
         V2D_CUDA_TRY(cudaMalloc(&w->V32, (m + 1) * n * sizeof(float)));
         V2D_CUDA_TRY(cudaMalloc(&w->w32, n * sizeof(float)));
@@ -607,14 +644,18 @@ int krylov_solve(KrylovWork *w, const CsrOp &A, const double *d_b, double *d_x,
     V2D_ARG_CHECK(A.n == w->n, "krylov_solve: operator size %d != workspace size %d", A.n, w->n);
     V2D_ARG_CHECK(prm.restart == w->m, "krylov_solve: restart changed (%d != %d)", prm.restart, w->m);
     const bool fp32 = prm.precision == V2D_PREC_MIXED;
-    V2D_ARG_CHECK(!fp32 || (A.val32 && (A.dinv32 || prm.precond == V2D_PC_NONE)),
+    const bool lu = prm.precond == V2D_PC_LU;
+    V2D_ARG_CHECK(!fp32 || (A.val32 && (A.dinv32 || prm.precond != V2D_PC_BJACOBI)),
                   "krylov_solve: mixed precision needs FP32 values");
-    V2D_TRY(ensure_basis(w, fp32));
+    V2D_ARG_CHECK(!lu || (A.lu && A.lu_plan && A.lu->fp32 == (fp32 ? 1 : 0)),
+                  "krylov_solve: LU preconditioner needs factors in the Krylov precision");
+    V2D_TRY(ensure_basis(w, fp32, lu));
     Desc hd;
     hd.n = A.n; hd.nblk = A.nblk; hd.layout = A.layout; hd.m = w->m;
     hd.rowptr = A.rowptr; hd.colind = A.colind; hd.val = A.val; hd.val32 = A.val32;
     hd.dinv = A.dinv; hd.dinv32 = A.dinv32; hd.b = d_b; hd.x = d_x;
-    hd.precond = prm.precond == V2D_PC_BJACOBI ? V2D_PC_BJACOBI : V2D_PC_NONE;
+    hd.precond = (prm.precond == V2D_PC_BJACOBI || prm.precond == V2D_PC_LU) ? prm.precond
+                                                                              : V2D_PC_NONE;
     V2D_CUDA_TRY(cudaMemcpyAsync(w->desc, &hd, sizeof(Desc), cudaMemcpyHostToDevice, s));
     Ctl c{};
     c.tol_abs = prm.rtol;  // scaled by ||b|| in the first residual pass (atol applied below)
@@ -638,8 +679,10 @@ int krylov_solve(KrylovWork *w, const CsrOp &A, const double *d_b, double *d_x,
     int batch = 1;
     int guard = 0;
     while (!h.conv) {
-        int status = fp32 ? run_cycles<float>(w, 1, w->V32, w->w32, w->z32, d_x, batch, s)
-                          : run_cycles<double>(w, 0, w->V64, w->w64, w->z64, d_x, batch, s);
+        int status = fp32 ? run_cycles<float>(w, 1, w->V32, w->w32, w->z32, w->Z32, d_x, batch, A,
+                                              hd.precond, s)
+                          : run_cycles<double>(w, 0, w->V64, w->w64, w->z64, w->Z64, d_x, batch, A,
+                                               hd.precond, s);
         if (status != V2D_OK) return status;
         V2D_CUDA_TRY(cudaMemcpyAsync(w->ctl_host, w->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
         V2D_CUDA_TRY(cudaStreamSynchronize(s));

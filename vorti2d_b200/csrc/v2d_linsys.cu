@@ -177,7 +177,7 @@ extern "C" int v2d_linsys_create(int n, int block_layout, const v2d_krylov_param
     V2D_ARG_CHECK(n > 0, "linsys_create: n must be positive (got %d)", n);
     V2D_ARG_CHECK(block_layout >= 0 && block_layout <= 2, "linsys_create: layout %d", block_layout);
     V2D_ARG_CHECK(block_layout == 0 || n % 2 == 0, "linsys_create: 2x2 layouts need an even n");
-    V2D_ARG_CHECK(p->precond != V2D_PC_MG, "linsys_create: multigrid needs the grid (use the solver API)");
+    V2D_ARG_CHECK(p->precond != V2D_PC_LU, "linsys_create: the LU preconditioner needs the grid (use the solver API)");
     v2d_linsys *L = new v2d_linsys();
     L->n = n;
     L->layout = block_layout;

@@ -1,0 +1,1038 @@
+// Sparse direct factorization of the Newton system on the device: a
+// multifrontal LU over a nested-dissection separator tree of the O-grid.
+//
+// It takes the place of the direct LU (MUMPS) of the reference's replicated
+// solve (vorti2d/petsc_solver.py:55-61, 97-115): pure Newton (dtau = inf)
+// systems of this discretisation defeat point / line block Jacobi and
+// multigrid preconditioners, so every Newton iteration factors the current
+// Jacobian and uses the factors as the right preconditioner of GMRES(m) (FP32
+// factors inside FP64 defect correction in the mixed-precision form; FP64
+// factors in the plain form).
+//
+// Symbolic phase (host, once per mesh and sparsity pattern):
+//  * the separator tree is geometric: the root separator is the two seam
+//    columns i = 0, imax-1 plus column imax/2, which cut the periodic ring into
+//    two rectangles; each rectangle is split recursively by its middle column
+//    or row (never rows 1 or jmax-2, whose boundary rows reach two rows away:
+//    the Thom wall row, vorti2d_core.f90:322-339, and the outflow rows,
+//    :254-269, :307-321) until it holds at most `leaf` nodes;
+//  * fronts are numbered level by level (level = height above the leaves), so
+//    the fronts of one level, their dense storage and their assembly entries
+//    are contiguous and each level is processed by a fixed set of batched
+//    launches;
+//  * struct(front) = (struct(children) U adj(separator)) minus the subtree,
+//    over the symmetrised node graph of the CSR pattern; each CSR entry goes
+//    to the front of whichever of its two nodes is eliminated first.
+//
+// Numeric phase (device, per Newton iteration), per level bottom-up:
+//  row-scaled CSR values scattered into the zeroed fronts, children's
+//  contribution blocks added (one child slot per launch: deterministic, no
+//  atomics), then a blocked right-looking partial LU of each front: panel
+//  (one CTA per front, partial pivoting among the fully summed rows, the panel
+//  held in shared memory), row swaps + TRSM for the U12 block row, GEMM update
+//  of the trailing block (which leaves the Schur complement for the parent).
+//
+// Solve (device): forward per level bottom-up (gather, permute, unit-lower
+// solve, contribution vector for the parent), backward top-down (U12 x_struct,
+// upper solve, scatter).  One CTA per front, blocked 32 rows at a time.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <vector>
+
+#include "v2d_internal.cuh"
+
+namespace v2d {
+
+// ================================================================ symbolic
+namespace {
+
+struct TreeNode {
+    std::vector<int> sep;   // node ids (pointer order K = imax*j + i)
+    int kid[2] = {-1, -1};
+    int parent = -1;
+};
+
+struct TreeBuilder {
+    int imax, jmax, leaf;
+    std::vector<TreeNode> t;  // postorder
+
+    int add(std::vector<int> &&sep, int a, int b)
+    {
+        TreeNode nd;
+        nd.sep = std::move(sep);
+        int q = 0;
+        if (a >= 0) nd.kid[q++] = a;
+        if (b >= 0) nd.kid[q++] = b;
+        t.push_back(std::move(nd));
+        const int id = (int)t.size() - 1;
+        for (int c : t[id].kid)
+            if (c >= 0) t[c].parent = id;
+        return id;
+    }
+    std::vector<int> block(int i0, int i1, int j0, int j1) const
+    {
+        std::vector<int> v;
+        for (int j = j0; j < j1; ++j)
+            for (int i = i0; i < i1; ++i) v.push_back(j * imax + i);
+        return v;
+    }
+    int col_cut(int i0, int i1, int j0, int j1)
+    {
+        const int c = (i0 + i1) / 2;
+        int a = rect(i0, c, j0, j1);
+        int b = rect(c + 1, i1, j0, j1);
+        return add(block(c, c + 1, j0, j1), a, b);
+    }
+    // Rectangle [i0,i1) x [j0,j1) of the non-periodic part of the ring.
+    int rect(int i0, int i1, int j0, int j1)
+    {
+        const int w = i1 - i0, h = j1 - j0;
+        if (w <= 0 || h <= 0) return -1;
+        if (w * h <= leaf) return add(block(i0, i1, j0, j1), -1, -1);
+        if (w >= h && w >= 3) return col_cut(i0, i1, j0, j1);
+        int best = -1;
+        const int mid = (j0 + j1) / 2;
+        for (int r = j0 + 1; r < j1 - 1; ++r) {
+            if (r == 1 || r == jmax - 2) continue;
+            if (best < 0 || std::abs(r - mid) < std::abs(best - mid)) best = r;
+        }
+        if (best < 0) {
+            if (w >= 3) return col_cut(i0, i1, j0, j1);
+            return add(block(i0, i1, j0, j1), -1, -1);
+        }
+        int a = rect(i0, i1, j0, best);
+        int b = rect(i0, i1, best + 1, j1);
+        return add(block(i0, i1, best, best + 1), a, b);
+    }
+    void build()
+    {
+        const int mid = imax / 2;
+        int a = rect(1, mid, 0, jmax);
+        int b = rect(mid + 1, imax - 1, 0, jmax);
+        std::vector<int> root;
+        for (int c : {0, mid, imax - 1})
+            for (int j = 0; j < jmax; ++j) root.push_back(j * imax + c);
+        add(std::move(root), a, b);
+    }
+};
+
+template <class T>
+int upload_vec(T **d, const std::vector<T> &h)
+{
+    *d = nullptr;
+    const size_t bytes = std::max<size_t>(1, h.size()) * sizeof(T);
+    V2D_CUDA_TRY(cudaMalloc((void **)d, bytes));
+    if (!h.empty()) V2D_CUDA_TRY(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return V2D_OK;
+}
+
+}  // namespace
+
+void mf_plan_destroy(MfPlan *p)
+{
+    if (!p) return;
+    void *ptrs[] = {p->d_S, p->d_f, p->d_voff, p->d_uoff, p->d_child0, p->d_child1, p->d_foff,
+                    p->d_vars, p->d_cbmap, p->d_asm_csr, p->d_asm_row, p->d_asm_pos};
+    for (void *q : ptrs)
+        if (q) cudaFree(q);
+    delete p;
+}
+
+int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_colind,
+                  int leaf, MfPlan **out)
+{
+    *out = nullptr;
+    const int N = imax * jmax;
+    V2D_ARG_CHECK(n == 2 * N, "mf_plan: system size %d != 2 * %d nodes", n, N);
+    V2D_ARG_CHECK(imax >= 5 && jmax >= 4, "mf_plan: grid %d x %d too small", imax, jmax);
+    TreeBuilder tb{imax, jmax, std::max(4, leaf), {}};
+    tb.build();
+    const int nf = (int)tb.t.size();
+    // --- symmetrised node graph (CSR)
+    std::vector<std::vector<int>> adj(N);
+    for (int r = 0; r < n; ++r)
+        for (int p = h_rowptr[r]; p < h_rowptr[r + 1]; ++p) {
+            int a = r % N, b = h_colind[p] % N;
+            if (a != b) {
+                adj[a].push_back(b);
+                adj[b].push_back(a);
+            }
+        }
+    for (auto &v : adj) {
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+    }
+    // --- elimination order (postorder of the tree)
+    std::vector<int> elim(N, -1), owner(N, -1), last_elim(nf);
+    int order = 0;
+    for (int q = 0; q < nf; ++q) {
+        for (int v : tb.t[q].sep) {
+            if (elim[v] >= 0) {
+                set_error("mf_plan: node %d in two separators", v);
+                return V2D_EARG;
+            }
+            elim[v] = order++;
+            owner[v] = q;
+        }
+        last_elim[q] = order - 1;
+    }
+    if (order != N) {
+        set_error("mf_plan: tree covers %d of %d nodes", order, N);
+        return V2D_EARG;
+    }
+    // --- struct sets
+    std::vector<std::vector<int>> st(nf);
+    std::vector<int> stamp(N, -1);
+    for (int q = 0; q < nf; ++q) {
+        std::vector<int> s;
+        auto take = [&](int u) {
+            if (elim[u] > last_elim[q] && stamp[u] != q) {
+                stamp[u] = q;
+                s.push_back(u);
+            }
+        };
+        for (int c : tb.t[q].kid)
+            if (c >= 0)
+                for (int u : st[c]) take(u);
+        for (int v : tb.t[q].sep)
+            for (int u : adj[v]) take(u);
+        std::sort(s.begin(), s.end(), [&](int a, int b) { return elim[a] < elim[b]; });
+        st[q] = std::move(s);
+    }
+    // a separator may couple only into its own subtree or to ancestors
+    std::vector<int> first_elim(nf);
+    for (int q = 0; q < nf; ++q) {
+        int fe = last_elim[q] - (int)tb.t[q].sep.size() + 1;
+        for (int c : tb.t[q].kid)
+            if (c >= 0) fe = std::min(fe, first_elim[c]);
+        first_elim[q] = fe;
+    }
+    for (int q = 0; q < nf; ++q)
+        for (int v : tb.t[q].sep)
+            for (int u : adj[v])
+                if (elim[u] < first_elim[q]) {
+                    set_error("mf_plan: node %d couples to node %d of a sibling subtree", v, u);
+                    return V2D_EARG;
+                }
+    // every struct node must belong to an ancestor (no coupling across subtrees)
+    for (int q = 0; q < nf; ++q)
+        for (int u : st[q]) {
+            int a = tb.t[q].parent;
+            while (a >= 0 && a != owner[u]) a = tb.t[a].parent;
+            if (a < 0) {
+                set_error("mf_plan: node %d couples across sibling subtrees", u);
+                return V2D_EARG;
+            }
+        }
+    // --- levels and level-major numbering
+    std::vector<int> height(nf, 0);
+    int nlevel = 0;
+    for (int q = 0; q < nf; ++q) {
+        int h = 0;
+        for (int c : tb.t[q].kid)
+            if (c >= 0) h = std::max(h, height[c] + 1);
+        height[q] = h;
+        nlevel = std::max(nlevel, h + 1);
+    }
+    std::vector<int> newid(nf), oldid;
+    for (int L = 0; L < nlevel; ++L)
+        for (int q = 0; q < nf; ++q)
+            if (height[q] == L) {
+                newid[q] = (int)oldid.size();
+                oldid.push_back(q);
+            }
+    MfPlan *P = new MfPlan();
+    P->N = N; P->n = n; P->nfront = nf; P->nlevel = nlevel;
+    P->S.resize(nf); P->f.resize(nf); P->voff.resize(nf); P->uoff.resize(nf);
+    P->child0.assign(nf, -1); P->child1.assign(nf, -1); P->parent.assign(nf, -1);
+    P->foff.resize(nf);
+    P->lvl_off.assign(nlevel + 1, 0);
+    P->lvl_fbeg.assign(nlevel, 0); P->lvl_fend.assign(nlevel, 0);
+    P->lvl_abeg.assign(nlevel, 0); P->lvl_aend.assign(nlevel, 0);
+    P->lvl_maxS.assign(nlevel, 0); P->lvl_maxf.assign(nlevel, 0); P->lvl_maxm_child.assign(nlevel, 0);
+    std::vector<int> vars, cbmap;
+    long long ftot = 0;
+    int vtot = 0, utot = 0;
+    for (int id = 0; id < nf; ++id) {
+        const int q = oldid[id];
+        const int s = (int)tb.t[q].sep.size(), m = (int)st[q].size();
+        const int S = 2 * s, f = 2 * (s + m);
+        P->S[id] = S; P->f[id] = f;
+        P->voff[id] = vtot; vtot += f;
+        P->uoff[id] = utot; utot += f - S;
+        P->foff[id] = ftot; ftot += (long long)f * f;
+        const int L = height[q];
+        P->lvl_off[L + 1]++;
+        P->lvl_maxS[L] = std::max(P->lvl_maxS[L], S);
+        P->lvl_maxf[L] = std::max(P->lvl_maxf[L], f);
+        if (tb.t[q].parent >= 0) P->parent[id] = newid[tb.t[q].parent];
+        if (tb.t[q].kid[0] >= 0) P->child0[id] = newid[tb.t[q].kid[0]];
+        if (tb.t[q].kid[1] >= 0) P->child1[id] = newid[tb.t[q].kid[1]];
+        // front-local variables: node p -> vars 2p (psi, row/col p) and 2p+1 (ome, N+p)
+        for (int u : tb.t[q].sep) { vars.push_back(u); vars.push_back(N + u); }
+        for (int u : st[q]) { vars.push_back(u); vars.push_back(N + u); }
+        P->maxS = std::max(P->maxS, S);
+        P->maxf = std::max(P->maxf, f);
+    }
+    for (int L = 0; L < nlevel; ++L) P->lvl_off[L + 1] += P->lvl_off[L];
+    for (int L = 0; L < nlevel; ++L) {
+        const int a = P->lvl_off[L], b = P->lvl_off[L + 1];
+        P->lvl_fbeg[L] = P->foff[a];
+        P->lvl_fend[L] = P->foff[b - 1] + (long long)P->f[b - 1] * P->f[b - 1];
+        for (int id = a; id < b; ++id)
+            for (int c : {P->child0[id], P->child1[id]})
+                if (c >= 0) P->lvl_maxm_child[L] = std::max(P->lvl_maxm_child[L], P->f[c] - P->S[c]);
+    }
+    // contribution-block maps: struct var of child -> local index in parent
+    cbmap.assign(utot, -1);
+    std::vector<int> loc(n, -1);
+    for (int id = 0; id < nf; ++id) {
+        const int pa = P->parent[id];
+        if (pa < 0) continue;
+        for (int t = 0; t < P->f[pa]; ++t) loc[vars[P->voff[pa] + t]] = t;
+        for (int t = P->S[id]; t < P->f[id]; ++t) {
+            const int li = loc[vars[P->voff[id] + t]];
+            if (li < 0) {
+                set_error("mf_plan: struct variable of front %d missing in its parent", id);
+                mf_plan_destroy(P);
+                return V2D_EARG;
+            }
+            cbmap[P->uoff[id] + t - P->S[id]] = li;
+        }
+        for (int t = 0; t < P->f[pa]; ++t) loc[vars[P->voff[pa] + t]] = -1;
+    }
+    // assembly entries grouped by front (level-major)
+    std::vector<int> cnt(nf + 1, 0), entry_front(h_rowptr[n]);
+    for (int r = 0; r < n; ++r)
+        for (int p = h_rowptr[r]; p < h_rowptr[r + 1]; ++p) {
+            const int a = r % N, b = h_colind[p] % N;
+            const int fr = newid[elim[a] < elim[b] ? owner[a] : owner[b]];
+            entry_front[p] = fr;
+            cnt[fr + 1]++;
+        }
+    for (int q = 0; q < nf; ++q) cnt[q + 1] += cnt[q];
+    const long long nnz = h_rowptr[n];
+    std::vector<int> asm_csr(nnz), asm_row(nnz);
+    std::vector<long long> asm_pos(nnz);
+    {
+        std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+        std::vector<std::vector<int>> rows_of_front;  // unused; positions computed below
+        // local index lookup per front: scan fronts, mark their vars
+        std::vector<std::vector<int>> ent(nf);
+        for (int r = 0; r < n; ++r)
+            for (int p = h_rowptr[r]; p < h_rowptr[r + 1]; ++p) ent[entry_front[p]].push_back(p);
+        std::vector<int> row_of(nnz);
+        for (int r = 0; r < n; ++r)
+            for (int p = h_rowptr[r]; p < h_rowptr[r + 1]; ++p) row_of[p] = r;
+        for (int id = 0; id < nf; ++id) {
+            const int f = P->f[id];
+            for (int t = 0; t < f; ++t) loc[vars[P->voff[id] + t]] = t;
+            int o = cnt[id];
+            for (int p : ent[id]) {
+                const int r = row_of[p], c = h_colind[p];
+                const int lr = loc[r], lc = loc[c];
+                if (lr < 0 || lc < 0) {
+                    set_error("mf_plan: entry (%d, %d) outside its front", r, c);
+                    mf_plan_destroy(P);
+                    return V2D_EARG;
+                }
+                asm_csr[o] = p;
+                asm_row[o] = r;
+                asm_pos[o] = P->foff[id] + (long long)lr * f + lc;
+                ++o;
+            }
+            for (int t = 0; t < f; ++t) loc[vars[P->voff[id] + t]] = -1;
+        }
+    }
+    for (int L = 0; L < nlevel; ++L) {
+        P->lvl_abeg[L] = cnt[P->lvl_off[L]];
+        P->lvl_aend[L] = cnt[P->lvl_off[L + 1]];
+    }
+    P->ftotal = ftot; P->vtotal = vtot; P->utotal = utot; P->nasm = nnz;
+    double fl = 0.0;
+    for (int id = 0; id < nf; ++id) fl += 2.0 * P->S[id] * (double)P->f[id] * P->f[id];
+    P->flops = fl;
+    // every index the kernels dereference stays inside its buffer
+    bool ok = (long long)vars.size() == vtot && (long long)cbmap.size() == utot;
+    for (int v : vars) ok = ok && v >= 0 && v < n;
+    for (int id = 0; id < nf && ok; ++id) {
+        ok = ok && P->S[id] > 0 && P->S[id] <= P->f[id] && P->S[id] % 2 == 0;
+        const int pa = P->parent[id];
+        if (pa >= 0)
+            for (int t = 0; t < P->f[id] - P->S[id]; ++t) {
+                const int li = cbmap[P->uoff[id] + t];
+                ok = ok && li >= 0 && li < P->f[pa];
+            }
+        else
+            ok = ok && P->f[id] == P->S[id];   // the root has no contribution block
+        for (int c : {P->child0[id], P->child1[id]}) ok = ok && (c < 0 || (c < id && P->parent[c] == id));
+    }
+    for (long long e = 0; e < nnz && ok; ++e)
+        ok = asm_pos[e] >= 0 && asm_pos[e] < ftot && asm_csr[e] >= 0 && asm_csr[e] < nnz &&
+             asm_row[e] >= 0 && asm_row[e] < n;
+    if (!ok) {
+        set_error("mf_plan: internal index check failed (%d x %d grid)", imax, jmax);
+        mf_plan_destroy(P);
+        return V2D_EARG;
+    }
+    P->h_vars = std::move(vars);
+    P->h_cbmap = std::move(cbmap);
+    P->h_asm_csr = std::move(asm_csr);
+    P->h_asm_row = std::move(asm_row);
+    P->h_asm_pos = std::move(asm_pos);
+    *out = P;
+    return V2D_OK;
+}
+
+int mf_plan_create(int imax, int jmax, int n, const int *h_rowptr, const int *h_colind,
+                   int leaf, MfPlan **out)
+{
+    *out = nullptr;
+    MfPlan *P = nullptr;
+    V2D_TRY(mf_plan_build(imax, jmax, n, h_rowptr, h_colind, leaf, &P));
+    int st_up = V2D_OK;
+    if (st_up == V2D_OK) st_up = upload_vec(&P->d_S, P->S);
+    if (st_up == V2D_OK) st_up = upload_vec(&P->d_f, P->f);
+    if (st_up == V2D_OK) st_up = upload_vec(&P->d_voff, P->voff);
+    if (st_up == V2D_OK) st_up = upload_vec(&P->d_uoff, P->uoff);
+    if (st_up == V2D_OK) st_up = upload_vec(&P->d_child0, P->child0);
+    if (st_up == V2D_OK) st_up = upload_vec(&P->d_child1, P->child1);
+    if (st_up == V2D_OK) st_up = upload_vec(&P->d_foff, P->foff);
+    if (st_up == V2D_OK) st_up = upload_vec(&P->d_vars, P->h_vars);
+    if (st_up == V2D_OK) st_up = upload_vec(&P->d_cbmap, P->h_cbmap);
+    if (st_up == V2D_OK) st_up = upload_vec(&P->d_asm_csr, P->h_asm_csr);
+    if (st_up == V2D_OK) st_up = upload_vec(&P->d_asm_row, P->h_asm_row);
+    if (st_up == V2D_OK) st_up = upload_vec(&P->d_asm_pos, P->h_asm_pos);
+    if (st_up != V2D_OK) {
+        mf_plan_destroy(P);
+        return st_up;
+    }
+    // host copies are not needed once uploaded
+    std::vector<int>().swap(P->h_vars);
+    std::vector<int>().swap(P->h_cbmap);
+    std::vector<int>().swap(P->h_asm_csr);
+    std::vector<int>().swap(P->h_asm_row);
+    std::vector<long long>().swap(P->h_asm_pos);
+    *out = P;
+    return V2D_OK;
+}
+
+}  // namespace v2d
+
+// Planning aid (no reference counterpart): runs only the host symbolic phase.
+extern "C" int v2d_lu_plan_info(int imax, int jmax, const int *indptr, const int *indices,
+                                int leaf, long long *out8)
+{
+    using namespace v2d;
+    V2D_ARG_CHECK(indptr && indices && out8, "lu_plan_info: null pointer");
+    MfPlan *P = nullptr;
+    V2D_TRY(mf_plan_build(imax, jmax, 2 * imax * jmax, indptr, indices, leaf, &P));
+    out8[0] = P->nfront;
+    out8[1] = P->nlevel;
+    out8[2] = P->maxS;
+    out8[3] = P->maxf;
+    out8[4] = P->ftotal;
+    out8[5] = (long long)P->flops;
+    out8[6] = P->vtotal;
+    out8[7] = P->utotal;
+    mf_plan_destroy(P);
+    return V2D_OK;
+}
+
+namespace v2d {
+
+// ================================================================ numeric
+namespace {
+
+constexpr int kMfThreads = 256;
+constexpr int kTrsmCols = 128;
+constexpr int kGemmTile = 64;
+
+template <class T> struct PanelWidth;
+template <> struct PanelWidth<float> { static constexpr int v = 32; };
+template <> struct PanelWidth<double> { static constexpr int v = 16; };
+
+// rs[r] = 1 / max_c |a_rc| (1 for an empty row).
+__global__ void k_rowscale(int n, const int *__restrict__ rowptr, const double *__restrict__ val,
+                           double *rs)
+{
+    V2D_GRID_STRIDE(r, n)
+    {
+        double m = 0.0;
+        for (int p = rowptr[r]; p < rowptr[r + 1]; ++p) m = fmax(m, fabs(val[p]));
+        rs[r] = m > 0.0 ? 1.0 / m : 1.0;
+    }
+}
+
+template <class T>
+__global__ void k_scatter(long long a0, long long a1, const int *__restrict__ csr,
+                          const int *__restrict__ row, const long long *__restrict__ pos,
+                          const double *__restrict__ val, const double *__restrict__ rs, T *F)
+{
+    for (long long e = a0 + (long long)blockIdx.x * blockDim.x + threadIdx.x; e < a1;
+         e += (long long)gridDim.x * blockDim.x)
+        F[pos[e]] += (T)(val[csr[e]] * rs[row[e]]);
+}
+
+// Add child `slot`'s contribution block into each front of the level.
+template <class T>
+__global__ void k_extend_add(int q0, int slot, const int *__restrict__ S, const int *__restrict__ f,
+                             const long long *__restrict__ foff, const int *__restrict__ uoff,
+                             const int *__restrict__ child0, const int *__restrict__ child1,
+                             const int *__restrict__ cbmap, T *F)
+{
+    const int P = q0 + blockIdx.y;
+    const int c = slot == 0 ? child0[P] : child1[P];
+    if (c < 0) return;
+    const int Sc = S[c], fc = f[c], m = fc - Sc, fp = f[P];
+    const T *src = F + foff[c];
+    T *dst = F + foff[P];
+    const int *map = cbmap + uoff[c];
+    const long long tot = (long long)m * m;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int a = (int)(e / m), b = (int)(e - (long long)a * m);
+        dst[(long long)map[a] * fp + map[b]] += src[(long long)(Sc + a) * fc + Sc + b];
+    }
+}
+
+// Block argmax of |v| (ties -> smallest index).
+template <class T>
+__device__ __forceinline__ void argmax_merge(T &bv, int &bi, T v, int i)
+{
+    if (v > bv || (v == bv && i < bi)) {
+        bv = v;
+        bi = i;
+    }
+}
+
+// Panel factorization of columns [k, k+w) of every front of the level with
+// S > k.  Rows [k, S) (fully summed) live in shared memory; row pivoting is
+// restricted to them.  Rows [S, f) get L21 = A21 U11^-1 (no pivoting).
+template <class T>
+__global__ void __launch_bounds__(kMfThreads) k_panel(int q0, int k, const int *__restrict__ S_,
+                                                      const int *__restrict__ f_,
+                                                      const long long *__restrict__ foff,
+                                                      const int *__restrict__ voff, T *F,
+                                                      int *ipiv, int *flag)
+{
+    constexpr int NB = PanelWidth<T>::v;
+    extern __shared__ unsigned char smem_raw[];
+    T *sp = reinterpret_cast<T *>(smem_raw);
+    __shared__ T red_v[kMfThreads / 32];
+    __shared__ int red_i[kMfThreads / 32];
+    __shared__ int piv_s;
+    const int q = q0 + blockIdx.x;
+    const int S = S_[q], f = f_[q];
+    if (S <= k) return;
+    const int w = min(NB, S - k);
+    const int R = S - k;  // fully summed rows in the panel
+    T *A = F + foff[q];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int e = tid; e < R * NB; e += blockDim.x) {
+        const int r = e / NB, c = e - r * NB;
+        sp[e] = c < w ? A[(long long)(k + r) * f + k + c] : T(0);
+    }
+    __syncthreads();
+    for (int c = 0; c < w; ++c) {
+        // pivot search over rows [c, R)
+        T bv = T(-1);
+        int bi = 0x7fffffff;
+        for (int r = c + tid; r < R; r += blockDim.x) argmax_merge(bv, bi, (T)fabs(sp[r * NB + c]), r);
+        for (int o = 16; o > 0; o >>= 1) {
+            T ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            argmax_merge(bv, bi, ov, oi);
+        }
+        if (lane == 0) { red_v[wid] = bv; red_i[wid] = bi; }
+        __syncthreads();
+        if (tid == 0) {
+            T v = red_v[0];
+            int i = red_i[0];
+            for (int u = 1; u < (int)(blockDim.x >> 5); ++u) argmax_merge(v, i, red_v[u], red_i[u]);
+            if (!(v > T(0))) atomicOr(flag, 1);   // zero (or NaN) pivot column
+            if (i < c || i >= R) i = c;           // all-NaN column: keep the diagonal
+            piv_s = i;
+            ipiv[voff[q] + k + c] = k + i;
+        }
+        __syncthreads();
+        const int p = piv_s;
+        if (p != c)
+            for (int u = tid; u < NB; u += blockDim.x) {
+                T t = sp[c * NB + u];
+                sp[c * NB + u] = sp[p * NB + u];
+                sp[p * NB + u] = t;
+            }
+        __syncthreads();
+        const T d = sp[c * NB + c];
+        const T inv = d != T(0) ? T(1) / d : T(0);
+        for (int r = c + 1 + tid; r < R; r += blockDim.x) sp[r * NB + c] *= inv;
+        __syncthreads();
+        const int nr = R - c - 1, ncol = w - c - 1;
+        for (int e = tid; e < nr * ncol; e += blockDim.x) {
+            const int r = c + 1 + e / ncol, cc = c + 1 + e % ncol;
+            sp[r * NB + cc] -= sp[r * NB + c] * sp[c * NB + cc];
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < R * w; e += blockDim.x) {
+        const int r = e / w, c = e - r * w;
+        A[(long long)(k + r) * f + k + c] = sp[r * NB + c];
+    }
+    // rows [S, f): x U = a  (U = upper triangle of the panel's top w rows)
+    for (int r = S + tid; r < f; r += blockDim.x) {
+        T x[NB];
+        T *row = A + (long long)r * f + k;
+#pragma unroll
+        for (int c = 0; c < NB; ++c) x[c] = c < w ? row[c] : T(0);
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+            if (c < w) {
+                T s = x[c];
+                for (int t = 0; t < c; ++t) s -= x[t] * sp[t * NB + c];
+                const T d = sp[c * NB + c];
+                x[c] = d != T(0) ? s / d : T(0);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+            if (c < w) row[c] = x[c];
+    }
+}
+
+// Row swaps of panel k applied to every column outside the panel (rows
+// [k, S)), then U12 = L11^-1 A12 for the panel's block row.
+template <class T>
+__global__ void __launch_bounds__(kTrsmCols) k_swap_trsm(int q0, int k, const int *__restrict__ S_,
+                                                         const int *__restrict__ f_,
+                                                         const long long *__restrict__ foff,
+                                                         const int *__restrict__ voff,
+                                                         T *F, const int *__restrict__ ipiv)
+{
+    constexpr int NB = PanelWidth<T>::v;
+    __shared__ T Ld[NB * NB];
+    __shared__ int pv[NB];
+    const int q = q0 + blockIdx.y;
+    const int S = S_[q], f = f_[q];
+    if (S <= k) return;
+    const int w = min(NB, S - k);
+    T *A = F + foff[q];
+    for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+        const int r = e / NB, c = e - r * NB;
+        Ld[e] = (r < w && c < w) ? A[(long long)(k + r) * f + k + c] : T(0);
+    }
+    for (int e = threadIdx.x; e < NB; e += blockDim.x) pv[e] = e < w ? ipiv[voff[q] + k + e] : 0;
+    __syncthreads();
+    const int col = blockIdx.x * kTrsmCols + threadIdx.x;
+    if (col >= f || (col >= k && col < k + w)) return;
+    for (int t = 0; t < w; ++t) {
+        const int p = pv[t];
+        if (p != k + t) {
+            T a = A[(long long)(k + t) * f + col];
+            A[(long long)(k + t) * f + col] = A[(long long)p * f + col];
+            A[(long long)p * f + col] = a;
+        }
+    }
+    if (col < k + w) return;
+    T x[NB];
+#pragma unroll
+    for (int t = 0; t < NB; ++t) {
+        if (t < w) {
+            T s = A[(long long)(k + t) * f + col];
+            for (int u = 0; u < t; ++u) s -= Ld[t * NB + u] * x[u];
+            x[t] = s;
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < NB; ++t)
+        if (t < w) A[(long long)(k + t) * f + col] = x[t];
+}
+
+// Trailing update A22 -= L21 U12 over rows/cols [k+w, f), 64x64 tiles.
+template <class T>
+__global__ void __launch_bounds__(256) k_gemm(int q0, int k, const int *__restrict__ S_,
+                                              const int *__restrict__ f_,
+                                              const long long *__restrict__ foff, T *F)
+{
+    constexpr int NB = PanelWidth<T>::v;
+    __shared__ T As[NB][kGemmTile + 1];
+    __shared__ T Bs[NB][kGemmTile];
+    const int q = q0 + blockIdx.y;
+    const int S = S_[q], f = f_[q];
+    if (S <= k) return;
+    const int w = min(NB, S - k);
+    const int base = k + w, rem = f - base;
+    if (rem <= 0) return;
+    const int nt = (rem + kGemmTile - 1) / kGemmTile;
+    if ((int)blockIdx.x >= nt * nt) return;
+    const int tr = blockIdx.x / nt, tc = blockIdx.x - tr * nt;
+    const int r0 = base + tr * kGemmTile, c0 = base + tc * kGemmTile;
+    T *A = F + foff[q];
+    const int tid = threadIdx.x;
+    for (int e = tid; e < kGemmTile * NB; e += blockDim.x) {
+        const int rr = e / NB, t = e - rr * NB;   // A tile: rows r0+rr, cols k+t
+        const int r = r0 + rr;
+        As[t][rr] = (r < f && t < w) ? A[(long long)r * f + k + t] : T(0);
+    }
+    for (int e = tid; e < NB * kGemmTile; e += blockDim.x) {
+        const int t = e / kGemmTile, cc = e - t * kGemmTile;
+        const int c = c0 + cc;
+        Bs[t][cc] = (c < f && t < w) ? A[(long long)(k + t) * f + c] : T(0);
+    }
+    __syncthreads();
+    const int ty = tid / 16, tx = tid % 16;  // 16x16 threads, 4x4 outputs each
+    T acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
+#pragma unroll 4
+    for (int t = 0; t < NB; ++t) {
+        T av[4], bv[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) av[a] = As[t][ty + 16 * a];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) bv[b] = Bs[t][tx + 16 * b];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int r = r0 + ty + 16 * a;
+        if (r >= f) continue;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int c = c0 + tx + 16 * b;
+            if (c < f) A[(long long)r * f + c] -= acc[a][b];
+        }
+    }
+}
+
+// ipiv (sequential swaps) -> perm (row i of the factors came from local row perm[i]).
+__global__ void k_perm(int q0, int q1, const int *__restrict__ S_, const int *__restrict__ voff,
+                       const int *__restrict__ ipiv, int *perm)
+{
+    const int q = q0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= q1) return;
+    const int S = S_[q], o = voff[q];
+    for (int i = 0; i < S; ++i) perm[o + i] = i;
+    for (int i = 0; i < S; ++i) {
+        const int p = ipiv[o + i];
+        const int t = perm[o + i];
+        perm[o + i] = perm[o + p];
+        perm[o + p] = t;
+    }
+}
+
+// ------------------------------------------------------------------ solve
+constexpr int kSolveThreads = 512;
+
+__device__ __forceinline__ bool stopped(const int *a, const int *b)
+{
+    return (a && *a) || (b && *b);
+}
+
+// Forward: w = P (rs .* b)|FS + children's updates; L11 z = w; upd = w2 - L21 z.
+template <class T>
+__global__ void __launch_bounds__(kSolveThreads) k_fwd(int q0, const MfDev D, const T *F, const T *b,
+                                                       const double *__restrict__ rs, T *zbuf,
+                                                       T *upd, const int *stop_a, const int *stop_b)
+{
+    if (stopped(stop_a, stop_b)) return;
+    extern __shared__ unsigned char smem_raw[];
+    T *w = reinterpret_cast<T *>(smem_raw);       // f
+    T *t2 = w + D.maxf;                             // S
+    const int q = q0 + blockIdx.x;
+    const int S = D.S[q], f = D.f[q], vo = D.voff[q];
+    const T *A = F + D.foff[q];
+    const int *vars = D.vars + vo;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+    for (int p = tid; p < f; p += blockDim.x) w[p] = p < S ? (T)(rs[vars[p]] * (double)b[vars[p]]) : T(0);
+    __syncthreads();
+    for (int slot = 0; slot < 2; ++slot) {
+        const int c = slot == 0 ? D.child0[q] : D.child1[q];
+        if (c >= 0) {
+            const int m = D.f[c] - D.S[c];
+            const int *map = D.cbmap + D.uoff[c];
+            const T *u = upd + D.uoff[c];
+            for (int e = tid; e < m; e += blockDim.x) w[map[e]] += u[e];
+        }
+        __syncthreads();
+    }
+    const int *perm = D.perm + vo;
+    for (int i = tid; i < S; i += blockDim.x) t2[i] = w[perm[i]];
+    __syncthreads();
+    for (int i = tid; i < S; i += blockDim.x) w[i] = t2[i];
+    __syncthreads();
+    // blocked unit-lower solve; rows below each block (FS and CB) updated by warps
+    for (int ib = 0; ib < S; ib += 32) {
+        const int bs = min(32, S - ib);
+        if (wid == 0) {
+            for (int t = 0; t < bs; ++t) {
+                const T zt = w[ib + t];
+                __syncwarp();
+                if (lane > t && lane < bs) w[ib + lane] -= A[(long long)(ib + lane) * f + ib + t] * zt;
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        const T zl = lane < bs ? w[ib + lane] : T(0);
+        for (int r = ib + bs + wid; r < f; r += nw) {
+            T v = lane < bs ? A[(long long)r * f + ib + lane] * zl : T(0);
+            v = warp_sum(v);
+            if (lane == 0) w[r] -= v;
+        }
+        __syncthreads();
+    }
+    for (int i = tid; i < S; i += blockDim.x) zbuf[vo + i] = w[i];
+    T *uo = upd + D.uoff[q];
+    for (int i = tid; i < f - S; i += blockDim.x) uo[i] = w[S + i];
+}
+
+// Backward: y = z - U12 x_struct; U11 x_FS = y; scatter.
+template <class T>
+__global__ void __launch_bounds__(kSolveThreads) k_bwd(int q0, const MfDev D, const T *F, const T *zbuf,
+                                                       T *x, const int *stop_a, const int *stop_b)
+{
+    if (stopped(stop_a, stop_b)) return;
+    extern __shared__ unsigned char smem_raw[];
+    T *y = reinterpret_cast<T *>(smem_raw);   // S
+    T *xs = y + D.maxS;                         // f - S
+    const int q = q0 + blockIdx.x;
+    const int S = D.S[q], f = D.f[q], vo = D.voff[q], m = f - S;
+    const T *A = F + D.foff[q];
+    const int *vars = D.vars + vo;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+    for (int i = tid; i < m; i += blockDim.x) xs[i] = x[vars[S + i]];
+    __syncthreads();
+    for (int r = wid; r < S; r += nw) {
+        T v = T(0);
+        for (int c = lane; c < m; c += 32) v += A[(long long)r * f + S + c] * xs[c];
+        v = warp_sum(v);
+        if (lane == 0) y[r] = zbuf[vo + r] - v;
+    }
+    __syncthreads();
+    const int nblk = (S + 31) / 32;
+    for (int bb = nblk - 1; bb >= 0; --bb) {
+        const int ib = bb * 32, bs = min(32, S - ib);
+        if (wid == 0) {
+            for (int t = bs - 1; t >= 0; --t) {
+                __syncwarp();
+                const T d = A[(long long)(ib + t) * f + ib + t];
+                const T xt = d != T(0) ? y[ib + t] / d : T(0);
+                __syncwarp();
+                if (lane == t) y[ib + t] = xt;
+                if (lane < t) y[ib + lane] -= A[(long long)(ib + lane) * f + ib + t] * xt;
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        const T xl = lane < bs ? y[ib + lane] : T(0);
+        for (int r = wid; r < ib; r += nw) {
+            T v = lane < bs ? A[(long long)r * f + ib + lane] * xl : T(0);
+            v = warp_sum(v);
+            if (lane == 0) y[r] -= v;
+        }
+        __syncthreads();
+    }
+    for (int i = tid; i < S; i += blockDim.x) x[vars[i]] = y[i];
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ host drivers
+int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
+{
+    *out = nullptr;
+    MfFactor *M = new MfFactor();
+    M->fp32 = fp32;
+    const size_t es = fp32 ? sizeof(float) : sizeof(double);
+    cudaError_t e = cudaSuccess;
+    auto grab = [&](void **p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+    };
+    grab(&M->F, (size_t)P->ftotal * es);
+    grab(&M->upd, (size_t)P->utotal * es);
+    grab(&M->z, (size_t)P->vtotal * es);
+    grab((void **)&M->rs, (size_t)P->n * sizeof(double));
+    grab((void **)&M->ipiv, (size_t)P->vtotal * sizeof(int));
+    grab((void **)&M->perm, (size_t)P->vtotal * sizeof(int));
+    grab((void **)&M->flag, sizeof(int));
+    if (e != cudaSuccess) {
+        set_error("mf_factor: allocation of %.1f MB failed: %s",
+                  ((double)P->ftotal * es) / 1e6, cudaGetErrorString(e));
+        mf_factor_destroy(M);
+        return V2D_ENOMEM;
+    }
+    // dynamic shared memory of the panel and solve kernels (set once, outside
+    // any stream capture)
+    const size_t panel = (size_t)P->maxS * (fp32 ? PanelWidth<float>::v * sizeof(float)
+                                                  : PanelWidth<double>::v * sizeof(double));
+    const size_t solve = (size_t)(P->maxf + P->maxS) * es;
+    if (panel > 227 * 1024 || solve > 227 * 1024) {
+        set_error("mf_factor: separator of %d / front of %d unknowns exceeds shared memory",
+                  P->maxS, P->maxf);
+        mf_factor_destroy(M);
+        return V2D_EARG;
+    }
+    if (fp32) {
+        e = cudaFuncSetAttribute(k_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_bwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve);
+    } else {
+        e = cudaFuncSetAttribute(k_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_bwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve);
+    }
+    if (e != cudaSuccess) {
+        set_error("mf_factor: %s", cudaGetErrorString(e));
+        mf_factor_destroy(M);
+        return V2D_ECUDA;
+    }
+    *out = M;
+    return V2D_OK;
+}
+
+void mf_factor_destroy(MfFactor *M)
+{
+    if (!M) return;
+    if (M->graph) cudaGraphExecDestroy(M->graph);
+    void *ptrs[] = {M->F, M->upd, M->z, M->rs, M->ipiv, M->perm, M->flag};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    delete M;
+}
+
+MfDev mf_dev(const MfPlan *P, const MfFactor *M)
+{
+    MfDev D;
+    D.S = P->d_S; D.f = P->d_f; D.voff = P->d_voff; D.uoff = P->d_uoff;
+    D.child0 = P->d_child0; D.child1 = P->d_child1; D.foff = P->d_foff;
+    D.vars = P->d_vars; D.cbmap = P->d_cbmap; D.perm = M->perm;
+    D.maxS = P->maxS; D.maxf = P->maxf;
+    return D;
+}
+
+template <class T>
+static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, const double *val,
+                           cudaStream_t s)
+{
+    constexpr int NB = PanelWidth<T>::v;
+    T *F = (T *)M->F;
+    long long launches = 0;
+    k_rowscale<<<grid_for(P->n, 256), 256, 0, s>>>(P->n, rowptr, val, M->rs);
+    ++launches;
+    const size_t panel_smem = (size_t)P->maxS * NB * sizeof(T);
+    for (int L = 0; L < P->nlevel; ++L) {
+        const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
+        V2D_CUDA_TRY(cudaMemsetAsync(F + P->lvl_fbeg[L], 0,
+                                     (size_t)(P->lvl_fend[L] - P->lvl_fbeg[L]) * sizeof(T), s));
+        const long long na = P->lvl_aend[L] - P->lvl_abeg[L];
+        if (na > 0) {
+            k_scatter<T><<<grid_for(na, 256), 256, 0, s>>>(P->lvl_abeg[L], P->lvl_aend[L],
+                                                         P->d_asm_csr, P->d_asm_row,
+                                                         P->d_asm_pos, val, M->rs, F);
+            ++launches;
+        }
+        if (L > 0) {
+            const long long mm = (long long)P->lvl_maxm_child[L] * P->lvl_maxm_child[L];
+            const int gx = (int)std::max(1LL, std::min<long long>((mm + 255) / 256, 64));
+            for (int slot = 0; slot < 2; ++slot) {
+                k_extend_add<T><<<dim3(gx, nq), 256, 0, s>>>(q0, slot, P->d_S, P->d_f, P->d_foff,
+                                                             P->d_uoff, P->d_child0, P->d_child1,
+                                                             P->d_cbmap, F);
+                ++launches;
+            }
+        }
+        const int maxf = P->lvl_maxf[L];
+        for (int k = 0; k < P->lvl_maxS[L]; k += NB) {
+            k_panel<T><<<nq, kMfThreads, panel_smem, s>>>(q0, k, P->d_S, P->d_f, P->d_foff,
+                                                          P->d_voff, F, M->ipiv, M->flag);
+            const int gcol = (maxf + kTrsmCols - 1) / kTrsmCols;
+            k_swap_trsm<T><<<dim3(gcol, nq), kTrsmCols, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff,
+                                                                P->d_voff, F, M->ipiv);
+            const int rem = std::max(1, maxf - k - 1);
+            const int nt = (rem + kGemmTile - 1) / kGemmTile;
+            k_gemm<T><<<dim3(nt * nt, nq), 256, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff, F);
+            launches += 3;
+        }
+        k_perm<<<(nq + 127) / 128, 128, 0, s>>>(q0, q0 + nq, P->d_S, P->d_voff, M->ipiv, M->perm);
+        ++launches;
+    }
+    V2D_CUDA_TRY(cudaGetLastError());
+    M->launches_per_factor = launches;
+    return V2D_OK;
+}
+
+int mf_factor(const MfPlan *P, MfFactor *M, const int *rowptr, const double *val, cudaStream_t s)
+{
+    if (!M->graph || M->graph_val != val || M->graph_rowptr != rowptr) {
+        if (M->graph) cudaGraphExecDestroy(M->graph);
+        M->graph = nullptr;
+        cudaGraph_t g = nullptr;
+        V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        int st = M->fp32 ? factor_launches<float>(P, M, rowptr, val, s)
+                         : factor_launches<double>(P, M, rowptr, val, s);
+        cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (st != V2D_OK) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        if (e != cudaSuccess) {
+            set_error("mf_factor: graph capture failed: %s", cudaGetErrorString(e));
+            return V2D_ECUDA;
+        }
+        e = cudaGraphInstantiate(&M->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            set_error("mf_factor: graph instantiate failed: %s", cudaGetErrorString(e));
+            return V2D_ECUDA;
+        }
+        M->graph_val = val;
+        M->graph_rowptr = rowptr;
+    }
+    V2D_CUDA_TRY(cudaMemsetAsync(M->flag, 0, sizeof(int), s));
+    V2D_CUDA_TRY(cudaGraphLaunch(M->graph, s));
+    count_launches(M->launches_per_factor);
+    return V2D_OK;
+}
+
+template <class T>
+static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, const int *stop_a,
+                          const int *stop_b, cudaStream_t s)
+{
+    const MfDev D = mf_dev(P, M);
+    const T *F = (const T *)M->F;
+    const size_t smf = (size_t)(P->maxf + P->maxS) * sizeof(T);
+    for (int L = 0; L < P->nlevel; ++L) {
+        const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
+        k_fwd<T><<<nq, kSolveThreads, smf, s>>>(q0, D, F, b, M->rs, (T *)M->z, (T *)M->upd, stop_a,
+                                                stop_b);
+    }
+    for (int L = P->nlevel - 1; L >= 0; --L) {
+        const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
+        k_bwd<T><<<nq, kSolveThreads, smf, s>>>(q0, D, F, (const T *)M->z, x, stop_a, stop_b);
+    }
+    V2D_CUDA_TRY(cudaGetLastError());
+    count_launches(2LL * P->nlevel);
+    return V2D_OK;
+}
+
+int mf_apply(const MfPlan *P, const MfFactor *M, const void *b, void *x, const int *stop_a,
+             const int *stop_b, cudaStream_t s)
+{
+    if (M->fp32) return apply_launches<float>(P, M, (const float *)b, (float *)x, stop_a, stop_b, s);
+    return apply_launches<double>(P, M, (const double *)b, (double *)x, stop_a, stop_b, s);
+}
+
+int mf_flag(const MfFactor *M, int *flag, cudaStream_t s)
+{
+    V2D_CUDA_TRY(cudaMemcpyAsync(flag, M->flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    return V2D_OK;
+}
+
+}  // namespace v2d

@@ -4,11 +4,13 @@
 // the canonical CSR Jacobian, right-hand side, block inverses and the Krylov
 // workspace -- lives in HBM behind one handle.  One Newton iteration is:
 // fused assembly kernel (values written into fixed CSR slots + b + 2x2 block
-// inverses), GMRES(m) on the device, and a fused update kernel
-// (q += dq and ||dq||_2 in one pass).  The host reads one scalar per Newton
+// inverses), with the LU preconditioner the multifrontal factorization of the
+// new Jacobian (one CUDA graph), GMRES(m) on the device, and a fused update
+// kernel (q += dq and ||dq||_2 in one pass).  The host reads one scalar per Newton
 // iteration to decide whether to continue, as the reference's loop does.
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "v2d_internal.cuh"
 
@@ -29,6 +31,9 @@ struct v2d_solver {
     int pattern_ff_bc = -1;
     double pattern_ca = 0, pattern_sa = 0;
     bool assembled = false;
+    MfPlan *plan = nullptr;        // multifrontal plan of the current pattern
+    int plan_leaf = 0;
+    MfFactor *lu[2] = {nullptr, nullptr};  // [0] FP64 factors, [1] FP32 factors
 };
 
 namespace {
@@ -96,11 +101,21 @@ int check_params(const v2d_solver_params *p)
                   "krylov restart must be in [1, 256] (got %d)", p->krylov.restart);
     V2D_ARG_CHECK(p->krylov.max_it >= 1, "krylov max_it must be >= 1");
     V2D_ARG_CHECK(p->krylov.precond == V2D_PC_NONE || p->krylov.precond == V2D_PC_BJACOBI ||
-                      p->krylov.precond == V2D_PC_MG,
+                      p->krylov.precond == V2D_PC_LU,
                   "unknown preconditioner %d", p->krylov.precond);
     V2D_ARG_CHECK(p->krylov.precision == V2D_PREC_FP64 || p->krylov.precision == V2D_PREC_MIXED,
                   "unknown precision %d", p->krylov.precision);
     return V2D_OK;
+}
+
+void drop_lu(v2d_solver *S)
+{
+    for (int q = 0; q < 2; ++q) {
+        mf_factor_destroy(S->lu[q]);
+        S->lu[q] = nullptr;
+    }
+    mf_plan_destroy(S->plan);
+    S->plan = nullptr;
 }
 
 int ensure_pattern(v2d_solver *S)
@@ -113,6 +128,28 @@ int ensure_pattern(v2d_solver *S)
     S->pattern_ca = p.ca;
     S->pattern_sa = p.sa;
     S->assembled = false;
+    drop_lu(S);   // the multifrontal plan follows the pattern
+    return V2D_OK;
+}
+
+// Multifrontal plan (once per pattern) and factor storage of the current precision.
+int ensure_lu(v2d_solver *S)
+{
+    const v2d_krylov_params &k = S->prm.krylov;
+    if (k.precond != V2D_PC_LU) return V2D_OK;
+    const int leaf = k.lu_leaf > 0 ? k.lu_leaf : 64;
+    if (S->plan && S->plan_leaf != leaf) drop_lu(S);
+    if (!S->plan) {
+        const GridDev &g = S->g;
+        std::vector<int> rp(g.n + 1), ci(g.nnz);
+        V2D_CUDA_TRY(cudaMemcpyAsync(rp.data(), g.rowptr, (g.n + 1) * sizeof(int), cudaMemcpyDeviceToHost, S->s));
+        V2D_CUDA_TRY(cudaMemcpyAsync(ci.data(), g.colind, g.nnz * sizeof(int), cudaMemcpyDeviceToHost, S->s));
+        V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+        V2D_TRY(mf_plan_create(g.imax, g.jmax, g.n, rp.data(), ci.data(), leaf, &S->plan));
+        S->plan_leaf = leaf;
+    }
+    const int q = k.precision == V2D_PREC_MIXED ? 1 : 0;
+    if (!S->lu[q]) V2D_TRY(mf_factor_create(S->plan, q, &S->lu[q]));
     return V2D_OK;
 }
 
@@ -145,9 +182,7 @@ extern "C" void v2d_krylov_defaults(v2d_krylov_params *p)
     p->precision = V2D_PREC_FP64;
     p->inner_rtol = 1e-5;
     p->dc_max_it = 20;
-    p->mg_levels = 0;
-    p->mg_smooth = 2;
-    p->mg_omega = 0.7;
+    p->lu_leaf = 64;
 }
 
 extern "C" int v2d_solver_destroy(v2d_solver *S)
@@ -155,6 +190,7 @@ extern "C" int v2d_solver_destroy(v2d_solver *S)
     if (!S) return V2D_OK;
     if (S->s) cudaStreamSynchronize(S->s);
     GridDev &g = S->g;
+    drop_lu(S);
     void *ptrs[] = {g.x, g.rowptr, g.colind, g.val, g.val32, g.b, g.dinv, g.dinv32,
                     S->delta, S->partial, S->scal, S->flag, S->counter};
     for (void *p : ptrs)
@@ -218,6 +254,7 @@ extern "C" int v2d_solver_create(int imax, int jmax, const double *xg, const dou
         if (cudaGetLastError() != cudaSuccess) st = V2D_ECUDA;
     }
     if (st == V2D_OK) st = ensure_pattern(S);
+    if (st == V2D_OK) st = ensure_lu(S);
     if (st == V2D_OK) st = krylov_create(&S->kw, g.n, p->krylov.restart, S->s);
     if (st == V2D_OK && cudaStreamSynchronize(S->s) != cudaSuccess) {
         set_error("solver_create: %s", cudaGetErrorString(cudaGetLastError()));
@@ -238,6 +275,7 @@ extern "C" int v2d_solver_set_params(v2d_solver *S, const v2d_solver_params *p)
     const int old_m = S->prm.krylov.restart;
     S->prm = *p;
     V2D_TRY(ensure_pattern(S));
+    V2D_TRY(ensure_lu(S));
     if (p->krylov.restart != old_m) {
         V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
         krylov_destroy(S->kw);
@@ -313,6 +351,13 @@ extern "C" int v2d_solver_newton(v2d_solver *S, double urot, double *res, v2d_li
     CsrOp A;
     A.n = g.n; A.nnz = g.nnz; A.rowptr = g.rowptr; A.colind = g.colind; A.val = g.val;
     A.val32 = g.val32; A.dinv = g.dinv; A.dinv32 = g.dinv32; A.layout = 1; A.nblk = g.N;
+    if (S->prm.krylov.precond == V2D_PC_LU) {
+        V2D_TRY(ensure_lu(S));
+        MfFactor *M = S->lu[S->prm.krylov.precision == V2D_PREC_MIXED ? 1 : 0];
+        V2D_TRY(mf_factor(S->plan, M, g.rowptr, g.val, S->s));
+        A.lu_plan = S->plan;
+        A.lu = M;
+    }
     v2d_lin_stats ls{};
     V2D_TRY(krylov_solve(S->kw, A, g.b, S->delta, S->prm.krylov, &ls, S->s));
     if (st) *st = ls;
