@@ -1,6 +1,10 @@
 """Benchmark: unsteady BDF2 dual-time cylinder (181x181 O-grid, Re=100,
 dt=0.2, rotational kick 0.5 until t=2, outflow far field, <=5 Newton
-iterations per step, GMRES(30) with 2x2 block Jacobi).
+iterations per step, GMRES(30)).  The Krylov solve is preconditioned with
+the multifrontal LU of each Newton Jacobian: GMRES(30) with 2x2 block Jacobi
+does not converge on these pure-Newton (dtau = inf) systems (it stops at the
+iteration limit every Newton step), so it would not reproduce the reference's
+direct-solve results.
 
 One "step" is one BDF2 physical time step through the device solver.
 ``value`` = whole-job BDF2 steps/s with the state resident in HBM (headline:
@@ -33,8 +37,8 @@ IMAX = JMAX = 181
 WORKLOAD = dict(re=100.0, steady=False, dt_phys=0.2, rot_speed=0.5, rot_until=2.0,
                 farfield_bc="outflow")
 SOLVER = dict(ksp_restart=30, ksp_rtol=1e-10, krylov_max_it=3000, pseudo_tol=1e-10,
-              max_pseudo_iter=5, precond="bjacobi")
-METRIC = "BDF2 steps/s, 181x181 cylinder O-grid Re=100 dt=0.2 (<=5 Newton, GMRES(30)+block-Jacobi)"
+              max_pseudo_iter=5, precond="lu")
+METRIC = "BDF2 steps/s, 181x181 cylinder O-grid Re=100 dt=0.2 (<=5 Newton, GMRES(30))"
 L2_FLUSH_BYTES = 256 << 20
 SPMV_BYTES_PER_NNZ = {"fp64": 8 + 4, "fp32": 4 + 4}
 
@@ -165,6 +169,37 @@ def timed_steps(torch, s, times, k0, K, flush_buf):
     return ms, newton, krylov
 
 
+def phase_times(_lib, s, reset=False):
+    """(assembly, factorization, Krylov, update) device ms summed over Newton
+    iterations, and the iteration count."""
+    import ctypes
+    out = (ctypes.c_double * 5)()
+    _lib.check(_lib.lib().v2d_solver_phase_times(s.dev.h, out, int(reset)))
+    return list(out)
+
+
+def profile_newton(args):
+    """One warm-up BDF2 step of the workload (captures the CUDA graphs), then
+    exactly one Newton iteration inside the NVTX range "v2d_newton"; for
+    `ncu --nvtx --nvtx-include v2d_newton/` launch lists of one iteration."""
+    import torch
+    import vorti2d_b200 as v
+    torch.cuda.set_device(0)
+    xg, yg = v.generate_cylinder(IMAX, JMAX)
+    prec = "mixed" if args.precision == "both" else args.precision
+    s = make_solver(v, xg, yg, prec)
+    times = s.times()
+    s.advance(times[0])
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("v2d_newton")
+    code, res, lin = s.dev.newton(s.cfg.u_rot(times[1]))
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    print(json.dumps({"profile": "one Newton iteration", "precision": prec, "code": code,
+                      "res": res, "krylov_its": lin.iterations}), flush=True)
+    s.close()
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import vorti2d_b200 as v
@@ -184,19 +219,24 @@ def run_ours(args, rank, world, local_rank):
         barrier(world)
         torch.cuda.synchronize()
         clocks = ClockSampler(local_rank).start() if prec == legs[0] else None
+        phase_times(_lib, s, reset=True)
         c0 = _lib.lib().v2d_launch_count()
         t0 = time.perf_counter()
         ms, nit, kit = timed_steps(torch, s, times, W, K, flush_buf)
         wall = time.perf_counter() - t0
         c1 = _lib.lib().v2d_launch_count()
+        ph = phase_times(_lib, s)
         if clocks is not None:
             results["clocks"] = clocks.stop()
         torch.cuda.synchronize()
         barrier(world)
         tot_ms = max_over_ranks(sum(ms), world, "cuda")
         fc = s.force_coeffs()
+        nn = max(ph[4], 1.0)
         results[prec] = dict(ms_per_step=tot_ms / K, newton=nit / K, krylov=kit / K,
-                             cd=fc.cd, cl=fc.cl, wall_s=wall, t_end=times[W + K - 1])
+                             cd=fc.cd, cl=fc.cl, wall_s=wall, t_end=times[W + K - 1],
+                             ms_per_newton={"assembly": ph[0] / nn, "factor": ph[1] / nn,
+                                            "krylov": ph[2] / nn, "update": ph[3] / nn})
         launches[prec] = c1 - c0
         if prec == legs[0]:
             # dominant kernel (SpMV of the Krylov loop), timed alone after L2 flushes
@@ -266,8 +306,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
     ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--profile-newton", action="store_true",
+                    help="one warm-up step, then one Newton iteration in NVTX range v2d_newton")
     args = ap.parse_args()
     rank, world, local_rank = dist_env()
+    if args.profile_newton:
+        profile_newton(args)
+        return
 
     if args.impl == "reference":
         # CPU restatement on rank 0 only; other ranks exit without work
@@ -317,7 +362,8 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32-krylov/f64" if head == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": "unsteady BDF2 cylinder 181x181 Re=100 dt=0.2 kick 0.5<=2 outflow",
-                   "precision": head, "newton_max": 5, "krylov": "GMRES(30)+2x2 block Jacobi",
+                   "precision": head, "newton_max": 5,
+                   "krylov": "GMRES(30), multifrontal LU preconditioner (FP32 factors in mixed)",
                    "l2": "flushed (256 MiB write) before every timed step",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": world * res["e2e"]["steps_per_s"], "unit": "steps/s",

@@ -131,7 +131,11 @@ int v2d_force_coeffs(int imax, int jmax, double re, double dksi, double deta,
 typedef struct {
     int restart;          /* GMRES(m) restart length                  (30)   */
     int max_it;           /* max Krylov iterations per solve          (5000) */
-    double rtol;          /* relative residual tolerance              (1e-10)*/
+    double rtol;          /* relative residual tolerance (1e-10); a solve whose
+                             FP64 residual stops halving per restart cycle
+                             within 100x of the target has reached the
+                             attainable accuracy: it ends there and counts
+                             as converged                                    */
     double atol;          /* absolute residual tolerance              (1e-50)*/
     int precond;          /* V2D_PC_*                                         */
     int precision;        /* V2D_PREC_*                                       */
@@ -247,6 +251,12 @@ int v2d_solver_time_spmv(v2d_solver *s, int fp32, int reps, long long flush_byte
  * entries. */
 int v2d_lu_plan_info(int imax, int jmax, const int *indptr, const int *indices, int leaf,
                      long long *out8);
+
+/* Measurement aid (no reference counterpart): device time in ms, summed over
+ * the Newton iterations since the last reset, of the four phases of a Newton
+ * iteration (CUDA events on the handle's stream): out5 = assembly,
+ * factorization (LU preconditioner), Krylov solve, update, iteration count. */
+int v2d_solver_phase_times(v2d_solver *s, double *out5, int reset);
 
 /* The stream the handle's kernels run on (cudaStream_t as void*). */
 int v2d_solver_stream(v2d_solver *s, void **stream);

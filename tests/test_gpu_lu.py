@@ -66,7 +66,8 @@ def test_config1_steady_129_matches_oracle(v2d, oracle_mod):
     xg, yg = oracle_mod.generate_cylinder(imax, jmax)
     ref = oracle_mod.OracleSolver(xg, yg, re=40.0, steady=True, pseudo_tol=1e-12,
                                   max_pseudo_iter=40).run()
-    s = v2d.Solver(cfg(v2d, re=40.0, steady=True, max_pseudo_iter=40), mesh=(xg, yg))
+    s = v2d.Solver(cfg(v2d, re=40.0, steady=True, max_pseudo_iter=40, ksp_rtol=1e-10),
+                   mesh=(xg, yg))
     s.advance(0.0)
     assert s.newton_log[-1][3] <= 1e-12
     assert _close(s.psi, ref.psi, 1e-9) and _close(s.ome, ref.ome, 1e-9)

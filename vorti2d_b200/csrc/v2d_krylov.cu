@@ -13,7 +13,9 @@
 //    updated by the last block of a reduction, so a whole restart cycle runs
 //    without the host; a device control block makes the remaining kernels of
 //    a cycle exit at once after convergence or breakdown.
-//  * Each cycle is captured once as a CUDA graph and replayed.
+//  * Each cycle is captured once as a few CUDA graphs (Arnoldi segments of
+//    growing length + a finishing graph) and replayed; the host checks the
+//    control block between segments.
 //  * Preconditioners: 2x2 (psi, ome) block Jacobi applied inline, or the
 //    multifrontal LU of the current Jacobian (v2d_mf.cu) applied by its own
 //    per-level kernels; with LU the preconditioned vectors Z_j = M^-1 v_j are
@@ -52,6 +54,8 @@ struct Ctl {
     int breakdown;
     int cycles;
     int nonfinite;
+    int stagnated;       // a cycle failed to halve the residual near the target
+    double prev_beta;
     unsigned int cnt[4]; // last-block counters
 };
 
@@ -82,7 +86,9 @@ struct KrylovWork {
     Ctl *ctl = nullptr;
     Ctl *ctl_host = nullptr;      // pinned mirror
     Desc *desc = nullptr;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    std::vector<cudaGraphExec_t> seg[2];   // Arnoldi segments per precision
+    std::vector<int> seg_bounds[2];
+    cudaGraphExec_t fin[2] = {nullptr, nullptr};
     int graph_m[2] = {0, 0};
     int graph_pc[2] = {-1, -1};
     const void *graph_lu[2] = {nullptr, nullptr};
@@ -475,9 +481,14 @@ __global__ void __launch_bounds__(kSpmvThreads) k_residual(const Desc *d, Ctl *c
                 ctl->conv = 1;
             } else if (beta <= ctl->tol_abs || beta == 0.0) {
                 ctl->conv = 1;
+            } else if (!first && beta > 0.5 * ctl->prev_beta && beta <= 100.0 * ctl->tol_abs) {
+                // the FP64 residual has reached the attainable accuracy
+                ctl->stagnated = 1;
+                ctl->conv = 1;
             } else if (ctl->its >= ctl->max_it || ctl->breakdown) {
                 ctl->conv = 1;  // stop: not converged (host reads beta)
             }
+            ctl->prev_beta = beta;
             // next cycle
             g[0] = beta;
             for (int i = 1; i <= m; ++i) g[i] = 0.0;
@@ -509,9 +520,54 @@ static int tile_grid(long long n)
     return (int)std::max(1LL, std::min<long long>(kTileBlocks, g));
 }
 
+// A restart cycle runs as a few captured segments of Arnoldi steps of
+// growing length ([0,2), [2,6), [6,14), ...), then a finishing graph
+// (back-substitution, correction, FP64 residual).  The host reads the control
+// block after each segment and skips the remaining segments once the cycle
+// has stopped, so a cycle that converges in a few steps (the usual case with
+// the LU preconditioner) does not pay for launching m steps.
+static std::vector<int> segment_bounds(int m)
+{
+    std::vector<int> b{0};
+    int len = 2;
+    while (b.back() < m) {
+        b.push_back(std::min(m, b.back() + len));
+        len *= 2;
+    }
+    return b;
+}
+
+static int end_capture(cudaStream_t s, cudaGraphExec_t *out)
+{
+    cudaGraph_t gph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &gph);
+    if (e != cudaSuccess) {
+        if (gph) cudaGraphDestroy(gph);
+        set_error("GMRES graph capture failed: %s", cudaGetErrorString(e));
+        return V2D_ECUDA;
+    }
+    e = cudaGraphInstantiate(out, gph, 0);
+    cudaGraphDestroy(gph);
+    if (e != cudaSuccess) {
+        *out = nullptr;
+        set_error("GMRES graph instantiate failed: %s", cudaGetErrorString(e));
+        return V2D_ECUDA;
+    }
+    return V2D_OK;
+}
+
+static void drop_graphs(KrylovWork *w, int which)
+{
+    for (cudaGraphExec_t g : w->seg[which])
+        if (g) cudaGraphExecDestroy(g);
+    w->seg[which].clear();
+    if (w->fin[which]) cudaGraphExecDestroy(w->fin[which]);
+    w->fin[which] = nullptr;
+}
+
 template <class T>
-static int run_cycles(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, double *x, int ncycles,
-                      const CsrOp &A, int precond, cudaStream_t s)
+static int capture_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, double *x,
+                         const CsrOp &A, int precond, cudaStream_t s)
 {
     const int n = w->n;
     const int gp = grid_for(n, 256);
@@ -519,14 +575,11 @@ static int run_cycles(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, double 
     const int gr = red_grid(n);
     const int gt = tile_grid(n);
     const bool lu = precond == V2D_PC_LU;
-    long long per_cycle = 6LL * w->m + 3;
-    if (!w->graph[which] || w->graph_m[which] != w->m || w->graph_pc[which] != precond ||
-        w->graph_lu[which] != (lu ? (const void *)A.lu : nullptr)) {
-        if (w->graph[which]) cudaGraphExecDestroy(w->graph[which]);
-        w->graph[which] = nullptr;
-        cudaGraph_t gph;
+    drop_graphs(w, which);
+    const std::vector<int> bnd = segment_bounds(w->m);
+    for (size_t q = 0; q + 1 < bnd.size(); ++q) {
         V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        for (int j = 0; j < w->m; ++j) {
+        for (int j = bnd[q]; j < bnd[q + 1]; ++j) {
             k_scale_precond<T><<<gp, 256, 0, s>>>(w->desc, w->ctl, j, w->r, wv, V, w->H, z);
             T *zj = z;
             if (lu) {
@@ -534,7 +587,7 @@ static int run_cycles(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, double 
                 int st = mf_apply(A.lu_plan, A.lu, V + (size_t)j * n, zj, &w->ctl->conv,
                                   &w->ctl->cyc_stop, s);
                 if (st != V2D_OK) {
-                    cudaGraph_t junk;
+                    cudaGraph_t junk = nullptr;
                     cudaStreamEndCapture(s, &junk);
                     if (junk) cudaGraphDestroy(junk);
                     return st;
@@ -549,27 +602,46 @@ static int run_cycles(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, double 
                                                        w->H, w->hcur, w->g, w->cs, w->sn);
             }
         }
-        k_backsolve<<<1, 32, 0, s>>>(w->desc, w->ctl, w->H, w->g, w->y);
-        k_correct<T><<<gp, 256, 0, s>>>(w->desc, w->ctl, V, w->y, z, x, Z);
-        k_residual<<<gr, kSpmvThreads, 0, s>>>(w->desc, w->ctl, w->r, w->partial, w->g, 0);
-        cudaError_t e = cudaStreamEndCapture(s, &gph);
-        if (e != cudaSuccess) {
-            set_error("GMRES graph capture failed: %s", cudaGetErrorString(e));
-            return V2D_ECUDA;
-        }
-        e = cudaGraphInstantiate(&w->graph[which], gph, 0);
-        cudaGraphDestroy(gph);
-        if (e != cudaSuccess) {
-            set_error("GMRES graph instantiate failed: %s", cudaGetErrorString(e));
-            return V2D_ECUDA;
-        }
-        w->graph_m[which] = w->m;
-        w->graph_pc[which] = precond;
-        w->graph_lu[which] = lu ? (const void *)A.lu : nullptr;
+        cudaGraphExec_t ge = nullptr;
+        V2D_TRY(end_capture(s, &ge));
+        w->seg[which].push_back(ge);
     }
-    if (lu) per_cycle += 2LL * A.lu_plan->nlevel * w->m;
-    for (int c = 0; c < ncycles; ++c) V2D_CUDA_TRY(cudaGraphLaunch(w->graph[which], s));
-    count_launches((long long)ncycles * per_cycle);
+    V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    k_backsolve<<<1, 32, 0, s>>>(w->desc, w->ctl, w->H, w->g, w->y);
+    k_correct<T><<<gp, 256, 0, s>>>(w->desc, w->ctl, V, w->y, z, x, Z);
+    k_residual<<<gr, kSpmvThreads, 0, s>>>(w->desc, w->ctl, w->r, w->partial, w->g, 0);
+    V2D_TRY(end_capture(s, &w->fin[which]));
+    w->seg_bounds[which] = bnd;
+    w->graph_m[which] = w->m;
+    w->graph_pc[which] = precond;
+    w->graph_lu[which] = lu ? (const void *)A.lu : nullptr;
+    return V2D_OK;
+}
+
+// One restart cycle; *h receives the control block at its end.
+template <class T>
+static int run_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, double *x, const CsrOp &A,
+                     int precond, cudaStream_t s, Ctl *h)
+{
+    const bool lu = precond == V2D_PC_LU;
+    if (w->seg[which].empty() || !w->fin[which] || w->graph_m[which] != w->m ||
+        w->graph_pc[which] != precond ||
+        w->graph_lu[which] != (lu ? (const void *)A.lu : nullptr))
+        V2D_TRY(capture_cycle<T>(w, which, V, wv, z, Z, x, A, precond, s));
+    const long long per_step = 6 + (lu ? 2LL * A.lu_plan->nlevel : 0);
+    const std::vector<int> &bnd = w->seg_bounds[which];
+    for (size_t q = 0; q < w->seg[which].size(); ++q) {
+        V2D_CUDA_TRY(cudaGraphLaunch(w->seg[which][q], s));
+        count_launches(per_step * (bnd[q + 1] - bnd[q]));
+        V2D_CUDA_TRY(cudaMemcpyAsync(w->ctl_host, w->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+        V2D_CUDA_TRY(cudaStreamSynchronize(s));
+        if (w->ctl_host->cyc_stop || w->ctl_host->conv) break;
+    }
+    V2D_CUDA_TRY(cudaGraphLaunch(w->fin[which], s));
+    count_launches(3);
+    V2D_CUDA_TRY(cudaMemcpyAsync(w->ctl_host, w->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(s));
+    *h = *w->ctl_host;
     return V2D_OK;
 }
 
@@ -610,8 +682,7 @@ int krylov_create(KrylovWork **out, int n, int restart, cudaStream_t s)
 void krylov_destroy(KrylovWork *w)
 {
     if (!w) return;
-    for (int q = 0; q < 2; ++q)
-        if (w->graph[q]) cudaGraphExecDestroy(w->graph[q]);
+    for (int q = 0; q < 2; ++q) drop_graphs(w, q);
     void *ptrs[] = {w->V64, w->w64, w->z64, w->Z64, w->V32, w->w32, w->z32, w->Z32, w->r, w->H, w->g,
                     w->cs, w->sn, w->y, w->hcur, w->partial, w->ctl, w->desc};
     for (void *p : ptrs)
@@ -676,21 +747,16 @@ int krylov_solve(KrylovWork *w, const CsrOp &A, const double *d_b, double *d_x,
         V2D_CUDA_TRY(cudaMemcpyAsync(&w->ctl->tol_abs, &ta, sizeof(double), cudaMemcpyHostToDevice, s));
         if (h.beta <= ta) h.conv = 1;
     }
-    int batch = 1;
     int guard = 0;
     while (!h.conv) {
-        int status = fp32 ? run_cycles<float>(w, 1, w->V32, w->w32, w->z32, w->Z32, d_x, batch, A,
-                                              hd.precond, s)
-                          : run_cycles<double>(w, 0, w->V64, w->w64, w->z64, w->Z64, d_x, batch, A,
-                                               hd.precond, s);
+        int status = fp32 ? run_cycle<float>(w, 1, w->V32, w->w32, w->z32, w->Z32, d_x, A,
+                                             hd.precond, s, &h)
+                          : run_cycle<double>(w, 0, w->V64, w->w64, w->z64, w->Z64, d_x, A,
+                                              hd.precond, s, &h);
         if (status != V2D_OK) return status;
-        V2D_CUDA_TRY(cudaMemcpyAsync(w->ctl_host, w->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
-        V2D_CUDA_TRY(cudaStreamSynchronize(s));
-        h = *w->ctl_host;
-        batch = std::min(batch * 2, 8);
         if (++guard > 1000000) break;
     }
-    const bool converged = h.beta <= fmax(h.tol_abs, prm.atol) && !h.nonfinite;
+    const bool converged = (h.beta <= fmax(h.tol_abs, prm.atol) || h.stagnated) && !h.nonfinite;
     if (st) {
         st->iterations = h.its;
         st->restarts = h.cycles;

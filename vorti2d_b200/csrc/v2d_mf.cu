@@ -28,9 +28,10 @@
 //  row-scaled CSR values scattered into the zeroed fronts, children's
 //  contribution blocks added (one child slot per launch: deterministic, no
 //  atomics), then a blocked right-looking partial LU of each front: panel
-//  (one CTA per front, partial pivoting among the fully summed rows, the panel
-//  held in shared memory), row swaps + TRSM for the U12 block row, GEMM update
-//  of the trailing block (which leaves the Schur complement for the parent).
+//  (one CTA per front; one warp factors the diagonal block in registers with
+//  pivoting among the block's rows, the other rows get L by a TRSM), row
+//  swaps + TRSM for the U12 block row, GEMM update of the trailing block
+//  (which leaves the Schur complement for the parent).
 //
 // Solve (device): forward per level bottom-up (gather, permute, unit-lower
 // solve, contribution vector for the parent), backward top-down (U12 x_struct,
@@ -498,19 +499,13 @@ __global__ void k_extend_add(int q0, int slot, const int *__restrict__ S, const 
     }
 }
 
-// Block argmax of |v| (ties -> smallest index).
-template <class T>
-__device__ __forceinline__ void argmax_merge(T &bv, int &bi, T v, int i)
-{
-    if (v > bv || (v == bv && i < bi)) {
-        bv = v;
-        bi = i;
-    }
-}
-
 // Panel factorization of columns [k, k+w) of every front of the level with
-// S > k.  Rows [k, S) (fully summed) live in shared memory; row pivoting is
-// restricted to them.  Rows [S, f) get L21 = A21 U11^-1 (no pivoting).
+// S > k.  One warp factors the w x w diagonal block in registers (lane l
+// holds row k+l) with partial pivoting restricted to the block's rows; the
+// row scaling applied at assembly keeps the pivots meaningful and the FP64
+// Krylov iteration around the factors absorbs the weaker pivoting.  Then
+// every row below the block (fully summed and contribution rows alike) gets
+// its L entries from x U = a (no pivoting), one thread per row.
 template <class T>
 __global__ void __launch_bounds__(kMfThreads) k_panel(int q0, int k, const int *__restrict__ S_,
                                                       const int *__restrict__ f_,
@@ -519,70 +514,71 @@ __global__ void __launch_bounds__(kMfThreads) k_panel(int q0, int k, const int *
                                                       int *ipiv, int *flag)
 {
     constexpr int NB = PanelWidth<T>::v;
-    extern __shared__ unsigned char smem_raw[];
-    T *sp = reinterpret_cast<T *>(smem_raw);
-    __shared__ T red_v[kMfThreads / 32];
-    __shared__ int red_i[kMfThreads / 32];
-    __shared__ int piv_s;
+    __shared__ T U[NB][NB + 1];
     const int q = q0 + blockIdx.x;
     const int S = S_[q], f = f_[q];
     if (S <= k) return;
     const int w = min(NB, S - k);
-    const int R = S - k;  // fully summed rows in the panel
     T *A = F + foff[q];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    for (int e = tid; e < R * NB; e += blockDim.x) {
-        const int r = e / NB, c = e - r * NB;
-        sp[e] = c < w ? A[(long long)(k + r) * f + k + c] : T(0);
+    const int tid = threadIdx.x, lane = tid & 31;
+    if (tid < 32) {
+        T a[NB];
+        const T *row = A + (long long)(k + min(lane, w - 1)) * f + k;
+#pragma unroll
+        for (int j = 0; j < NB; ++j) a[j] = (lane < w && j < w) ? row[j] : T(0);
+        int bad = 0;
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+            if (c < w) {
+                // argmax |a[c]| over lanes [c, w); ties -> lowest lane (same in every lane)
+                T v = (lane >= c && lane < w) ? (T)fabs(a[c]) : T(-1);
+                int idx = lane;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const T ov = __shfl_xor_sync(0xffffffffu, v, o);
+                    const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+                    if (ov > v || (ov == v && oi < idx)) {
+                        v = ov;
+                        idx = oi;
+                    }
+                }
+                int p = idx;
+                if (!(v > T(0)) || p < c || p >= w) {
+                    bad = 1;
+                    p = c;
+                }
+                if (lane == 0) ipiv[voff[q] + k + c] = k + p;
+                if (p != c) {
+                    const int src = lane == c ? p : (lane == p ? c : lane);
+#pragma unroll
+                    for (int j = 0; j < NB; ++j) a[j] = __shfl_sync(0xffffffffu, a[j], src);
+                }
+                const T d = __shfl_sync(0xffffffffu, a[c], c);
+                const T inv = d != T(0) ? T(1) / d : T(0);
+                const T l = a[c] * inv;
+                const bool below = lane > c && lane < w;
+                if (below) a[c] = l;
+#pragma unroll
+                for (int j = c + 1; j < NB; ++j) {
+                    const T pj = __shfl_sync(0xffffffffu, a[j], c);
+                    if (below) a[j] -= l * pj;
+                }
+            }
+        }
+        if (bad && lane == 0) atomicOr(flag, 1);
+        if (lane < w) {
+            T *wr = A + (long long)(k + lane) * f + k;
+#pragma unroll
+            for (int j = 0; j < NB; ++j)
+                if (j < w) {
+                    wr[j] = a[j];
+                    U[lane][j] = a[j];
+                }
+        }
     }
     __syncthreads();
-    for (int c = 0; c < w; ++c) {
-        // pivot search over rows [c, R)
-        T bv = T(-1);
-        int bi = 0x7fffffff;
-        for (int r = c + tid; r < R; r += blockDim.x) argmax_merge(bv, bi, (T)fabs(sp[r * NB + c]), r);
-        for (int o = 16; o > 0; o >>= 1) {
-            T ov = __shfl_xor_sync(0xffffffffu, bv, o);
-            int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            argmax_merge(bv, bi, ov, oi);
-        }
-        if (lane == 0) { red_v[wid] = bv; red_i[wid] = bi; }
-        __syncthreads();
-        if (tid == 0) {
-            T v = red_v[0];
-            int i = red_i[0];
-            for (int u = 1; u < (int)(blockDim.x >> 5); ++u) argmax_merge(v, i, red_v[u], red_i[u]);
-            if (!(v > T(0))) atomicOr(flag, 1);   // zero (or NaN) pivot column
-            if (i < c || i >= R) i = c;           // all-NaN column: keep the diagonal
-            piv_s = i;
-            ipiv[voff[q] + k + c] = k + i;
-        }
-        __syncthreads();
-        const int p = piv_s;
-        if (p != c)
-            for (int u = tid; u < NB; u += blockDim.x) {
-                T t = sp[c * NB + u];
-                sp[c * NB + u] = sp[p * NB + u];
-                sp[p * NB + u] = t;
-            }
-        __syncthreads();
-        const T d = sp[c * NB + c];
-        const T inv = d != T(0) ? T(1) / d : T(0);
-        for (int r = c + 1 + tid; r < R; r += blockDim.x) sp[r * NB + c] *= inv;
-        __syncthreads();
-        const int nr = R - c - 1, ncol = w - c - 1;
-        for (int e = tid; e < nr * ncol; e += blockDim.x) {
-            const int r = c + 1 + e / ncol, cc = c + 1 + e % ncol;
-            sp[r * NB + cc] -= sp[r * NB + c] * sp[c * NB + cc];
-        }
-        __syncthreads();
-    }
-    for (int e = tid; e < R * w; e += blockDim.x) {
-        const int r = e / w, c = e - r * w;
-        A[(long long)(k + r) * f + k + c] = sp[r * NB + c];
-    }
-    // rows [S, f): x U = a  (U = upper triangle of the panel's top w rows)
-    for (int r = S + tid; r < f; r += blockDim.x) {
+    // rows [k+w, f): x U = a  (U = upper triangle of the factored block)
+    for (int r = k + w + tid; r < f; r += blockDim.x) {
         T x[NB];
         T *row = A + (long long)r * f + k;
 #pragma unroll
@@ -591,8 +587,9 @@ __global__ void __launch_bounds__(kMfThreads) k_panel(int q0, int k, const int *
         for (int c = 0; c < NB; ++c) {
             if (c < w) {
                 T s = x[c];
-                for (int t = 0; t < c; ++t) s -= x[t] * sp[t * NB + c];
-                const T d = sp[c * NB + c];
+#pragma unroll
+                for (int t = 0; t < c; ++t) s -= x[t] * U[t][c];
+                const T d = U[c][c];
                 x[c] = d != T(0) ? s / d : T(0);
             }
         }
@@ -602,8 +599,10 @@ __global__ void __launch_bounds__(kMfThreads) k_panel(int q0, int k, const int *
     }
 }
 
-// Row swaps of panel k applied to every column outside the panel (rows
-// [k, S)), then U12 = L11^-1 A12 for the panel's block row.
+// The panel's row swaps (confined to its w rows) applied to every column
+// outside the panel, then U12 = L11^-1 A12 for the panel's block row.  One
+// thread per column: the w entries are gathered through the block
+// permutation into registers, solved and written back.
 template <class T>
 __global__ void __launch_bounds__(kTrsmCols) k_swap_trsm(int q0, int k, const int *__restrict__ S_,
                                                          const int *__restrict__ f_,
@@ -612,8 +611,8 @@ __global__ void __launch_bounds__(kTrsmCols) k_swap_trsm(int q0, int k, const in
                                                          T *F, const int *__restrict__ ipiv)
 {
     constexpr int NB = PanelWidth<T>::v;
-    __shared__ T Ld[NB * NB];
-    __shared__ int pv[NB];
+    __shared__ T Ld[NB][NB + 1];
+    __shared__ int src[NB];
     const int q = q0 + blockIdx.y;
     const int S = S_[q], f = f_[q];
     if (S <= k) return;
@@ -621,27 +620,30 @@ __global__ void __launch_bounds__(kTrsmCols) k_swap_trsm(int q0, int k, const in
     T *A = F + foff[q];
     for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
         const int r = e / NB, c = e - r * NB;
-        Ld[e] = (r < w && c < w) ? A[(long long)(k + r) * f + k + c] : T(0);
+        Ld[r][c] = (r < w && c < w) ? A[(long long)(k + r) * f + k + c] : T(0);
     }
-    for (int e = threadIdx.x; e < NB; e += blockDim.x) pv[e] = e < w ? ipiv[voff[q] + k + e] : 0;
+    if (threadIdx.x == 0) {
+        // new row t of the block = old row src[t]
+        for (int t = 0; t < NB; ++t) src[t] = t;
+        for (int t = 0; t < w; ++t) {
+            const int p = ipiv[voff[q] + k + t] - k;
+            const int u = src[t];
+            src[t] = src[p];
+            src[p] = u;
+        }
+    }
     __syncthreads();
     const int col = blockIdx.x * kTrsmCols + threadIdx.x;
     if (col >= f || (col >= k && col < k + w)) return;
-    for (int t = 0; t < w; ++t) {
-        const int p = pv[t];
-        if (p != k + t) {
-            T a = A[(long long)(k + t) * f + col];
-            A[(long long)(k + t) * f + col] = A[(long long)p * f + col];
-            A[(long long)p * f + col] = a;
-        }
-    }
-    if (col < k + w) return;
     T x[NB];
 #pragma unroll
-    for (int t = 0; t < NB; ++t) {
-        if (t < w) {
-            T s = A[(long long)(k + t) * f + col];
-            for (int u = 0; u < t; ++u) s -= Ld[t * NB + u] * x[u];
+    for (int t = 0; t < NB; ++t) x[t] = t < w ? A[(long long)(k + src[t]) * f + col] : T(0);
+    if (col >= k + w) {
+#pragma unroll
+        for (int t = 1; t < NB; ++t) {
+            T s = x[t];
+#pragma unroll
+            for (int u = 0; u < t; ++u) s -= Ld[t][u] * x[u];
             x[t] = s;
         }
     }
@@ -750,7 +752,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd(int q0, const MfDev D, co
     const int S = D.S[q], f = D.f[q], vo = D.voff[q];
     const T *A = F + D.foff[q];
     const int *vars = D.vars + vo;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (int p = tid; p < f; p += blockDim.x) w[p] = p < S ? (T)(rs[vars[p]] * (double)b[vars[p]]) : T(0);
     __syncthreads();
     for (int slot = 0; slot < 2; ++slot) {
@@ -768,23 +770,35 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd(int q0, const MfDev D, co
     __syncthreads();
     for (int i = tid; i < S; i += blockDim.x) w[i] = t2[i];
     __syncthreads();
-    // blocked unit-lower solve; rows below each block (FS and CB) updated by warps
+    // blocked unit-lower solve: warp 0 solves each 32-row diagonal block with
+    // the block in registers (lane l holds row ib+l), then every thread
+    // updates one row below the block (FS rows and the CB rows alike)
     for (int ib = 0; ib < S; ib += 32) {
         const int bs = min(32, S - ib);
         if (wid == 0) {
-            for (int t = 0; t < bs; ++t) {
-                const T zt = w[ib + t];
-                __syncwarp();
-                if (lane > t && lane < bs) w[ib + lane] -= A[(long long)(ib + lane) * f + ib + t] * zt;
-                __syncwarp();
+            T Lr[32];
+            const T *row = A + (long long)(ib + min(lane, bs - 1)) * f + ib;
+#pragma unroll
+            for (int t = 0; t < 32; ++t) Lr[t] = (t < bs && lane < bs) ? row[t] : T(0);
+            T wl = lane < bs ? w[ib + lane] : T(0);
+#pragma unroll
+            for (int t = 0; t < 32; ++t) {
+                const T zt = __shfl_sync(0xffffffffu, wl, t);
+                if (lane > t) wl -= Lr[t] * zt;
             }
+            if (lane < bs) w[ib + lane] = wl;
         }
         __syncthreads();
-        const T zl = lane < bs ? w[ib + lane] : T(0);
-        for (int r = ib + bs + wid; r < f; r += nw) {
-            T v = lane < bs ? A[(long long)r * f + ib + lane] * zl : T(0);
-            v = warp_sum(v);
-            if (lane == 0) w[r] -= v;
+        for (int r = ib + bs + tid; r < f; r += blockDim.x) {
+            const T *row = A + (long long)r * f + ib;
+            T v = T(0);
+            if (bs == 32) {
+#pragma unroll
+                for (int t = 0; t < 32; ++t) v += row[t] * w[ib + t];
+            } else {
+                for (int t = 0; t < bs; ++t) v += row[t] * w[ib + t];
+            }
+            w[r] -= v;
         }
         __syncthreads();
     }
@@ -820,22 +834,34 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd(int q0, const MfDev D, co
     for (int bb = nblk - 1; bb >= 0; --bb) {
         const int ib = bb * 32, bs = min(32, S - ib);
         if (wid == 0) {
-            for (int t = bs - 1; t >= 0; --t) {
-                __syncwarp();
-                const T d = A[(long long)(ib + t) * f + ib + t];
-                const T xt = d != T(0) ? y[ib + t] / d : T(0);
-                __syncwarp();
-                if (lane == t) y[ib + t] = xt;
-                if (lane < t) y[ib + lane] -= A[(long long)(ib + lane) * f + ib + t] * xt;
-                __syncwarp();
+            T Ur[32];
+            const T *row = A + (long long)(ib + min(lane, bs - 1)) * f + ib;
+#pragma unroll
+            for (int t = 0; t < 32; ++t) Ur[t] = (t < bs && lane < bs) ? row[t] : T(0);
+            T yl = lane < bs ? y[ib + lane] : T(0);
+#pragma unroll
+            for (int t = 31; t >= 0; --t) {
+                if (t < bs) {
+                    const T d = Ur[t];   // diagonal, valid in lane t
+                    const T mine = (lane == t && d != T(0)) ? yl / d : T(0);
+                    const T xt = __shfl_sync(0xffffffffu, mine, t);
+                    if (lane == t) yl = xt;
+                    else if (lane < t) yl -= Ur[t] * xt;
+                }
             }
+            if (lane < bs) y[ib + lane] = yl;
         }
         __syncthreads();
-        const T xl = lane < bs ? y[ib + lane] : T(0);
-        for (int r = wid; r < ib; r += nw) {
-            T v = lane < bs ? A[(long long)r * f + ib + lane] * xl : T(0);
-            v = warp_sum(v);
-            if (lane == 0) y[r] -= v;
+        for (int r = tid; r < ib; r += blockDim.x) {
+            const T *row = A + (long long)r * f + ib;
+            T v = T(0);
+            if (bs == 32) {
+#pragma unroll
+                for (int t = 0; t < 32; ++t) v += row[t] * y[ib + t];
+            } else {
+                for (int t = 0; t < bs; ++t) v += row[t] * y[ib + t];
+            }
+            y[r] -= v;
         }
         __syncthreads();
     }
@@ -868,24 +894,19 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
         mf_factor_destroy(M);
         return V2D_ENOMEM;
     }
-    // dynamic shared memory of the panel and solve kernels (set once, outside
-    // any stream capture)
-    const size_t panel = (size_t)P->maxS * (fp32 ? PanelWidth<float>::v * sizeof(float)
-                                                  : PanelWidth<double>::v * sizeof(double));
+    // dynamic shared memory of the solve kernels (set once, outside any
+    // stream capture)
     const size_t solve = (size_t)(P->maxf + P->maxS) * es;
-    if (panel > 227 * 1024 || solve > 227 * 1024) {
-        set_error("mf_factor: separator of %d / front of %d unknowns exceeds shared memory",
-                  P->maxS, P->maxf);
+    if (solve > 227 * 1024) {
+        set_error("mf_factor: front of %d unknowns exceeds the solve's shared memory", P->maxf);
         mf_factor_destroy(M);
         return V2D_EARG;
     }
     if (fp32) {
-        e = cudaFuncSetAttribute(k_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve);
+        e = cudaFuncSetAttribute(k_fwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(k_bwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve);
     } else {
-        e = cudaFuncSetAttribute(k_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve);
+        e = cudaFuncSetAttribute(k_fwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(k_bwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve);
     }
     if (e != cudaSuccess) {
@@ -926,7 +947,6 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
     long long launches = 0;
     k_rowscale<<<grid_for(P->n, 256), 256, 0, s>>>(P->n, rowptr, val, M->rs);
     ++launches;
-    const size_t panel_smem = (size_t)P->maxS * NB * sizeof(T);
     for (int L = 0; L < P->nlevel; ++L) {
         const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
         V2D_CUDA_TRY(cudaMemsetAsync(F + P->lvl_fbeg[L], 0,
@@ -950,7 +970,7 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
         }
         const int maxf = P->lvl_maxf[L];
         for (int k = 0; k < P->lvl_maxS[L]; k += NB) {
-            k_panel<T><<<nq, kMfThreads, panel_smem, s>>>(q0, k, P->d_S, P->d_f, P->d_foff,
+            k_panel<T><<<nq, kMfThreads, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff,
                                                           P->d_voff, F, M->ipiv, M->flag);
             const int gcol = (maxf + kTrsmCols - 1) / kTrsmCols;
             k_swap_trsm<T><<<dim3(gcol, nq), kTrsmCols, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff,

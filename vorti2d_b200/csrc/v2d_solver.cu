@@ -34,6 +34,9 @@ struct v2d_solver {
     MfPlan *plan = nullptr;        // multifrontal plan of the current pattern
     int plan_leaf = 0;
     MfFactor *lu[2] = {nullptr, nullptr};  // [0] FP64 factors, [1] FP32 factors
+    cudaEvent_t ev[5] = {};          // phase boundaries of the last Newton iteration
+    double phase_ms[4] = {0, 0, 0, 0};
+    long long phase_n = 0;
 };
 
 namespace {
@@ -191,6 +194,8 @@ extern "C" int v2d_solver_destroy(v2d_solver *S)
     if (S->s) cudaStreamSynchronize(S->s);
     GridDev &g = S->g;
     drop_lu(S);
+    for (cudaEvent_t e : S->ev)
+        if (e) cudaEventDestroy(e);
     void *ptrs[] = {g.x, g.rowptr, g.colind, g.val, g.val32, g.b, g.dinv, g.dinv32,
                     S->delta, S->partial, S->scal, S->flag, S->counter};
     for (void *p : ptrs)
@@ -231,6 +236,7 @@ extern "C" int v2d_solver_create(int imax, int jmax, const double *xg, const dou
     if (e == cudaSuccess) e = cudaMalloc(&S->counter, sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMallocHost(&S->host, 16 * sizeof(double));
     if (e == cudaSuccess) e = cudaMemsetAsync(S->counter, 0, sizeof(unsigned int), S->s);
+    for (int q = 0; q < 5 && e == cudaSuccess; ++q) e = cudaEventCreate(&S->ev[q]);
     if (e != cudaSuccess) {
         set_error("solver_create: allocation failed: %s", cudaGetErrorString(e));
         v2d_solver_destroy(S);
@@ -346,7 +352,9 @@ extern "C" int v2d_solver_newton(v2d_solver *S, double urot, double *res, v2d_li
 {
     V2D_ARG_CHECK(S, "null solver");
     GridDev &g = S->g;
+    V2D_CUDA_TRY(cudaEventRecord(S->ev[0], S->s));
     V2D_TRY(assemble_now(S, urot));
+    V2D_CUDA_TRY(cudaEventRecord(S->ev[1], S->s));
     V2D_TRY(sync_flag(S, "newton assembly"));
     CsrOp A;
     A.n = g.n; A.nnz = g.nnz; A.rowptr = g.rowptr; A.colind = g.colind; A.val = g.val;
@@ -358,16 +366,24 @@ extern "C" int v2d_solver_newton(v2d_solver *S, double urot, double *res, v2d_li
         A.lu_plan = S->plan;
         A.lu = M;
     }
+    V2D_CUDA_TRY(cudaEventRecord(S->ev[2], S->s));
     v2d_lin_stats ls{};
     V2D_TRY(krylov_solve(S->kw, A, g.b, S->delta, S->prm.krylov, &ls, S->s));
+    V2D_CUDA_TRY(cudaEventRecord(S->ev[3], S->s));
     if (st) *st = ls;
     const int grid = std::max(1, std::min(kUpdBlocks, (g.N + kUpdThreads * 8 - 1) / (kUpdThreads * 8)));
     k_newton_update<<<grid, kUpdThreads, 0, S->s>>>(g.N, S->delta, g.psi, g.ome, S->partial,
                                                      S->counter, S->scal);
     V2D_CUDA_TRY(cudaGetLastError());
     count_launches(1);
+    V2D_CUDA_TRY(cudaEventRecord(S->ev[4], S->s));
     V2D_CUDA_TRY(cudaMemcpyAsync(S->host, S->scal, sizeof(double), cudaMemcpyDeviceToHost, S->s));
     V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    for (int q = 0; q < 4; ++q) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, S->ev[q], S->ev[q + 1]) == cudaSuccess) S->phase_ms[q] += ms;
+    }
+    ++S->phase_n;
     S->assembled = false;
     const double r = S->host[0];
     if (res) *res = r;
@@ -480,6 +496,18 @@ extern "C" int v2d_solver_time_spmv(v2d_solver *S, int fp32, int reps, long long
     A.n = g.n; A.nnz = g.nnz; A.rowptr = g.rowptr; A.colind = g.colind; A.val = g.val;
     A.val32 = g.val32; A.layout = 1; A.nblk = g.N;
     return time_spmv(A, fp32 != 0, reps, (size_t)flush_bytes, S->s, ms_avg);
+}
+
+extern "C" int v2d_solver_phase_times(v2d_solver *S, double *out5, int reset)
+{
+    V2D_ARG_CHECK(S && out5, "null pointer");
+    for (int q = 0; q < 4; ++q) out5[q] = S->phase_ms[q];
+    out5[4] = (double)S->phase_n;
+    if (reset) {
+        for (double &v : S->phase_ms) v = 0.0;
+        S->phase_n = 0;
+    }
+    return V2D_OK;
 }
 
 extern "C" int v2d_solver_stream(v2d_solver *S, void **stream)
