@@ -103,6 +103,31 @@ int v2d_assemble_coo_local(int gxm, int jmax, int il0, int il1, double re,
                            int maxnnz, int ff_bc, double ca, double sa, int *coo_i,
                            int *coo_j, double *coo_v, int *nnz, double *bvec);
 
+/* Allocation-free variant of v2d_assemble_coo.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory where
+ * they assemble -- a framework that owns the GPU's memory through its own pool
+ * and budget, or a time-critical loop that must avoid cudaMalloc/cudaFree,
+ * which can synchronize the device and can fail under memory pressure.
+ * Same rows, COO push order and right-hand side as v2d_assemble_coo, but every
+ * array is a DEVICE pointer: d_fields14 is a host array of the 14 device input
+ * fields in v2d_assemble_coo's order (jac ... omeoldold, imax*jmax doubles
+ * each); d_coo_i/j/v have room for maxnnz entries, d_bvec for r1-r0; *nnz is
+ * a host int.  The call allocates nothing: its only scratch (row offsets and
+ * scan sums) is a fixed 4 MiB array in the library's device memory, which
+ * every GPU that loads the library holds until the process exits.  It limits
+ * a call to r1 - r0 <= 1048576 rows (larger ranges return V2D_EARG: assemble
+ * them in pieces).  The first call on a device looks up that array's address
+ * (cudaGetSymbolAddress) with the device current; make that first call before
+ * any stream capture.  All calls share the array, so calls whose work
+ * overlaps on the GPU (concurrent streams or host threads on one device) race
+ * and must be serialized by the caller.  The call
+ * synchronizes `stream` (a cudaStream_t, may be 0) to read the entry count. */
+int v2d_assemble_coo_noalloc(int imax, int jmax, double re, double invdtau, double inv2dt,
+                             double urot, double dksi, double deta,
+                             const double *const *d_fields14, int r0, int r1, int maxnnz,
+                             int ff_bc, double ca, double sa, int *d_coo_i, int *d_coo_j,
+                             double *d_coo_v, int *nnz, double *d_bvec, void *stream);
+
 /* Device-pointer form of v2d_compute_metrics (same layouts; stream may be 0). */
 int v2d_compute_metrics_dev(int imax, int jmax, double dksi, double deta,
                             const double *d_xg, const double *d_yg, double *const *d_out10,

@@ -78,6 +78,8 @@ _SIGS = {
     "v2d_assemble_coo_local": (_i, [_i] * 4 + [_d] * 6 + [_dp] * 14 + [_i, _i, _ip, _i, _i]
                                + [_d] * 2 + [_ip, _ip, _dp, _ip, _dp]),
     "v2d_compute_metrics_dev": (_i, [_i, _i, _d, _d, _vp, _vp, _vp, _vp]),
+    "v2d_assemble_coo_noalloc": (_i, [_i, _i] + [_d] * 6 + [ctypes.POINTER(_vp)] + [_i] * 4
+                                 + [_d] * 2 + [_vp, _vp, _vp, _ip, _vp, _vp]),
     "v2d_force_coeffs": (_i, [_i, _i, _d, _d, _d] + [_dp] * 7 + [_d, _d, _d, _dp]),
     "v2d_krylov_defaults": (None, [ctypes.POINTER(KrylovParams)]),
     "v2d_linsys_create": (_i, [_i, _i, ctypes.POINTER(KrylovParams), ctypes.POINTER(_vp)]),

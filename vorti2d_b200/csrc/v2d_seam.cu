@@ -2,6 +2,8 @@
 // (src/fortran/vorti2d_core.f90:24-25) as sm_100a kernels plus host entry
 // points with the f2py argument order.  Built with -fmad=false: the values are
 // bit-identical to the CPU restatement of the Fortran.
+#include <mutex>
+
 #include "v2d_stencil.cuh"
 #include "v2d_util.cuh"
 
@@ -381,6 +383,104 @@ extern "C" int v2d_assemble_coo_local(int gxm, int jmax, int il0, int il1, doubl
                   r0 + nloc);
         return V2D_EARG;
     }
+    *nnz = m;
+    return V2D_OK;
+}
+
+// ------------------------------------------- allocation-free COO assembly
+// Some callers cannot allocate device memory at the point where they
+// assemble: a framework that owns all of the GPU's memory through its own pool
+// and budget, or a time-critical loop that must not hit cudaMalloc/cudaFree
+// (both can synchronize the device and cudaMalloc can fail under memory
+// pressure).  v2d_assemble_coo_noalloc serves them: the caller passes device
+// buffers for every input and output, and the only scratch the kernels need
+// (per-row entry counts turned into row offsets, plus the scan's tile sums)
+// lives in the file-scope array below, which every GPU that loads this
+// library holds until the process exits.
+namespace v2d {
+
+constexpr int kNoAllocMaxRows = 1 << 20;
+static __device__ __align__(256) int g_coo_scratch[kNoAllocMaxRows + 2048];
+
+}  // namespace v2d
+
+extern "C" int v2d_assemble_coo_noalloc(int imax, int jmax, double re, double invdtau,
+                                        double inv2dt, double urot, double dksi, double deta,
+                                        const double *const *d_fields14, int r0, int r1,
+                                        int maxnnz, int ff_bc, double ca, double sa, int *d_coo_i,
+                                        int *d_coo_j, double *d_coo_v, int *nnz, double *d_bvec,
+                                        void *stream)
+{
+    using namespace v2d;
+    static std::mutex mu;
+    static int *scratch_of_device[256] = {};
+    V2D_TRY(check_finite_mesh(imax, jmax));
+    const int N = imax * jmax;
+    V2D_ARG_CHECK(d_fields14 && nnz, "assemble_coo_noalloc: null pointer");
+    for (int q = 0; q < 14; ++q)
+        V2D_ARG_CHECK(d_fields14[q], "assemble_coo_noalloc: field %d is null", q);
+    V2D_ARG_CHECK(r0 >= 0 && r1 <= 2 * N && r0 <= r1,
+                  "assemble_coo_noalloc: rows [%d,%d) outside [0,%d)", r0, r1, 2 * N);
+    const int nrows = r1 - r0;
+    V2D_ARG_CHECK(nrows <= kNoAllocMaxRows,
+                  "assemble_coo_noalloc: %d rows exceed the fixed scratch of %d rows; use "
+                  "v2d_assemble_coo or assemble in row ranges of at most %d rows",
+                  nrows, kNoAllocMaxRows, kNoAllocMaxRows);
+    V2D_ARG_CHECK(nrows == 0 || d_bvec, "assemble_coo_noalloc: null bvec");
+    // device address of the scratch array, looked up once per device with
+    // that device current
+    int dev = 0;
+    V2D_CUDA_TRY(cudaGetDevice(&dev));
+    V2D_ARG_CHECK(dev >= 0 && dev < 256, "assemble_coo_noalloc: device %d out of range", dev);
+    int *scratch_base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!scratch_of_device[dev]) {
+            void *p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_coo_scratch);
+            if (e != cudaSuccess || !p) {
+                set_error("assemble_coo_noalloc: cudaGetSymbolAddress failed on device %d: %s",
+                          dev, cudaGetErrorString(e));
+                return V2D_ECUDA;
+            }
+            scratch_of_device[dev] = (int *)p;
+        }
+        scratch_base = scratch_of_device[dev];
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    Fields f;
+    f.jac = d_fields14[0]; f.alfa = d_fields14[1]; f.beta = d_fields14[2]; f.gama = d_fields14[3];
+    f.pmet = d_fields14[4]; f.qmet = d_fields14[5]; f.detadx = d_fields14[6];
+    f.detady = d_fields14[7]; f.xphys = d_fields14[8]; f.yphys = d_fields14[9];
+    f.psi = d_fields14[10]; f.ome = d_fields14[11]; f.omeold = d_fields14[12];
+    f.omeoldold = d_fields14[13];
+    GlobalTopo T{imax, jmax, N};
+    Coeffs c{re, invdtau, inv2dt, urot, dksi, deta, ca, sa, ff_bc};
+    // counts -> offsets in place; the total after them; then the scan's tile
+    // sums.  Every entry the kernels read is written earlier in this call, so
+    // nothing left by a previous call is used.
+    int *cnt = scratch_base, *total = scratch_base + nrows, *tiles = total + 1;
+    if (nrows > 0) {
+        coo_count_global<<<grid_for(nrows, 256), 256, 0, s>>>(T, c, f, r0, r1, cnt);
+        V2D_CUDA_TRY(cudaGetLastError());
+    }
+    V2D_TRY(exclusive_scan_i32(cnt, cnt, nrows, total, tiles, s));
+    int m = 0;
+    V2D_CUDA_TRY(cudaMemcpyAsync(&m, total, sizeof(int), cudaMemcpyDeviceToHost, s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(s));
+    *nnz = 0;
+    if (m > maxnnz) {
+        set_error("assemble_coo_noalloc: %d entries exceed maxnnz=%d", m, maxnnz);
+        return V2D_ECAPACITY;
+    }
+    V2D_ARG_CHECK(m == 0 || (d_coo_i && d_coo_j && d_coo_v), "assemble_coo_noalloc: null COO pointer");
+    if (nrows > 0) {
+        coo_fill_global<<<grid_for(nrows, 256), 256, 0, s>>>(T, c, f, r0, r1, cnt, d_coo_i,
+                                                              d_coo_j, d_coo_v, d_bvec);
+        V2D_CUDA_TRY(cudaGetLastError());
+    }
+    count_launches(nrows > 0 ? 5 : 3);
+    V2D_CUDA_TRY(cudaStreamSynchronize(s));
     *nnz = m;
     return V2D_OK;
 }
