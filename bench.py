@@ -135,9 +135,10 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------- our arm
-def make_solver(v, xg, yg, precision):
+def make_solver(v, xg, yg, precision, lu_reuse=0):
     cfg = v.Config(verbose=False, write_csv=False, write_xdmf=False, compute_forces=False,
-                   raise_on_linear_failure=False, precision=precision, **WORKLOAD, **SOLVER)
+                   raise_on_linear_failure=False, precision=precision, lu_reuse_its=lu_reuse,
+                   **WORKLOAD, **SOLVER)
     return v.Solver(cfg, mesh=(xg, yg))
 
 
@@ -173,7 +174,7 @@ def phase_times(_lib, s, reset=False):
     """(assembly, factorization, Krylov, update) device ms summed over Newton
     iterations, and the iteration count."""
     import ctypes
-    out = (ctypes.c_double * 5)()
+    out = (ctypes.c_double * 6)()
     _lib.check(_lib.lib().v2d_solver_phase_times(s.dev.h, out, int(reset)))
     return list(out)
 
@@ -212,7 +213,7 @@ def run_ours(args, rank, world, local_rank):
     legs = ["mixed", "fp64"] if args.precision == "both" else [args.precision]
     launches = {}
     for prec in legs:
-        s = make_solver(v, xg, yg, prec)
+        s = make_solver(v, xg, yg, prec, args.lu_reuse)
         times = s.times()
         for m in range(W):
             s.advance(times[m])
@@ -236,7 +237,8 @@ def run_ours(args, rank, world, local_rank):
         results[prec] = dict(ms_per_step=tot_ms / K, newton=nit / K, krylov=kit / K,
                              cd=fc.cd, cl=fc.cl, wall_s=wall, t_end=times[W + K - 1],
                              ms_per_newton={"assembly": ph[0] / nn, "factor": ph[1] / nn,
-                                            "krylov": ph[2] / nn, "update": ph[3] / nn})
+                                            "krylov": ph[2] / nn, "update": ph[3] / nn},
+                             factorizations_per_step=ph[5] / K)
         launches[prec] = c1 - c0
         if prec == legs[0]:
             # dominant kernel (SpMV of the Krylov loop), timed alone after L2 flushes
@@ -246,8 +248,13 @@ def run_ours(args, rank, world, local_rank):
             nnz = ctypes.c_longlong()
             _lib.check(_lib.lib().v2d_solver_nnz(s.dev.h, ctypes.byref(nnz)))
             results["nnz"] = nnz.value
-            # e2e: the public API with host state every step
-            results["e2e"] = _e2e(torch, v, s, times, W + K, min(K, 5))
+            # e2e: the same steps again through the public API, with the
+            # state copied host->device and back every step
+            s2 = make_solver(v, xg, yg, prec, args.lu_reuse)
+            for m in range(W):
+                s2.advance(times[m])
+            results["e2e"] = _e2e(torch, v, s2, times, W, K)
+            s2.close()
         s.close()
     return results, launches
 
@@ -261,8 +268,9 @@ def _spmv_time(_lib, s, fp32, reps=20):
 
 
 def _e2e(torch, v, s, times, k0, K):
-    """Steps through Solver.set_state / advance / state readback with pinned
-    host buffers; the copies are inside the timed region."""
+    """Steps k0 .. k0+K-1 (the timed steps of the device-resident leg) through
+    Solver.set_state / advance / state readback with pinned host buffers; the
+    copies are inside the timed region."""
     N = s.ndof
     host = [torch.empty(N, dtype=torch.float64, pin_memory=True) for _ in range(4)]
     st = s.dev.get_state()
@@ -306,6 +314,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
     ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--lu-reuse", type=int, default=20,
+                    help="keep LU factors while GMRES needs at most this many iterations "
+                         "(0: factor every Newton Jacobian)")
     ap.add_argument("--profile-newton", action="store_true",
                     help="one warm-up step, then one Newton iteration in NVTX range v2d_newton")
     args = ap.parse_args()
@@ -364,6 +375,7 @@ def main():
         "config": {"workload": "unsteady BDF2 cylinder 181x181 Re=100 dt=0.2 kick 0.5<=2 outflow",
                    "precision": head, "newton_max": 5,
                    "krylov": "GMRES(30), multifrontal LU preconditioner (FP32 factors in mixed)",
+                   "lu_reuse_its": args.lu_reuse,
                    "l2": "flushed (256 MiB write) before every timed step",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": world * res["e2e"]["steps_per_s"], "unit": "steps/s",

@@ -167,6 +167,12 @@ typedef struct {
     double inner_rtol;    /* mixed: FP32 GMRES tolerance per correction (1e-5)*/
     int dc_max_it;        /* mixed: max defect-correction passes       (20)  */
     int lu_leaf;          /* LU: max nodes of a leaf subdomain         (64)  */
+    int lu_reuse_its;     /* LU: 0 factors every Newton Jacobian (default);
+                             k > 0 keeps the factors across Newton iterations
+                             and time steps while the last solve with them
+                             took at most k Krylov iterations, and refactors
+                             (re-solving once) when a solve with stale factors
+                             fails.  Newton steps are still solved to rtol. */
 } v2d_krylov_params;
 
 void v2d_krylov_defaults(v2d_krylov_params *p);
@@ -279,9 +285,10 @@ int v2d_lu_plan_info(int imax, int jmax, const int *indptr, const int *indices, 
 
 /* Measurement aid (no reference counterpart): device time in ms, summed over
  * the Newton iterations since the last reset, of the four phases of a Newton
- * iteration (CUDA events on the handle's stream): out5 = assembly,
- * factorization (LU preconditioner), Krylov solve, update, iteration count. */
-int v2d_solver_phase_times(v2d_solver *s, double *out5, int reset);
+ * iteration (CUDA events on the handle's stream): out6 = assembly,
+ * factorization (LU preconditioner), Krylov solve, update, iteration count,
+ * LU factorizations performed. */
+int v2d_solver_phase_times(v2d_solver *s, double *out6, int reset);
 
 /* The stream the handle's kernels run on (cudaStream_t as void*). */
 int v2d_solver_stream(v2d_solver *s, void **stream);

@@ -51,11 +51,13 @@ struct MfPlan {
     double flops = 0.0;   // 2 * sum S f^2 (upper bound of the factorization flops)
     std::vector<int> S, f, voff, uoff, child0, child1, parent;
     std::vector<long long> foff;
-    std::vector<int> lvl_off, lvl_maxS, lvl_maxf, lvl_maxm_child;
+    std::vector<long long> toff;   // offset of the front's S x S block in the level's scratch
+    long long tmax = 0;            // largest sum of S^2 over the fronts of one level
+    std::vector<int> lvl_off, lvl_maxS, lvl_maxf, lvl_maxm, lvl_maxm_child;
     std::vector<long long> lvl_fbeg, lvl_fend, lvl_abeg, lvl_aend;
     int *d_S = nullptr, *d_f = nullptr, *d_voff = nullptr, *d_uoff = nullptr;
     int *d_child0 = nullptr, *d_child1 = nullptr;
-    long long *d_foff = nullptr;
+    long long *d_foff = nullptr, *d_toff = nullptr;
     int *d_vars = nullptr, *d_cbmap = nullptr, *d_asm_csr = nullptr, *d_asm_row = nullptr;
     long long *d_asm_pos = nullptr;
     // host copies, kept only between the build and the upload
@@ -67,6 +69,7 @@ struct MfPlan {
 struct MfFactor {
     int fp32 = 0;
     void *F = nullptr, *upd = nullptr, *z = nullptr;
+    void *tmp = nullptr;        // triangular inverses of one level before they replace L11 / U11
     double *rs = nullptr;       // row scaling 1 / max |a_r.|
     int *ipiv = nullptr, *perm = nullptr, *flag = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -96,9 +99,10 @@ MfDev mf_dev(const MfPlan *P, const MfFactor *M);
 // Factor the CSR values (FP64, row-scaled and rounded to the factor's precision).
 int mf_factor(const MfPlan *P, MfFactor *M, const int *rowptr, const double *val, cudaStream_t s);
 // x = A^-1 b with the factors (vectors in the factor's precision).  The
-// kernels exit at once while *stop_a or *stop_b is non-zero (either may be null).
+// kernels exit at once while *stop_a or *stop_b is non-zero (either may be
+// null).  *n_launches (if given) receives the number of kernels launched.
 int mf_apply(const MfPlan *P, const MfFactor *M, const void *b, void *x, const int *stop_a,
-             const int *stop_b, cudaStream_t s);
+             const int *stop_b, cudaStream_t s, long long *n_launches);
 int mf_flag(const MfFactor *M, int *flag, cudaStream_t s);
 
 // ------------------------------------------------------------- Krylov

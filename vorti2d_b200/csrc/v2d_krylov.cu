@@ -88,6 +88,7 @@ struct KrylovWork {
     Desc *desc = nullptr;
     std::vector<cudaGraphExec_t> seg[2];   // Arnoldi segments per precision
     std::vector<int> seg_bounds[2];
+    std::vector<long long> seg_launches[2];  // kernels per segment replay
     cudaGraphExec_t fin[2] = {nullptr, nullptr};
     int graph_m[2] = {0, 0};
     int graph_pc[2] = {-1, -1};
@@ -576,16 +577,21 @@ static int capture_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, doub
     const int gt = tile_grid(n);
     const bool lu = precond == V2D_PC_LU;
     drop_graphs(w, which);
+    w->seg_launches[which].clear();
     const std::vector<int> bnd = segment_bounds(w->m);
     for (size_t q = 0; q + 1 < bnd.size(); ++q) {
+        long long nl = 0;
         V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         for (int j = bnd[q]; j < bnd[q + 1]; ++j) {
+            nl += 6;
             k_scale_precond<T><<<gp, 256, 0, s>>>(w->desc, w->ctl, j, w->r, wv, V, w->H, z);
             T *zj = z;
             if (lu) {
                 zj = Z + (size_t)j * n;
+                long long na = 0;
                 int st = mf_apply(A.lu_plan, A.lu, V + (size_t)j * n, zj, &w->ctl->conv,
-                                  &w->ctl->cyc_stop, s);
+                                  &w->ctl->cyc_stop, s, &na);
+                nl += na;
                 if (st != V2D_OK) {
                     cudaGraph_t junk = nullptr;
                     cudaStreamEndCapture(s, &junk);
@@ -605,6 +611,7 @@ static int capture_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, doub
         cudaGraphExec_t ge = nullptr;
         V2D_TRY(end_capture(s, &ge));
         w->seg[which].push_back(ge);
+        w->seg_launches[which].push_back(nl);
     }
     V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     k_backsolve<<<1, 32, 0, s>>>(w->desc, w->ctl, w->H, w->g, w->y);
@@ -628,11 +635,9 @@ static int run_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, double *
         w->graph_pc[which] != precond ||
         w->graph_lu[which] != (lu ? (const void *)A.lu : nullptr))
         V2D_TRY(capture_cycle<T>(w, which, V, wv, z, Z, x, A, precond, s));
-    const long long per_step = 6 + (lu ? 2LL * A.lu_plan->nlevel : 0);
-    const std::vector<int> &bnd = w->seg_bounds[which];
     for (size_t q = 0; q < w->seg[which].size(); ++q) {
         V2D_CUDA_TRY(cudaGraphLaunch(w->seg[which][q], s));
-        count_launches(per_step * (bnd[q + 1] - bnd[q]));
+        count_launches(w->seg_launches[which][q]);
         V2D_CUDA_TRY(cudaMemcpyAsync(w->ctl_host, w->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
         V2D_CUDA_TRY(cudaStreamSynchronize(s));
         if (w->ctl_host->cyc_stop || w->ctl_host->conv) break;

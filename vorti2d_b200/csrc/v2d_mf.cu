@@ -10,12 +10,15 @@
 // factors in the plain form).
 //
 // Symbolic phase (host, once per mesh and sparsity pattern):
-//  * the separator tree is geometric: the root separator is the two seam
-//    columns i = 0, imax-1 plus column imax/2, which cut the periodic ring into
-//    two rectangles; each rectangle is split recursively by its middle column
+//  * the separator tree is geometric: the root separator is the
+//    circumferential row jmax/2, which splits the O-grid into an inner and an
+//    outer annulus; each annulus is opened by its two seam columns into one
+//    rectangle, and rectangles are split recursively by their middle column
 //    or row (never rows 1 or jmax-2, whose boundary rows reach two rows away:
 //    the Thom wall row, vorti2d_core.f90:322-339, and the outflow rows,
-//    :254-269, :307-321) until it holds at most `leaf` nodes;
+//    :254-269, :307-321) until they hold at most `leaf` nodes.  Every
+//    separator thus spans at most one row or two half-columns, which keeps
+//    the dense top fronts small;
 //  * fronts are numbered level by level (level = height above the leaves), so
 //    the fronts of one level, their dense storage and their assembly entries
 //    are contiguous and each level is processed by a fixed set of batched
@@ -27,15 +30,21 @@
 // Numeric phase (device, per Newton iteration), per level bottom-up:
 //  row-scaled CSR values scattered into the zeroed fronts, children's
 //  contribution blocks added (one child slot per launch: deterministic, no
-//  atomics), then a blocked right-looking partial LU of each front: panel
-//  (one CTA per front; one warp factors the diagonal block in registers with
-//  pivoting among the block's rows, the other rows get L by a TRSM), row
-//  swaps + TRSM for the U12 block row, GEMM update of the trailing block
-//  (which leaves the Schur complement for the parent).
+//  atomics), then a blocked right-looking partial LU of each front, four
+//  batched launches per 32-column panel: the diagonal block (one CTA per
+//  front, pivoting among the block's rows), L21 for the rows below (row
+//  chunks), row swaps + TRSM for the U12 block row (column chunks), GEMM
+//  update of the trailing block (which leaves the Schur complement for the
+//  parent).
 //
-// Solve (device): forward per level bottom-up (gather, permute, unit-lower
-// solve, contribution vector for the parent), backward top-down (U12 x_struct,
-// upper solve, scatter).  One CTA per front, blocked 32 rows at a time.
+// After each level's factorization the S x S pivot block of every front is
+// replaced by the explicit inverses of its triangular factors (L11^-1 below
+// the diagonal, U11^-1 on and above it).
+//
+// Solve (device): forward per level bottom-up (gather, permute, z = L11^-1 w,
+// contribution vector for the parent), backward top-down (U12 x_struct,
+// x = U11^-1 y, scatter).  Every step is a row-parallel product split over
+// CTAs of 8 rows, so the large top fronts spread over many SMs.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -107,8 +116,34 @@ struct TreeBuilder {
         int b = rect(i0, i1, best + 1, j1);
         return add(block(i0, i1, best, best + 1), a, b);
     }
+    // Annulus rows [j0, j1): cutting the two seam columns leaves one
+    // (non-periodic) rectangle [1, imax-1) x [j0, j1).
+    int annulus(int j0, int j1)
+    {
+        if (j1 <= j0) return -1;
+        int kid = rect(1, imax - 1, j0, j1);
+        std::vector<int> sep;
+        for (int c : {0, imax - 1})
+            for (int j = j0; j < j1; ++j) sep.push_back(j * imax + c);
+        return add(std::move(sep), kid, -1);
+    }
     void build()
     {
+        // Ring first: the root is the circumferential row jc, which splits the
+        // O-grid into an inner and an outer annulus (each keeps the wall or the
+        // far-field rows and their two-row reach); every separator then spans
+        // at most one row or two half-columns.  Grids with too few rows for
+        // that use the seam columns plus the middle column as the root.
+        int jc = jmax / 2;
+        if (jc == 1 || jc == jmax - 2) ++jc;
+        if (jmax >= 8 && jc >= 2 && jc <= jmax - 4) {
+            int a = annulus(0, jc);
+            int b = annulus(jc + 1, jmax);
+            std::vector<int> root;
+            for (int i = 0; i < imax; ++i) root.push_back(jc * imax + i);
+            add(std::move(root), a, b);
+            return;
+        }
         const int mid = imax / 2;
         int a = rect(1, mid, 0, jmax);
         int b = rect(mid + 1, imax - 1, 0, jmax);
@@ -134,7 +169,7 @@ int upload_vec(T **d, const std::vector<T> &h)
 void mf_plan_destroy(MfPlan *p)
 {
     if (!p) return;
-    void *ptrs[] = {p->d_S, p->d_f, p->d_voff, p->d_uoff, p->d_child0, p->d_child1, p->d_foff,
+    void *ptrs[] = {p->d_S, p->d_f, p->d_voff, p->d_uoff, p->d_child0, p->d_child1, p->d_foff, p->d_toff,
                     p->d_vars, p->d_cbmap, p->d_asm_csr, p->d_asm_row, p->d_asm_pos};
     for (void *q : ptrs)
         if (q) cudaFree(q);
@@ -252,7 +287,8 @@ int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_c
     P->lvl_off.assign(nlevel + 1, 0);
     P->lvl_fbeg.assign(nlevel, 0); P->lvl_fend.assign(nlevel, 0);
     P->lvl_abeg.assign(nlevel, 0); P->lvl_aend.assign(nlevel, 0);
-    P->lvl_maxS.assign(nlevel, 0); P->lvl_maxf.assign(nlevel, 0); P->lvl_maxm_child.assign(nlevel, 0);
+    P->lvl_maxS.assign(nlevel, 0); P->lvl_maxf.assign(nlevel, 0); P->lvl_maxm.assign(nlevel, 0);
+    P->lvl_maxm_child.assign(nlevel, 0);
     std::vector<int> vars, cbmap;
     long long ftot = 0;
     int vtot = 0, utot = 0;
@@ -268,6 +304,7 @@ int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_c
         P->lvl_off[L + 1]++;
         P->lvl_maxS[L] = std::max(P->lvl_maxS[L], S);
         P->lvl_maxf[L] = std::max(P->lvl_maxf[L], f);
+        P->lvl_maxm[L] = std::max(P->lvl_maxm[L], f - S);
         if (tb.t[q].parent >= 0) P->parent[id] = newid[tb.t[q].parent];
         if (tb.t[q].kid[0] >= 0) P->child0[id] = newid[tb.t[q].kid[0]];
         if (tb.t[q].kid[1] >= 0) P->child1[id] = newid[tb.t[q].kid[1]];
@@ -278,6 +315,15 @@ int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_c
         P->maxf = std::max(P->maxf, f);
     }
     for (int L = 0; L < nlevel; ++L) P->lvl_off[L + 1] += P->lvl_off[L];
+    P->toff.assign(nf, 0);
+    for (int L = 0; L < nlevel; ++L) {
+        long long t = 0;
+        for (int id = P->lvl_off[L]; id < P->lvl_off[L + 1]; ++id) {
+            P->toff[id] = t;
+            t += (long long)P->S[id] * P->S[id];
+        }
+        P->tmax = std::max(P->tmax, t);
+    }
     for (int L = 0; L < nlevel; ++L) {
         const int a = P->lvl_off[L], b = P->lvl_off[L + 1];
         P->lvl_fbeg[L] = P->foff[a];
@@ -401,6 +447,7 @@ int mf_plan_create(int imax, int jmax, int n, const int *h_rowptr, const int *h_
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_child0, P->child0);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_child1, P->child1);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_foff, P->foff);
+    if (st_up == V2D_OK) st_up = upload_vec(&P->d_toff, P->toff);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_vars, P->h_vars);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_cbmap, P->h_cbmap);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_asm_csr, P->h_asm_csr);
@@ -448,7 +495,7 @@ namespace v2d {
 namespace {
 
 constexpr int kMfThreads = 256;
-constexpr int kTrsmCols = 128;
+constexpr int kTrsmCols = 32;
 constexpr int kGemmTile = 64;
 
 template <class T> struct PanelWidth;
@@ -500,18 +547,18 @@ __global__ void k_extend_add(int q0, int slot, const int *__restrict__ S, const 
 }
 
 // Panel factorization of columns [k, k+w) of every front of the level with
-// S > k.  One warp factors the w x w diagonal block in registers (lane l
-// holds row k+l) with partial pivoting restricted to the block's rows; the
-// row scaling applied at assembly keeps the pivots meaningful and the FP64
-// Krylov iteration around the factors absorbs the weaker pivoting.  Then
-// every row below the block (fully summed and contribution rows alike) gets
-// its L entries from x U = a (no pivoting), one thread per row.
+// S > k.  One warp factors the w x w diagonal block in shared memory with
+// partial pivoting restricted to the block's rows and records both the swap
+// sequence (ipiv) and the block's part of the row permutation; the row scaling applied at
+// assembly keeps the pivots meaningful and the FP64 Krylov iteration around
+// the factors absorbs the weaker pivoting.  The rows below the block (fully
+// summed and contribution rows alike) get their L entries from k_l21.
 template <class T>
 __global__ void __launch_bounds__(kMfThreads) k_panel(int q0, int k, const int *__restrict__ S_,
                                                       const int *__restrict__ f_,
                                                       const long long *__restrict__ foff,
                                                       const int *__restrict__ voff, T *F,
-                                                      int *ipiv, int *flag)
+                                                      int *ipiv, int *perm, int *flag)
 {
     constexpr int NB = PanelWidth<T>::v;
     __shared__ T U[NB][NB + 1];
@@ -521,82 +568,108 @@ __global__ void __launch_bounds__(kMfThreads) k_panel(int q0, int k, const int *
     const int w = min(NB, S - k);
     T *A = F + foff[q];
     const int tid = threadIdx.x, lane = tid & 31;
-    if (tid < 32) {
-        T a[NB];
-        const T *row = A + (long long)(k + min(lane, w - 1)) * f + k;
-#pragma unroll
-        for (int j = 0; j < NB; ++j) a[j] = (lane < w && j < w) ? row[j] : T(0);
-        int bad = 0;
-#pragma unroll
-        for (int c = 0; c < NB; ++c) {
-            if (c < w) {
-                // argmax |a[c]| over lanes [c, w); ties -> lowest lane (same in every lane)
-                T v = (lane >= c && lane < w) ? (T)fabs(a[c]) : T(-1);
-                int idx = lane;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    const T ov = __shfl_xor_sync(0xffffffffu, v, o);
-                    const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
-                    if (ov > v || (ov == v && oi < idx)) {
-                        v = ov;
-                        idx = oi;
-                    }
-                }
-                int p = idx;
-                if (!(v > T(0)) || p < c || p >= w) {
-                    bad = 1;
-                    p = c;
-                }
-                if (lane == 0) ipiv[voff[q] + k + c] = k + p;
-                if (p != c) {
-                    const int src = lane == c ? p : (lane == p ? c : lane);
-#pragma unroll
-                    for (int j = 0; j < NB; ++j) a[j] = __shfl_sync(0xffffffffu, a[j], src);
-                }
-                const T d = __shfl_sync(0xffffffffu, a[c], c);
-                const T inv = d != T(0) ? T(1) / d : T(0);
-                const T l = a[c] * inv;
-                const bool below = lane > c && lane < w;
-                if (below) a[c] = l;
-#pragma unroll
-                for (int j = c + 1; j < NB; ++j) {
-                    const T pj = __shfl_sync(0xffffffffu, a[j], c);
-                    if (below) a[j] -= l * pj;
-                }
-            }
-        }
-        if (bad && lane == 0) atomicOr(flag, 1);
-        if (lane < w) {
-            T *wr = A + (long long)(k + lane) * f + k;
-#pragma unroll
-            for (int j = 0; j < NB; ++j)
-                if (j < w) {
-                    wr[j] = a[j];
-                    U[lane][j] = a[j];
-                }
-        }
+    __shared__ int pv[NB];
+    for (int e = tid; e < NB * NB; e += blockDim.x) {
+        const int r = e / NB, c = e - r * NB;
+        U[r][c] = (r < w && c < w) ? A[(long long)(k + r) * f + k + c] : T(0);
     }
     __syncthreads();
-    // rows [k+w, f): x U = a  (U = upper triangle of the factored block)
-    for (int r = k + w + tid; r < f; r += blockDim.x) {
-        T x[NB];
-        T *row = A + (long long)r * f + k;
-#pragma unroll
-        for (int c = 0; c < NB; ++c) x[c] = c < w ? row[c] : T(0);
-#pragma unroll
-        for (int c = 0; c < NB; ++c) {
-            if (c < w) {
-                T s = x[c];
-#pragma unroll
-                for (int t = 0; t < c; ++t) s -= x[t] * U[t][c];
-                const T d = U[c][c];
-                x[c] = d != T(0) ? s / d : T(0);
+    if (tid < 32) {
+        // one warp; lane = row for the pivot search and the elimination,
+        // lane = column for the row swap
+        int bad = 0;
+        if (lane < NB) pv[lane] = lane;
+        __syncwarp();
+        for (int c = 0; c < w; ++c) {
+            T v = (lane >= c && lane < w) ? (T)fabs(U[lane][c]) : T(-1);
+            int idx = lane;
+            for (int o = 16; o > 0; o >>= 1) {
+                const T ov = __shfl_xor_sync(0xffffffffu, v, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+                if (ov > v || (ov == v && oi < idx)) {
+                    v = ov;
+                    idx = oi;
+                }
             }
+            int p = idx;
+            if (!(v > T(0)) || p < c || p >= w) {
+                p = c;
+                bad = 1;
+            }
+            if (lane == 0) {
+                ipiv[voff[q] + k + c] = k + p;
+                const int t = pv[c];
+                pv[c] = pv[p];
+                pv[p] = t;
+            }
+            if (p != c && lane < NB) {
+                const T t = U[c][lane];
+                U[c][lane] = U[p][lane];
+                U[p][lane] = t;
+            }
+            __syncwarp();
+            const T d = U[c][c];
+            const T inv = d != T(0) ? T(1) / d : T(0);
+            if (lane > c && lane < w) {
+                const T l = U[lane][c] * inv;
+                U[lane][c] = l;
+                for (int j = c + 1; j < w; ++j) U[lane][j] -= l * U[c][j];
+            }
+            __syncwarp();
         }
-#pragma unroll
-        for (int c = 0; c < NB; ++c)
-            if (c < w) row[c] = x[c];
+        if (bad && lane == 0) atomicOr(flag, 1);
+        // row i of the factored front came from local row perm[i]; the swaps
+        // stay inside the panel's rows, so the panel fixes its own entries
+        if (lane < w) perm[voff[q] + k + lane] = k + pv[lane];
     }
+    __syncthreads();
+    for (int e = tid; e < w * w; e += blockDim.x) {
+        const int r = e / w, c = e - r * w;
+        A[(long long)(k + r) * f + k + c] = U[r][c];
+    }
+}
+
+// L entries of the panel for the rows below its diagonal block: x U = a with
+// U the upper triangle of the factored block (no pivoting outside the block).
+// Grid: (chunks of kL21Rows rows, fronts); one thread per row.
+constexpr int kL21Rows = 64;
+
+template <class T>
+__global__ void __launch_bounds__(kL21Rows) k_l21(int q0, int k, const int *__restrict__ S_,
+                                                  const int *__restrict__ f_,
+                                                  const long long *__restrict__ foff, T *F)
+{
+    constexpr int NB = PanelWidth<T>::v;
+    __shared__ T U[NB][NB + 1];
+    const int q = q0 + blockIdx.y;
+    const int S = S_[q], f = f_[q];
+    if (S <= k) return;
+    const int w = min(NB, S - k);
+    const int rbeg = k + w + blockIdx.x * kL21Rows;
+    if (rbeg >= f) return;
+    T *A = F + foff[q];
+    for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+        const int r = e / NB, c = e - r * NB;
+        U[r][c] = (r < w && c < w) ? A[(long long)(k + r) * f + k + c] : T(0);
+    }
+    __syncthreads();
+    const int r = rbeg + threadIdx.x;
+    if (r >= f) return;
+    T x[NB];
+    T *row = A + (long long)r * f + k;
+#pragma unroll
+    for (int c = 0; c < NB; ++c) x[c] = c < w ? row[c] : T(0);
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        T sacc = x[c];
+#pragma unroll
+        for (int t = 0; t < c; ++t) sacc -= x[t] * U[t][c];
+        const T d = U[c][c];
+        x[c] = (c < w && d != T(0)) ? sacc / d : T(0);
+    }
+#pragma unroll
+    for (int c = 0; c < NB; ++c)
+        if (c < w) row[c] = x[c];
 }
 
 // The panel's row swaps (confined to its w rows) applied to every column
@@ -714,42 +787,200 @@ __global__ void __launch_bounds__(256) k_gemm(int q0, int k, const int *__restri
     }
 }
 
-// ipiv (sequential swaps) -> perm (row i of the factors came from local row perm[i]).
-__global__ void k_perm(int q0, int q1, const int *__restrict__ S_, const int *__restrict__ voff,
-                       const int *__restrict__ ipiv, int *perm)
+// Explicit inverses of the factored S x S block of every front of a level:
+// strictly lower part <- L11^-1 (unit diagonal implied), upper part incl. the
+// diagonal <- U11^-1, written to the level's scratch and copied back by
+// k_trcopy.  One CTA per (front, column block of CW columns); the column
+// block of each inverse is solved against the identity right-looking: the CTA
+// keeps the S x CW block in shared memory, solves one 32-row diagonal block
+// (one thread per column), then updates every remaining row with a rank-32
+// product (all threads).  With the inverses the solve applies each front by
+// row-parallel products instead of a chain of dependent triangular blocks.
+constexpr int kTrinvThreads = 512;
+template <class T> struct InvWidth;
+template <> struct InvWidth<float> { static constexpr int v = 32; };
+template <> struct InvWidth<double> { static constexpr int v = 16; };
+
+template <class T>
+__global__ void __launch_bounds__(kTrinvThreads) k_trinv(int q0, const int *__restrict__ S_,
+                                                         const long long *__restrict__ foff,
+                                                         const int *__restrict__ f_,
+                                                         const long long *__restrict__ toff,
+                                                         const T *__restrict__ F, T *tmp)
 {
-    const int q = q0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= q1) return;
-    const int S = S_[q], o = voff[q];
-    for (int i = 0; i < S; ++i) perm[o + i] = i;
-    for (int i = 0; i < S; ++i) {
-        const int p = ipiv[o + i];
-        const int t = perm[o + i];
-        perm[o + i] = perm[o + p];
-        perm[o + p] = t;
+    constexpr int CW = InvWidth<T>::v;
+    extern __shared__ unsigned char smem_raw[];
+    T *Xs = reinterpret_cast<T *>(smem_raw);    // S x CW
+    T *Lp = Xs + (size_t)S_[q0 + blockIdx.y] * CW;   // S x 33: the 32 columns of the current step
+    __shared__ T Dg[32][33];                     // current 32 x 32 diagonal block
+    const int q = q0 + blockIdx.y;
+    const int S = S_[q], f = f_[q];
+    const int c0 = blockIdx.x * CW;
+    if (c0 >= S) return;
+    const int cw = min(CW, S - c0);
+    const T *A = F + foff[q];
+    T *X = tmp + toff[q];
+    const int tid = threadIdx.x;
+    // ---------------- L11^-1 (unit lower): rows [c0, S)
+    for (int e = tid; e < S * CW; e += blockDim.x) {
+        const int r = e / CW, cc = e - r * CW;
+        Xs[e] = (r == c0 + cc) ? T(1) : T(0);
+    }
+    __syncthreads();
+    for (int r0 = (c0 / 32) * 32; r0 < S; r0 += 32) {
+        const int bh = min(32, S - r0);
+        for (int e = tid; e < 1024; e += blockDim.x) {
+            const int rr = e >> 5, cc = e & 31;
+            Dg[rr][cc] = (rr < bh && cc < bh) ? A[(long long)(r0 + rr) * f + r0 + cc] : T(0);
+        }
+        __syncthreads();
+        if (tid < CW) {   // diagonal block, one thread per column
+            for (int r = 1; r < bh; ++r) {
+                T v = Xs[(r0 + r) * CW + tid];
+                for (int t = 0; t < r; ++t) v -= Dg[r][t] * Xs[(r0 + t) * CW + tid];
+                Xs[(r0 + r) * CW + tid] = v;
+            }
+        }
+        __syncthreads();
+        const int rows = S - r0 - bh;
+        for (int e = tid; e < rows * 32; e += blockDim.x) {    // stage L[r0+bh.., r0..r0+32)
+            const int rr = e >> 5, t = e & 31;
+            Lp[rr * 33 + t] = t < bh ? A[(long long)(r0 + bh + rr) * f + r0 + t] : T(0);
+        }
+        __syncthreads();
+        for (int e = tid; e < rows * CW; e += blockDim.x) {   // rank-bh update below
+            const int rr = e / CW, cc = e % CW;
+            const T *lr = Lp + rr * 33;
+            T v0 = T(0), v1 = T(0);
+            int t = 0;
+            for (; t + 1 < bh; t += 2) {   // rows r0 .. r0+bh-1 of Xs only
+                v0 += lr[t] * Xs[(r0 + t) * CW + cc];
+                v1 += lr[t + 1] * Xs[(r0 + t + 1) * CW + cc];
+            }
+            if (t < bh) v0 += lr[t] * Xs[(r0 + t) * CW + cc];
+            Xs[(r0 + bh + rr) * CW + cc] -= v0 + v1;
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < S * CW; e += blockDim.x) {
+        const int r = e / CW, cc = e - r * CW;
+        if (cc < cw && r > c0 + cc) X[(long long)r * S + c0 + cc] = Xs[e];
+    }
+    __syncthreads();
+    // ---------------- U11^-1 (upper): rows [0, c0 + cw)
+    const int rtop = c0 + cw;
+    for (int e = tid; e < rtop * CW; e += blockDim.x) {
+        const int r = e / CW, cc = e - r * CW;
+        Xs[e] = (r == c0 + cc) ? T(1) : T(0);
+    }
+    __syncthreads();
+    for (int r0 = ((rtop - 1) / 32) * 32; r0 >= 0; r0 -= 32) {
+        const int r1 = min(r0 + 32, rtop);
+        const int bh = r1 - r0;
+        for (int e = tid; e < 1024; e += blockDim.x) {
+            const int rr = e >> 5, cc = e & 31;
+            Dg[rr][cc] = (rr < bh && cc < bh) ? A[(long long)(r0 + rr) * f + r0 + cc] : T(0);
+        }
+        __syncthreads();
+        if (tid < CW) {
+            for (int r = bh - 1; r >= 0; --r) {
+                T v = Xs[(r0 + r) * CW + tid];
+                for (int t = r + 1; t < bh; ++t) v -= Dg[r][t] * Xs[(r0 + t) * CW + tid];
+                const T d = Dg[r][r];
+                Xs[(r0 + r) * CW + tid] = d != T(0) ? v / d : T(0);
+            }
+        }
+        __syncthreads();
+        for (int e = tid; e < r0 * 32; e += blockDim.x) {      // stage U[0..r0, r0..r0+32)
+            const int rr = e >> 5, t = e & 31;
+            Lp[rr * 33 + t] = t < bh ? A[(long long)rr * f + r0 + t] : T(0);
+        }
+        __syncthreads();
+        for (int e = tid; e < r0 * CW; e += blockDim.x) {   // rank update above
+            const int r = e / CW, cc = e % CW;
+            const T *ur = Lp + r * 33;
+            T v0 = T(0), v1 = T(0);
+            int t = 0;
+            for (; t + 1 < bh; t += 2) {   // rows r0 .. r0+bh-1 of Xs only
+                v0 += ur[t] * Xs[(r0 + t) * CW + cc];
+                v1 += ur[t + 1] * Xs[(r0 + t + 1) * CW + cc];
+            }
+            if (t < bh) v0 += ur[t] * Xs[(r0 + t) * CW + cc];
+            Xs[r * CW + cc] -= v0 + v1;
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < rtop * CW; e += blockDim.x) {
+        const int r = e / CW, cc = e - r * CW;
+        if (cc < cw && r <= c0 + cc) X[(long long)r * S + c0 + cc] = Xs[e];
+    }
+}
+
+// Inverted S x S blocks of the level's fronts: scratch -> factor storage.
+template <class T>
+__global__ void k_trcopy(int q0, const int *__restrict__ S_, const int *__restrict__ f_,
+                         const long long *__restrict__ foff, const long long *__restrict__ toff,
+                         const T *__restrict__ tmp, T *F)
+{
+    const int q = q0 + blockIdx.y;
+    const int S = S_[q], f = f_[q];
+    const T *src = tmp + toff[q];
+    T *dst = F + foff[q];
+    const long long tot = (long long)S * S;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(e / S), c = (int)(e - (long long)r * S);
+        dst[(long long)r * f + c] = src[e];
     }
 }
 
 // ------------------------------------------------------------------ solve
-constexpr int kSolveThreads = 512;
 
 __device__ __forceinline__ bool stopped(const int *a, const int *b)
 {
     return (a && *a) || (b && *b);
 }
 
-// Forward: w = P (rs .* b)|FS + children's updates; L11 z = w; upd = w2 - L21 z.
+// The solve runs every step of a front as row-parallel products split over
+// CTAs of kSolveRows rows (one warp per row, lanes across the columns, four
+// independent partial sums), so the large top fronts use many SMs.
+constexpr int kSolveRows = 8;
+constexpr int kSolveThreads2 = 32 * kSolveRows;
+
 template <class T>
-__global__ void __launch_bounds__(kSolveThreads) k_fwd(int q0, const MfDev D, const T *F, const T *b,
-                                                       const double *__restrict__ rs, T *zbuf,
-                                                       T *upd, const int *stop_a, const int *stop_b)
+__device__ __forceinline__ T row_dot(const T *__restrict__ row, const T *v, int c0, int c1)
+{
+    const int lane = threadIdx.x & 31;
+    T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+    int c = c0 + lane;
+    for (; c + 96 < c1; c += 128) {
+        a0 += row[c] * v[c];
+        a1 += row[c + 32] * v[c + 32];
+        a2 += row[c + 64] * v[c + 64];
+        a3 += row[c + 96] * v[c + 96];
+    }
+    for (; c < c1; c += 32) a0 += row[c] * v[c];
+    return warp_sum((a0 + a1) + (a2 + a3));
+}
+
+// Forward, part 1 (grid: row chunks x fronts): every CTA gathers the front's
+// right-hand side w = rs .* b on the fully summed rows plus the children's
+// contribution vectors, permutes the fully summed part, and computes its rows
+// of z = L11^-1 P w (unit diagonal).  CTA 0 also stores w on the
+// contribution rows in the front's update vector for part 2.
+template <class T>
+__global__ void __launch_bounds__(kSolveThreads2) k_fwd_z(int q0, const MfDev D, const T *F, const T *b,
+                                                          const double *__restrict__ rs, T *zbuf,
+                                                          T *upd, const int *stop_a, const int *stop_b)
 {
     if (stopped(stop_a, stop_b)) return;
+    const int q = q0 + blockIdx.y;
+    const int S = D.S[q], f = D.f[q], vo = D.voff[q];
+    const int rbeg = blockIdx.x * kSolveRows;
+    if (rbeg >= S && blockIdx.x != 0) return;
     extern __shared__ unsigned char smem_raw[];
     T *w = reinterpret_cast<T *>(smem_raw);       // f
     T *t2 = w + D.maxf;                             // S
-    const int q = q0 + blockIdx.x;
-    const int S = D.S[q], f = D.f[q], vo = D.voff[q];
     const T *A = F + D.foff[q];
     const int *vars = D.vars + vo;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -768,104 +999,91 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd(int q0, const MfDev D, co
     const int *perm = D.perm + vo;
     for (int i = tid; i < S; i += blockDim.x) t2[i] = w[perm[i]];
     __syncthreads();
-    for (int i = tid; i < S; i += blockDim.x) w[i] = t2[i];
-    __syncthreads();
-    // blocked unit-lower solve: warp 0 solves each 32-row diagonal block with
-    // the block in registers (lane l holds row ib+l), then every thread
-    // updates one row below the block (FS rows and the CB rows alike)
-    for (int ib = 0; ib < S; ib += 32) {
-        const int bs = min(32, S - ib);
-        if (wid == 0) {
-            T Lr[32];
-            const T *row = A + (long long)(ib + min(lane, bs - 1)) * f + ib;
-#pragma unroll
-            for (int t = 0; t < 32; ++t) Lr[t] = (t < bs && lane < bs) ? row[t] : T(0);
-            T wl = lane < bs ? w[ib + lane] : T(0);
-#pragma unroll
-            for (int t = 0; t < 32; ++t) {
-                const T zt = __shfl_sync(0xffffffffu, wl, t);
-                if (lane > t) wl -= Lr[t] * zt;
-            }
-            if (lane < bs) w[ib + lane] = wl;
-        }
-        __syncthreads();
-        for (int r = ib + bs + tid; r < f; r += blockDim.x) {
-            const T *row = A + (long long)r * f + ib;
-            T v = T(0);
-            if (bs == 32) {
-#pragma unroll
-                for (int t = 0; t < 32; ++t) v += row[t] * w[ib + t];
-            } else {
-                for (int t = 0; t < bs; ++t) v += row[t] * w[ib + t];
-            }
-            w[r] -= v;
-        }
-        __syncthreads();
+    const int r = rbeg + wid;
+    if (r < S) {
+        const T v = row_dot(A + (long long)r * f, t2, 0, r);
+        if (lane == 0) zbuf[vo + r] = t2[r] + v;
     }
-    for (int i = tid; i < S; i += blockDim.x) zbuf[vo + i] = w[i];
-    T *uo = upd + D.uoff[q];
-    for (int i = tid; i < f - S; i += blockDim.x) uo[i] = w[S + i];
+    if (blockIdx.x == 0) {
+        T *uo = upd + D.uoff[q];
+        for (int i = tid; i < f - S; i += blockDim.x) uo[i] = w[S + i];
+    }
 }
 
-// Backward: y = z - U12 x_struct; U11 x_FS = y; scatter.
+// Forward, part 2 (grid: contribution-row chunks x fronts):
+// upd = w_CB - L21 z, in place in the front's update vector.
 template <class T>
-__global__ void __launch_bounds__(kSolveThreads) k_bwd(int q0, const MfDev D, const T *F, const T *zbuf,
-                                                       T *x, const int *stop_a, const int *stop_b)
+__global__ void __launch_bounds__(kSolveThreads2) k_fwd_u(int q0, const MfDev D, const T *F,
+                                                          const T *zbuf, T *upd, const int *stop_a,
+                                                          const int *stop_b)
 {
     if (stopped(stop_a, stop_b)) return;
-    extern __shared__ unsigned char smem_raw[];
-    T *y = reinterpret_cast<T *>(smem_raw);   // S
-    T *xs = y + D.maxS;                         // f - S
-    const int q = q0 + blockIdx.x;
+    const int q = q0 + blockIdx.y;
     const int S = D.S[q], f = D.f[q], vo = D.voff[q], m = f - S;
+    const int rbeg = blockIdx.x * kSolveRows;
+    if (rbeg >= m) return;
+    extern __shared__ unsigned char smem_raw[];
+    T *z = reinterpret_cast<T *>(smem_raw);   // S
+    const T *A = F + D.foff[q];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int i = tid; i < S; i += blockDim.x) z[i] = zbuf[vo + i];
+    __syncthreads();
+    const int i = rbeg + wid;
+    if (i < m) {
+        const T v = row_dot(A + (long long)(S + i) * f, z, 0, S);
+        if (lane == 0) upd[D.uoff[q] + i] -= v;
+    }
+}
+
+// Backward, part 1 (grid: row chunks x fronts): y = z - U12 x_struct, in
+// place in zbuf.
+template <class T>
+__global__ void __launch_bounds__(kSolveThreads2) k_bwd_y(int q0, const MfDev D, const T *F, T *zbuf,
+                                                          const T *x, const int *stop_a,
+                                                          const int *stop_b)
+{
+    if (stopped(stop_a, stop_b)) return;
+    const int q = q0 + blockIdx.y;
+    const int S = D.S[q], f = D.f[q], vo = D.voff[q], m = f - S;
+    const int rbeg = blockIdx.x * kSolveRows;
+    if (rbeg >= S || m == 0) return;
+    extern __shared__ unsigned char smem_raw[];
+    T *xs = reinterpret_cast<T *>(smem_raw);  // m
     const T *A = F + D.foff[q];
     const int *vars = D.vars + vo;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (int i = tid; i < m; i += blockDim.x) xs[i] = x[vars[S + i]];
     __syncthreads();
-    for (int r = wid; r < S; r += nw) {
-        T v = T(0);
-        for (int c = lane; c < m; c += 32) v += A[(long long)r * f + S + c] * xs[c];
-        v = warp_sum(v);
-        if (lane == 0) y[r] = zbuf[vo + r] - v;
+    const int r = rbeg + wid;
+    if (r < S) {
+        const T v = row_dot(A + (long long)r * f + S, xs, 0, m);
+        if (lane == 0) zbuf[vo + r] -= v;
     }
+}
+
+// Backward, part 2 (grid: row chunks x fronts): x_FS = U11^-1 y, scattered
+// to the solution vector.
+template <class T>
+__global__ void __launch_bounds__(kSolveThreads2) k_bwd_x(int q0, const MfDev D, const T *F,
+                                                          const T *zbuf, T *x, const int *stop_a,
+                                                          const int *stop_b)
+{
+    if (stopped(stop_a, stop_b)) return;
+    const int q = q0 + blockIdx.y;
+    const int S = D.S[q], f = D.f[q], vo = D.voff[q];
+    const int rbeg = blockIdx.x * kSolveRows;
+    if (rbeg >= S) return;
+    extern __shared__ unsigned char smem_raw[];
+    T *y = reinterpret_cast<T *>(smem_raw);   // S
+    const T *A = F + D.foff[q];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int i = tid; i < S; i += blockDim.x) y[i] = zbuf[vo + i];
     __syncthreads();
-    const int nblk = (S + 31) / 32;
-    for (int bb = nblk - 1; bb >= 0; --bb) {
-        const int ib = bb * 32, bs = min(32, S - ib);
-        if (wid == 0) {
-            T Ur[32];
-            const T *row = A + (long long)(ib + min(lane, bs - 1)) * f + ib;
-#pragma unroll
-            for (int t = 0; t < 32; ++t) Ur[t] = (t < bs && lane < bs) ? row[t] : T(0);
-            T yl = lane < bs ? y[ib + lane] : T(0);
-#pragma unroll
-            for (int t = 31; t >= 0; --t) {
-                if (t < bs) {
-                    const T d = Ur[t];   // diagonal, valid in lane t
-                    const T mine = (lane == t && d != T(0)) ? yl / d : T(0);
-                    const T xt = __shfl_sync(0xffffffffu, mine, t);
-                    if (lane == t) yl = xt;
-                    else if (lane < t) yl -= Ur[t] * xt;
-                }
-            }
-            if (lane < bs) y[ib + lane] = yl;
-        }
-        __syncthreads();
-        for (int r = tid; r < ib; r += blockDim.x) {
-            const T *row = A + (long long)r * f + ib;
-            T v = T(0);
-            if (bs == 32) {
-#pragma unroll
-                for (int t = 0; t < 32; ++t) v += row[t] * y[ib + t];
-            } else {
-                for (int t = 0; t < bs; ++t) v += row[t] * y[ib + t];
-            }
-            y[r] -= v;
-        }
-        __syncthreads();
+    const int r = rbeg + wid;
+    if (r < S) {
+        const T v = row_dot(A + (long long)r * f, y, r, S);
+        if (lane == 0) x[D.vars[vo + r]] = v;
     }
-    for (int i = tid; i < S; i += blockDim.x) x[vars[i]] = y[i];
 }
 
 }  // namespace
@@ -884,6 +1102,7 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
     grab(&M->F, (size_t)P->ftotal * es);
     grab(&M->upd, (size_t)P->utotal * es);
     grab(&M->z, (size_t)P->vtotal * es);
+    grab(&M->tmp, (size_t)P->tmax * es);
     grab((void **)&M->rs, (size_t)P->n * sizeof(double));
     grab((void **)&M->ipiv, (size_t)P->vtotal * sizeof(int));
     grab((void **)&M->perm, (size_t)P->vtotal * sizeof(int));
@@ -894,20 +1113,33 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
         mf_factor_destroy(M);
         return V2D_ENOMEM;
     }
-    // dynamic shared memory of the solve kernels (set once, outside any
-    // stream capture)
+    // dynamic shared memory of the solve and inversion kernels (set once,
+    // outside any stream capture)
     const size_t solve = (size_t)(P->maxf + P->maxS) * es;
-    if (solve > 227 * 1024) {
-        set_error("mf_factor: front of %d unknowns exceeds the solve's shared memory", P->maxf);
+    const size_t inv = (size_t)P->maxS * (fp32 ? (InvWidth<float>::v + 33) * sizeof(float)
+                                               : (InvWidth<double>::v + 33) * sizeof(double));
+    if (solve > 227 * 1024 || inv > 227 * 1024) {
+        set_error("mf_factor: front of %d unknowns (separator %d) exceeds shared memory",
+                  P->maxf, P->maxS);
         mf_factor_destroy(M);
         return V2D_EARG;
     }
+    auto attr = [&](const void *fn, size_t bytes) {
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    };
     if (fp32) {
-        e = cudaFuncSetAttribute(k_fwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_bwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve);
+        attr((const void *)k_fwd_z<float>, solve);
+        attr((const void *)k_fwd_u<float>, solve);
+        attr((const void *)k_bwd_y<float>, solve);
+        attr((const void *)k_bwd_x<float>, solve);
+        attr((const void *)k_trinv<float>, inv);
     } else {
-        e = cudaFuncSetAttribute(k_fwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_bwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve);
+        attr((const void *)k_fwd_z<double>, solve);
+        attr((const void *)k_fwd_u<double>, solve);
+        attr((const void *)k_bwd_y<double>, solve);
+        attr((const void *)k_bwd_x<double>, solve);
+        attr((const void *)k_trinv<double>, inv);
     }
     if (e != cudaSuccess) {
         set_error("mf_factor: %s", cudaGetErrorString(e));
@@ -922,7 +1154,7 @@ void mf_factor_destroy(MfFactor *M)
 {
     if (!M) return;
     if (M->graph) cudaGraphExecDestroy(M->graph);
-    void *ptrs[] = {M->F, M->upd, M->z, M->rs, M->ipiv, M->perm, M->flag};
+    void *ptrs[] = {M->F, M->upd, M->z, M->tmp, M->rs, M->ipiv, M->perm, M->flag};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     delete M;
@@ -970,18 +1202,28 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
         }
         const int maxf = P->lvl_maxf[L];
         for (int k = 0; k < P->lvl_maxS[L]; k += NB) {
-            k_panel<T><<<nq, kMfThreads, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff,
-                                                          P->d_voff, F, M->ipiv, M->flag);
+            k_panel<T><<<nq, kMfThreads, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff, P->d_voff, F,
+                                                 M->ipiv, M->perm, M->flag);
+            const int below = std::max(1, maxf - k - 1);
+            k_l21<T><<<dim3((below + kL21Rows - 1) / kL21Rows, nq), kL21Rows, 0, s>>>(
+                q0, k, P->d_S, P->d_f, P->d_foff, F);
             const int gcol = (maxf + kTrsmCols - 1) / kTrsmCols;
             k_swap_trsm<T><<<dim3(gcol, nq), kTrsmCols, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff,
                                                                 P->d_voff, F, M->ipiv);
             const int rem = std::max(1, maxf - k - 1);
             const int nt = (rem + kGemmTile - 1) / kGemmTile;
             k_gemm<T><<<dim3(nt * nt, nq), 256, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff, F);
-            launches += 3;
+            launches += 4;
         }
-        k_perm<<<(nq + 127) / 128, 128, 0, s>>>(q0, q0 + nq, P->d_S, P->d_voff, M->ipiv, M->perm);
-        ++launches;
+        const int nbc = (P->lvl_maxS[L] + InvWidth<T>::v - 1) / InvWidth<T>::v;
+        k_trinv<T><<<dim3(nbc, nq), kTrinvThreads,
+                     (size_t)P->lvl_maxS[L] * (InvWidth<T>::v + 33) * sizeof(T), s>>>(
+            q0, P->d_S, P->d_foff, P->d_f, P->d_toff, F, (T *)M->tmp);
+        const long long ss = (long long)P->lvl_maxS[L] * P->lvl_maxS[L];
+        const int gcp = (int)std::max(1LL, std::min<long long>((ss + 255) / 256, 256));
+        k_trcopy<T><<<dim3(gcp, nq), 256, 0, s>>>(q0, P->d_S, P->d_f, P->d_foff, P->d_toff,
+                                                  (const T *)M->tmp, F);
+        launches += 2;
     }
     V2D_CUDA_TRY(cudaGetLastError());
     M->launches_per_factor = launches;
@@ -1023,30 +1265,49 @@ int mf_factor(const MfPlan *P, MfFactor *M, const int *rowptr, const double *val
 
 template <class T>
 static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, const int *stop_a,
-                          const int *stop_b, cudaStream_t s)
+                          const int *stop_b, cudaStream_t s, long long *n_launches)
 {
     const MfDev D = mf_dev(P, M);
     const T *F = (const T *)M->F;
-    const size_t smf = (size_t)(P->maxf + P->maxS) * sizeof(T);
+    T *z = (T *)M->z, *upd = (T *)M->upd;
+    long long launches = 0;
+    auto chunks = [](int rows) { return std::max(1, (rows + kSolveRows - 1) / kSolveRows); };
     for (int L = 0; L < P->nlevel; ++L) {
         const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
-        k_fwd<T><<<nq, kSolveThreads, smf, s>>>(q0, D, F, b, M->rs, (T *)M->z, (T *)M->upd, stop_a,
-                                                stop_b);
+        k_fwd_z<T><<<dim3(chunks(P->lvl_maxS[L]), nq), kSolveThreads2,
+                     (size_t)(P->maxf + P->maxS) * sizeof(T), s>>>(q0, D, F, b, M->rs, z, upd,
+                                                                   stop_a, stop_b);
+        ++launches;
+        if (P->lvl_maxm[L] > 0) {
+            k_fwd_u<T><<<dim3(chunks(P->lvl_maxm[L]), nq), kSolveThreads2,
+                         (size_t)P->maxS * sizeof(T), s>>>(q0, D, F, z, upd, stop_a, stop_b);
+            ++launches;
+        }
     }
     for (int L = P->nlevel - 1; L >= 0; --L) {
         const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
-        k_bwd<T><<<nq, kSolveThreads, smf, s>>>(q0, D, F, (const T *)M->z, x, stop_a, stop_b);
+        if (P->lvl_maxm[L] > 0) {
+            k_bwd_y<T><<<dim3(chunks(P->lvl_maxS[L]), nq), kSolveThreads2,
+                         (size_t)P->maxf * sizeof(T), s>>>(q0, D, F, z, x, stop_a, stop_b);
+            ++launches;
+        }
+        k_bwd_x<T><<<dim3(chunks(P->lvl_maxS[L]), nq), kSolveThreads2,
+                     (size_t)P->maxS * sizeof(T), s>>>(q0, D, F, z, x, stop_a, stop_b);
+        ++launches;
     }
     V2D_CUDA_TRY(cudaGetLastError());
-    count_launches(2LL * P->nlevel);
+    if (n_launches) *n_launches = launches;
     return V2D_OK;
 }
 
 int mf_apply(const MfPlan *P, const MfFactor *M, const void *b, void *x, const int *stop_a,
-             const int *stop_b, cudaStream_t s)
+             const int *stop_b, cudaStream_t s, long long *n_launches)
 {
-    if (M->fp32) return apply_launches<float>(P, M, (const float *)b, (float *)x, stop_a, stop_b, s);
-    return apply_launches<double>(P, M, (const double *)b, (double *)x, stop_a, stop_b, s);
+    if (M->fp32)
+        return apply_launches<float>(P, M, (const float *)b, (float *)x, stop_a, stop_b, s,
+                                     n_launches);
+    return apply_launches<double>(P, M, (const double *)b, (double *)x, stop_a, stop_b, s,
+                                  n_launches);
 }
 
 int mf_flag(const MfFactor *M, int *flag, cudaStream_t s)

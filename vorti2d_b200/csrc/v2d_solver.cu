@@ -34,6 +34,9 @@ struct v2d_solver {
     MfPlan *plan = nullptr;        // multifrontal plan of the current pattern
     int plan_leaf = 0;
     MfFactor *lu[2] = {nullptr, nullptr};  // [0] FP64 factors, [1] FP32 factors
+    bool lu_valid = false;           // factors of an earlier Jacobian kept for reuse
+    int lu_last_its = 0;             // Krylov iterations of the last solve with them
+    long long lu_factorizations = 0;
     cudaEvent_t ev[5] = {};          // phase boundaries of the last Newton iteration
     double phase_ms[4] = {0, 0, 0, 0};
     long long phase_n = 0;
@@ -113,6 +116,7 @@ int check_params(const v2d_solver_params *p)
 
 void drop_lu(v2d_solver *S)
 {
+    S->lu_valid = false;
     for (int q = 0; q < 2; ++q) {
         mf_factor_destroy(S->lu[q]);
         S->lu[q] = nullptr;
@@ -186,6 +190,7 @@ extern "C" void v2d_krylov_defaults(v2d_krylov_params *p)
     p->inner_rtol = 1e-5;
     p->dc_max_it = 20;
     p->lu_leaf = 64;
+    p->lu_reuse_its = 0;
 }
 
 extern "C" int v2d_solver_destroy(v2d_solver *S)
@@ -280,6 +285,7 @@ extern "C" int v2d_solver_set_params(v2d_solver *S, const v2d_solver_params *p)
     V2D_TRY(check_params(p));
     const int old_m = S->prm.krylov.restart;
     S->prm = *p;
+    S->lu_valid = false;
     V2D_TRY(ensure_pattern(S));
     V2D_TRY(ensure_lu(S));
     if (p->krylov.restart != old_m) {
@@ -302,6 +308,7 @@ extern "C" int v2d_solver_set_state(v2d_solver *S, const double *psi, const doub
         if (src[q]) V2D_CUDA_TRY(cudaMemcpyAsync(dst[q], src[q], bytes, cudaMemcpyHostToDevice, S->s));
     V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
     S->assembled = false;
+    S->lu_valid = false;   // a new state: do not precondition with old factors
     return V2D_OK;
 }
 
@@ -359,16 +366,43 @@ extern "C" int v2d_solver_newton(v2d_solver *S, double urot, double *res, v2d_li
     CsrOp A;
     A.n = g.n; A.nnz = g.nnz; A.rowptr = g.rowptr; A.colind = g.colind; A.val = g.val;
     A.val32 = g.val32; A.dinv = g.dinv; A.dinv32 = g.dinv32; A.layout = 1; A.nblk = g.N;
-    if (S->prm.krylov.precond == V2D_PC_LU) {
+    const v2d_krylov_params &kp = S->prm.krylov;
+    const bool lu = kp.precond == V2D_PC_LU;
+    const int mixed = kp.precision == V2D_PREC_MIXED ? 1 : 0;
+    bool refactored = false;
+    if (lu) {
         V2D_TRY(ensure_lu(S));
-        MfFactor *M = S->lu[S->prm.krylov.precision == V2D_PREC_MIXED ? 1 : 0];
-        V2D_TRY(mf_factor(S->plan, M, g.rowptr, g.val, S->s));
+        const bool reuse = kp.lu_reuse_its > 0 && S->lu_valid && S->lu_last_its <= kp.lu_reuse_its;
+        if (!reuse) {
+            V2D_TRY(mf_factor(S->plan, S->lu[mixed], g.rowptr, g.val, S->s));
+            ++S->lu_factorizations;
+            refactored = true;
+        }
         A.lu_plan = S->plan;
-        A.lu = M;
+        A.lu = S->lu[mixed];
     }
     V2D_CUDA_TRY(cudaEventRecord(S->ev[2], S->s));
     v2d_lin_stats ls{};
-    V2D_TRY(krylov_solve(S->kw, A, g.b, S->delta, S->prm.krylov, &ls, S->s));
+    if (lu && !refactored) {
+        // stale factors: bounded attempt, then refactor and solve again
+        v2d_krylov_params k2 = kp;
+        k2.max_it = std::min(kp.max_it, std::max(2 * kp.lu_reuse_its, kp.restart));
+        V2D_TRY(krylov_solve(S->kw, A, g.b, S->delta, k2, &ls, S->s));
+        if (!ls.converged) {
+            const int its0 = ls.iterations;
+            V2D_TRY(mf_factor(S->plan, S->lu[mixed], g.rowptr, g.val, S->s));
+            ++S->lu_factorizations;
+            refactored = true;
+            V2D_TRY(krylov_solve(S->kw, A, g.b, S->delta, kp, &ls, S->s));
+            ls.iterations += its0;
+        }
+    } else {
+        V2D_TRY(krylov_solve(S->kw, A, g.b, S->delta, kp, &ls, S->s));
+    }
+    if (lu) {
+        S->lu_valid = true;
+        S->lu_last_its = refactored ? 0 : ls.iterations;
+    }
     V2D_CUDA_TRY(cudaEventRecord(S->ev[3], S->s));
     if (st) *st = ls;
     const int grid = std::max(1, std::min(kUpdBlocks, (g.N + kUpdThreads * 8 - 1) / (kUpdThreads * 8)));
@@ -498,14 +532,17 @@ extern "C" int v2d_solver_time_spmv(v2d_solver *S, int fp32, int reps, long long
     return time_spmv(A, fp32 != 0, reps, (size_t)flush_bytes, S->s, ms_avg);
 }
 
-extern "C" int v2d_solver_phase_times(v2d_solver *S, double *out5, int reset)
+extern "C" int v2d_solver_phase_times(v2d_solver *S, double *out6, int reset)
 {
-    V2D_ARG_CHECK(S && out5, "null pointer");
+    V2D_ARG_CHECK(S && out6, "null pointer");
+    double *out5 = out6;
     for (int q = 0; q < 4; ++q) out5[q] = S->phase_ms[q];
     out5[4] = (double)S->phase_n;
+    out5[5] = (double)S->lu_factorizations;
     if (reset) {
         for (double &v : S->phase_ms) v = 0.0;
         S->phase_n = 0;
+        S->lu_factorizations = 0;
     }
     return V2D_OK;
 }

@@ -42,6 +42,7 @@ def solver_params(cfg: Config) -> _lib.SolverParams:
     k.precision = cfg.precision_code()
     k.precond = cfg.precond_code()
     k.inner_rtol = float(cfg.inner_rtol)
+    k.lu_reuse_its = int(cfg.lu_reuse_its)
     p.krylov = k
     return p
 
