@@ -41,6 +41,10 @@ SOLVER = dict(ksp_restart=30, ksp_rtol=1e-10, krylov_max_it=3000, pseudo_tol=1e-
 METRIC = "BDF2 steps/s, 181x181 cylinder O-grid Re=100 dt=0.2 (<=5 Newton, GMRES(30))"
 L2_FLUSH_BYTES = 256 << 20
 SPMV_BYTES_PER_NNZ = {"fp64": 8 + 4, "fp32": 4 + 4}
+# DRAM bytes (read + write) of one LU apply, summed over its kernels in the
+# ncu capture summarised in profiles/lu_apply_181_mixed_traffic.md; None until
+# captured
+TRAFFIC_LU = None
 
 
 # ------------------------------------------------------------------ ranks
@@ -241,7 +245,13 @@ def run_ours(args, rank, world, local_rank):
                              factorizations_per_step=ph[5] / K)
         launches[prec] = c1 - c0
         if prec == legs[0]:
-            # dominant kernel (SpMV of the Krylov loop), timed alone after L2 flushes
+            # dominant unit: the LU preconditioner solve of a GMRES iteration,
+            # timed alone after L2 flushes; the Krylov SpMV beside it
+            import ctypes
+            ms_lu, fb = ctypes.c_double(), ctypes.c_longlong()
+            _lib.check(_lib.lib().v2d_solver_time_lu_apply(s.dev.h, 20, L2_FLUSH_BYTES,
+                                                           ctypes.byref(ms_lu), ctypes.byref(fb)))
+            results["lu_apply_ms"], results["lu_factor_bytes"] = ms_lu.value, fb.value
             ms_spmv = _spmv_time(_lib, s, fp32=(prec == "mixed"))
             results["spmv_ms"] = ms_spmv
             import ctypes
@@ -253,7 +263,7 @@ def run_ours(args, rank, world, local_rank):
             s2 = make_solver(v, xg, yg, prec, args.lu_reuse)
             for m in range(W):
                 s2.advance(times[m])
-            results["e2e"] = _e2e(torch, v, s2, times, W, K)
+            results["e2e"] = _e2e(torch, v, s2, times, W, K, flush_buf)
             s2.close()
         s.close()
     return results, launches
@@ -267,25 +277,26 @@ def _spmv_time(_lib, s, fp32, reps=20):
     return out.value
 
 
-def _e2e(torch, v, s, times, k0, K):
+def _e2e(torch, v, s, times, k0, K, flush_buf):
     """Steps k0 .. k0+K-1 (the timed steps of the device-resident leg) through
     Solver.set_state / advance / state readback with pinned host buffers; the
-    copies are inside the timed region."""
+    copies are inside the timed region, the L2 flush before each step is not."""
     N = s.ndof
     host = [torch.empty(N, dtype=torch.float64, pin_memory=True) for _ in range(4)]
     st = s.dev.get_state()
     for h, a in zip(host, st):
         h.numpy()[:] = a
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    dt = 0.0
     for m in range(K):
+        flush_l2(torch, flush_buf)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         s.set_state(*[h.numpy() for h in host])
         s.advance(times[k0 + m])
         out = s.dev.get_state()
         for h, a in zip(host, out):
             h.numpy()[:] = a
-    torch.cuda.synchronize()
-    dt = time.perf_counter() - t0
+        dt += time.perf_counter() - t0
     return dict(steps_per_s=K / dt, h2d=4 * N * 8, d2h=4 * N * 8, steps=K)
 
 
@@ -314,7 +325,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
     ap.add_argument("--cpu-steps", type=int, default=2)
-    ap.add_argument("--lu-reuse", type=int, default=20,
+    ap.add_argument("--lu-reuse", type=int, default=8,
                     help="keep LU factors while GMRES needs at most this many iterations "
                          "(0: factor every Newton Jacobian)")
     ap.add_argument("--profile-newton", action="store_true",
@@ -364,9 +375,15 @@ def main():
     n = 2 * IMAX * JMAX
     prec_key = "fp32" if head == "mixed" else "fp64"
     bytes_spmv = nnz * SPMV_BYTES_PER_NNZ[prec_key] + (n + 1) * 4 + 2 * n * (4 if prec_key == "fp32" else 8)
-    with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
-        peaks = json.load(fh)
+    peaks, peak_src = {"hbm_gbs": 6650.0}, "fallback 6.65 TB/s (no measured peaks file)"
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peaks, peak_src = json.load(fh), "measured hbm_gbs"
+    except (OSError, ValueError):
+        pass
     achieved = bytes_spmv / (res["spmv_ms"] * 1e-3) / 1e9
+    lu_bytes = res["lu_factor_bytes"]
+    achieved_lu = lu_bytes / (res["lu_apply_ms"] * 1e-3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_head,
@@ -380,10 +397,16 @@ def main():
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": world * res["e2e"]["steps_per_s"], "unit": "steps/s",
                 "h2d_bytes_per_step": res["e2e"]["h2d"], "d2h_bytes_per_step": res["e2e"]["d2h"]},
-        "roofline": {"bound": "hbm", "kernel": f"spmv_csr_{prec_key}",
-                     "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": None,
-                     "bytes_per_launch": bytes_spmv, "ms_per_launch": res["spmv_ms"]},
+        "roofline": {"bound": "hbm", "kernel": f"lu_apply_{prec_key} (forward + backward "
+                     "sweep over all levels: k_fwd_z, k_fwd_u, k_bwd_y, k_bwd_x)",
+                     "achieved": achieved_lu, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved_lu / peaks["hbm_gbs"], "traffic": TRAFFIC_LU,
+                     "bytes_per_launch": lu_bytes, "ms_per_launch": res["lu_apply_ms"],
+                     "peak_note": peak_src},
+        "roofline_spmv": {"bound": "hbm", "kernel": f"spmv_csr_{prec_key}",
+                          "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                          "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                          "bytes_per_launch": bytes_spmv, "ms_per_launch": res["spmv_ms"]},
         "cpu_baseline": cpu,
         "gpu_launches": int(launches.get(head, 0)),
         "clocks": res.get("clocks"),

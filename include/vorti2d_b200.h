@@ -168,11 +168,13 @@ typedef struct {
     int dc_max_it;        /* mixed: max defect-correction passes       (20)  */
     int lu_leaf;          /* LU: max nodes of a leaf subdomain         (64)  */
     int lu_reuse_its;     /* LU: 0 factors every Newton Jacobian (default);
-                             k > 0 keeps the factors across Newton iterations
-                             and time steps while the last solve with them
-                             took at most k Krylov iterations, and refactors
-                             (re-solving once) when a solve with stale factors
-                             fails.  Newton steps are still solved to rtol. */
+                             k > 0 keeps the factors across the Newton
+                             iterations of one time step (the BDF2 history
+                             shift refreshes them) while the last solve with
+                             them took at most k Krylov iterations; a solve
+                             with kept factors that needs more than k+5
+                             iterations refactors and solves again.  Newton
+                             steps are still solved to rtol.                */
 } v2d_krylov_params;
 
 void v2d_krylov_defaults(v2d_krylov_params *p);
@@ -289,6 +291,14 @@ int v2d_lu_plan_info(int imax, int jmax, const int *indptr, const int *indices, 
  * factorization (LU preconditioner), Krylov solve, update, iteration count,
  * LU factorizations performed. */
 int v2d_solver_phase_times(v2d_solver *s, double *out6, int reset);
+
+/* Measurement aid (no reference counterpart): average duration in ms of
+ * `reps` applications of the current LU factors (the preconditioner solve of
+ * one GMRES iteration), each preceded by a write of flush_bytes to evict L2;
+ * *factor_bytes receives the bytes of factor entries one application reads
+ * (per front the pivot-block inverses and the L21 / U12 blocks). */
+int v2d_solver_time_lu_apply(v2d_solver *s, int reps, long long flush_bytes, double *ms_avg,
+                             long long *factor_bytes);
 
 /* The stream the handle's kernels run on (cudaStream_t as void*). */
 int v2d_solver_stream(v2d_solver *s, void **stream);

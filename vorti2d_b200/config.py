@@ -74,9 +74,9 @@ class Config:
     """Mixed precision: relative residual reduction asked of each FP32 cycle."""
     lu_reuse_its: int = 0
     """LU preconditioner: 0 factors every Newton Jacobian; k > 0 keeps the
-    factors across Newton iterations and time steps while the last solve with
-    them needed at most k Krylov iterations (each Newton step is still solved
-    to ``ksp_rtol``)."""
+    factors across the Newton iterations of one time step while the last
+    solve with them needed at most k Krylov iterations (each Newton step is
+    still solved to ``ksp_rtol``)."""
     raise_on_linear_failure: bool = True
     """Raise if a Krylov solve misses ``ksp_rtol`` (the reference raises on a
     failed PETSc solve, vorti2d/petsc_solver.py:103-105)."""

@@ -49,6 +49,7 @@ struct MfPlan {
     long long ftotal = 0, nasm = 0;
     int vtotal = 0, utotal = 0;
     double flops = 0.0;   // 2 * sum S f^2 (upper bound of the factorization flops)
+    long long apply_entries = 0;   // factor entries one solve reads: sum S (2f - S)
     std::vector<int> S, f, voff, uoff, child0, child1, parent;
     std::vector<long long> foff;
     std::vector<long long> toff;   // offset of the front's S x S block in the level's scratch
@@ -58,11 +59,18 @@ struct MfPlan {
     int *d_S = nullptr, *d_f = nullptr, *d_voff = nullptr, *d_uoff = nullptr;
     int *d_child0 = nullptr, *d_child1 = nullptr;
     long long *d_foff = nullptr, *d_toff = nullptr;
+    int *d_lvl4 = nullptr;         // per level: first front, fronts, row chunks (S, CB)
     int *d_vars = nullptr, *d_cbmap = nullptr, *d_asm_csr = nullptr, *d_asm_row = nullptr;
     long long *d_asm_pos = nullptr;
     // host copies, kept only between the build and the upload
     std::vector<int> h_vars, h_cbmap, h_asm_csr, h_asm_row;
     std::vector<long long> h_asm_pos;
+};
+
+// Grid barrier state of the persistent solve (cooperative launch).
+struct MfBarrier {
+    unsigned int count, gen;
+    int err, pad;
 };
 
 // Numeric factors of one plan in one precision.
@@ -72,6 +80,8 @@ struct MfFactor {
     void *tmp = nullptr;        // triangular inverses of one level before they replace L11 / U11
     double *rs = nullptr;       // row scaling 1 / max |a_r.|
     int *ipiv = nullptr, *perm = nullptr, *flag = nullptr;
+    MfBarrier *bar = nullptr;
+    int coop_grid = 0;          // CTAs of the one-launch persistent solve (0: per-phase launches)
     cudaGraphExec_t graph = nullptr;
     const double *graph_val = nullptr;
     const int *graph_rowptr = nullptr;
@@ -104,6 +114,13 @@ int mf_factor(const MfPlan *P, MfFactor *M, const int *rowptr, const double *val
 int mf_apply(const MfPlan *P, const MfFactor *M, const void *b, void *x, const int *stop_a,
              const int *stop_b, cudaStream_t s, long long *n_launches);
 int mf_flag(const MfFactor *M, int *flag, cudaStream_t s);
+// V2D_ETIMEOUT (and a reset barrier) if a grid barrier of the persistent solve
+// timed out since the last check.
+int mf_check_barrier(MfFactor *M, cudaStream_t s);
+// Average device time (ms) of `reps` LU applies to a zero vector, each after a
+// write of flush_bytes (evicts L2); CUDA events on stream s.
+int mf_time_apply(const MfPlan *P, const MfFactor *M, int reps, size_t flush_bytes, cudaStream_t s,
+                  double *ms_avg);
 
 // ------------------------------------------------------------- Krylov
 // A CSR operator with optional FP32 copy and 2x2 block inverse.

@@ -47,6 +47,7 @@
 // CTAs of 8 rows, so the large top fronts spread over many SMs.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <vector>
@@ -54,6 +55,9 @@
 #include "v2d_internal.cuh"
 
 namespace v2d {
+
+// rows per work item of the solve (kSolveRows below; also the level table's unit)
+constexpr int kSolveRowsHost = 8;
 
 // ================================================================ symbolic
 namespace {
@@ -169,7 +173,7 @@ int upload_vec(T **d, const std::vector<T> &h)
 void mf_plan_destroy(MfPlan *p)
 {
     if (!p) return;
-    void *ptrs[] = {p->d_S, p->d_f, p->d_voff, p->d_uoff, p->d_child0, p->d_child1, p->d_foff, p->d_toff,
+    void *ptrs[] = {p->d_S, p->d_f, p->d_voff, p->d_uoff, p->d_child0, p->d_child1, p->d_foff, p->d_toff, p->d_lvl4,
                     p->d_vars, p->d_cbmap, p->d_asm_csr, p->d_asm_row, p->d_asm_pos};
     for (void *q : ptrs)
         if (q) cudaFree(q);
@@ -399,7 +403,10 @@ int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_c
     }
     P->ftotal = ftot; P->vtotal = vtot; P->utotal = utot; P->nasm = nnz;
     double fl = 0.0;
-    for (int id = 0; id < nf; ++id) fl += 2.0 * P->S[id] * (double)P->f[id] * P->f[id];
+    for (int id = 0; id < nf; ++id) {
+        fl += 2.0 * P->S[id] * (double)P->f[id] * P->f[id];
+        P->apply_entries += (long long)P->S[id] * (2LL * P->f[id] - P->S[id]);
+    }
     P->flops = fl;
     // every index the kernels dereference stays inside its buffer
     bool ok = (long long)vars.size() == vtot && (long long)cbmap.size() == utot;
@@ -448,6 +455,16 @@ int mf_plan_create(int imax, int jmax, int n, const int *h_rowptr, const int *h_
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_child1, P->child1);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_foff, P->foff);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_toff, P->toff);
+    if (st_up == V2D_OK) {
+        std::vector<int> l4(4 * P->nlevel);
+        for (int L = 0; L < P->nlevel; ++L) {
+            l4[4 * L] = P->lvl_off[L];
+            l4[4 * L + 1] = P->lvl_off[L + 1] - P->lvl_off[L];
+            l4[4 * L + 2] = std::max(1, (P->lvl_maxS[L] + kSolveRowsHost - 1) / kSolveRowsHost);
+            l4[4 * L + 3] = (P->lvl_maxm[L] + kSolveRowsHost - 1) / kSolveRowsHost;
+        }
+        st_up = upload_vec(&P->d_lvl4, l4);
+    }
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_vars, P->h_vars);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_cbmap, P->h_cbmap);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_asm_csr, P->h_asm_csr);
@@ -944,7 +961,9 @@ __device__ __forceinline__ bool stopped(const int *a, const int *b)
 // The solve runs every step of a front as row-parallel products split over
 // CTAs of kSolveRows rows (one warp per row, lanes across the columns, four
 // independent partial sums), so the large top fronts use many SMs.
-constexpr int kSolveRows = 8;
+constexpr int kSolveRows = kSolveRowsHost;
+// levels with at least this many fronts are solved with one CTA per front
+constexpr int kFrontPerCta = 64;
 constexpr int kSolveThreads2 = 32 * kSolveRows;
 
 template <class T>
@@ -963,27 +982,169 @@ __device__ __forceinline__ T row_dot(const T *__restrict__ row, const T *v, int 
     return warp_sum((a0 + a1) + (a2 + a3));
 }
 
-// Forward, part 1 (grid: row chunks x fronts): every CTA gathers the front's
-// right-hand side w = rs .* b on the fully summed rows plus the children's
-// contribution vectors, permutes the fully summed part, and computes its rows
-// of z = L11^-1 P w (unit diagonal).  CTA 0 also stores w on the
-// contribution rows in the front's update vector for part 2.
+// Forward, part 1 (one work item = one row chunk of one front): gather the
+// front's right-hand side w = rs .* b on the fully summed rows plus the
+// children's contribution vectors, permute the fully summed part, and compute
+// the chunk's rows of z = L11^-1 P w (unit diagonal).  Chunk 0 also stores w
+// on the contribution rows in the front's update vector for part 2.
+template <class T>
+__device__ __forceinline__ void fz_item(const MfDev &D, const T *F, const T *b,
+                                        const double *__restrict__ rs, T *zbuf, T *upd, int q,
+                                        int chunk, T *w, T *t2)
+{
+    const int S = D.S[q], f = D.f[q], vo = D.voff[q];
+    const int rbeg = chunk * kSolveRows;
+    if (rbeg >= S && chunk != 0) return;
+    const T *A = F + D.foff[q];
+    const int *vars = D.vars + vo;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int p = tid; p < f; p += blockDim.x) w[p] = p < S ? (T)(rs[vars[p]] * (double)b[vars[p]]) : T(0);
+    __syncthreads();
+    for (int slot = 0; slot < 2; ++slot) {
+        const int c = slot == 0 ? D.child0[q] : D.child1[q];
+        if (c >= 0) {
+            const int m = D.f[c] - D.S[c];
+            const int *map = D.cbmap + D.uoff[c];
+            const T *u = upd + D.uoff[c];
+            for (int e = tid; e < m; e += blockDim.x) w[map[e]] += __ldcg(u + e);
+        }
+        __syncthreads();
+    }
+    const int *perm = D.perm + vo;
+    for (int i = tid; i < S; i += blockDim.x) t2[i] = w[perm[i]];
+    __syncthreads();
+    const int r = rbeg + wid;
+    if (r < S) {
+        const T v = row_dot(A + (long long)r * f, t2, 0, r);
+        if (lane == 0) zbuf[vo + r] = t2[r] + v;
+    }
+    if (chunk == 0) {
+        T *uo = upd + D.uoff[q];
+        for (int i = tid; i < f - S; i += blockDim.x) uo[i] = w[S + i];
+    }
+}
+
+// Forward, part 2 (item = contribution-row chunk): upd = w_CB - L21 z, in
+// place in the front's update vector.
+template <class T>
+__device__ __forceinline__ void fu_item(const MfDev &D, const T *F, const T *zbuf, T *upd, int q,
+                                        int chunk, T *z)
+{
+    const int S = D.S[q], f = D.f[q], vo = D.voff[q], m = f - S;
+    const int rbeg = chunk * kSolveRows;
+    if (rbeg >= m) return;
+    const T *A = F + D.foff[q];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int i = tid; i < S; i += blockDim.x) z[i] = __ldcg(zbuf + vo + i);
+    __syncthreads();
+    const int i = rbeg + wid;
+    if (i < m) {
+        const T v = row_dot(A + (long long)(S + i) * f, z, 0, S);
+        T *u = upd + D.uoff[q] + i;
+        if (lane == 0) *u = __ldcg(u) - v;
+    }
+}
+
+// Backward, part 1 (item = row chunk): y = z - U12 x_struct, in place in zbuf.
+template <class T>
+__device__ __forceinline__ void by_item(const MfDev &D, const T *F, T *zbuf, const T *x, int q,
+                                        int chunk, T *xs)
+{
+    const int S = D.S[q], f = D.f[q], vo = D.voff[q], m = f - S;
+    const int rbeg = chunk * kSolveRows;
+    if (rbeg >= S || m == 0) return;
+    const T *A = F + D.foff[q];
+    const int *vars = D.vars + vo;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int i = tid; i < m; i += blockDim.x) xs[i] = __ldcg(x + vars[S + i]);
+    __syncthreads();
+    const int r = rbeg + wid;
+    if (r < S) {
+        const T v = row_dot(A + (long long)r * f + S, xs, 0, m);
+        if (lane == 0) zbuf[vo + r] = __ldcg(zbuf + vo + r) - v;
+    }
+}
+
+// Backward, part 2 (item = row chunk): x_FS = U11^-1 y, scattered to x.
+template <class T>
+__device__ __forceinline__ void bx_item(const MfDev &D, const T *F, const T *zbuf, T *x, int q,
+                                        int chunk, T *y)
+{
+    const int S = D.S[q], f = D.f[q], vo = D.voff[q];
+    const int rbeg = chunk * kSolveRows;
+    if (rbeg >= S) return;
+    const T *A = F + D.foff[q];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int i = tid; i < S; i += blockDim.x) y[i] = __ldcg(zbuf + vo + i);
+    __syncthreads();
+    const int r = rbeg + wid;
+    if (r < S) {
+        const T v = row_dot(A + (long long)r * f, y, r, S);
+        if (lane == 0) x[D.vars[vo + r]] = v;
+    }
+}
+
+// One launch per phase and level (grid: chunks x fronts).
 template <class T>
 __global__ void __launch_bounds__(kSolveThreads2) k_fwd_z(int q0, const MfDev D, const T *F, const T *b,
                                                           const double *__restrict__ rs, T *zbuf,
                                                           T *upd, const int *stop_a, const int *stop_b)
 {
     if (stopped(stop_a, stop_b)) return;
-    const int q = q0 + blockIdx.y;
-    const int S = D.S[q], f = D.f[q], vo = D.voff[q];
-    const int rbeg = blockIdx.x * kSolveRows;
-    if (rbeg >= S && blockIdx.x != 0) return;
     extern __shared__ unsigned char smem_raw[];
-    T *w = reinterpret_cast<T *>(smem_raw);       // f
-    T *t2 = w + D.maxf;                             // S
+    T *w = reinterpret_cast<T *>(smem_raw);
+    fz_item<T>(D, F, b, rs, zbuf, upd, q0 + blockIdx.y, blockIdx.x, w, w + D.maxf);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kSolveThreads2) k_fwd_u(int q0, const MfDev D, const T *F,
+                                                          const T *zbuf, T *upd, const int *stop_a,
+                                                          const int *stop_b)
+{
+    if (stopped(stop_a, stop_b)) return;
+    extern __shared__ unsigned char smem_raw[];
+    fu_item<T>(D, F, zbuf, upd, q0 + blockIdx.y, blockIdx.x, reinterpret_cast<T *>(smem_raw));
+}
+
+template <class T>
+__global__ void __launch_bounds__(kSolveThreads2) k_bwd_y(int q0, const MfDev D, const T *F, T *zbuf,
+                                                          const T *x, const int *stop_a,
+                                                          const int *stop_b)
+{
+    if (stopped(stop_a, stop_b)) return;
+    extern __shared__ unsigned char smem_raw[];
+    by_item<T>(D, F, zbuf, x, q0 + blockIdx.y, blockIdx.x, reinterpret_cast<T *>(smem_raw));
+}
+
+template <class T>
+__global__ void __launch_bounds__(kSolveThreads2) k_bwd_x(int q0, const MfDev D, const T *F,
+                                                          const T *zbuf, T *x, const int *stop_a,
+                                                          const int *stop_b)
+{
+    if (stopped(stop_a, stop_b)) return;
+    extern __shared__ unsigned char smem_raw[];
+    bx_item<T>(D, F, zbuf, x, q0 + blockIdx.y, blockIdx.x, reinterpret_cast<T *>(smem_raw));
+}
+
+// Levels with many small fronts: one CTA per front does the whole forward
+// (gather, z, contribution vector) or backward (y, x) step, so the right-hand
+// side is gathered once per front instead of once per row chunk.
+template <class T>
+__global__ void __launch_bounds__(kSolveThreads2) k_fwd_front(int q0, const MfDev D, const T *F,
+                                                              const T *b,
+                                                              const double *__restrict__ rs,
+                                                              T *zbuf, T *upd, const int *stop_a,
+                                                              const int *stop_b)
+{
+    if (stopped(stop_a, stop_b)) return;
+    extern __shared__ unsigned char smem_raw[];
+    T *w = reinterpret_cast<T *>(smem_raw);   // f
+    T *t2 = w + D.maxf;                         // S
+    const int q = q0 + blockIdx.x;
+    const int S = D.S[q], f = D.f[q], vo = D.voff[q];
     const T *A = F + D.foff[q];
     const int *vars = D.vars + vo;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
     for (int p = tid; p < f; p += blockDim.x) w[p] = p < S ? (T)(rs[vars[p]] * (double)b[vars[p]]) : T(0);
     __syncthreads();
     for (int slot = 0; slot < 2; ++slot) {
@@ -999,90 +1160,131 @@ __global__ void __launch_bounds__(kSolveThreads2) k_fwd_z(int q0, const MfDev D,
     const int *perm = D.perm + vo;
     for (int i = tid; i < S; i += blockDim.x) t2[i] = w[perm[i]];
     __syncthreads();
-    const int r = rbeg + wid;
-    if (r < S) {
+    for (int r = wid; r < S; r += nw) {            // z = Linv t2 (unit diagonal)
         const T v = row_dot(A + (long long)r * f, t2, 0, r);
-        if (lane == 0) zbuf[vo + r] = t2[r] + v;
+        if (lane == 0) w[r] = t2[r] + v;
     }
-    if (blockIdx.x == 0) {
-        T *uo = upd + D.uoff[q];
-        for (int i = tid; i < f - S; i += blockDim.x) uo[i] = w[S + i];
-    }
-}
-
-// Forward, part 2 (grid: contribution-row chunks x fronts):
-// upd = w_CB - L21 z, in place in the front's update vector.
-template <class T>
-__global__ void __launch_bounds__(kSolveThreads2) k_fwd_u(int q0, const MfDev D, const T *F,
-                                                          const T *zbuf, T *upd, const int *stop_a,
-                                                          const int *stop_b)
-{
-    if (stopped(stop_a, stop_b)) return;
-    const int q = q0 + blockIdx.y;
-    const int S = D.S[q], f = D.f[q], vo = D.voff[q], m = f - S;
-    const int rbeg = blockIdx.x * kSolveRows;
-    if (rbeg >= m) return;
-    extern __shared__ unsigned char smem_raw[];
-    T *z = reinterpret_cast<T *>(smem_raw);   // S
-    const T *A = F + D.foff[q];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    for (int i = tid; i < S; i += blockDim.x) z[i] = zbuf[vo + i];
     __syncthreads();
-    const int i = rbeg + wid;
-    if (i < m) {
-        const T v = row_dot(A + (long long)(S + i) * f, z, 0, S);
-        if (lane == 0) upd[D.uoff[q] + i] -= v;
+    for (int r = S + wid; r < f; r += nw) {        // upd = w_CB - L21 z
+        const T v = row_dot(A + (long long)r * f, w, 0, S);
+        if (lane == 0) w[r] -= v;
     }
-}
-
-// Backward, part 1 (grid: row chunks x fronts): y = z - U12 x_struct, in
-// place in zbuf.
-template <class T>
-__global__ void __launch_bounds__(kSolveThreads2) k_bwd_y(int q0, const MfDev D, const T *F, T *zbuf,
-                                                          const T *x, const int *stop_a,
-                                                          const int *stop_b)
-{
-    if (stopped(stop_a, stop_b)) return;
-    const int q = q0 + blockIdx.y;
-    const int S = D.S[q], f = D.f[q], vo = D.voff[q], m = f - S;
-    const int rbeg = blockIdx.x * kSolveRows;
-    if (rbeg >= S || m == 0) return;
-    extern __shared__ unsigned char smem_raw[];
-    T *xs = reinterpret_cast<T *>(smem_raw);  // m
-    const T *A = F + D.foff[q];
-    const int *vars = D.vars + vo;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    for (int i = tid; i < m; i += blockDim.x) xs[i] = x[vars[S + i]];
     __syncthreads();
-    const int r = rbeg + wid;
-    if (r < S) {
-        const T v = row_dot(A + (long long)r * f + S, xs, 0, m);
-        if (lane == 0) zbuf[vo + r] -= v;
-    }
+    for (int i = tid; i < S; i += blockDim.x) zbuf[vo + i] = w[i];
+    T *uo = upd + D.uoff[q];
+    for (int i = tid; i < f - S; i += blockDim.x) uo[i] = w[S + i];
 }
 
-// Backward, part 2 (grid: row chunks x fronts): x_FS = U11^-1 y, scattered
-// to the solution vector.
 template <class T>
-__global__ void __launch_bounds__(kSolveThreads2) k_bwd_x(int q0, const MfDev D, const T *F,
-                                                          const T *zbuf, T *x, const int *stop_a,
-                                                          const int *stop_b)
+__global__ void __launch_bounds__(kSolveThreads2) k_bwd_front(int q0, const MfDev D, const T *F,
+                                                              const T *zbuf, T *x,
+                                                              const int *stop_a, const int *stop_b)
 {
     if (stopped(stop_a, stop_b)) return;
-    const int q = q0 + blockIdx.y;
-    const int S = D.S[q], f = D.f[q], vo = D.voff[q];
-    const int rbeg = blockIdx.x * kSolveRows;
-    if (rbeg >= S) return;
     extern __shared__ unsigned char smem_raw[];
     T *y = reinterpret_cast<T *>(smem_raw);   // S
+    T *xs = y + D.maxS;                         // f - S
+    const int q = q0 + blockIdx.x;
+    const int S = D.S[q], f = D.f[q], vo = D.voff[q], m = f - S;
     const T *A = F + D.foff[q];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    for (int i = tid; i < S; i += blockDim.x) y[i] = zbuf[vo + i];
+    const int *vars = D.vars + vo;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+    for (int i = tid; i < m; i += blockDim.x) xs[i] = x[vars[S + i]];
     __syncthreads();
-    const int r = rbeg + wid;
-    if (r < S) {
+    for (int r = wid; r < S; r += nw) {
+        const T v = m > 0 ? row_dot(A + (long long)r * f + S, xs, 0, m) : T(0);
+        if (lane == 0) y[r] = zbuf[vo + r] - v;
+    }
+    __syncthreads();
+    for (int r = wid; r < S; r += nw) {            // x = Uinv y (upper incl. diagonal)
         const T v = row_dot(A + (long long)r * f, y, r, S);
-        if (lane == 0) x[D.vars[vo + r]] = v;
+        if (lane == 0) x[vars[r]] = v;
+    }
+}
+
+// Grid-wide barrier of a cooperative launch (all CTAs resident): a
+// generation counter in global memory.  The wait is bounded: after
+// kBarrierSpins polls the CTA records a timeout in bar->err and reports
+// failure, and the kernel returns; the host checks bar->err after the solve.
+constexpr long long kBarrierSpins = 1LL << 24;
+
+__device__ __forceinline__ bool grid_barrier(MfBarrier *bar)
+{
+    __shared__ int ok_s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        volatile unsigned int *gen = &bar->gen;
+        const unsigned int g = *gen;
+        __threadfence();
+        const unsigned int arrived = atomicAdd(&bar->count, 1u) + 1u;
+        if (arrived == gridDim.x) {
+            atomicExch(&bar->count, 0u);
+            __threadfence();
+            atomicAdd(&bar->gen, 1u);
+        } else {
+            long long spins = 0;
+            while (*gen == g) {
+                if (++spins > kBarrierSpins) {
+                    atomicOr(&bar->err, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        ok_s = ok;
+    }
+    __syncthreads();
+    return ok_s != 0;
+}
+
+// The whole solve in one cooperative launch: each phase of each level is a
+// loop over its (front, chunk) work items, separated by grid barriers.  Data
+// written by other CTAs in earlier phases (contribution vectors, z, x) is
+// read with L1-bypassing loads in the item functions.
+template <class T>
+__global__ void __launch_bounds__(kSolveThreads2) k_apply_all(const MfDev D, const T *F, const T *b,
+                                                              const double *__restrict__ rs,
+                                                              T *zbuf, T *upd, T *x,
+                                                              const int4 *__restrict__ lvl, int nlevel,
+                                                              MfBarrier *bar, const int *stop_a,
+                                                              const int *stop_b)
+{
+    if (stopped(stop_a, stop_b)) return;   // the flags are the same for every CTA
+    extern __shared__ unsigned char smem_raw[];
+    T *w = reinterpret_cast<T *>(smem_raw);
+    T *t2 = w + D.maxf;
+    for (int L = 0; L < nlevel; ++L) {
+        const int4 v = lvl[L];   // q0, fronts, chunks over S, chunks over the contribution rows
+        for (int it = blockIdx.x; it < v.y * v.z; it += gridDim.x) {
+            fz_item<T>(D, F, b, rs, zbuf, upd, v.x + it / v.z, it % v.z, w, t2);
+            __syncthreads();
+        }
+        if (!grid_barrier(bar)) return;
+        if (v.w > 0) {
+            for (int it = blockIdx.x; it < v.y * v.w; it += gridDim.x) {
+                fu_item<T>(D, F, zbuf, upd, v.x + it / v.w, it % v.w, w);
+                __syncthreads();
+            }
+            if (!grid_barrier(bar)) return;
+        }
+    }
+    for (int L = nlevel - 1; L >= 0; --L) {
+        const int4 v = lvl[L];
+        if (v.w > 0) {
+            for (int it = blockIdx.x; it < v.y * v.z; it += gridDim.x) {
+                by_item<T>(D, F, zbuf, x, v.x + it / v.z, it % v.z, w);
+                __syncthreads();
+            }
+            if (!grid_barrier(bar)) return;
+        }
+        for (int it = blockIdx.x; it < v.y * v.z; it += gridDim.x) {
+            bx_item<T>(D, F, zbuf, x, v.x + it / v.z, it % v.z, w);
+            __syncthreads();
+        }
+        if (L > 0 && !grid_barrier(bar)) return;
     }
 }
 
@@ -1107,6 +1309,8 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
     grab((void **)&M->ipiv, (size_t)P->vtotal * sizeof(int));
     grab((void **)&M->perm, (size_t)P->vtotal * sizeof(int));
     grab((void **)&M->flag, sizeof(int));
+    grab((void **)&M->bar, sizeof(MfBarrier));
+    if (e == cudaSuccess) e = cudaMemset(M->bar, 0, sizeof(MfBarrier));
     if (e != cudaSuccess) {
         set_error("mf_factor: allocation of %.1f MB failed: %s",
                   ((double)P->ftotal * es) / 1e6, cudaGetErrorString(e));
@@ -1129,12 +1333,18 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
             e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     };
     if (fp32) {
+        attr((const void *)k_apply_all<float>, solve);
+        attr((const void *)k_fwd_front<float>, solve);
+        attr((const void *)k_bwd_front<float>, solve);
         attr((const void *)k_fwd_z<float>, solve);
         attr((const void *)k_fwd_u<float>, solve);
         attr((const void *)k_bwd_y<float>, solve);
         attr((const void *)k_bwd_x<float>, solve);
         attr((const void *)k_trinv<float>, inv);
     } else {
+        attr((const void *)k_apply_all<double>, solve);
+        attr((const void *)k_fwd_front<double>, solve);
+        attr((const void *)k_bwd_front<double>, solve);
         attr((const void *)k_fwd_z<double>, solve);
         attr((const void *)k_fwd_u<double>, solve);
         attr((const void *)k_bwd_y<double>, solve);
@@ -1146,6 +1356,23 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
         mf_factor_destroy(M);
         return V2D_ECUDA;
     }
+    // persistent solve: as many CTAs as can be resident at once (at most 2 per
+    // SM); 0 keeps the one-launch-per-phase path (the default)
+    int dev = 0, coop = 0, nsm = 0, per_sm = 0;
+    // opt-in (V2D_LU_PERSISTENT=1): on 181x181 the per-phase launches were
+    // faster than one cooperative launch with a grid barrier per phase
+    const char *env = getenv("V2D_LU_PERSISTENT");
+    const bool allow = env && env[0] == '1';
+    if (allow && cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && coop) {
+        cudaError_t oe = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                    &per_sm, k_apply_all<float>, kSolveThreads2, solve)
+                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                    &per_sm, k_apply_all<double>, kSolveThreads2, solve);
+        if (oe == cudaSuccess && per_sm > 0) M->coop_grid = nsm * std::min(per_sm, 2);
+    }
+    cudaGetLastError();
     *out = M;
     return V2D_OK;
 }
@@ -1154,7 +1381,7 @@ void mf_factor_destroy(MfFactor *M)
 {
     if (!M) return;
     if (M->graph) cudaGraphExecDestroy(M->graph);
-    void *ptrs[] = {M->F, M->upd, M->z, M->tmp, M->rs, M->ipiv, M->perm, M->flag};
+    void *ptrs[] = {M->F, M->upd, M->z, M->tmp, M->rs, M->ipiv, M->perm, M->flag, M->bar};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     delete M;
@@ -1271,9 +1498,34 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
     const T *F = (const T *)M->F;
     T *z = (T *)M->z, *upd = (T *)M->upd;
     long long launches = 0;
+    if (M->coop_grid > 0) {
+        // the whole solve as one cooperative launch (graph-capturable)
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(M->coop_grid);
+        cfg.blockDim = dim3(kSolveThreads2);
+        cfg.dynamicSmemBytes = (size_t)(P->maxf + P->maxS) * sizeof(T);
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        V2D_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_apply_all<T>, D, F, b, (const double *)M->rs, z,
+                                        upd, x, (const int4 *)P->d_lvl4, P->nlevel, M->bar,
+                                        stop_a, stop_b));
+        if (n_launches) *n_launches = 1;
+        return V2D_OK;
+    }
     auto chunks = [](int rows) { return std::max(1, (rows + kSolveRows - 1) / kSolveRows); };
+    const size_t smf = (size_t)(P->maxf + P->maxS) * sizeof(T);
     for (int L = 0; L < P->nlevel; ++L) {
         const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
+        if (nq >= kFrontPerCta) {
+            k_fwd_front<T><<<nq, kSolveThreads2, smf, s>>>(q0, D, F, b, M->rs, z, upd, stop_a,
+                                                           stop_b);
+            ++launches;
+            continue;
+        }
         k_fwd_z<T><<<dim3(chunks(P->lvl_maxS[L]), nq), kSolveThreads2,
                      (size_t)(P->maxf + P->maxS) * sizeof(T), s>>>(q0, D, F, b, M->rs, z, upd,
                                                                    stop_a, stop_b);
@@ -1286,6 +1538,11 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
     }
     for (int L = P->nlevel - 1; L >= 0; --L) {
         const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
+        if (nq >= kFrontPerCta) {
+            k_bwd_front<T><<<nq, kSolveThreads2, smf, s>>>(q0, D, F, z, x, stop_a, stop_b);
+            ++launches;
+            continue;
+        }
         if (P->lvl_maxm[L] > 0) {
             k_bwd_y<T><<<dim3(chunks(P->lvl_maxS[L]), nq), kSolveThreads2,
                          (size_t)P->maxf * sizeof(T), s>>>(q0, D, F, z, x, stop_a, stop_b);
@@ -1313,6 +1570,50 @@ int mf_apply(const MfPlan *P, const MfFactor *M, const void *b, void *x, const i
 int mf_flag(const MfFactor *M, int *flag, cudaStream_t s)
 {
     V2D_CUDA_TRY(cudaMemcpyAsync(flag, M->flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    return V2D_OK;
+}
+
+int mf_time_apply(const MfPlan *P, const MfFactor *M, int reps, size_t flush_bytes, cudaStream_t s,
+                  double *ms_avg)
+{
+    const size_t es = M->fp32 ? sizeof(float) : sizeof(double);
+    DevBuf<char> buf;
+    V2D_TRY(buf.alloc(2 * P->n * es + flush_bytes + 256, s));
+    V2D_CUDA_TRY(cudaMemsetAsync(buf.p, 0, 2 * P->n * es, s));
+    char *fl = buf.p + 2 * P->n * es;
+    cudaEvent_t e0, e1;
+    V2D_CUDA_TRY(cudaEventCreate(&e0));
+    V2D_CUDA_TRY(cudaEventCreate(&e1));
+    double total = 0.0;
+    int st = V2D_OK;
+    for (int r = 0; r < reps && st == V2D_OK; ++r) {
+        if (flush_bytes) cudaMemsetAsync(fl, r & 0xff, flush_bytes, s);
+        cudaEventRecord(e0, s);
+        st = mf_apply(P, M, buf.p, buf.p + P->n * es, nullptr, nullptr, s, nullptr);
+        cudaEventRecord(e1, s);
+        if (cudaEventSynchronize(e1) != cudaSuccess) st = V2D_ECUDA;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        total += ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != V2D_OK) return st;
+    *ms_avg = total / reps;
+    return V2D_OK;
+}
+
+int mf_check_barrier(MfFactor *M, cudaStream_t s)
+{
+    if (!M->bar) return V2D_OK;
+    int err = 0;
+    V2D_CUDA_TRY(cudaMemcpyAsync(&err, &M->bar->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(s));
+    if (err) {
+        V2D_CUDA_TRY(cudaMemsetAsync(M->bar, 0, sizeof(MfBarrier), s));
+        set_error("LU solve: a grid barrier of the persistent solve timed out");
+        return V2D_ETIMEOUT;
+    }
     return V2D_OK;
 }
 

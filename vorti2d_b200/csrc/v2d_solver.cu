@@ -35,6 +35,7 @@ struct v2d_solver {
     int plan_leaf = 0;
     MfFactor *lu[2] = {nullptr, nullptr};  // [0] FP64 factors, [1] FP32 factors
     bool lu_valid = false;           // factors of an earlier Jacobian kept for reuse
+    bool lu_ready = false;           // the factor storage holds some factorization
     int lu_last_its = 0;             // Krylov iterations of the last solve with them
     long long lu_factorizations = 0;
     cudaEvent_t ev[5] = {};          // phase boundaries of the last Newton iteration
@@ -117,6 +118,7 @@ int check_params(const v2d_solver_params *p)
 void drop_lu(v2d_solver *S)
 {
     S->lu_valid = false;
+    S->lu_ready = false;
     for (int q = 0; q < 2; ++q) {
         mf_factor_destroy(S->lu[q]);
         S->lu[q] = nullptr;
@@ -376,6 +378,7 @@ extern "C" int v2d_solver_newton(v2d_solver *S, double urot, double *res, v2d_li
         if (!reuse) {
             V2D_TRY(mf_factor(S->plan, S->lu[mixed], g.rowptr, g.val, S->s));
             ++S->lu_factorizations;
+            S->lu_ready = true;
             refactored = true;
         }
         A.lu_plan = S->plan;
@@ -386,12 +389,13 @@ extern "C" int v2d_solver_newton(v2d_solver *S, double urot, double *res, v2d_li
     if (lu && !refactored) {
         // stale factors: bounded attempt, then refactor and solve again
         v2d_krylov_params k2 = kp;
-        k2.max_it = std::min(kp.max_it, std::max(2 * kp.lu_reuse_its, kp.restart));
+        k2.max_it = std::min(kp.max_it, kp.lu_reuse_its + 5);
         V2D_TRY(krylov_solve(S->kw, A, g.b, S->delta, k2, &ls, S->s));
         if (!ls.converged) {
             const int its0 = ls.iterations;
             V2D_TRY(mf_factor(S->plan, S->lu[mixed], g.rowptr, g.val, S->s));
             ++S->lu_factorizations;
+            S->lu_ready = true;
             refactored = true;
             V2D_TRY(krylov_solve(S->kw, A, g.b, S->delta, kp, &ls, S->s));
             ls.iterations += its0;
@@ -400,6 +404,7 @@ extern "C" int v2d_solver_newton(v2d_solver *S, double urot, double *res, v2d_li
         V2D_TRY(krylov_solve(S->kw, A, g.b, S->delta, kp, &ls, S->s));
     }
     if (lu) {
+        V2D_TRY(mf_check_barrier(S->lu[mixed], S->s));
         S->lu_valid = true;
         S->lu_last_its = refactored ? 0 : ls.iterations;
     }
@@ -463,6 +468,7 @@ extern "C" int v2d_solver_shift_history(v2d_solver *S)
     const size_t bytes = (size_t)S->g.N * sizeof(double);
     V2D_CUDA_TRY(cudaMemcpyAsync(S->g.omeoldold, S->g.omeold, bytes, cudaMemcpyDeviceToDevice, S->s));
     V2D_CUDA_TRY(cudaMemcpyAsync(S->g.omeold, S->g.ome, bytes, cudaMemcpyDeviceToDevice, S->s));
+    S->lu_valid = false;   // factors are reused within a time step, refreshed at the next
     return V2D_OK;
 }
 
@@ -545,6 +551,19 @@ extern "C" int v2d_solver_phase_times(v2d_solver *S, double *out6, int reset)
         S->lu_factorizations = 0;
     }
     return V2D_OK;
+}
+
+extern "C" int v2d_solver_time_lu_apply(v2d_solver *S, int reps, long long flush_bytes,
+                                        double *ms_avg, long long *factor_bytes)
+{
+    V2D_ARG_CHECK(S && ms_avg && factor_bytes && reps > 0 && flush_bytes >= 0,
+                  "time_lu_apply: bad arguments");
+    V2D_ARG_CHECK(S->prm.krylov.precond == V2D_PC_LU && S->plan,
+                  "time_lu_apply: the handle does not use the LU preconditioner");
+    const int q = S->prm.krylov.precision == V2D_PREC_MIXED ? 1 : 0;
+    V2D_ARG_CHECK(S->lu[q] && S->lu_ready, "time_lu_apply: no factors yet (run a Newton iteration)");
+    *factor_bytes = S->plan->apply_entries * (long long)(q ? sizeof(float) : sizeof(double));
+    return mf_time_apply(S->plan, S->lu[q], reps, (size_t)flush_bytes, S->s, ms_avg);
 }
 
 extern "C" int v2d_solver_stream(v2d_solver *S, void **stream)
