@@ -143,6 +143,14 @@ int v2d_force_coeffs(int imax, int jmax, double re, double dksi, double deta,
                      const double *ome, double ref_length, double x0, double y0,
                      double *out10);
 
+/* Replaces vorti2d.velocity.compute_velocity (vorti2d/velocity.py:76-93):
+ * Cartesian velocity from the streamfunction, computed on the device from host
+ * arrays of imax*jmax doubles (pointer order).  vmag may be null. */
+int v2d_compute_velocity(int imax, int jmax, double dksi, double deta, const double *jac,
+                         const double *beta, const double *gama, const double *detadx,
+                         const double *detady, const double *psi, double *u, double *v,
+                         double *vmag);
+
 /* ------------------------------------------------ Krylov solver parameters */
 #define V2D_PC_NONE 0
 #define V2D_PC_BJACOBI 1   /* 2x2 (psi, ome) node blocks                     */
@@ -260,6 +268,24 @@ int v2d_solver_step(v2d_solver *s, double urot, double pseudo_tol, int max_iter,
  * out10 = cd, cl, cm, cdp, cdf, clp, clf, cmp, cmf, ref_length. */
 int v2d_solver_forces(v2d_solver *s, double re, double ref_length, double x0, double y0,
                       double *out10);
+/* Velocity of the current state (vorti2d/velocity.py:76-93) into host arrays
+ * of N doubles; vmag may be null. */
+int v2d_solver_velocity(v2d_solver *s, double *u, double *v, double *vmag);
+/* Discrete adjoint (no reference counterpart; the reference has no adjoint):
+ * J^T lambda = g for the Jacobian J = dR/dq of the current state (rotation
+ * urot), R = -b the residual of the field-blocked 2N system.  FP64 multifrontal
+ * factors of J are computed, the transposed solve is refined against J^T
+ * products until ||g - J^T lambda|| <= rtol ||g||, max_refine passes, or a
+ * pass no longer halves the residual (the attainable accuracy; accepted when
+ * below 1e-8).
+ * g and lambda: host arrays of 2N doubles. */
+int v2d_solver_adjoint(v2d_solver *s, double urot, const double *g, double *lambda, double rtol,
+                       int max_refine, int *refinements, double *rel_res);
+/* b = -R of the current state for the given scalar parameters (same far-field
+ * BC and pattern as the handle), into a host array of 2N doubles: the
+ * parameter derivatives of the residual for the adjoint. */
+int v2d_solver_residual(v2d_solver *s, double re, double invdtau, double inv2dt, double urot,
+                        double ca, double sa, double *b);
 /* Current system (after the last assembly): canonical CSR of the 2N system
  * and its right-hand side.  Sizes: 2N+1, nnz, nnz, 2N. */
 int v2d_solver_nnz(const v2d_solver *s, long long *nnz);

@@ -244,6 +244,32 @@ def compute_force_coeffs(imax, jmax, re, dksi, deta, beta, gama, detadx, detady,
                        clp=clp, clf=clf, cmp=cmp_, cmf=cmf, ref_length=d)
 
 
+# ----------------------------------------------------------------- velocity
+def compute_velocity(imax, jmax, dksi, deta, jac, beta, gama, detadx, detady, psi,
+                     want_mag=False):
+    """Restates vorti2d/velocity.py:38-93: grad(xi) from the exported metrics,
+    psi_xi central with the branch-cut wrap, psi_eta central inside and
+    one-sided 2nd order at j = 0 and j = jmax-1."""
+    xix = (gama * detadx + jac * detady) / beta
+    xiy = (gama * detady - jac * detadx) / beta
+    p = np.asarray(psi, dtype=np.float64).reshape(jmax, imax)
+    i = np.arange(imax)
+    e, w = i + 1, i - 1
+    e[0] = e[imax - 1] = 1
+    w[0] = w[imax - 1] = imax - 2
+    pxi = ((p[:, e] - p[:, w]) / (2.0 * dksi)).reshape(-1)
+    pe = np.empty_like(p)
+    pe[1:-1] = (p[2:] - p[:-2]) / (2.0 * deta)
+    pe[0] = (-3.0 * p[0] + 4.0 * p[1] - p[2]) / (2.0 * deta)
+    pe[-1] = (3.0 * p[-1] - 4.0 * p[-2] + p[-3]) / (2.0 * deta)
+    pe = pe.reshape(-1)
+    u = pxi * xiy + pe * detady
+    v = -(pxi * xix + pe * detadx)
+    if want_mag:
+        return u, v, np.sqrt(u * u + v * v)
+    return u, v
+
+
 # ------------------------------------------------------------- config scalars
 def config_scalars(re=60.0, steady=False, dt_phys=0.2, dtau=math.inf, alpha_deg=0.0,
                    farfield_bc="dirichlet"):

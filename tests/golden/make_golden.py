@@ -5,14 +5,15 @@ pure-NumPy modules (run in a checkout that has the reference next to it):
 
 The reference's Fortran core and PETSc layer cannot be built without a Fortran
 compiler and petsc4py, but ``vorti2d/mesh.py``, ``vorti2d/forces.py``,
-``vorti2d/config.py``, ``vorti2d/restart.py`` and ``vorti2d/velocity.py``
-import only numpy, so they are loaded unmodified by file path and run here.
-Their outputs pin the oracle's restatements (mesh generator, force integrals,
-configuration scalars) and the product's host-side mirrors of them.
+``vorti2d/config.py`` and ``vorti2d/velocity.py`` import only numpy, so they
+are loaded unmodified by file path and run here.  Their outputs pin the
+oracle's restatements (mesh generator, force integrals, configuration
+scalars, velocity reconstruction) and the product's kernels and host-side
+mirrors of them.
 
-Forces need metric arrays as input; those come from the oracle's C
-restatement of ``compute_metrics`` and are stored next to the outputs, so the
-golden force values depend only on the reference's ``forces.py``.
+Forces and velocities need metric arrays as input; those come from the
+oracle's C restatement of ``compute_metrics`` and are stored next to the
+outputs, so the golden values depend only on the reference's modules.
 """
 from __future__ import annotations
 
@@ -101,6 +102,20 @@ def main(ref_root):
                              fc.cmf, fc.ref_length])
             out[f"{key}_out_{tag}"] = np.array(rows)
     out["force_columns"] = np.array(forces.FORCE_COLUMNS)
+    velocity = load(ref_root, "velocity")
+    for (im, jm) in FORCE_MESHES:
+        xg, yg = mesh.generate_cylinder(im, jm, 0.5, 50.0)
+        dk, de = 1.0 / (im - 1), 1.0 / (jm - 1)
+        M = O.core().compute_metrics(dk, de, xg, yg)
+        psi, _ = smooth_state(M[8], M[9])
+        key = f"velocity_{im}x{jm}"
+        for name, a in zip(("jac", "beta", "gama", "detadx", "detady"), (M[0], M[2], M[3], M[6],
+                                                                          M[7])):
+            out[f"{key}_in_{name}"] = a
+        out[f"{key}_in_psi"] = psi
+        u, v, mag = velocity.compute_velocity(im, jm, dk, de, M[0], M[2], M[3], M[6], M[7], psi,
+                                              want_mag=True)
+        out[f"{key}_out"] = np.stack([u, v, mag])
     rows = []
     for kw in CONFIGS:
         c = config.Config(**kw)

@@ -12,12 +12,14 @@ from .mesh import (generate_cylinder, generate_naca0012, load_cgns_ogrid, load_m
                    save_mesh)
 from .solver import Solver, run
 from .forces import compute_force_coeffs, ForceCoeffs
+from . import velocity
+from .velocity import compute_velocity
 from .petsc_solver import GpuLinearSolver, MumpsSolver
 
 __all__ = [
     "Config", "Solver", "run", "generate_cylinder", "generate_naca0012", "load_mesh",
     "load_cgns_ogrid", "save_mesh", "compute_force_coeffs", "ForceCoeffs", "mesh", "core",
-    "GpuLinearSolver", "MumpsSolver",
+    "GpuLinearSolver", "MumpsSolver", "velocity", "compute_velocity",
 ]
 
 __version__ = "0.1.0"

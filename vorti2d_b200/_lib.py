@@ -81,6 +81,10 @@ _SIGS = {
     "v2d_assemble_coo_noalloc": (_i, [_i, _i] + [_d] * 6 + [ctypes.POINTER(_vp)] + [_i] * 4
                                  + [_d] * 2 + [_vp, _vp, _vp, _ip, _vp, _vp]),
     "v2d_force_coeffs": (_i, [_i, _i, _d, _d, _d] + [_dp] * 7 + [_d, _d, _d, _dp]),
+    "v2d_compute_velocity": (_i, [_i, _i, _d, _d] + [_dp] * 9),
+    "v2d_solver_velocity": (_i, [_vp, _dp, _dp, _dp]),
+    "v2d_solver_adjoint": (_i, [_vp, _d, _dp, _dp, _d, _i, _ip, _dp]),
+    "v2d_solver_residual": (_i, [_vp, _d, _d, _d, _d, _d, _d, _dp]),
     "v2d_krylov_defaults": (None, [ctypes.POINTER(KrylovParams)]),
     "v2d_linsys_create": (_i, [_i, _i, ctypes.POINTER(KrylovParams), ctypes.POINTER(_vp)]),
     "v2d_linsys_assemble": (_i, [_vp, _ip, _ip, _dp, _ll, _dp]),

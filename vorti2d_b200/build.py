@@ -28,6 +28,7 @@ SOURCES = [
     ("v2d_mf.cu", []),
     ("v2d_solver.cu", []),
     ("v2d_forces.cu", []),
+    ("v2d_velocity.cu", ["-fmad=false"]),
     ("v2d_linsys.cu", []),
 ]
 

@@ -164,6 +164,36 @@ __global__ void __launch_bounds__(128) assemble_newton(GlobalTopo T, Coeffs c, F
     }
 }
 
+// Right-hand side b = -R of the Newton system only (no Jacobian values), for
+// scalar parameters that may differ from the handle's: the parameter
+// derivatives of the residual used by the adjoint.
+__global__ void __launch_bounds__(128) residual_only(GlobalTopo T, Coeffs c, Fields f,
+                                                     double *__restrict__ b)
+{
+    V2D_GRID_STRIDE(t, T.N)
+    {
+        const int K = (int)t;
+        int col[kOmeMax];
+        double v[kOmeMax];
+        double bk;
+        psi_row<true>(T, c, f, K, col, v, &bk);
+        b[K] = bk;
+        ome_row<true>(T, c, f, K, col, v, &bk);
+        b[T.N + K] = bk;
+    }
+}
+
+int launch_residual(const GridDev &g, const AsmParams &p, double *d_b, cudaStream_t s)
+{
+    GlobalTopo T{g.imax, g.jmax, g.N};
+    Coeffs c{p.re, p.invdtau, p.inv2dt, p.urot, g.dksi, g.deta, p.ca, p.sa, p.ff_bc};
+    Fields f = fields_of(g);
+    residual_only<<<grid_for(g.N, 128), 128, 0, s>>>(T, c, f, d_b);
+    V2D_CUDA_TRY(cudaGetLastError());
+    count_launches(1);
+    return V2D_OK;
+}
+
 int launch_assemble(GridDev &g, const AsmParams &p, bool want32, int *d_flag, cudaStream_t s)
 {
     GlobalTopo T{g.imax, g.jmax, g.N};

@@ -34,6 +34,14 @@ struct AsmParams {
 int build_pattern(GridDev &g, const AsmParams &p, cudaStream_t s);  // rowptr/colind/nnz
 int launch_metrics(GridDev &g, cudaStream_t s);
 int launch_assemble(GridDev &g, const AsmParams &p, bool want32, int *d_flag, cudaStream_t s);
+// b = -R at the handle's state for the given scalar parameters (no CSR writes).
+int launch_residual(const GridDev &g, const AsmParams &p, double *d_b, cudaStream_t s);
+
+// v2d_velocity.cu (vorti2d/velocity.py:76-93); vmag may be null
+int launch_velocity(int imax, int jmax, double dksi, double deta, const double *jac,
+                    const double *beta, const double *gama, const double *detadx,
+                    const double *detady, const double *psi, double *u, double *v, double *vmag,
+                    cudaStream_t s);
 
 // v2d_forces.cu
 int launch_forces(const GridDev &g, double re, double ref_length, double x0, double y0,
@@ -57,7 +65,7 @@ struct MfPlan {
     std::vector<int> lvl_off, lvl_maxS, lvl_maxf, lvl_maxm, lvl_maxm_child;
     std::vector<long long> lvl_fbeg, lvl_fend, lvl_abeg, lvl_aend;
     int *d_S = nullptr, *d_f = nullptr, *d_voff = nullptr, *d_uoff = nullptr;
-    int *d_child0 = nullptr, *d_child1 = nullptr;
+    int *d_child0 = nullptr, *d_child1 = nullptr, *d_parent = nullptr;
     long long *d_foff = nullptr, *d_toff = nullptr;
     int *d_lvl4 = nullptr;         // per level: first front, fronts, row chunks (S, CB)
     int *d_vars = nullptr, *d_cbmap = nullptr, *d_asm_csr = nullptr, *d_asm_row = nullptr;
@@ -78,6 +86,7 @@ struct MfFactor {
     int fp32 = 0;
     void *F = nullptr, *upd = nullptr, *z = nullptr;
     void *tmp = nullptr;        // triangular inverses of one level before they replace L11 / U11
+    void *wb = nullptr;         // transposed solve: per-front adjoint right-hand sides (vtotal)
     double *rs = nullptr;       // row scaling 1 / max |a_r.|
     int *ipiv = nullptr, *perm = nullptr, *flag = nullptr;
     MfBarrier *bar = nullptr;
@@ -90,7 +99,7 @@ struct MfFactor {
 
 // Kernel-side view of a plan + factor (passed by value).
 struct MfDev {
-    const int *S, *f, *voff, *uoff, *child0, *child1;
+    const int *S, *f, *voff, *uoff, *child0, *child1, *parent;
     const long long *foff;
     const int *vars, *cbmap, *perm;
     int maxS, maxf;
@@ -113,6 +122,9 @@ int mf_factor(const MfPlan *P, MfFactor *M, const int *rowptr, const double *val
 // null).  *n_launches (if given) receives the number of kernels launched.
 int mf_apply(const MfPlan *P, const MfFactor *M, const void *b, void *x, const int *stop_a,
              const int *stop_b, cudaStream_t s, long long *n_launches);
+// lambda = A^-T g with the factors (the transposed solve: a bottom-up sweep
+// with U11^-T / U12^T, then a top-down sweep with L21^T / L11^-T).
+int mf_apply_transpose(const MfPlan *P, MfFactor *M, const void *g, void *lambda, cudaStream_t s);
 int mf_flag(const MfFactor *M, int *flag, cudaStream_t s);
 // V2D_ETIMEOUT (and a reset barrier) if a grid barrier of the persistent solve
 // timed out since the last check.

@@ -173,7 +173,8 @@ int upload_vec(T **d, const std::vector<T> &h)
 void mf_plan_destroy(MfPlan *p)
 {
     if (!p) return;
-    void *ptrs[] = {p->d_S, p->d_f, p->d_voff, p->d_uoff, p->d_child0, p->d_child1, p->d_foff, p->d_toff, p->d_lvl4,
+    void *ptrs[] = {p->d_S, p->d_f, p->d_voff, p->d_uoff, p->d_child0, p->d_child1, p->d_parent,
+                    p->d_foff, p->d_toff, p->d_lvl4,
                     p->d_vars, p->d_cbmap, p->d_asm_csr, p->d_asm_row, p->d_asm_pos};
     for (void *q : ptrs)
         if (q) cudaFree(q);
@@ -453,6 +454,7 @@ int mf_plan_create(int imax, int jmax, int n, const int *h_rowptr, const int *h_
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_uoff, P->uoff);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_child0, P->child0);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_child1, P->child1);
+    if (st_up == V2D_OK) st_up = upload_vec(&P->d_parent, P->parent);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_foff, P->foff);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_toff, P->toff);
     if (st_up == V2D_OK) {
@@ -1202,6 +1204,91 @@ __global__ void __launch_bounds__(kSolveThreads2) k_bwd_front(int q0, const MfDe
     }
 }
 
+// ---------------------------------------------------------- transposed solve
+// The transposed solve is the adjoint of the solve's steps taken in reverse
+// order.  Bottom-up (adjoint of the backward sweep): the front gathers g on
+// its fully summed variables plus its children's contributions (the same
+// contribution-block maps as the forward sweep), forms ybar = U11^-T acc_FS
+// (kept in zbuf) and passes acc_CB - U12^T ybar up.  Top-down (adjoint of the
+// forward sweep): the front takes its parent's adjoint right-hand side on its
+// contribution rows, zbar = ybar - L21^T upd_bar, t = L11^-T zbar (unit
+// diagonal), scatters t through the row permutation and writes
+// lambda = rs .* w_bar on its fully summed variables.  One CTA per front; the
+// transposed products read the factor rows column-wise (one thread per
+// column, coalesced across the warp).
+template <class T>
+__global__ void __launch_bounds__(kSolveThreads2) k_tup_front(int q0, const MfDev D, const T *F,
+                                                              const T *g, T *zbuf, T *upd)
+{
+    extern __shared__ unsigned char smem_raw[];
+    T *acc = reinterpret_cast<T *>(smem_raw);   // f
+    T *yb = acc + D.maxf;                         // S
+    const int q = q0 + blockIdx.x;
+    const int S = D.S[q], f = D.f[q], vo = D.voff[q], m = f - S;
+    const T *A = F + D.foff[q];
+    const int *vars = D.vars + vo;
+    const int tid = threadIdx.x;
+    for (int p = tid; p < f; p += blockDim.x) acc[p] = p < S ? g[vars[p]] : T(0);
+    __syncthreads();
+    for (int slot = 0; slot < 2; ++slot) {
+        const int c = slot == 0 ? D.child0[q] : D.child1[q];
+        if (c >= 0) {
+            const int mc = D.f[c] - D.S[c];
+            const int *map = D.cbmap + D.uoff[c];
+            const T *u = upd + D.uoff[c];
+            for (int e = tid; e < mc; e += blockDim.x) acc[map[e]] += u[e];
+        }
+        __syncthreads();
+    }
+    for (int j = tid; j < S; j += blockDim.x) {     // ybar = Uinv^T acc_FS
+        T v = T(0);
+        for (int i = 0; i <= j; ++i) v += A[(long long)i * f + j] * acc[i];
+        yb[j] = v;
+    }
+    __syncthreads();
+    for (int j = tid; j < S; j += blockDim.x) zbuf[vo + j] = yb[j];
+    T *uo = upd + D.uoff[q];
+    for (int k = tid; k < m; k += blockDim.x) {     // acc_CB - U12^T ybar
+        T v = T(0);
+        for (int i = 0; i < S; ++i) v += A[(long long)i * f + S + k] * yb[i];
+        uo[k] = acc[S + k] - v;
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kSolveThreads2) k_tdown_front(int q0, const MfDev D, const T *F,
+                                                                const double *__restrict__ rs,
+                                                                const T *zbuf, T *wb, T *lam)
+{
+    extern __shared__ unsigned char smem_raw[];
+    T *wbar = reinterpret_cast<T *>(smem_raw);  // f
+    T *zb = wbar + D.maxf;                        // S
+    const int q = q0 + blockIdx.x;
+    const int S = D.S[q], f = D.f[q], vo = D.voff[q], m = f - S;
+    const T *A = F + D.foff[q];
+    const int *vars = D.vars + vo;
+    const int tid = threadIdx.x;
+    const int pa = D.parent[q];
+    for (int k = tid; k < m; k += blockDim.x)       // upd_bar from the parent
+        wbar[S + k] = pa >= 0 ? wb[D.voff[pa] + D.cbmap[D.uoff[q] + k]] : T(0);
+    __syncthreads();
+    for (int j = tid; j < S; j += blockDim.x) {     // zbar = ybar - L21^T upd_bar
+        T v = T(0);
+        for (int k = 0; k < m; ++k) v += A[(long long)(S + k) * f + j] * wbar[S + k];
+        zb[j] = zbuf[vo + j] - v;
+    }
+    __syncthreads();
+    const int *perm = D.perm + vo;
+    for (int i = tid; i < S; i += blockDim.x) {     // t = Linv^T zbar; w_bar[perm[i]] = t
+        T v = zb[i];
+        for (int j = i + 1; j < S; ++j) v += A[(long long)j * f + i] * zb[j];
+        wbar[perm[i]] = v;
+    }
+    __syncthreads();
+    for (int p = tid; p < f; p += blockDim.x) wb[vo + p] = wbar[p];
+    for (int p = tid; p < S; p += blockDim.x) lam[vars[p]] = (T)(rs[vars[p]] * (double)wbar[p]);
+}
+
 // Grid-wide barrier of a cooperative launch (all CTAs resident): a
 // generation counter in global memory.  The wait is bounded: after
 // kBarrierSpins polls the CTA records a timeout in bar->err and reports
@@ -1305,6 +1392,7 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
     grab(&M->upd, (size_t)P->utotal * es);
     grab(&M->z, (size_t)P->vtotal * es);
     grab(&M->tmp, (size_t)P->tmax * es);
+    grab(&M->wb, (size_t)P->vtotal * es);
     grab((void **)&M->rs, (size_t)P->n * sizeof(double));
     grab((void **)&M->ipiv, (size_t)P->vtotal * sizeof(int));
     grab((void **)&M->perm, (size_t)P->vtotal * sizeof(int));
@@ -1335,6 +1423,8 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
     if (fp32) {
         attr((const void *)k_apply_all<float>, solve);
         attr((const void *)k_fwd_front<float>, solve);
+        attr((const void *)k_tup_front<float>, solve);
+        attr((const void *)k_tdown_front<float>, solve);
         attr((const void *)k_bwd_front<float>, solve);
         attr((const void *)k_fwd_z<float>, solve);
         attr((const void *)k_fwd_u<float>, solve);
@@ -1344,6 +1434,8 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
     } else {
         attr((const void *)k_apply_all<double>, solve);
         attr((const void *)k_fwd_front<double>, solve);
+        attr((const void *)k_tup_front<double>, solve);
+        attr((const void *)k_tdown_front<double>, solve);
         attr((const void *)k_bwd_front<double>, solve);
         attr((const void *)k_fwd_z<double>, solve);
         attr((const void *)k_fwd_u<double>, solve);
@@ -1381,7 +1473,7 @@ void mf_factor_destroy(MfFactor *M)
 {
     if (!M) return;
     if (M->graph) cudaGraphExecDestroy(M->graph);
-    void *ptrs[] = {M->F, M->upd, M->z, M->tmp, M->rs, M->ipiv, M->perm, M->flag, M->bar};
+    void *ptrs[] = {M->F, M->upd, M->z, M->tmp, M->wb, M->rs, M->ipiv, M->perm, M->flag, M->bar};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     delete M;
@@ -1391,7 +1483,7 @@ MfDev mf_dev(const MfPlan *P, const MfFactor *M)
 {
     MfDev D;
     D.S = P->d_S; D.f = P->d_f; D.voff = P->d_voff; D.uoff = P->d_uoff;
-    D.child0 = P->d_child0; D.child1 = P->d_child1; D.foff = P->d_foff;
+    D.child0 = P->d_child0; D.child1 = P->d_child1; D.parent = P->d_parent; D.foff = P->d_foff;
     D.vars = P->d_vars; D.cbmap = P->d_cbmap; D.perm = M->perm;
     D.maxS = P->maxS; D.maxf = P->maxf;
     return D;
@@ -1565,6 +1657,34 @@ int mf_apply(const MfPlan *P, const MfFactor *M, const void *b, void *x, const i
                                      n_launches);
     return apply_launches<double>(P, M, (const double *)b, (double *)x, stop_a, stop_b, s,
                                   n_launches);
+}
+
+template <class T>
+static int apply_transpose_launches(const MfPlan *P, MfFactor *M, const T *g, T *lam,
+                                    cudaStream_t s)
+{
+    const MfDev D = mf_dev(P, M);
+    const T *F = (const T *)M->F;
+    const size_t smf = (size_t)(P->maxf + P->maxS) * sizeof(T);
+    for (int L = 0; L < P->nlevel; ++L) {
+        const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
+        k_tup_front<T><<<nq, kSolveThreads2, smf, s>>>(q0, D, F, g, (T *)M->z, (T *)M->upd);
+    }
+    for (int L = P->nlevel - 1; L >= 0; --L) {
+        const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
+        k_tdown_front<T><<<nq, kSolveThreads2, smf, s>>>(q0, D, F, M->rs, (const T *)M->z,
+                                                         (T *)M->wb, lam);
+    }
+    V2D_CUDA_TRY(cudaGetLastError());
+    count_launches(2LL * P->nlevel);
+    return V2D_OK;
+}
+
+int mf_apply_transpose(const MfPlan *P, MfFactor *M, const void *g, void *lambda, cudaStream_t s)
+{
+    if (M->fp32)
+        return apply_transpose_launches<float>(P, M, (const float *)g, (float *)lambda, s);
+    return apply_transpose_launches<double>(P, M, (const double *)g, (double *)lambda, s);
 }
 
 int mf_flag(const MfFactor *M, int *flag, cudaStream_t s)

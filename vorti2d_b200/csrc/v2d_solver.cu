@@ -38,6 +38,7 @@ struct v2d_solver {
     bool lu_ready = false;           // the factor storage holds some factorization
     int lu_last_its = 0;             // Krylov iterations of the last solve with them
     long long lu_factorizations = 0;
+    int *tptr = nullptr, *tind = nullptr, *tperm = nullptr;   // transposed CSR pattern (adjoint)
     cudaEvent_t ev[5] = {};          // phase boundaries of the last Newton iteration
     double phase_ms[4] = {0, 0, 0, 0};
     long long phase_n = 0;
@@ -115,8 +116,16 @@ int check_params(const v2d_solver_params *p)
     return V2D_OK;
 }
 
+void drop_transpose(v2d_solver *S)
+{
+    for (int *p : {S->tptr, S->tind, S->tperm})
+        if (p) cudaFree(p);
+    S->tptr = S->tind = S->tperm = nullptr;
+}
+
 void drop_lu(v2d_solver *S)
 {
+    drop_transpose(S);   // follows the pattern like the plan
     S->lu_valid = false;
     S->lu_ready = false;
     for (int q = 0; q < 2; ++q) {
@@ -490,6 +499,165 @@ extern "C" int v2d_solver_forces(v2d_solver *S, double re, double ref_length, do
                                  cudaMemcpyDeviceToHost, S->s));
     V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
     std::memcpy(out10, S->host + 1, 10 * sizeof(double));
+    return V2D_OK;
+}
+
+extern "C" int v2d_solver_velocity(v2d_solver *S, double *u, double *v, double *vmag)
+{
+    V2D_ARG_CHECK(S && u && v, "solver_velocity: null pointer");
+    const GridDev &g = S->g;
+    const size_t N = g.N;
+    DevBuf<double> buf;
+    V2D_TRY(buf.alloc(3 * N, S->s));
+    V2D_TRY(launch_velocity(g.imax, g.jmax, g.dksi, g.deta, g.met[0], g.met[2], g.met[3], g.met[6],
+                            g.met[7], g.psi, buf.p, buf.p + N, vmag ? buf.p + 2 * N : nullptr,
+                            S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(u, buf.p, N * sizeof(double), cudaMemcpyDeviceToHost, S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(v, buf.p + N, N * sizeof(double), cudaMemcpyDeviceToHost, S->s));
+    if (vmag)
+        V2D_CUDA_TRY(cudaMemcpyAsync(vmag, buf.p + 2 * N, N * sizeof(double), cudaMemcpyDeviceToHost, S->s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    return V2D_OK;
+}
+
+// ------------------------------------------------------------------ adjoint
+namespace {
+
+// y = J^T x over the transposed pattern (values gathered through tperm).
+__global__ void k_spmv_t(int n, const int *__restrict__ tptr, const int *__restrict__ tind,
+                         const int *__restrict__ tperm, const double *__restrict__ val,
+                         const double *__restrict__ x, double *y)
+{
+    V2D_GRID_STRIDE(r, n)
+    {
+        double s = 0.0;
+        for (int e = tptr[r]; e < tptr[r + 1]; ++e) s += val[tperm[e]] * x[tind[e]];
+        y[r] = s;
+    }
+}
+
+__global__ void k_axpy_res(int n, const double *__restrict__ g, const double *__restrict__ jtl,
+                           const double *__restrict__ d, double *lam, double *r, int mode)
+{
+    V2D_GRID_STRIDE(i, n)
+    {
+        if (mode == 0) lam[i] += d[i];          // lambda += delta
+        else r[i] = g[i] - jtl[i];               // r = g - J^T lambda
+    }
+}
+
+int ensure_transpose(v2d_solver *S)
+{
+    if (S->tptr) return V2D_OK;
+    const GridDev &g = S->g;
+    std::vector<int> rp(g.n + 1), ci(g.nnz);
+    V2D_CUDA_TRY(cudaMemcpyAsync(rp.data(), g.rowptr, (g.n + 1) * sizeof(int), cudaMemcpyDeviceToHost, S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(ci.data(), g.colind, g.nnz * sizeof(int), cudaMemcpyDeviceToHost, S->s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    std::vector<int> tp(g.n + 1, 0), ti(g.nnz), tq(g.nnz);
+    for (long long e = 0; e < g.nnz; ++e) tp[ci[e] + 1]++;
+    for (int r = 0; r < g.n; ++r) tp[r + 1] += tp[r];
+    std::vector<int> fill(tp.begin(), tp.end() - 1);
+    for (int r = 0; r < g.n; ++r)
+        for (int e = rp[r]; e < rp[r + 1]; ++e) {
+            const int o = fill[ci[e]]++;
+            ti[o] = r;
+            tq[o] = e;
+        }
+    V2D_CUDA_TRY(cudaMalloc(&S->tptr, (g.n + 1) * sizeof(int)));
+    V2D_CUDA_TRY(cudaMalloc(&S->tind, g.nnz * sizeof(int)));
+    V2D_CUDA_TRY(cudaMalloc(&S->tperm, g.nnz * sizeof(int)));
+    V2D_CUDA_TRY(cudaMemcpy(S->tptr, tp.data(), (g.n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    V2D_CUDA_TRY(cudaMemcpy(S->tind, ti.data(), g.nnz * sizeof(int), cudaMemcpyHostToDevice));
+    V2D_CUDA_TRY(cudaMemcpy(S->tperm, tq.data(), g.nnz * sizeof(int), cudaMemcpyHostToDevice));
+    return V2D_OK;
+}
+
+double host_norm(const std::vector<double> &v)
+{
+    double s = 0.0;
+    for (double x : v) s += x * x;
+    return std::sqrt(s);
+}
+
+}  // namespace
+
+extern "C" int v2d_solver_residual(v2d_solver *S, double re, double invdtau, double inv2dt,
+                                   double urot, double ca, double sa, double *b)
+{
+    V2D_ARG_CHECK(S && b, "solver_residual: null pointer");
+    V2D_ARG_CHECK(re > 0.0, "solver_residual: re must be positive");
+    const GridDev &g = S->g;
+    DevBuf<double> d;
+    V2D_TRY(d.alloc(g.n, S->s));
+    AsmParams ap{re, invdtau, inv2dt, urot, ca, sa, S->prm.ff_bc};
+    V2D_TRY(launch_residual(g, ap, d.p, S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(b, d.p, g.n * sizeof(double), cudaMemcpyDeviceToHost, S->s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    return V2D_OK;
+}
+
+extern "C" int v2d_solver_adjoint(v2d_solver *S, double urot, const double *g_host, double *lam_host,
+                                  double rtol, int max_refine, int *refinements, double *rel_res)
+{
+    V2D_ARG_CHECK(S && g_host && lam_host, "solver_adjoint: null pointer");
+    V2D_ARG_CHECK(S->plan || S->prm.krylov.precond == V2D_PC_LU,
+                  "solver_adjoint: needs the LU preconditioner");
+    V2D_ARG_CHECK(max_refine >= 1, "solver_adjoint: max_refine must be >= 1");
+    GridDev &g = S->g;
+    // FP64 factors of the Jacobian at the current state
+    V2D_TRY(assemble_now(S, urot));
+    V2D_TRY(sync_flag(S, "adjoint assembly"));
+    if (!S->plan) {
+        v2d_krylov_params keep = S->prm.krylov;
+        S->prm.krylov.precond = V2D_PC_LU;
+        const int st = ensure_lu(S);
+        S->prm.krylov = keep;
+        V2D_TRY(st);
+    }
+    if (!S->lu[0]) V2D_TRY(mf_factor_create(S->plan, 0, &S->lu[0]));
+    V2D_TRY(mf_factor(S->plan, S->lu[0], g.rowptr, g.val, S->s));
+    S->lu_valid = false;   // lu[0] no longer holds the Newton solve's factors
+    V2D_TRY(ensure_transpose(S));
+    const size_t n = g.n;
+    DevBuf<double> buf;
+    V2D_TRY(buf.alloc(5 * n, S->s));
+    double *dg = buf.p, *lam = dg + n, *r = lam + n, *del = r + n, *jtl = del + n;
+    V2D_CUDA_TRY(cudaMemcpyAsync(dg, g_host, n * sizeof(double), cudaMemcpyHostToDevice, S->s));
+    V2D_CUDA_TRY(cudaMemsetAsync(lam, 0, n * sizeof(double), S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(r, dg, n * sizeof(double), cudaMemcpyDeviceToDevice, S->s));
+    std::vector<double> hr(n), hg(g_host, g_host + n);
+    const double gn = host_norm(hg);
+    double rel = gn > 0.0 ? 1.0 : 0.0, prev = HUGE_VAL;
+    int it = 0;
+    const int grid = grid_for(n, 256);
+    // refine until rtol, or until a pass no longer halves the residual (the
+    // attainable accuracy of the FP64 factors)
+    while (rel > rtol && it < max_refine && rel < 0.5 * prev) {
+        prev = rel;
+        V2D_TRY(mf_apply_transpose(S->plan, S->lu[0], r, del, S->s));
+        k_axpy_res<<<grid, 256, 0, S->s>>>(g.n, dg, jtl, del, lam, r, 0);
+        k_spmv_t<<<grid, 256, 0, S->s>>>(g.n, S->tptr, S->tind, S->tperm, g.val, lam, jtl);
+        k_axpy_res<<<grid, 256, 0, S->s>>>(g.n, dg, jtl, del, lam, r, 1);
+        V2D_CUDA_TRY(cudaGetLastError());
+        count_launches(3);
+        V2D_CUDA_TRY(cudaMemcpyAsync(hr.data(), r, n * sizeof(double), cudaMemcpyDeviceToHost, S->s));
+        V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+        rel = gn > 0.0 ? host_norm(hr) / gn : 0.0;
+        ++it;
+        if (!std::isfinite(rel)) {
+            set_error("solver_adjoint: non-finite residual");
+            return V2D_ENONFINITE;
+        }
+    }
+    V2D_CUDA_TRY(cudaMemcpyAsync(lam_host, lam, n * sizeof(double), cudaMemcpyDeviceToHost, S->s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    if (refinements) *refinements = it;
+    if (rel_res) *rel_res = rel;
+    if (rel > rtol && rel > 1e-8) {
+        set_error("solver_adjoint: residual %.3e after %d refinements", rel, it);
+        return V2D_ENOTCONVERGED;
+    }
     return V2D_OK;
 }
 

@@ -88,6 +88,14 @@ class DeviceState:
     def shift_history(self):
         check(lib().v2d_solver_shift_history(self.h), "shift_history")
 
+    def velocity(self, want_mag=False):
+        N = self.N
+        u, v = np.empty(N), np.empty(N)
+        mag = np.empty(N) if want_mag else None
+        check(lib().v2d_solver_velocity(self.h, dptr(u), dptr(v), dptr(mag) if want_mag else None),
+              "velocity")
+        return (u, v, mag) if want_mag else (u, v)
+
     def forces(self, re, ref_length, moment_ref):
         out = np.zeros(10)
         rl = -1.0 if ref_length is None else float(ref_length)
@@ -312,6 +320,11 @@ class Solver:
         (vorti2d/solver.py:272-283 -> vorti2d/forces.py:82-194)."""
         cfg = self.cfg
         return self.dev.forces(cfg.re, cfg.ref_length, cfg.moment_center)
+
+    def velocity(self, want_mag: bool = False):
+        """Cartesian velocity of the current state, on the device
+        (vorti2d/velocity.py:76-93)."""
+        return self.dev.velocity(want_mag)
 
     def close(self):
         self.dev.close()
