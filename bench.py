@@ -174,6 +174,106 @@ def timed_steps(torch, s, times, k0, K, flush_buf):
     return ms, newton, krylov
 
 
+# Algorithmic bytes per node of the HBM-bound kernels (read inputs + write
+# outputs once): metrics x, y -> 10 arrays; assembly 6 metrics + 4 state
+# fields -> 23 Jacobian values + 2 right-hand sides (+ 4 block inverses and,
+# mixed, an FP32 copy); velocity 5 metrics + psi -> u, v, |V|; SpMV per nnz
+# value + column index, plus row pointers and the two vectors.
+KERNEL_BYTES = {"metrics": 96, "assemble_fp64": 8 * (6 + 4) + 8 * 23 + 8 * 2 + 8 * 4,
+                "assemble_mixed": 8 * (6 + 4) + 12 * 23 + 8 * 2 + 12 * 4, "velocity": 8 * 6 + 8 * 3}
+
+
+def kernel_rooflines(n_side, hbm_gbs, reps=10):
+    """Metrics, assembly, velocity and Krylov SpMV on an n_side x n_side
+    cylinder O-grid (state: the far-field initial condition), each timed
+    alone after L2 flushes, against the HBM roofline."""
+    import ctypes
+    import vorti2d_b200 as v
+    from vorti2d_b200 import _lib
+    xg, yg = v.generate_cylinder(n_side, n_side)
+    cfg = v.Config(verbose=False, write_csv=False, write_xdmf=False, compute_forces=False,
+                   precond="bjacobi", precision="mixed", **WORKLOAD)
+    s = v.Solver(cfg, mesh=(xg, yg))
+    N = s.ndof
+    nnz = ctypes.c_longlong()
+    _lib.check(_lib.lib().v2d_solver_nnz(s.dev.h, ctypes.byref(nnz)))
+    out = {}
+    for name, which in (("metrics", 0), ("assemble_fp64", 1), ("assemble_mixed", 2),
+                        ("velocity", 3)):
+        ms = ctypes.c_double()
+        _lib.check(_lib.lib().v2d_solver_time_kernel(s.dev.h, which, reps, L2_FLUSH_BYTES,
+                                                     ctypes.byref(ms)))
+        b = KERNEL_BYTES[name] * N
+        out[name] = {"ms": ms.value, "bytes": b, "GBs": b / ms.value / 1e6,
+                     "frac": b / ms.value / 1e6 / hbm_gbs}
+    _lib.check(_lib.lib().v2d_solver_assemble(s.dev.h, 0.0))
+    for prec, fp32 in (("fp64", 0), ("fp32", 1)):
+        ms = ctypes.c_double()
+        _lib.check(_lib.lib().v2d_solver_time_spmv(s.dev.h, fp32, reps, L2_FLUSH_BYTES,
+                                                   ctypes.byref(ms)))
+        n = 2 * N
+        b = nnz.value * SPMV_BYTES_PER_NNZ[prec] + (n + 1) * 4 + 2 * n * (4 if fp32 else 8)
+        out[f"spmv_{prec}"] = {"ms": ms.value, "bytes": b, "GBs": b / ms.value / 1e6,
+                               "frac": b / ms.value / 1e6 / hbm_gbs}
+    s.close()
+    return {"grid": f"{n_side}x{n_side}", "nodes": N, "nnz": nnz.value, "kernels": out}
+
+
+def run_sweep_workload(args):
+    """Batched steady sweep: 96 instances (32 cylinders 129x129, 32 cylinders
+    181x181, 32 NACA-0012 257x129; Re ~ U[50,1000], alpha ~ U[-8,8] deg from
+    seed 0), steady pure Newton (at most 20 iterations), FP32 Krylov + LU
+    inside FP64 defect correction, solved concurrently.  Plain Newton from the
+    free stream converges only on part of that Re range, so value = Newton
+    iterations per second summed over the instances (the work done), with
+    converged solves per second beside it."""
+    import torch
+    import vorti2d_b200 as v
+    from vorti2d_b200.batch import run_sweep, sweep_cases
+    torch.cuda.set_device(0)
+    cases = sweep_cases(seed=0)
+    res = run_sweep(cases, workers=args.sweep_workers, precision="mixed")
+    kinds = {}
+    for r in res.results:
+        k = r.name.rsplit("_", 1)[0]
+        d = kinds.setdefault(k, {"instances": 0, "converged": 0, "diverged": 0, "errors": 0,
+                                 "newton": 0, "krylov": 0})
+        d["instances"] += 1
+        d["converged"] += int(r.converged)
+        d["diverged"] += int(r.diverged)
+        d["errors"] += int(bool(r.error))
+        d["newton"] += r.newton_iters
+        d["krylov"] += r.krylov_iters
+    cpu = None
+    if args.cpu_steps > 0:
+        from oracle import oracle as O
+        sample = [c for c in cases if c.name.startswith("cyl129")][:2]
+        t0 = time.perf_counter()
+        its = 0
+        for c in sample:
+            o = O.OracleSolver(c.xg, c.yg, re=c.re, alpha_deg=c.alpha_deg, steady=True,
+                               pseudo_tol=1e-10, max_pseudo_iter=5)
+            its += o.advance(0.0)[1]
+        dt = time.perf_counter() - t0
+        cpu = {"value": its / dt, "unit": "Newton iterations/s", "cores": 1, "kind": "port",
+               "sample": f"{its} Newton iterations of {len(sample)} 129x129 cylinder instances "
+                         "of the sweep, serial (C assembly + SuperLU)"}
+    line = {"metric": "Newton iterations/s, 96-instance steady sweep (cylinders 129^2/181^2, "
+                      "NACA-0012 257x129)",
+            "value": res.newton_per_s, "unit": "Newton iterations/s", "n_gpus": 1,
+            "converged_solves_per_s": res.solves_per_s, "newton_iters": res.newton_iters,
+            "higher_is_better": True, "dtype": "f32-krylov/f64", "data": "synthetic",
+            "config": {"workload": "batched steady sweep, seed 0", "workers": res.workers,
+                       "precond": "multifrontal LU per Newton iteration",
+                       "newton": "<=20 iterations, stop when ||dq|| > 1e3 x the first",
+                       "krylov_max_it": 300},
+            "krylov_iters": res.krylov_iters,
+            "errors": sorted({r.error for r in res.results if r.error})[:4],
+            "converged": res.converged, "instances": len(cases), "solve_s": res.solve_s,
+            "setup_s": res.setup_s, "by_kind": kinds, "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+
+
 def phase_times(_lib, s, reset=False):
     """(assembly, factorization, Krylov, update) device ms summed over Newton
     iterations, and the iteration count."""
@@ -328,12 +428,33 @@ def main():
     ap.add_argument("--lu-reuse", type=int, default=8,
                     help="keep LU factors while GMRES needs at most this many iterations "
                          "(0: factor every Newton Jacobian)")
+    ap.add_argument("--kernels-grid", type=int, default=2049,
+                    help="grid side of the HBM-bound kernel roofline table (0: skip)")
+    ap.add_argument("--workload", default="unsteady", choices=["unsteady", "sweep"],
+                    help="unsteady: the BDF2 benchmark; sweep: the batched steady sweep")
+    ap.add_argument("--sweep-workers", type=int, default=16)
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="print only the HBM-bound kernel roofline table (--kernels-grid)")
     ap.add_argument("--profile-newton", action="store_true",
                     help="one warm-up step, then one Newton iteration in NVTX range v2d_newton")
     args = ap.parse_args()
     rank, world, local_rank = dist_env()
     if args.profile_newton:
         profile_newton(args)
+        return
+    if args.workload == "sweep" and args.impl == "ours":
+        run_sweep_workload(args)
+        return
+    if args.kernels_only:
+        import torch
+        torch.cuda.set_device(0)
+        hbm = 6650.0
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+                hbm = json.load(fh)["hbm_gbs"]
+        except (OSError, ValueError, KeyError):
+            pass
+        print(json.dumps(kernel_rooflines(args.kernels_grid, hbm, reps=3)), flush=True)
         return
 
     if args.impl == "reference":
@@ -408,6 +529,8 @@ def main():
                           "frac": achieved / peaks["hbm_gbs"], "traffic": None,
                           "bytes_per_launch": bytes_spmv, "ms_per_launch": res["spmv_ms"]},
         "cpu_baseline": cpu,
+        "kernel_rooflines": (kernel_rooflines(args.kernels_grid, peaks["hbm_gbs"])
+                             if args.kernels_grid > 0 else None),
         "gpu_launches": int(launches.get(head, 0)),
         "clocks": res.get("clocks"),
         "legs": {p: res[p] for p in ("mixed", "fp64") if p in res},

@@ -326,6 +326,13 @@ int v2d_solver_phase_times(v2d_solver *s, double *out6, int reset);
 int v2d_solver_time_lu_apply(v2d_solver *s, int reps, long long flush_bytes, double *ms_avg,
                              long long *factor_bytes);
 
+/* Measurement aid (no reference counterpart): average ms of `reps` launches
+ * of one kernel on the handle's data, each after a write of flush_bytes:
+ * which = 0 metrics, 1 Newton assembly (FP64 values), 2 Newton assembly with
+ * the FP32 copy, 3 velocity reconstruction. */
+int v2d_solver_time_kernel(v2d_solver *s, int which, int reps, long long flush_bytes,
+                           double *ms_avg);
+
 /* The stream the handle's kernels run on (cudaStream_t as void*). */
 int v2d_solver_stream(v2d_solver *s, void **stream);
 

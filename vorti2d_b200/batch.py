@@ -1,0 +1,178 @@
+"""Batched steady sweeps: many independent steady solves of uneven grid sizes
+(cylinders and NACA-0012 sections over a range of Reynolds numbers and
+angles of attack) run concurrently on one GPU.
+
+Every instance is its own device handle (state, CSR, multifrontal factors,
+Krylov workspace) with its own CUDA stream; a pool of host threads drives
+them (the C ABI releases the GIL).  One instance at these sizes occupies only
+a fraction of the B200's SMs -- its factor and solve kernels are
+latency-bound -- so the streams of the other instances fill the rest.
+
+Plain Newton from the free stream (the reference's steady method) does not
+reach a steady state at the higher Reynolds numbers of a sweep: each instance
+reports whether it converged, and the sweep's throughput is counted both in
+Newton iterations (the work done) and in converged solves.
+"""
+from __future__ import annotations
+
+import math
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from .config import Config
+from .mesh import generate_cylinder, generate_naca0012
+
+
+@dataclass
+class Case:
+    name: str
+    xg: np.ndarray
+    yg: np.ndarray
+    re: float
+    alpha_deg: float
+    ref_length: float | None = None
+
+
+@dataclass
+class CaseResult:
+    name: str
+    re: float
+    alpha_deg: float
+    nodes: int
+    converged: bool
+    newton_iters: int
+    res: float
+    krylov_iters: int = 0
+    diverged: bool = False
+    cd: float = math.nan
+    cl: float = math.nan
+    cm: float = math.nan
+    seconds: float = 0.0
+    error: str = ""
+
+
+def sweep_cases(seed: int = 0, n_each: int = 32):
+    """The batched sweep: n_each cylinders at 129x129, n_each at 181x181 and
+    n_each NACA-0012 sections at 257x129 (open trailing edge, far field 30
+    chords); Re ~ U[50, 1000], alpha ~ U[-8, 8] degrees from one seeded
+    generator."""
+    rng = np.random.default_rng(seed)
+    meshes = {"cyl129": generate_cylinder(129, 129), "cyl181": generate_cylinder(181, 181),
+              "naca257x129": generate_naca0012(257, 129)}
+    cases = []
+    for kind in ("cyl129", "cyl181", "naca257x129"):
+        xg, yg = meshes[kind]
+        for k in range(n_each):
+            re = float(rng.uniform(50.0, 1000.0))
+            alpha = float(rng.uniform(-8.0, 8.0))
+            cases.append(Case(f"{kind}_{k:02d}", xg, yg, re, alpha,
+                              1.0 if kind.startswith("naca") else None))
+    return cases
+
+
+def _config(case: Case, precision: str, max_newton: int, pseudo_tol: float,
+            krylov_max_it: int, **kw) -> Config:
+    return Config(re=case.re, alpha_deg=case.alpha_deg, steady=True, verbose=False,
+                  write_csv=False, write_xdmf=False, compute_forces=False,
+                  pseudo_tol=pseudo_tol, max_pseudo_iter=max_newton, ksp_rtol=1e-10,
+                  krylov_max_it=krylov_max_it, precision=precision,
+                  ref_length=case.ref_length, raise_on_linear_failure=False, **kw)
+
+
+@dataclass
+class SweepResult:
+    results: list = field(default_factory=list)
+    setup_s: float = 0.0
+    solve_s: float = 0.0
+    workers: int = 0
+
+    @property
+    def converged(self) -> int:
+        return sum(r.converged for r in self.results)
+
+    @property
+    def newton_iters(self) -> int:
+        return sum(r.newton_iters for r in self.results)
+
+    @property
+    def krylov_iters(self) -> int:
+        return sum(r.krylov_iters for r in self.results)
+
+    @property
+    def solves_per_s(self) -> float:
+        return self.converged / self.solve_s if self.solve_s > 0 else 0.0
+
+    @property
+    def newton_per_s(self) -> float:
+        return self.newton_iters / self.solve_s if self.solve_s > 0 else 0.0
+
+
+def run_sweep(cases, workers: int = 16, precision: str = "mixed", max_newton: int = 20,
+              pseudo_tol: float = 1e-10, krylov_max_it: int = 300,
+              diverge_factor: float = 1e3, **cfg_kw) -> SweepResult:
+    """Solve every case to a steady state, ``workers`` instances at a time.
+
+    Each instance runs the steady Newton loop (vorti2d/solver.py:136-145:
+    iterate while ||dq||/(2N) > pseudo_tol, at most max_newton times) and
+    additionally stops when the update norm exceeds ``diverge_factor`` times
+    the first one (a diverging instance), with GMRES capped at
+    ``krylov_max_it`` iterations per Newton step.  Handles are created first
+    (device allocation synchronises the device, so it is kept out of the
+    timed solve phase); ``solve_s`` is the wall time of the concurrent
+    solves."""
+    from .solver import Solver
+    out = SweepResult(workers=workers)
+    t0 = time.perf_counter()
+    solvers = [Solver(_config(c, precision, max_newton, pseudo_tol, krylov_max_it, **cfg_kw),
+                      mesh=(c.xg, c.yg))
+               for c in cases]
+    out.setup_s = time.perf_counter() - t0
+    results = [None] * len(cases)
+    lock = threading.Lock()
+
+    def newton_loop(s, r):
+        cfg = s.cfg
+        urot = cfg.u_rot(cfg.t_start)
+        res, first = math.inf, None
+        while r.newton_iters < max_newton:
+            res = s._assemble_and_solve_once(cfg.inv_dtau(), cfg.inv_2dt(), urot)
+            r.newton_iters += 1
+            r.krylov_iters += s._last_lin.iterations
+            r.res = res
+            first = res if first is None else first
+            if not np.isfinite(res) or res > diverge_factor * first:
+                r.diverged = True
+                break
+            if res <= pseudo_tol:
+                break
+        return res
+
+    def work(i):
+        c, s = cases[i], solvers[i]
+        t = time.perf_counter()
+        r = CaseResult(c.name, c.re, c.alpha_deg, s.ndof, False, 0, math.inf)
+        try:
+            res = newton_loop(s, r)
+            r.converged = bool(np.isfinite(res) and res <= pseudo_tol)
+            if r.converged:
+                fc = s.force_coeffs()
+                r.cd, r.cl, r.cm = fc.cd, fc.cl, fc.cm
+        except (_lib.V2DError, ValueError) as exc:
+            r.error = str(exc)[:200]
+        r.seconds = time.perf_counter() - t
+        with lock:
+            results[i] = r
+
+    t1 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        list(pool.map(work, range(len(cases))))
+    out.solve_s = time.perf_counter() - t1
+    for s in solvers:
+        s.close()
+    out.results = results
+    return out

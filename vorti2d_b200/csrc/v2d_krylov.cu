@@ -27,6 +27,7 @@
 //    FP32 cycles act as inner solves of an FP64 defect correction.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "v2d_internal.cuh"
@@ -581,7 +582,7 @@ static int capture_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, doub
     const std::vector<int> bnd = segment_bounds(w->m);
     for (size_t q = 0; q + 1 < bnd.size(); ++q) {
         long long nl = 0;
-        V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
         for (int j = bnd[q]; j < bnd[q + 1]; ++j) {
             nl += 6;
             k_scale_precond<T><<<gp, 256, 0, s>>>(w->desc, w->ctl, j, w->r, wv, V, w->H, z);
@@ -613,7 +614,7 @@ static int capture_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, doub
         w->seg[which].push_back(ge);
         w->seg_launches[which].push_back(nl);
     }
-    V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
     k_backsolve<<<1, 32, 0, s>>>(w->desc, w->ctl, w->H, w->g, w->y);
     k_correct<T><<<gp, 256, 0, s>>>(w->desc, w->ctl, V, w->y, z, x, Z);
     k_residual<<<gr, kSpmvThreads, 0, s>>>(w->desc, w->ctl, w->r, w->partial, w->g, 0);
@@ -650,8 +651,35 @@ static int run_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, double *
     return V2D_OK;
 }
 
+// Kernels are loaded lazily on first launch; every kernel that the restart
+// cycle graphs hold is loaded here first, outside any stream capture, so that
+// no module load happens while a stream is capturing.
+static int krylov_preload()
+{
+    static std::once_flag once;
+    static cudaError_t status = cudaSuccess;
+    std::call_once(once, [] {
+        const void *fns[] = {
+            (const void *)k_scale_precond<float>, (const void *)k_scale_precond<double>,
+            (const void *)k_spmv<float>, (const void *)k_spmv<double>,
+            (const void *)k_mdot<float>, (const void *)k_mdot<double>,
+            (const void *)k_update<float>, (const void *)k_update<double>,
+            (const void *)k_correct<float>, (const void *)k_correct<double>,
+            (const void *)k_backsolve, (const void *)k_residual};
+        cudaFuncAttributes a;
+        for (const void *f : fns)
+            if (status == cudaSuccess) status = cudaFuncGetAttributes(&a, f);
+    });
+    if (status != cudaSuccess) {
+        set_error("krylov: kernel load failed: %s", cudaGetErrorString(status));
+        return V2D_ECUDA;
+    }
+    return V2D_OK;
+}
+
 int krylov_create(KrylovWork **out, int n, int restart, cudaStream_t s)
 {
+    V2D_TRY(krylov_preload());
     V2D_ARG_CHECK(n > 0 && restart >= 1 && restart <= kMaxRestart,
                   "krylov: n=%d restart=%d (restart must be in [1, %d])", n, restart, kMaxRestart);
     KrylovWork *w = new KrylovWork();

@@ -50,6 +50,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <mutex>
 #include <vector>
 
 #include "v2d_internal.cuh"
@@ -1378,9 +1379,45 @@ __global__ void __launch_bounds__(kSolveThreads2) k_apply_all(const MfDev D, con
 }  // namespace
 
 // ------------------------------------------------------------ host drivers
+// Kernels are loaded lazily on first launch; the factorization graph's
+// kernels are loaded here first, outside any stream capture.
+template <class T>
+static cudaError_t mf_preload_t()
+{
+    const void *fns[] = {(const void *)k_scatter<T>, (const void *)k_extend_add<T>,
+                         (const void *)k_panel<T>, (const void *)k_l21<T>,
+                         (const void *)k_swap_trsm<T>, (const void *)k_gemm<T>,
+                         (const void *)k_trinv<T>, (const void *)k_trcopy<T>,
+                         (const void *)k_fwd_z<T>, (const void *)k_fwd_u<T>,
+                         (const void *)k_bwd_y<T>, (const void *)k_bwd_x<T>,
+                         (const void *)k_fwd_front<T>, (const void *)k_bwd_front<T>,
+                         (const void *)k_tup_front<T>, (const void *)k_tdown_front<T>};
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, (const void *)k_rowscale);
+    for (const void *f : fns)
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, f);
+    return e;
+}
+
+static int mf_preload()
+{
+    static std::once_flag once;
+    static cudaError_t status = cudaSuccess;
+    std::call_once(once, [] {
+        status = mf_preload_t<float>();
+        if (status == cudaSuccess) status = mf_preload_t<double>();
+    });
+    if (status != cudaSuccess) {
+        set_error("mf_factor: kernel load failed: %s", cudaGetErrorString(status));
+        return V2D_ECUDA;
+    }
+    return V2D_OK;
+}
+
 int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
 {
     *out = nullptr;
+    V2D_TRY(mf_preload());
     MfFactor *M = new MfFactor();
     M->fp32 = fp32;
     const size_t es = fp32 ? sizeof(float) : sizeof(double);
@@ -1555,7 +1592,7 @@ int mf_factor(const MfPlan *P, MfFactor *M, const int *rowptr, const double *val
         if (M->graph) cudaGraphExecDestroy(M->graph);
         M->graph = nullptr;
         cudaGraph_t g = nullptr;
-        V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
         int st = M->fp32 ? factor_launches<float>(P, M, rowptr, val, s)
                          : factor_launches<double>(P, M, rowptr, val, s);
         cudaError_t e = cudaStreamEndCapture(s, &g);

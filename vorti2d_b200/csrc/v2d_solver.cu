@@ -734,6 +734,50 @@ extern "C" int v2d_solver_time_lu_apply(v2d_solver *S, int reps, long long flush
     return mf_time_apply(S->plan, S->lu[q], reps, (size_t)flush_bytes, S->s, ms_avg);
 }
 
+// Kernel timing (no reference counterpart): average ms of `reps` launches of
+// one kernel of the Newton iteration on the handle's current data, each after
+// a write of flush_bytes (evicts L2).
+extern "C" int v2d_solver_time_kernel(v2d_solver *S, int which, int reps, long long flush_bytes,
+                                      double *ms_avg)
+{
+    V2D_ARG_CHECK(S && ms_avg && reps > 0 && flush_bytes >= 0, "time_kernel: bad arguments");
+    V2D_ARG_CHECK(which >= 0 && which <= 3, "time_kernel: unknown kernel %d", which);
+    GridDev &g = S->g;
+    DevBuf<char> fl;
+    V2D_TRY(fl.alloc((size_t)flush_bytes + 16, S->s));
+    DevBuf<double> vel;
+    if (which == 3) V2D_TRY(vel.alloc(3 * (size_t)g.N, S->s));
+    V2D_TRY(ensure_pattern(S));
+    const v2d_solver_params &p = S->prm;
+    AsmParams ap{p.re, p.invdtau, p.inv2dt, 0.0, p.ca, p.sa, p.ff_bc};
+    cudaEvent_t e0, e1;
+    V2D_CUDA_TRY(cudaEventCreate(&e0));
+    V2D_CUDA_TRY(cudaEventCreate(&e1));
+    double total = 0.0;
+    int st = V2D_OK;
+    for (int r = 0; r < reps && st == V2D_OK; ++r) {
+        if (flush_bytes) cudaMemsetAsync(fl.p, r & 0xff, (size_t)flush_bytes, S->s);
+        cudaEventRecord(e0, S->s);
+        if (which == 0) st = launch_metrics(g, S->s);
+        else if (which == 1) st = launch_assemble(g, ap, false, S->flag, S->s);
+        else if (which == 2) st = launch_assemble(g, ap, true, S->flag, S->s);
+        else st = launch_velocity(g.imax, g.jmax, g.dksi, g.deta, g.met[0], g.met[2], g.met[3],
+                                  g.met[6], g.met[7], g.psi, vel.p, vel.p + g.N, vel.p + 2 * g.N,
+                                  S->s);
+        cudaEventRecord(e1, S->s);
+        if (cudaEventSynchronize(e1) != cudaSuccess) st = V2D_ECUDA;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        total += ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != V2D_OK) return st;
+    *ms_avg = total / reps;
+    S->assembled = false;
+    return V2D_OK;
+}
+
 extern "C" int v2d_solver_stream(v2d_solver *S, void **stream)
 {
     V2D_ARG_CHECK(S && stream, "null pointer");

@@ -120,7 +120,11 @@ def generate_naca0012(imax: int = 257, jmax: int = 129, chord: float = 1.0,
     dist *= R / dist[-1]
     w = dist / R                                   # 0 at the wall, 1 at the far field
     blend = w ** 2 * (3.0 - 2.0 * w)               # smooth transition to the circle
-    phi = np.arctan2(ys, xs)
+    # far-field circle at uniform angles in the surface parameter (clockwise,
+    # like the surface): arctan2 of the surface points would crowd the lines
+    # next to the thin trailing edge onto nearly one angle and fold the outer
+    # cells beside the seam
+    phi = -ang
     xo, yo = R * np.cos(phi), R * np.sin(phi)
     xg = np.empty((imax, jmax))
     yg = np.empty((imax, jmax))
