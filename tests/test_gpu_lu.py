@@ -57,6 +57,23 @@ def test_one_newton_update_matches_direct_solve(v2d, oracle_mod, imax, jmax, ff_
     s.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_handles_with_different_front_sizes_coexist(v2d, oracle_mod, precision):
+    """The solve kernels' dynamic shared memory limit holds for the whole
+    process: a handle with smaller fronts, created after one with larger
+    fronts, must not lower it below what the larger one launches with."""
+    big = v2d.Solver(cfg(v2d, re=40.0, steady=True, precision=precision),
+                     mesh=oracle_mod.generate_cylinder(65, 49))
+    small = v2d.Solver(cfg(v2d, re=40.0, steady=True, precision=precision),
+                       mesh=oracle_mod.generate_cylinder(33, 25))
+    for s in (big, small, big):
+        code, res, lin = s.dev.newton(0.0)
+        assert code == 0, v2d._lib.last_error()
+        assert lin.converged and np.isfinite(res)
+    big.close()
+    small.close()
+
+
 def test_config1_steady_129_matches_oracle(v2d, oracle_mod):
     """Plain FP64 steady Newton, 129x129 cylinder, Re=40, Dirichlet far field,
     pure Newton (dtau = inf) to ||dq||/(2N) < 1e-12: psi/omega within 1e-9,

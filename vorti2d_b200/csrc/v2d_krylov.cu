@@ -27,7 +27,6 @@
 //    FP32 cycles act as inner solves of an FP64 defect correction.
 #include <algorithm>
 #include <cmath>
-#include <mutex>
 #include <vector>
 
 #include "v2d_internal.cuh"
@@ -558,6 +557,22 @@ static int end_capture(cudaStream_t s, cudaGraphExec_t *out)
     return V2D_OK;
 }
 
+// A launch that fails during a capture invalidates it, and every later call
+// reports only "a previous error during capture": each launch is checked as
+// it is captured, so the error names the first one that failed.
+static bool capture_launch_failed(cudaStream_t s, const char *what, int j)
+{
+    const cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) return false;
+    cudaGraph_t junk = nullptr;
+    cudaStreamEndCapture(s, &junk);
+    if (junk) cudaGraphDestroy(junk);
+    cudaGetLastError();
+    set_error("GMRES graph capture: launch of %s (basis column %d) failed: %s", what, j,
+              cudaGetErrorString(e));
+    return true;
+}
+
 static void drop_graphs(KrylovWork *w, int which)
 {
     for (cudaGraphExec_t g : w->seg[which])
@@ -582,10 +597,12 @@ static int capture_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, doub
     const std::vector<int> bnd = segment_bounds(w->m);
     for (size_t q = 0; q + 1 < bnd.size(); ++q) {
         long long nl = 0;
-        V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+        V2D_CUDA_TRY(cudaGetLastError());
+        V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         for (int j = bnd[q]; j < bnd[q + 1]; ++j) {
             nl += 6;
             k_scale_precond<T><<<gp, 256, 0, s>>>(w->desc, w->ctl, j, w->r, wv, V, w->H, z);
+            if (capture_launch_failed(s, "k_scale_precond", j)) return V2D_ECUDA;
             T *zj = z;
             if (lu) {
                 zj = Z + (size_t)j * n;
@@ -601,12 +618,15 @@ static int capture_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, doub
                 }
             }
             k_spmv<T><<<gs, kSpmvThreads, 0, s>>>(w->desc, w->ctl, zj, wv);
+            if (capture_launch_failed(s, "k_spmv", j)) return V2D_ECUDA;
             const dim3 gdot(gt, (j + 1 + kDotChunk - 1) / kDotChunk);
             for (int pass = 0; pass < 2; ++pass) {
                 k_mdot<T><<<gdot, kRedThreads, 0, s>>>(w->desc, w->ctl, j, pass, V, wv, w->partial,
                                                        w->H, w->hcur);
+                if (capture_launch_failed(s, "k_mdot", j)) return V2D_ECUDA;
                 k_update<T><<<gt, kRedThreads, 0, s>>>(w->desc, w->ctl, j, pass, V, wv, w->partial,
                                                        w->H, w->hcur, w->g, w->cs, w->sn);
+                if (capture_launch_failed(s, "k_update", j)) return V2D_ECUDA;
             }
         }
         cudaGraphExec_t ge = nullptr;
@@ -614,7 +634,7 @@ static int capture_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, doub
         w->seg[which].push_back(ge);
         w->seg_launches[which].push_back(nl);
     }
-    V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+    V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     k_backsolve<<<1, 32, 0, s>>>(w->desc, w->ctl, w->H, w->g, w->y);
     k_correct<T><<<gp, 256, 0, s>>>(w->desc, w->ctl, V, w->y, z, x, Z);
     k_residual<<<gr, kSpmvThreads, 0, s>>>(w->desc, w->ctl, w->r, w->partial, w->g, 0);
@@ -651,35 +671,8 @@ static int run_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, double *
     return V2D_OK;
 }
 
-// Kernels are loaded lazily on first launch; every kernel that the restart
-// cycle graphs hold is loaded here first, outside any stream capture, so that
-// no module load happens while a stream is capturing.
-static int krylov_preload()
-{
-    static std::once_flag once;
-    static cudaError_t status = cudaSuccess;
-    std::call_once(once, [] {
-        const void *fns[] = {
-            (const void *)k_scale_precond<float>, (const void *)k_scale_precond<double>,
-            (const void *)k_spmv<float>, (const void *)k_spmv<double>,
-            (const void *)k_mdot<float>, (const void *)k_mdot<double>,
-            (const void *)k_update<float>, (const void *)k_update<double>,
-            (const void *)k_correct<float>, (const void *)k_correct<double>,
-            (const void *)k_backsolve, (const void *)k_residual};
-        cudaFuncAttributes a;
-        for (const void *f : fns)
-            if (status == cudaSuccess) status = cudaFuncGetAttributes(&a, f);
-    });
-    if (status != cudaSuccess) {
-        set_error("krylov: kernel load failed: %s", cudaGetErrorString(status));
-        return V2D_ECUDA;
-    }
-    return V2D_OK;
-}
-
 int krylov_create(KrylovWork **out, int n, int restart, cudaStream_t s)
 {
-    V2D_TRY(krylov_preload());
     V2D_ARG_CHECK(n > 0 && restart >= 1 && restart <= kMaxRestart,
                   "krylov: n=%d restart=%d (restart must be in [1, %d])", n, restart, kMaxRestart);
     KrylovWork *w = new KrylovWork();

@@ -50,7 +50,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include "v2d_internal.cuh"
@@ -1379,45 +1381,29 @@ __global__ void __launch_bounds__(kSolveThreads2) k_apply_all(const MfDev D, con
 }  // namespace
 
 // ------------------------------------------------------------ host drivers
-// Kernels are loaded lazily on first launch; the factorization graph's
-// kernels are loaded here first, outside any stream capture.
-template <class T>
-static cudaError_t mf_preload_t()
+// The dynamic shared memory limit of a kernel (cudaFuncSetAttribute) holds
+// per function and device for the whole process, so every handle shares it:
+// it is only ever raised, to the largest size any handle launches with, and
+// left at the 48 KB default below that.  Setting it to one handle's smaller
+// size would make the launches of a handle with larger fronts fail.
+static cudaError_t raise_dyn_smem(const void *fn, size_t bytes)
 {
-    const void *fns[] = {(const void *)k_scatter<T>, (const void *)k_extend_add<T>,
-                         (const void *)k_panel<T>, (const void *)k_l21<T>,
-                         (const void *)k_swap_trsm<T>, (const void *)k_gemm<T>,
-                         (const void *)k_trinv<T>, (const void *)k_trcopy<T>,
-                         (const void *)k_fwd_z<T>, (const void *)k_fwd_u<T>,
-                         (const void *)k_bwd_y<T>, (const void *)k_bwd_x<T>,
-                         (const void *)k_fwd_front<T>, (const void *)k_bwd_front<T>,
-                         (const void *)k_tup_front<T>, (const void *)k_tdown_front<T>};
-    cudaFuncAttributes a;
-    cudaError_t e = cudaFuncGetAttributes(&a, (const void *)k_rowscale);
-    for (const void *f : fns)
-        if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, f);
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> limit;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t &cur = limit[{fn, dev}];
+    if (bytes <= std::max<size_t>(cur, 48 * 1024)) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) cur = bytes;
     return e;
-}
-
-static int mf_preload()
-{
-    static std::once_flag once;
-    static cudaError_t status = cudaSuccess;
-    std::call_once(once, [] {
-        status = mf_preload_t<float>();
-        if (status == cudaSuccess) status = mf_preload_t<double>();
-    });
-    if (status != cudaSuccess) {
-        set_error("mf_factor: kernel load failed: %s", cudaGetErrorString(status));
-        return V2D_ECUDA;
-    }
-    return V2D_OK;
 }
 
 int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
 {
     *out = nullptr;
-    V2D_TRY(mf_preload());
     MfFactor *M = new MfFactor();
     M->fp32 = fp32;
     const size_t es = fp32 ? sizeof(float) : sizeof(double);
@@ -1454,8 +1440,7 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
         return V2D_EARG;
     }
     auto attr = [&](const void *fn, size_t bytes) {
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e == cudaSuccess) e = raise_dyn_smem(fn, bytes);
     };
     if (fp32) {
         attr((const void *)k_apply_all<float>, solve);
@@ -1592,7 +1577,7 @@ int mf_factor(const MfPlan *P, MfFactor *M, const int *rowptr, const double *val
         if (M->graph) cudaGraphExecDestroy(M->graph);
         M->graph = nullptr;
         cudaGraph_t g = nullptr;
-        V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+        V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         int st = M->fp32 ? factor_launches<float>(P, M, rowptr, val, s)
                          : factor_launches<double>(P, M, rowptr, val, s);
         cudaError_t e = cudaStreamEndCapture(s, &g);
@@ -1617,6 +1602,17 @@ int mf_factor(const MfPlan *P, MfFactor *M, const int *rowptr, const double *val
     V2D_CUDA_TRY(cudaGraphLaunch(M->graph, s));
     count_launches(M->launches_per_factor);
     return V2D_OK;
+}
+
+// Error of the launch just issued, named (the solve is usually issued inside
+// a stream capture, where a failed launch invalidates the capture and later
+// calls report only that).
+static int solve_launch(const char *what, int L)
+{
+    const cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) return V2D_OK;
+    set_error("LU solve: launch of %s (level %d) failed: %s", what, L, cudaGetErrorString(e));
+    return V2D_ECUDA;
 }
 
 template <class T>
@@ -1652,16 +1648,19 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
         if (nq >= kFrontPerCta) {
             k_fwd_front<T><<<nq, kSolveThreads2, smf, s>>>(q0, D, F, b, M->rs, z, upd, stop_a,
                                                            stop_b);
+            V2D_TRY(solve_launch("k_fwd_front", L));
             ++launches;
             continue;
         }
         k_fwd_z<T><<<dim3(chunks(P->lvl_maxS[L]), nq), kSolveThreads2,
                      (size_t)(P->maxf + P->maxS) * sizeof(T), s>>>(q0, D, F, b, M->rs, z, upd,
                                                                    stop_a, stop_b);
+        V2D_TRY(solve_launch("k_fwd_z", L));
         ++launches;
         if (P->lvl_maxm[L] > 0) {
             k_fwd_u<T><<<dim3(chunks(P->lvl_maxm[L]), nq), kSolveThreads2,
                          (size_t)P->maxS * sizeof(T), s>>>(q0, D, F, z, upd, stop_a, stop_b);
+            V2D_TRY(solve_launch("k_fwd_u", L));
             ++launches;
         }
     }
@@ -1669,16 +1668,19 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
         const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
         if (nq >= kFrontPerCta) {
             k_bwd_front<T><<<nq, kSolveThreads2, smf, s>>>(q0, D, F, z, x, stop_a, stop_b);
+            V2D_TRY(solve_launch("k_bwd_front", L));
             ++launches;
             continue;
         }
         if (P->lvl_maxm[L] > 0) {
             k_bwd_y<T><<<dim3(chunks(P->lvl_maxS[L]), nq), kSolveThreads2,
                          (size_t)P->maxf * sizeof(T), s>>>(q0, D, F, z, x, stop_a, stop_b);
+            V2D_TRY(solve_launch("k_bwd_y", L));
             ++launches;
         }
         k_bwd_x<T><<<dim3(chunks(P->lvl_maxS[L]), nq), kSolveThreads2,
                      (size_t)P->maxS * sizeof(T), s>>>(q0, D, F, z, x, stop_a, stop_b);
+        V2D_TRY(solve_launch("k_bwd_x", L));
         ++launches;
     }
     V2D_CUDA_TRY(cudaGetLastError());
