@@ -274,6 +274,61 @@ def run_sweep_workload(args):
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint_workload(args):
+    """Steady discrete adjoint: NACA-0012 257x193 (256 distinct wall nodes),
+    wall displaced by seeded Gaussian bumps of 1e-3 chord, alpha = 4 deg,
+    Re = --adjoint-re.  The steady Newton solve (FP64 LU-preconditioned GMRES)
+    is timed, then the gradients dCl/dalpha, dCd/dRe and dCd/d(256 wall-normal
+    displacements): one transposed solve per output weight plus central
+    differences of the residual and the wall forces on the displaced meshes.
+    value = gradient evaluations (all three) per second."""
+    import torch
+    import vorti2d_b200 as v
+    from vorti2d_b200.adjoint import deform_ogrid, force_vjp, gaussian_bumps, shape_vjp
+    torch.cuda.set_device(0)
+    base = v.generate_naca0012(257, 193)
+    d0 = gaussian_bumps(256, n_bumps=8, amplitude=1e-3, seed=0)
+    X, Y = deform_ogrid(*base, d0)
+    cfg = v.Config(verbose=False, write_csv=False, write_xdmf=False, compute_forces=False,
+                   re=args.adjoint_re, alpha_deg=4.0, steady=True, pseudo_tol=1e-12,
+                   max_pseudo_iter=30, ksp_rtol=1e-12, ref_length=1.0, precision="fp64",
+                   raise_on_linear_failure=False)
+    s = v.Solver(cfg, mesh=(X, Y))
+    t0 = time.perf_counter()
+    try:
+        res, its, _ = s.advance(0.0)
+    except v._lib.V2DError:
+        res, its = float("nan"), cfg.max_pseudo_iter
+    t_solve = time.perf_counter() - t0
+    converged = bool(np.isfinite(res) and res <= cfg.pseudo_tol)
+    line = {"metric": "steady adjoint gradients/s (dCl/dalpha, dCd/dRe, dCd/d(256 wall "
+                      "displacements)), NACA-0012 257x193",
+            "unit": "gradient sets/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "steady discrete adjoint, NACA-0012 257x193, alpha 4 deg, "
+                                   f"Re {args.adjoint_re:g}, 8 seeded 1e-3-chord wall bumps"},
+            "steady_newton_its": its, "steady_res": res, "steady_converged": converged,
+            "steady_solve_s": t_solve}
+    if not converged:
+        line.update(value=None, note="plain Newton from the free stream did not converge at "
+                                     "this Re; no gradient at an unconverged state")
+        print(json.dumps(line), flush=True)
+        s.close()
+        return
+    reps = max(1, args.steps // 5)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        d_alpha, _, info = force_vjp(s, (1.0, 0.0, 0.0))
+        _, d_re, _ = force_vjp(s, (0.0, 1.0, 0.0))
+        gshape, sinfo = shape_vjp(s, (0.0, 1.0, 0.0), base)
+    dt = (time.perf_counter() - t0) / reps
+    line.update(value=1.0 / dt, ms_per_gradient_set=1e3 * dt, reps=reps,
+                dCl_dalpha=d_alpha, dCd_dRe=d_re, dCd_dd_norm=float(np.linalg.norm(gshape)),
+                adjoint_refinements=sinfo["refinements"], adjoint_rel_res=sinfo["rel_res"])
+    print(json.dumps(line), flush=True)
+    s.close()
+
+
 def phase_times(_lib, s, reset=False):
     """(assembly, factorization, Krylov, update) device ms summed over Newton
     iterations, and the iteration count."""
@@ -430,9 +485,12 @@ def main():
                          "(0: factor every Newton Jacobian)")
     ap.add_argument("--kernels-grid", type=int, default=2049,
                     help="grid side of the HBM-bound kernel roofline table (0: skip)")
-    ap.add_argument("--workload", default="unsteady", choices=["unsteady", "sweep"],
-                    help="unsteady: the BDF2 benchmark; sweep: the batched steady sweep")
+    ap.add_argument("--workload", default="unsteady", choices=["unsteady", "sweep", "adjoint"],
+                    help="unsteady: the BDF2 benchmark; sweep: the batched steady sweep; "
+                         "adjoint: steady adjoint gradients")
     ap.add_argument("--sweep-workers", type=int, default=16)
+    ap.add_argument("--adjoint-re", type=float, default=500.0,
+                    help="Reynolds number of the adjoint workload (--workload adjoint)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="print only the HBM-bound kernel roofline table (--kernels-grid)")
     ap.add_argument("--profile-newton", action="store_true",
@@ -444,6 +502,9 @@ def main():
         return
     if args.workload == "sweep" and args.impl == "ours":
         run_sweep_workload(args)
+        return
+    if args.workload == "adjoint" and args.impl == "ours":
+        run_adjoint_workload(args)
         return
     if args.kernels_only:
         import torch

@@ -286,6 +286,17 @@ int v2d_solver_adjoint(v2d_solver *s, double urot, const double *g, double *lamb
  * parameter derivatives of the residual for the adjoint. */
 int v2d_solver_residual(v2d_solver *s, double re, double invdtau, double inv2dt, double urot,
                         double ca, double sa, double *b);
+/* The same right-hand side b = -R at the handle's state, but with the metrics
+ * of another mesh of the same shape (xg, yg: host, N doubles each, in the
+ * handle's pointer order): the mesh derivative of the residual for shape
+ * gradients (vorti2d_core.f90:66-189 then :219-381 on the given coordinates).
+ * The handle is not changed.  When met_rows > 0, met receives rows
+ * j < met_rows of the 10 metric arrays (10 blocks of imax*met_rows doubles, in
+ * the order of v2d_solver_get_metrics), enough for the wall force integrals
+ * with met_rows = 3. */
+int v2d_solver_residual_mesh(v2d_solver *s, const double *xg, const double *yg, double re,
+                             double invdtau, double inv2dt, double urot, double ca, double sa,
+                             double *b, int met_rows, double *met);
 /* Current system (after the last assembly): canonical CSR of the 2N system
  * and its right-hand side.  Sizes: 2N+1, nnz, nnz, 2N. */
 int v2d_solver_nnz(const v2d_solver *s, long long *nnz);

@@ -94,3 +94,117 @@ def test_torch_autograd_function(v2d, oracle_mod):
     assert abs(re.grad.item() - d_re) <= 1e-10 * max(1.0, abs(d_re))
     assert np.allclose(out.detach().numpy(),
                        coeffs(solve(v2d, xg, yg, RE, ADEG).force_coeffs()), rtol=1e-12)
+
+
+def test_residual_on_own_mesh_is_the_handles(v2d, oracle_mod):
+    """The residual and metrics on a given mesh equal the handle's own when
+    that mesh is the handle's, bit for bit; the wall force integral from the
+    three returned rows equals the solver's force coefficients."""
+    from vorti2d_b200.adjoint import _residual, _wall_forces, residual_on_mesh
+    xg, yg = oracle_mod.generate_cylinder(33, 25)
+    s = solve(v2d, xg, yg, RE, ADEG)
+    b, met = residual_on_mesh(s, xg, yg, 3)
+    want = _residual(s, RE, ADEG, s.cfg.u_rot(s.t))
+    assert np.array_equal(b, want)
+    own = s.dev.metrics()
+    for q in range(10):
+        assert np.array_equal(met[q], own[q][:3 * s.imax]), q
+    ome3 = s.ome[:3 * s.imax]
+    for w, key in (((1, 0, 0), "cl"), ((0, 1, 0), "cd"), ((0, 0, 1), "cm")):
+        got = _wall_forces(s, met, ome3, w)
+        ref = getattr(s.force_coeffs(), key)
+        assert abs(got - ref) <= 1e-14 * max(1.0, abs(ref)), key
+    s.close()
+
+
+SHAPE_CASES = [
+    # (kind, imax, jmax, Re, alpha, ref_length)
+    ("cylinder", 65, 49, 40.0, 4.0, None),
+    ("naca", 65, 33, 5.0, 3.0, 1.0),
+]
+
+
+def _base_mesh(v2d, oracle_mod, kind, im, jm):
+    if kind == "cylinder":
+        return oracle_mod.generate_cylinder(im, jm)
+    return v2d.generate_naca0012(im, jm)
+
+
+def _shape_solve(v2d, base, d, re, adeg, ref_length):
+    from vorti2d_b200.adjoint import deform_ogrid
+    X, Y = deform_ogrid(*base, d)
+    cfg = steady_cfg(v2d, re, adeg)
+    cfg.ref_length = ref_length
+    s = v2d.Solver(cfg, mesh=(X, Y))
+    s.advance(0.0)
+    return s
+
+
+@pytest.mark.parametrize("kind,im,jm,re,adeg,ref_length", SHAPE_CASES)
+def test_shape_gradient_matches_finite_differences(v2d, oracle_mod, kind, im, jm, re, adeg,
+                                                   ref_length):
+    """dCl/dd and dCd/dd for the wall-normal displacements d of all P wall
+    nodes (one adjoint solve) against central differences of full steady
+    solves along a bump direction and a single-node direction, on the GPU
+    and on the oracle, within 1e-5 relative."""
+    from vorti2d_b200.adjoint import deform_ogrid, gaussian_bumps, shape_vjp
+    base = _base_mesh(v2d, oracle_mod, kind, im, jm)
+    P = im - 1
+    d0 = gaussian_bumps(P, n_bumps=4, amplitude=1e-3, seed=1)
+    s = _shape_solve(v2d, base, d0, re, adeg, ref_length)
+    grads = {}
+    for w, key in (((1.0, 0.0, 0.0), "cl"), ((0.0, 1.0, 0.0), "cd")):
+        grads[key], info = shape_vjp(s, w, base)
+        assert grads[key].shape == (P,)
+    s.close()
+    e5 = np.zeros(P)
+    e5[5] = 1.0
+    # steps small enough that the O(eps^2) error of the full-solve difference
+    # is below 1e-7 relative: moving one wall node by 1e-4 is a sizeable part
+    # of the local cell there
+    for v, eps in ((gaussian_bumps(P, n_bumps=3, amplitude=1.0, seed=2), 1e-5), (e5, 1e-6)):
+        fd, fo = {}, {}
+        sp_ = _shape_solve(v2d, base, d0 + eps * v, re, adeg, ref_length)
+        sm_ = _shape_solve(v2d, base, d0 - eps * v, re, adeg, ref_length)
+        for key in ("cl", "cd"):
+            fd[key] = (getattr(sp_.force_coeffs(), key) - getattr(sm_.force_coeffs(), key)) / (2 * eps)
+        sp_.close()
+        sm_.close()
+        ov = []
+        for sg in (1.0, -1.0):
+            X, Y = deform_ogrid(*base, d0 + sg * eps * v)
+            o = oracle_mod.OracleSolver(X, Y, re=re, alpha_deg=adeg, steady=True,
+                                        pseudo_tol=1e-13, max_pseudo_iter=60).run()
+            ov.append(oracle_mod.compute_force_coeffs(
+                o.imax, o.jmax, o.re, o.dksi, o.deta, o.beta, o.gama, o.detadx, o.detady,
+                o.xphys, o.yphys, o.ome, ref_length=ref_length))
+        for key in ("cl", "cd"):
+            fo[key] = (getattr(ov[0], key) - getattr(ov[1], key)) / (2 * eps)
+            adj = float(grads[key] @ v)
+            scale = max(abs(fd[key]), 1e-3 * np.abs(grads[key]).sum())
+            assert abs(adj - fd[key]) <= 1e-5 * scale, (kind, key, adj, fd[key])
+            assert abs(adj - fo[key]) <= 1e-5 * scale, (kind, key, adj, fo[key])
+
+
+def test_torch_autograd_shape(v2d, oracle_mod):
+    import torch
+    from vorti2d_b200.adjoint import SteadyForces, deform_ogrid, gaussian_bumps, shape_vjp
+    base = oracle_mod.generate_cylinder(33, 25)
+    P = 32
+    d0 = gaussian_bumps(P, n_bumps=3, amplitude=1e-3, seed=4)
+
+    def make(adeg, re, d):
+        return v2d.Solver(steady_cfg(v2d, re, adeg), mesh=deform_ogrid(*base, d))
+
+    alpha = torch.tensor(ADEG, dtype=torch.float64, requires_grad=True)
+    re = torch.tensor(RE, dtype=torch.float64, requires_grad=True)
+    d = torch.tensor(d0, dtype=torch.float64, requires_grad=True)
+    out = SteadyForces.apply(alpha, re, make, d, base)
+    out[1].backward()
+    s = make(ADEG, RE, d0)
+    s.advance(0.0)
+    want, _ = shape_vjp(s, (0.0, 1.0, 0.0), base)
+    s.close()
+    assert d.grad is not None and d.grad.shape == (P,)
+    assert np.allclose(d.grad.numpy(), want, rtol=1e-10, atol=1e-12 * np.abs(want).max())
+    assert alpha.grad is not None and re.grad is not None

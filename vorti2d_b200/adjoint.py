@@ -21,6 +21,13 @@ C(q; p) has
   body-axis quantities, so dC/dalpha|_q = 0.  With an outflow far field the
   set of outflow rows itself depends on alpha; gradients in alpha are for the
   Dirichlet far field.
+* Shape: the P = imax-1 distinct wall nodes move along their outward normals
+  by d_i, and each grid line follows with a weight that decays from 1 at the
+  wall to 0 at the far field (``deform_ogrid``; linear in d).  dR/dd_i and
+  dC/dd_i|_q are central differences of the residual and of the force
+  integrals on the displaced meshes at the fixed converged state
+  (``v2d_solver_residual_mesh``: metrics and residual on the device); the one
+  adjoint solve is shared by all P components.
 """
 from __future__ import annotations
 
@@ -123,22 +130,161 @@ def force_vjp(solver, weights, alpha_h=1e-3):
     return d_alpha, d_re, dict(refinements=its, rel_res=rel)
 
 
+# ------------------------------------------------------------------ shape
+def wall_normals(xg, yg):
+    """Outward unit normals (nx, ny) of the P = imax-1 distinct wall nodes
+    (j = 0) of an O-grid (xg, yg of shape (imax, jmax)), from the periodic
+    central tangent, pointing toward the first grid line off the wall."""
+    xg, yg = np.asarray(xg, dtype=np.float64), np.asarray(yg, dtype=np.float64)
+    P = xg.shape[0] - 1
+    xw, yw = xg[:P, 0], yg[:P, 0]
+    tx = np.roll(xw, -1) - np.roll(xw, 1)
+    ty = np.roll(yw, -1) - np.roll(yw, 1)
+    tn = np.hypot(tx, ty)
+    nx, ny = ty / tn, -tx / tn
+    sgn = np.where(nx * (xg[:P, 1] - xw) + ny * (yg[:P, 1] - yw) < 0.0, -1.0, 1.0)
+    return nx * sgn, ny * sgn
+
+
+def deformation_weights(xg, yg):
+    """phi (imax, jmax): (1 - w)^2 with w the arclength fraction along each
+    grid line from the wall (1 at the wall, 0 at the far field)."""
+    xg, yg = np.asarray(xg, dtype=np.float64), np.asarray(yg, dtype=np.float64)
+    seg = np.hypot(np.diff(xg, axis=1), np.diff(yg, axis=1))
+    cum = np.concatenate([np.zeros((xg.shape[0], 1)), np.cumsum(seg, axis=1)], axis=1)
+    w = cum / cum[:, -1:]
+    return (1.0 - w) ** 2
+
+
+def deform_ogrid(xg, yg, d, normals=None, weights=None):
+    """The O-grid with wall node i moved by d[i] along its outward normal and
+    grid line i by d[i] * phi[i, j] (the seam column imax-1 moves with
+    column 0).
+    ``normals`` / ``weights`` default to those of (xg, yg), so the map is
+    linear in d."""
+    xg, yg = np.asarray(xg, dtype=np.float64), np.asarray(yg, dtype=np.float64)
+    P = xg.shape[0] - 1
+    d = np.asarray(d, dtype=np.float64)
+    if d.shape != (P,):
+        raise ValueError(f"d must have imax-1 = {P} entries (got shape {d.shape})")
+    nx, ny = normals if normals is not None else wall_normals(xg, yg)
+    phi = weights if weights is not None else deformation_weights(xg, yg)
+    X, Y = xg.copy(), yg.copy()
+    X[:P] += (d * nx)[:, None] * phi[:P]
+    Y[:P] += (d * ny)[:, None] * phi[:P]
+    X[P] += d[0] * nx[0] * phi[P]
+    Y[P] += d[0] * ny[0] * phi[P]
+    return X, Y
+
+
+def gaussian_bumps(P, n_bumps=8, amplitude=1e-3, width=None, seed=0):
+    """A seeded wall displacement: n_bumps periodic Gaussian bumps over the P
+    wall nodes, centres uniform, signs random, each of height ``amplitude``
+    and standard deviation ``width`` nodes (default P/32)."""
+    rng = np.random.default_rng(seed)
+    sigma = float(width) if width is not None else P / 32.0
+    centres = rng.uniform(0.0, P, n_bumps)
+    signs = rng.choice([-1.0, 1.0], n_bumps)
+    i = np.arange(P, dtype=np.float64)
+    d = np.zeros(P)
+    for c, sg in zip(centres, signs):
+        dist = np.abs(i - c)
+        dist = np.minimum(dist, P - dist)
+        d += sg * amplitude * np.exp(-0.5 * (dist / sigma) ** 2)
+    return d
+
+
+def residual_on_mesh(solver, xg, yg, met_rows=3):
+    """(b, wall metrics): b = -R at the solver's state with the metrics of
+    mesh (xg, yg), and rows j < met_rows of the 10 metric arrays, shape
+    (10, met_rows * imax)."""
+    cfg = solver.cfg
+    X = np.asfortranarray(xg, dtype=np.float64)
+    Y = np.asfortranarray(yg, dtype=np.float64)
+    if X.shape != (solver.imax, solver.jmax) or Y.shape != X.shape:
+        raise ValueError(f"mesh must be {solver.imax} x {solver.jmax}")
+    b = np.empty(2 * solver.ndof)
+    met = np.empty((10, met_rows * solver.imax))
+    a = math.radians(cfg.alpha_deg)
+    check(lib().v2d_solver_residual_mesh(solver.dev.h, dptr(X), dptr(Y), float(cfg.re),
+                                         cfg.inv_dtau(), cfg.inv_2dt(),
+                                         float(cfg.u_rot(solver.t)), math.cos(a), math.sin(a),
+                                         dptr(b), int(met_rows), dptr(met)),
+          "residual_mesh")
+    return b, met
+
+
+def _wall_forces(solver, met3, ome3, weights):
+    from .forces import compute_force_coeffs
+    cfg = solver.cfg
+    fc = compute_force_coeffs(solver.imax, 3, float(cfg.re), solver.dksi, solver.deta,
+                              met3[2], met3[3], met3[6], met3[7], met3[8], met3[9], ome3,
+                              ref_length=cfg.ref_length, moment_ref=cfg.moment_center)
+    w_cl, w_cd, w_cm = (float(v) for v in weights)
+    return w_cl * fc.cl + w_cd * fc.cd + w_cm * fc.cm
+
+
+def shape_vjp(solver, weights, base_mesh, h=None):
+    """d(w . (Cl, Cd, Cm))/d(d_i), i < P, at the solver's converged steady
+    state, for wall displacements d along the normals of ``base_mesh`` (the
+    undeformed (xg, yg) that ``deform_ogrid`` displaced to the solver's
+    mesh).  Central differences of step h (default 1e-6 of the wall's
+    extent) on the residual and the force integrals, one adjoint solve."""
+    xg0, yg0 = (np.asarray(a, dtype=np.float64) for a in base_mesh)
+    nx, ny = wall_normals(xg0, yg0)
+    phi = deformation_weights(xg0, yg0)
+    X = np.asarray(solver.xg, dtype=np.float64)
+    Y = np.asarray(solver.yg, dtype=np.float64)
+    P = solver.imax - 1
+    if h is None:
+        h = 1e-6 * max(np.ptp(X[:P, 0]), np.ptp(Y[:P, 0]))
+    cfg = solver.cfg
+    grads = force_gradients(solver.imax, solver.jmax, float(cfg.re), solver.dksi, solver.deta,
+                            solver.beta, solver.gama, solver.detadx, solver.detady,
+                            solver.xphys, solver.yphys, cfg.ref_length, cfg.moment_center)
+    w_cl, w_cd, w_cm = (float(v) for v in weights)
+    N = solver.ndof
+    g = np.zeros(2 * N)
+    g[N:] = w_cl * grads["cl"] + w_cd * grads["cd"] + w_cm * grads["cm"]
+    lam, its, rel = adjoint_solve(solver, g)
+    ome3 = np.asarray(solver.ome, dtype=np.float64).reshape(-1)[:3 * solver.imax]
+    out = np.empty(P)
+    for i in range(P):
+        vals, bs = [], []
+        for sg in (1.0, -1.0):
+            Xs, Ys = X.copy(), Y.copy()
+            Xs[i] += sg * h * nx[i] * phi[i]
+            Ys[i] += sg * h * ny[i] * phi[i]
+            if i == 0:
+                Xs[P] += sg * h * nx[0] * phi[P]
+                Ys[P] += sg * h * ny[0] * phi[P]
+            b, met = residual_on_mesh(solver, Xs, Ys, 3)
+            bs.append(b)
+            vals.append(_wall_forces(solver, met, ome3, weights))
+        out[i] = (vals[0] - vals[1]) / (2.0 * h) + float(lam @ (bs[0] - bs[1])) / (2.0 * h)
+    return out, dict(refinements=its, rel_res=rel, h=h)
+
+
 def _torch():
     import torch
     return torch
 
 
 class SteadyForces:
-    """(alpha_deg, Re) -> (Cl, Cd, Cm) of a converged steady solve, as a
-    torch.autograd.Function whose backward is the discrete adjoint.
+    """(alpha_deg, Re[, wall displacements d]) -> (Cl, Cd, Cm) of a converged
+    steady solve, as a torch.autograd.Function whose backward is the
+    discrete adjoint.
 
     Usage::
 
         out = SteadyForces.apply(alpha, re, make_solver)   # out = [Cl, Cd, Cm]
+        out = SteadyForces.apply(alpha, re, make_solver, d, base_mesh)
 
-    ``make_solver(alpha_deg, re)`` returns a ``vorti2d_b200.Solver`` configured
-    as a steady case; it is advanced once (the steady Newton solve) and kept
-    for the backward pass.
+    ``make_solver(alpha_deg, re)`` -- or ``make_solver(alpha_deg, re, d)``
+    when a displacement tensor d (P = imax-1 entries) is given -- returns a
+    ``vorti2d_b200.Solver`` configured as a steady case, on
+    ``deform_ogrid(*base_mesh, d)`` in the second form; it is advanced once
+    (the steady Newton solve) and kept for the backward pass.
     """
 
     _fn = None
@@ -150,24 +296,37 @@ class SteadyForces:
 
             class _Fn(torch.autograd.Function):
                 @staticmethod
-                def forward(ctx, alpha, re, make_solver):
-                    s = make_solver(float(alpha), float(re))
+                def forward(ctx, alpha, re, make_solver, disp, base_mesh):
+                    if disp is None:
+                        s = make_solver(float(alpha), float(re))
+                    else:
+                        s = make_solver(float(alpha), float(re),
+                                        disp.detach().cpu().numpy().astype(np.float64))
                     s.advance(s.times()[0])
                     fc = s.force_coeffs()
                     ctx.solver = s
+                    ctx.base_mesh = base_mesh
+                    ctx.has_disp = disp is not None
                     return torch.tensor([fc.cl, fc.cd, fc.cm], dtype=torch.float64)
 
                 @staticmethod
                 def backward(ctx, grad):
                     s = ctx.solver
-                    d_alpha, d_re, _ = force_vjp(s, grad.detach().cpu().numpy())
+                    w = grad.detach().cpu().numpy()
+                    d_alpha, d_re, _ = force_vjp(s, w)
+                    d_disp = None
+                    if ctx.has_disp:
+                        gs, _ = shape_vjp(s, w, ctx.base_mesh)
+                        d_disp = torch.tensor(gs, dtype=torch.float64)
                     s.close()
                     return (torch.tensor(d_alpha, dtype=torch.float64),
-                            torch.tensor(d_re, dtype=torch.float64), None)
+                            torch.tensor(d_re, dtype=torch.float64), None, d_disp, None)
 
             cls._fn = _Fn
         return cls._fn
 
     @classmethod
-    def apply(cls, alpha, re, make_solver):
-        return cls.function().apply(alpha, re, make_solver)
+    def apply(cls, alpha, re, make_solver, disp=None, base_mesh=None):
+        if disp is not None and base_mesh is None:
+            raise ValueError("a displacement needs the undeformed base_mesh")
+        return cls.function().apply(alpha, re, make_solver, disp, base_mesh)

@@ -597,6 +597,41 @@ extern "C" int v2d_solver_residual(v2d_solver *S, double re, double invdtau, dou
     return V2D_OK;
 }
 
+extern "C" int v2d_solver_residual_mesh(v2d_solver *S, const double *xg, const double *yg,
+                                        double re, double invdtau, double inv2dt, double urot,
+                                        double ca, double sa, double *b, int met_rows,
+                                        double *met)
+{
+    V2D_ARG_CHECK(S && xg && yg && b, "solver_residual_mesh: null pointer");
+    V2D_ARG_CHECK(re > 0.0, "solver_residual_mesh: re must be positive");
+    V2D_ARG_CHECK(met_rows >= 0 && met_rows <= S->g.jmax && (met_rows == 0 || met),
+                  "solver_residual_mesh: met_rows=%d outside [0, %d] or null output", met_rows,
+                  S->g.jmax);
+    // a copy of the grid description whose mesh and metric arrays point to
+    // scratch: the state is the handle's, the handle itself is not changed
+    GridDev g = S->g;
+    const size_t N = (size_t)g.N;
+    DevBuf<double> buf;
+    V2D_TRY(buf.alloc(12 * N + (size_t)g.n, S->s));
+    g.x = buf.p;
+    g.y = buf.p + N;
+    for (int q = 0; q < 10; ++q) g.met[q] = buf.p + (2 + q) * N;
+    double *d = buf.p + 12 * N;
+    V2D_CUDA_TRY(cudaMemcpyAsync(g.x, xg, N * sizeof(double), cudaMemcpyHostToDevice, S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(g.y, yg, N * sizeof(double), cudaMemcpyHostToDevice, S->s));
+    V2D_TRY(launch_metrics(g, S->s));
+    count_launches(1);
+    AsmParams ap{re, invdtau, inv2dt, urot, ca, sa, S->prm.ff_bc};
+    V2D_TRY(launch_residual(g, ap, d, S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(b, d, g.n * sizeof(double), cudaMemcpyDeviceToHost, S->s));
+    const size_t rows = (size_t)g.imax * met_rows;
+    for (int q = 0; q < 10 && rows > 0; ++q)
+        V2D_CUDA_TRY(cudaMemcpyAsync(met + q * rows, g.met[q], rows * sizeof(double),
+                                     cudaMemcpyDeviceToHost, S->s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    return V2D_OK;
+}
+
 extern "C" int v2d_solver_adjoint(v2d_solver *S, double urot, const double *g_host, double *lam_host,
                                   double rtol, int max_refine, int *refinements, double *rel_res)
 {
