@@ -360,6 +360,55 @@ def profile_newton(args):
     s.close()
 
 
+def profile_lu_launches(args):
+    """Per-launch device time of one LU preconditioner solve after two steps
+    of the workload, with the factors warm in L2 (as inside GMRES) and after
+    an L2 flush."""
+    import ctypes
+    import torch
+    import vorti2d_b200 as v
+    from vorti2d_b200 import _lib
+    torch.cuda.set_device(0)
+    xg, yg = v.generate_cylinder(IMAX, JMAX)
+    prec = "mixed" if args.precision == "both" else args.precision
+    s = make_solver(v, xg, yg, prec, args.lu_reuse)
+    times = s.times()
+    for m in range(2):
+        s.advance(times[m])
+    kinds = ["fwd_front", "fwd_z", "fwd_u", "bwd_front", "bwd_y", "bwd_x"]
+    out = {"profile": "LU solve launches", "precision": prec}
+    for label, flush in (("warm", 0), ("cold", L2_FLUSH_BYTES)):
+        cap = 256
+        ms = (ctypes.c_double * cap)()
+        codes = (ctypes.c_int * cap)()
+        n = ctypes.c_int()
+        _lib.check(_lib.lib().v2d_solver_time_lu_launches(s.dev.h, 20, flush, ms, codes, cap,
+                                                         ctypes.byref(n)))
+        rows = [(kinds[codes[k] // 1000], codes[k] % 1000, ms[k]) for k in range(n.value)]
+        by_kind = {}
+        for kind, _, t in rows:
+            by_kind[kind] = by_kind.get(kind, 0.0) + t
+        out[label] = {"total_ms": sum(t for _, _, t in rows), "launches": len(rows),
+                      "by_kind_ms": by_kind,
+                      "per_launch_us": [[kind, lvl, round(1e3 * t, 2)] for kind, lvl, t in rows]}
+    fkinds = ["rowscale", "scatter", "extend_add", "panel", "l21", "swap_trsm", "gemm", "trinv",
+              "trcopy"]
+    cap = 1024
+    ms = (ctypes.c_double * cap)()
+    codes = (ctypes.c_int * cap)()
+    n = ctypes.c_int()
+    _lib.check(_lib.lib().v2d_solver_time_lu_factor(s.dev.h, 5, ms, codes, cap, ctypes.byref(n)))
+    by_kind, by_level = {}, {}
+    for k in range(n.value):
+        kind, lvl = fkinds[codes[k] // 1000], codes[k] % 1000
+        by_kind[kind] = by_kind.get(kind, 0.0) + ms[k]
+        by_level[lvl] = by_level.get(lvl, 0.0) + ms[k]
+    out["factor"] = {"total_ms": sum(ms[k] for k in range(n.value)), "launches": n.value,
+                     "by_kind_ms": by_kind, "by_level_ms": by_level}
+    print(json.dumps(out), flush=True)
+    s.close()
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import vorti2d_b200 as v
@@ -493,12 +542,17 @@ def main():
                     help="Reynolds number of the adjoint workload (--workload adjoint)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="print only the HBM-bound kernel roofline table (--kernels-grid)")
+    ap.add_argument("--lu-launches", action="store_true",
+                    help="per-launch device time of one LU preconditioner solve, warm and cold")
     ap.add_argument("--profile-newton", action="store_true",
                     help="one warm-up step, then one Newton iteration in NVTX range v2d_newton")
     args = ap.parse_args()
     rank, world, local_rank = dist_env()
     if args.profile_newton:
         profile_newton(args)
+        return
+    if args.lu_launches:
+        profile_lu_launches(args)
         return
     if args.workload == "sweep" and args.impl == "ours":
         run_sweep_workload(args)

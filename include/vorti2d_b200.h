@@ -337,6 +337,21 @@ int v2d_solver_phase_times(v2d_solver *s, double *out6, int reset);
 int v2d_solver_time_lu_apply(v2d_solver *s, int reps, long long flush_bytes, double *ms_avg,
                              long long *factor_bytes);
 
+/* Measurement aid (no reference counterpart): the device time of each
+ * launch of one LU preconditioner solve, averaged over `reps` solves (each
+ * after a write of flush_bytes; 0 keeps the factors warm in L2).  ms[k] and
+ * codes[k] (kind * 1000 + level; kinds 0 forward per-front, 1 forward pivot
+ * rows, 2 forward contribution rows, 3 backward per-front, 4 backward
+ * contribution part, 5 backward pivot rows) for k < *n <= cap. */
+int v2d_solver_time_lu_launches(v2d_solver *s, int reps, long long flush_bytes, double *ms,
+                                int *codes, int cap, int *n);
+/* Measurement aid (no reference counterpart): the device time of each kernel
+ * of one LU factorization of the last assembled Jacobian, launched directly,
+ * averaged over `reps` (codes kind * 1000 + level; kinds 0 row scaling,
+ * 1 scatter, 2 extend-add, 3 panel, 4 L21, 5 row swaps + U12, 6 Schur update,
+ * 7 pivot-block inversion, 8 inverse copy). */
+int v2d_solver_time_lu_factor(v2d_solver *s, int reps, double *ms, int *codes, int cap, int *n);
+
 /* Measurement aid (no reference counterpart): average ms of `reps` launches
  * of one kernel on the handle's data, each after a write of flush_bytes:
  * which = 0 metrics, 1 Newton assembly (FP64 values), 2 Newton assembly with

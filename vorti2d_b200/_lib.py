@@ -112,6 +112,8 @@ _SIGS = {
     "v2d_solver_time_spmv": (_i, [_vp, _i, _i, _ll, _dp]),
     "v2d_solver_phase_times": (_i, [_vp, _dp, _i]),
     "v2d_solver_time_kernel": (_i, [_vp, _i, _i, _ll, _dp]),
+    "v2d_solver_time_lu_launches": (_i, [_vp, _i, _ll, _dp, _ip, _i, _ip]),
+    "v2d_solver_time_lu_factor": (_i, [_vp, _i, _dp, _ip, _i, _ip]),
     "v2d_solver_residual_mesh": (_i, [_vp, _dp, _dp, _d, _d, _d, _d, _d, _d, _dp, _i, _dp]),
     "v2d_solver_time_lu_apply": (_i, [_vp, _i, _ll, _dp, ctypes.POINTER(_ll)]),
     "v2d_lu_plan_info": (_i, [_i, _i, _ip, _ip, _i, ctypes.POINTER(_ll)]),

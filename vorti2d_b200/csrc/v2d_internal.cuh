@@ -133,6 +133,17 @@ int mf_check_barrier(MfFactor *M, cudaStream_t s);
 // write of flush_bytes (evicts L2); CUDA events on stream s.
 int mf_time_apply(const MfPlan *P, const MfFactor *M, int reps, size_t flush_bytes, cudaStream_t s,
                   double *ms_avg);
+// Per-launch device time of one solve (average of reps), with the launch
+// codes (kind * 1000 + level; kinds: 0 fwd_front, 1 fwd_z, 2 fwd_u,
+// 3 bwd_front, 4 bwd_y, 5 bwd_x); *n receives the number of launches.
+int mf_time_apply_launches(const MfPlan *P, const MfFactor *M, int reps, size_t flush_bytes,
+                           cudaStream_t s, double *ms, int *codes, int cap, int *n);
+// Per-kernel device time of one factorization launched directly (not from
+// its graph), average of reps; codes kind * 1000 + level (kinds 0 rowscale,
+// 1 scatter, 2 extend_add, 3 panel, 4 l21, 5 swap_trsm, 6 gemm, 7 trinv,
+// 8 trcopy).  The factors are recomputed from the same values.
+int mf_time_factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, const double *val,
+                            int reps, cudaStream_t s, double *ms, int *codes, int cap, int *n);
 
 // ------------------------------------------------------------- Krylov
 // A CSR operator with optional FP32 copy and 2x2 block inverse.

@@ -1513,12 +1513,29 @@ MfDev mf_dev(const MfPlan *P, const MfFactor *M)
 
 template <class T>
 static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, const double *val,
-                           cudaStream_t s)
+                           cudaStream_t s, cudaEvent_t *ev = nullptr, int *codes = nullptr,
+                           int cap = 0, int *nev_out = nullptr)
 {
     constexpr int NB = PanelWidth<T>::v;
     T *F = (T *)M->F;
     long long launches = 0;
+    // with ev: an event is recorded after each kernel (kind * 1000 + level;
+    // kinds 0 rowscale, 1 scatter, 2 extend_add, 3 panel, 4 l21, 5 swap_trsm,
+    // 6 gemm, 7 trinv, 8 trcopy)
+    int nev = 0;
+    auto mark = [&](int code) -> int {
+        if (!ev) return V2D_OK;
+        if (nev >= cap) {
+            set_error("LU factor timing: more than %d launches", cap);
+            return V2D_EARG;
+        }
+        codes[nev] = code;
+        V2D_CUDA_TRY(cudaEventRecord(ev[nev], s));
+        ++nev;
+        return V2D_OK;
+    };
     k_rowscale<<<grid_for(P->n, 256), 256, 0, s>>>(P->n, rowptr, val, M->rs);
+    V2D_TRY(mark(0));
     ++launches;
     for (int L = 0; L < P->nlevel; ++L) {
         const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
@@ -1529,6 +1546,7 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
             k_scatter<T><<<grid_for(na, 256), 256, 0, s>>>(P->lvl_abeg[L], P->lvl_aend[L],
                                                          P->d_asm_csr, P->d_asm_row,
                                                          P->d_asm_pos, val, M->rs, F);
+            V2D_TRY(mark(1000 + L));
             ++launches;
         }
         if (L > 0) {
@@ -1538,6 +1556,7 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
                 k_extend_add<T><<<dim3(gx, nq), 256, 0, s>>>(q0, slot, P->d_S, P->d_f, P->d_foff,
                                                              P->d_uoff, P->d_child0, P->d_child1,
                                                              P->d_cbmap, F);
+                V2D_TRY(mark(2000 + L));
                 ++launches;
             }
         }
@@ -1545,29 +1564,36 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
         for (int k = 0; k < P->lvl_maxS[L]; k += NB) {
             k_panel<T><<<nq, kMfThreads, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff, P->d_voff, F,
                                                  M->ipiv, M->perm, M->flag);
+            V2D_TRY(mark(3000 + L));
             const int below = std::max(1, maxf - k - 1);
             k_l21<T><<<dim3((below + kL21Rows - 1) / kL21Rows, nq), kL21Rows, 0, s>>>(
                 q0, k, P->d_S, P->d_f, P->d_foff, F);
+            V2D_TRY(mark(4000 + L));
             const int gcol = (maxf + kTrsmCols - 1) / kTrsmCols;
             k_swap_trsm<T><<<dim3(gcol, nq), kTrsmCols, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff,
                                                                 P->d_voff, F, M->ipiv);
+            V2D_TRY(mark(5000 + L));
             const int rem = std::max(1, maxf - k - 1);
             const int nt = (rem + kGemmTile - 1) / kGemmTile;
             k_gemm<T><<<dim3(nt * nt, nq), 256, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff, F);
+            V2D_TRY(mark(6000 + L));
             launches += 4;
         }
         const int nbc = (P->lvl_maxS[L] + InvWidth<T>::v - 1) / InvWidth<T>::v;
         k_trinv<T><<<dim3(nbc, nq), kTrinvThreads,
                      (size_t)P->lvl_maxS[L] * (InvWidth<T>::v + 33) * sizeof(T), s>>>(
             q0, P->d_S, P->d_foff, P->d_f, P->d_toff, F, (T *)M->tmp);
+        V2D_TRY(mark(7000 + L));
         const long long ss = (long long)P->lvl_maxS[L] * P->lvl_maxS[L];
         const int gcp = (int)std::max(1LL, std::min<long long>((ss + 255) / 256, 256));
         k_trcopy<T><<<dim3(gcp, nq), 256, 0, s>>>(q0, P->d_S, P->d_f, P->d_foff, P->d_toff,
                                                   (const T *)M->tmp, F);
+        V2D_TRY(mark(8000 + L));
         launches += 2;
     }
     V2D_CUDA_TRY(cudaGetLastError());
-    M->launches_per_factor = launches;
+    if (nev_out) *nev_out = nev;
+    if (!ev) M->launches_per_factor = launches;
     return V2D_OK;
 }
 
@@ -1615,10 +1641,28 @@ static int solve_launch(const char *what, int L)
     return V2D_ECUDA;
 }
 
+// Launch codes of the solve's kernels for per-launch timing (kind * 1000 + level).
+enum { kCodeFwdFront = 0, kCodeFwdZ = 1, kCodeFwdU = 2, kCodeBwdFront = 3, kCodeBwdY = 4,
+       kCodeBwdX = 5 };
+
 template <class T>
 static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, const int *stop_a,
-                          const int *stop_b, cudaStream_t s, long long *n_launches)
+                          const int *stop_b, cudaStream_t s, long long *n_launches,
+                          cudaEvent_t *ev = nullptr, int *codes = nullptr, int cap = 0)
 {
+    // with ev: an event is recorded after each launch (at most cap launches)
+    int nev = 0;
+    auto mark = [&](int code) -> int {
+        if (!ev) return V2D_OK;
+        if (nev >= cap) {
+            set_error("LU solve timing: more than %d launches", cap);
+            return V2D_EARG;
+        }
+        codes[nev] = code;
+        V2D_CUDA_TRY(cudaEventRecord(ev[nev], s));
+        ++nev;
+        return V2D_OK;
+    };
     const MfDev D = mf_dev(P, M);
     const T *F = (const T *)M->F;
     T *z = (T *)M->z, *upd = (T *)M->upd;
@@ -1649,6 +1693,7 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
             k_fwd_front<T><<<nq, kSolveThreads2, smf, s>>>(q0, D, F, b, M->rs, z, upd, stop_a,
                                                            stop_b);
             V2D_TRY(solve_launch("k_fwd_front", L));
+            V2D_TRY(mark(kCodeFwdFront * 1000 + L));
             ++launches;
             continue;
         }
@@ -1656,11 +1701,13 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
                      (size_t)(P->maxf + P->maxS) * sizeof(T), s>>>(q0, D, F, b, M->rs, z, upd,
                                                                    stop_a, stop_b);
         V2D_TRY(solve_launch("k_fwd_z", L));
+        V2D_TRY(mark(kCodeFwdZ * 1000 + L));
         ++launches;
         if (P->lvl_maxm[L] > 0) {
             k_fwd_u<T><<<dim3(chunks(P->lvl_maxm[L]), nq), kSolveThreads2,
                          (size_t)P->maxS * sizeof(T), s>>>(q0, D, F, z, upd, stop_a, stop_b);
             V2D_TRY(solve_launch("k_fwd_u", L));
+            V2D_TRY(mark(kCodeFwdU * 1000 + L));
             ++launches;
         }
     }
@@ -1669,6 +1716,7 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
         if (nq >= kFrontPerCta) {
             k_bwd_front<T><<<nq, kSolveThreads2, smf, s>>>(q0, D, F, z, x, stop_a, stop_b);
             V2D_TRY(solve_launch("k_bwd_front", L));
+            V2D_TRY(mark(kCodeBwdFront * 1000 + L));
             ++launches;
             continue;
         }
@@ -1676,15 +1724,17 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
             k_bwd_y<T><<<dim3(chunks(P->lvl_maxS[L]), nq), kSolveThreads2,
                          (size_t)P->maxf * sizeof(T), s>>>(q0, D, F, z, x, stop_a, stop_b);
             V2D_TRY(solve_launch("k_bwd_y", L));
+            V2D_TRY(mark(kCodeBwdY * 1000 + L));
             ++launches;
         }
         k_bwd_x<T><<<dim3(chunks(P->lvl_maxS[L]), nq), kSolveThreads2,
                      (size_t)P->maxS * sizeof(T), s>>>(q0, D, F, z, x, stop_a, stop_b);
         V2D_TRY(solve_launch("k_bwd_x", L));
+        V2D_TRY(mark(kCodeBwdX * 1000 + L));
         ++launches;
     }
     V2D_CUDA_TRY(cudaGetLastError());
-    if (n_launches) *n_launches = launches;
+    if (n_launches) *n_launches = ev ? nev : launches;
     return V2D_OK;
 }
 
@@ -1759,6 +1809,87 @@ int mf_time_apply(const MfPlan *P, const MfFactor *M, int reps, size_t flush_byt
     cudaEventDestroy(e1);
     if (st != V2D_OK) return st;
     *ms_avg = total / reps;
+    return V2D_OK;
+}
+
+// Keeps the device busy for about `us` microseconds (bounded), so that the
+// host can enqueue a whole solve before it starts and per-launch events then
+// time the device, not the host's submission.
+__global__ void k_delay(int us)
+{
+    for (int i = 0; i < us; ++i) __nanosleep(1000);
+}
+
+int mf_time_apply_launches(const MfPlan *P, const MfFactor *M, int reps, size_t flush_bytes,
+                           cudaStream_t s, double *ms, int *codes, int cap, int *n)
+{
+    if (M->coop_grid > 0) {
+        set_error("LU solve timing: per-launch timing needs the per-level launches");
+        return V2D_EARG;
+    }
+    const size_t es = M->fp32 ? sizeof(float) : sizeof(double);
+    DevBuf<char> buf;
+    V2D_TRY(buf.alloc(2 * P->n * es + flush_bytes + 256, s));
+    V2D_CUDA_TRY(cudaMemsetAsync(buf.p, 0, 2 * P->n * es, s));
+    char *fl = buf.p + 2 * P->n * es;
+    std::vector<cudaEvent_t> ev(cap + 1, nullptr);
+    int st = V2D_OK;
+    for (auto &e : ev)
+        if (st == V2D_OK && cudaEventCreate(&e) != cudaSuccess) st = V2D_ECUDA;
+    std::vector<double> acc(cap, 0.0);
+    long long nl = 0;
+    for (int r = 0; r < reps && st == V2D_OK; ++r) {
+        if (flush_bytes) cudaMemsetAsync(fl, r & 0xff, flush_bytes, s);
+        k_delay<<<1, 32, 0, s>>>(300);
+        cudaEventRecord(ev[0], s);
+        st = M->fp32 ? apply_launches<float>(P, M, (const float *)buf.p,
+                                             (float *)(buf.p + P->n * es), nullptr, nullptr, s,
+                                             &nl, ev.data() + 1, codes, cap)
+                     : apply_launches<double>(P, M, (const double *)buf.p,
+                                              (double *)(buf.p + P->n * es), nullptr, nullptr,
+                                              s, &nl, ev.data() + 1, codes, cap);
+        if (st == V2D_OK && cudaEventSynchronize(ev[nl]) != cudaSuccess) st = V2D_ECUDA;
+        for (long long k = 0; k < nl && st == V2D_OK; ++k) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+            acc[k] += t;
+        }
+    }
+    for (auto &e : ev)
+        if (e) cudaEventDestroy(e);
+    if (st != V2D_OK) return st;
+    for (long long k = 0; k < nl; ++k) ms[k] = acc[k] / reps;
+    *n = (int)nl;
+    return V2D_OK;
+}
+
+int mf_time_factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, const double *val,
+                            int reps, cudaStream_t s, double *ms, int *codes, int cap, int *n)
+{
+    std::vector<cudaEvent_t> ev(cap + 1, nullptr);
+    int st = V2D_OK;
+    for (auto &e : ev)
+        if (st == V2D_OK && cudaEventCreate(&e) != cudaSuccess) st = V2D_ECUDA;
+    std::vector<double> acc(cap, 0.0);
+    int nl = 0;
+    for (int r = 0; r < reps && st == V2D_OK; ++r) {
+        k_delay<<<1, 32, 0, s>>>(2000);
+        cudaEventRecord(ev[0], s);
+        st = M->fp32 ? factor_launches<float>(P, M, rowptr, val, s, ev.data() + 1, codes, cap, &nl)
+                     : factor_launches<double>(P, M, rowptr, val, s, ev.data() + 1, codes, cap,
+                                               &nl);
+        if (st == V2D_OK && cudaEventSynchronize(ev[nl]) != cudaSuccess) st = V2D_ECUDA;
+        for (int k = 0; k < nl && st == V2D_OK; ++k) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+            acc[k] += t;
+        }
+    }
+    for (auto &e : ev)
+        if (e) cudaEventDestroy(e);
+    if (st != V2D_OK) return st;
+    for (int k = 0; k < nl; ++k) ms[k] = acc[k] / reps;
+    *n = nl;
     return V2D_OK;
 }
 

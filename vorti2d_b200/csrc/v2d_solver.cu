@@ -769,6 +769,34 @@ extern "C" int v2d_solver_time_lu_apply(v2d_solver *S, int reps, long long flush
     return mf_time_apply(S->plan, S->lu[q], reps, (size_t)flush_bytes, S->s, ms_avg);
 }
 
+extern "C" int v2d_solver_time_lu_launches(v2d_solver *S, int reps, long long flush_bytes,
+                                           double *ms, int *codes, int cap, int *n)
+{
+    V2D_ARG_CHECK(S && ms && codes && n && reps > 0 && flush_bytes >= 0 && cap > 0,
+                  "time_lu_launches: bad arguments");
+    V2D_ARG_CHECK(S->prm.krylov.precond == V2D_PC_LU && S->plan,
+                  "time_lu_launches: the handle does not use the LU preconditioner");
+    const int q = S->prm.krylov.precision == V2D_PREC_MIXED ? 1 : 0;
+    V2D_ARG_CHECK(S->lu[q] && S->lu_ready,
+                  "time_lu_launches: no current factors (run a Newton iteration first)");
+    return mf_time_apply_launches(S->plan, S->lu[q], reps, (size_t)flush_bytes, S->s, ms, codes,
+                                  cap, n);
+}
+
+extern "C" int v2d_solver_time_lu_factor(v2d_solver *S, int reps, double *ms, int *codes, int cap,
+                                         int *n)
+{
+    V2D_ARG_CHECK(S && ms && codes && n && reps > 0 && cap > 0,
+                  "time_lu_factor: bad arguments");
+    V2D_ARG_CHECK(S->prm.krylov.precond == V2D_PC_LU && S->plan,
+                  "time_lu_factor: the handle does not use the LU preconditioner");
+    const int q = S->prm.krylov.precision == V2D_PREC_MIXED ? 1 : 0;
+    V2D_ARG_CHECK(S->lu[q] && S->lu_ready,
+                  "time_lu_factor: no current factors (run a Newton iteration first)");
+    return mf_time_factor_launches(S->plan, S->lu[q], S->g.rowptr, S->g.val, reps, S->s, ms,
+                                   codes, cap, n);
+}
+
 // Kernel timing (no reference counterpart): average ms of `reps` launches of
 // one kernel of the Newton iteration on the handle's current data, each after
 // a write of flush_bytes (evicts L2).
