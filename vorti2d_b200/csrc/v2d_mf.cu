@@ -517,7 +517,6 @@ namespace v2d {
 namespace {
 
 constexpr int kMfThreads = 256;
-constexpr int kTrsmCols = 32;
 constexpr int kGemmTile = 64;
 
 template <class T> struct PanelWidth;
@@ -574,23 +573,17 @@ __global__ void k_extend_add(int q0, int slot, const int *__restrict__ S, const 
 // sequence (ipiv) and the block's part of the row permutation; the row scaling applied at
 // assembly keeps the pivots meaningful and the FP64 Krylov iteration around
 // the factors absorbs the weaker pivoting.  The rows below the block (fully
-// summed and contribution rows alike) get their L entries from k_l21.
+// summed and contribution rows alike) get their L entries from l21_rows.
+// k_panel factors a level's first panel; every later panel is factored by
+// the trailing update of the panel before it (k_gemm).
 template <class T>
-__global__ void __launch_bounds__(kMfThreads) k_panel(int q0, int k, const int *__restrict__ S_,
-                                                      const int *__restrict__ f_,
-                                                      const long long *__restrict__ foff,
-                                                      const int *__restrict__ voff, T *F,
-                                                      int *ipiv, int *perm, int *flag)
+__device__ __forceinline__ void panel_factor(T *A, int f, int S, int k, int vo, int *ipiv,
+                                             int *perm, int *flag,
+                                             T (*U)[PanelWidth<T>::v + 1], int *pv)
 {
     constexpr int NB = PanelWidth<T>::v;
-    __shared__ T U[NB][NB + 1];
-    const int q = q0 + blockIdx.x;
-    const int S = S_[q], f = f_[q];
-    if (S <= k) return;
     const int w = min(NB, S - k);
-    T *A = F + foff[q];
     const int tid = threadIdx.x, lane = tid & 31;
-    __shared__ int pv[NB];
     for (int e = tid; e < NB * NB; e += blockDim.x) {
         const int r = e / NB, c = e - r * NB;
         U[r][c] = (r < w && c < w) ? A[(long long)(k + r) * f + k + c] : T(0);
@@ -619,7 +612,7 @@ __global__ void __launch_bounds__(kMfThreads) k_panel(int q0, int k, const int *
                 bad = 1;
             }
             if (lane == 0) {
-                ipiv[voff[q] + k + c] = k + p;
+                ipiv[vo + k + c] = k + p;
                 const int t = pv[c];
                 pv[c] = pv[p];
                 pv[p] = t;
@@ -642,7 +635,7 @@ __global__ void __launch_bounds__(kMfThreads) k_panel(int q0, int k, const int *
         if (bad && lane == 0) atomicOr(flag, 1);
         // row i of the factored front came from local row perm[i]; the swaps
         // stay inside the panel's rows, so the panel fixes its own entries
-        if (lane < w) perm[voff[q] + k + lane] = k + pv[lane];
+        if (lane < w) perm[vo + k + lane] = k + pv[lane];
     }
     __syncthreads();
     for (int e = tid; e < w * w; e += blockDim.x) {
@@ -651,25 +644,35 @@ __global__ void __launch_bounds__(kMfThreads) k_panel(int q0, int k, const int *
     }
 }
 
+template <class T>
+__global__ void __launch_bounds__(kMfThreads) k_panel(int q0, int k, const int *__restrict__ S_,
+                                                      const int *__restrict__ f_,
+                                                      const long long *__restrict__ foff,
+                                                      const int *__restrict__ voff, T *F,
+                                                      int *ipiv, int *perm, int *flag)
+{
+    constexpr int NB = PanelWidth<T>::v;
+    __shared__ T U[NB][NB + 1];
+    __shared__ int pv[NB];
+    const int q = q0 + blockIdx.x;
+    const int S = S_[q], f = f_[q];
+    if (S <= k) return;
+    panel_factor<T>(F + foff[q], f, S, k, voff[q], ipiv, perm, flag, U, pv);
+}
+
 // L entries of the panel for the rows below its diagonal block: x U = a with
 // U the upper triangle of the factored block (no pivoting outside the block).
 // Grid: (chunks of kL21Rows rows, fronts); one thread per row.
 constexpr int kL21Rows = 64;
 
 template <class T>
-__global__ void __launch_bounds__(kL21Rows) k_l21(int q0, int k, const int *__restrict__ S_,
-                                                  const int *__restrict__ f_,
-                                                  const long long *__restrict__ foff, T *F)
+__device__ __forceinline__ void l21_rows(T *A, int f, int S, int k, int chunk,
+                                         T (*U)[PanelWidth<T>::v + 1])
 {
     constexpr int NB = PanelWidth<T>::v;
-    __shared__ T U[NB][NB + 1];
-    const int q = q0 + blockIdx.y;
-    const int S = S_[q], f = f_[q];
-    if (S <= k) return;
     const int w = min(NB, S - k);
-    const int rbeg = k + w + blockIdx.x * kL21Rows;
+    const int rbeg = k + w + chunk * kL21Rows;
     if (rbeg >= f) return;
-    T *A = F + foff[q];
     for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
         const int r = e / NB, c = e - r * NB;
         U[r][c] = (r < w && c < w) ? A[(long long)(k + r) * f + k + c] : T(0);
@@ -699,20 +702,12 @@ __global__ void __launch_bounds__(kL21Rows) k_l21(int q0, int k, const int *__re
 // thread per column: the w entries are gathered through the block
 // permutation into registers, solved and written back.
 template <class T>
-__global__ void __launch_bounds__(kTrsmCols) k_swap_trsm(int q0, int k, const int *__restrict__ S_,
-                                                         const int *__restrict__ f_,
-                                                         const long long *__restrict__ foff,
-                                                         const int *__restrict__ voff,
-                                                         T *F, const int *__restrict__ ipiv)
+__device__ __forceinline__ void swap_trsm_cols(T *A, int f, int S, int k, int vo, int chunk,
+                                               const int *__restrict__ ipiv,
+                                               T (*Ld)[PanelWidth<T>::v + 1], int *src)
 {
     constexpr int NB = PanelWidth<T>::v;
-    __shared__ T Ld[NB][NB + 1];
-    __shared__ int src[NB];
-    const int q = q0 + blockIdx.y;
-    const int S = S_[q], f = f_[q];
-    if (S <= k) return;
     const int w = min(NB, S - k);
-    T *A = F + foff[q];
     for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
         const int r = e / NB, c = e - r * NB;
         Ld[r][c] = (r < w && c < w) ? A[(long long)(k + r) * f + k + c] : T(0);
@@ -721,14 +716,14 @@ __global__ void __launch_bounds__(kTrsmCols) k_swap_trsm(int q0, int k, const in
         // new row t of the block = old row src[t]
         for (int t = 0; t < NB; ++t) src[t] = t;
         for (int t = 0; t < w; ++t) {
-            const int p = ipiv[voff[q] + k + t] - k;
+            const int p = ipiv[vo + k + t] - k;
             const int u = src[t];
             src[t] = src[p];
             src[p] = u;
         }
     }
     __syncthreads();
-    const int col = blockIdx.x * kTrsmCols + threadIdx.x;
+    const int col = chunk * blockDim.x + threadIdx.x;
     if (col >= f || (col >= k && col < k + w)) return;
     T x[NB];
 #pragma unroll
@@ -747,15 +742,49 @@ __global__ void __launch_bounds__(kTrsmCols) k_swap_trsm(int q0, int k, const in
         if (t < w) A[(long long)(k + t) * f + col] = x[t];
 }
 
+// Both panel steps that only read the factored diagonal block, in one launch:
+// blocks [0, nl) compute L21 for kL21Rows rows each, blocks [nl, gridDim.x)
+// apply the row swaps and U12 for kL21Rows columns each.  The two write
+// disjoint parts of the front (rows below the block in its columns; the
+// block's rows outside its columns) and read neither's output.
+template <class T>
+__global__ void __launch_bounds__(kL21Rows) k_l21_trsm(int q0, int k, int nl,
+                                                       const int *__restrict__ S_,
+                                                       const int *__restrict__ f_,
+                                                       const long long *__restrict__ foff,
+                                                       const int *__restrict__ voff, T *F,
+                                                       const int *__restrict__ ipiv)
+{
+    constexpr int NB = PanelWidth<T>::v;
+    __shared__ T D[NB][NB + 1];
+    __shared__ int src[NB];
+    const int q = q0 + blockIdx.y;
+    const int S = S_[q], f = f_[q];
+    if (S <= k) return;
+    T *A = F + foff[q];
+    if ((int)blockIdx.x < nl)
+        l21_rows<T>(A, f, S, k, blockIdx.x, D);
+    else
+        swap_trsm_cols<T>(A, f, S, k, voff[q], blockIdx.x - nl, ipiv, D, src);
+}
+
 // Trailing update A22 -= L21 U12 over rows/cols [k+w, f), 64x64 tiles.
+// The next panel's diagonal block, rows and columns [k+w, k+w+w'), lies in
+// tile (0, 0), and no other tile reads or writes it: so the CTA of that tile
+// factors the next panel right after its own update (panel_factor), which
+// saves the next step's panel launch.
 template <class T>
 __global__ void __launch_bounds__(256) k_gemm(int q0, int k, const int *__restrict__ S_,
                                               const int *__restrict__ f_,
-                                              const long long *__restrict__ foff, T *F)
+                                              const long long *__restrict__ foff,
+                                              const int *__restrict__ voff, T *F, int *ipiv,
+                                              int *perm, int *flag)
 {
     constexpr int NB = PanelWidth<T>::v;
     __shared__ T As[NB][kGemmTile + 1];
     __shared__ T Bs[NB][kGemmTile];
+    __shared__ T U[NB][NB + 1];
+    __shared__ int pv[NB];
     const int q = q0 + blockIdx.y;
     const int S = S_[q], f = f_[q];
     if (S <= k) return;
@@ -806,6 +835,10 @@ __global__ void __launch_bounds__(256) k_gemm(int q0, int k, const int *__restri
             const int c = c0 + tx + 16 * b;
             if (c < f) A[(long long)r * f + c] -= acc[a][b];
         }
+    }
+    if (blockIdx.x == 0 && S > base) {
+        __syncthreads();   // the tile's updated entries are visible to the block
+        panel_factor<T>(A, f, S, base, voff[q], ipiv, perm, flag, U, pv);
     }
 }
 
@@ -1520,8 +1553,8 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
     T *F = (T *)M->F;
     long long launches = 0;
     // with ev: an event is recorded after each kernel (kind * 1000 + level;
-    // kinds 0 rowscale, 1 scatter, 2 extend_add, 3 panel, 4 l21, 5 swap_trsm,
-    // 6 gemm, 7 trinv, 8 trcopy)
+    // kinds 0 rowscale, 1 scatter, 2 extend_add, 3 first panel, 4 L21 + row
+    // swaps + U12, 6 trailing update + next panel, 7 trinv, 8 trcopy)
     int nev = 0;
     auto mark = [&](int code) -> int {
         if (!ev) return V2D_OK;
@@ -1562,22 +1595,26 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
         }
         const int maxf = P->lvl_maxf[L];
         for (int k = 0; k < P->lvl_maxS[L]; k += NB) {
-            k_panel<T><<<nq, kMfThreads, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff, P->d_voff, F,
-                                                 M->ipiv, M->perm, M->flag);
-            V2D_TRY(mark(3000 + L));
+            if (k == 0) {   // later panels are factored by the previous trailing update
+                k_panel<T><<<nq, kMfThreads, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff, P->d_voff,
+                                                     F, M->ipiv, M->perm, M->flag);
+                V2D_TRY(mark(3000 + L));
+                ++launches;
+            }
             const int below = std::max(1, maxf - k - 1);
-            k_l21<T><<<dim3((below + kL21Rows - 1) / kL21Rows, nq), kL21Rows, 0, s>>>(
-                q0, k, P->d_S, P->d_f, P->d_foff, F);
+            const int nl = (below + kL21Rows - 1) / kL21Rows;
+            const int ncol = (maxf + kL21Rows - 1) / kL21Rows;
+            k_l21_trsm<T><<<dim3(nl + ncol, nq), kL21Rows, 0, s>>>(q0, k, nl, P->d_S, P->d_f,
+                                                                   P->d_foff, P->d_voff, F,
+                                                                   M->ipiv);
             V2D_TRY(mark(4000 + L));
-            const int gcol = (maxf + kTrsmCols - 1) / kTrsmCols;
-            k_swap_trsm<T><<<dim3(gcol, nq), kTrsmCols, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff,
-                                                                P->d_voff, F, M->ipiv);
-            V2D_TRY(mark(5000 + L));
             const int rem = std::max(1, maxf - k - 1);
             const int nt = (rem + kGemmTile - 1) / kGemmTile;
-            k_gemm<T><<<dim3(nt * nt, nq), 256, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff, F);
+            k_gemm<T><<<dim3(nt * nt, nq), 256, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff,
+                                                        P->d_voff, F, M->ipiv, M->perm,
+                                                        M->flag);
             V2D_TRY(mark(6000 + L));
-            launches += 4;
+            launches += 2;
         }
         const int nbc = (P->lvl_maxS[L] + InvWidth<T>::v - 1) / InvWidth<T>::v;
         k_trinv<T><<<dim3(nbc, nq), kTrinvThreads,
