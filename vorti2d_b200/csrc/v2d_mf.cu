@@ -889,12 +889,20 @@ __global__ void __launch_bounds__(kTrinvThreads) k_trinv(int q0, const int *__re
             Dg[rr][cc] = (rr < bh && cc < bh) ? A[(long long)(r0 + rr) * f + r0 + cc] : T(0);
         }
         __syncthreads();
-        if (tid < CW) {   // diagonal block, one thread per column
-            for (int r = 1; r < bh; ++r) {
-                T v = Xs[(r0 + r) * CW + tid];
-                for (int t = 0; t < r; ++t) v -= Dg[r][t] * Xs[(r0 + t) * CW + tid];
-                Xs[(r0 + r) * CW + tid] = v;
+        if (tid < CW) {   // diagonal block, one thread per column, column in registers
+            T xr[32];
+#pragma unroll
+            for (int r = 0; r < 32; ++r) xr[r] = r < bh ? Xs[(r0 + r) * CW + tid] : T(0);
+#pragma unroll
+            for (int r = 1; r < 32; ++r) {
+                T v = xr[r];
+#pragma unroll
+                for (int t = 0; t < r; ++t) v -= Dg[r][t] * xr[t];
+                xr[r] = v;
             }
+#pragma unroll
+            for (int r = 1; r < 32; ++r)
+                if (r < bh) Xs[(r0 + r) * CW + tid] = xr[r];
         }
         __syncthreads();
         const int rows = S - r0 - bh;
@@ -937,13 +945,24 @@ __global__ void __launch_bounds__(kTrinvThreads) k_trinv(int q0, const int *__re
             Dg[rr][cc] = (rr < bh && cc < bh) ? A[(long long)(r0 + rr) * f + r0 + cc] : T(0);
         }
         __syncthreads();
-        if (tid < CW) {
-            for (int r = bh - 1; r >= 0; --r) {
-                T v = Xs[(r0 + r) * CW + tid];
-                for (int t = r + 1; t < bh; ++t) v -= Dg[r][t] * Xs[(r0 + t) * CW + tid];
-                const T d = Dg[r][r];
-                Xs[(r0 + r) * CW + tid] = d != T(0) ? v / d : T(0);
+        if (tid < CW) {   // column in registers
+            T xr[32];
+#pragma unroll
+            for (int r = 0; r < 32; ++r) xr[r] = r < bh ? Xs[(r0 + r) * CW + tid] : T(0);
+#pragma unroll
+            for (int r = 31; r >= 0; --r) {
+                if (r < bh) {
+                    T v = xr[r];
+#pragma unroll
+                    for (int t = r + 1; t < 32; ++t)
+                        if (t < bh) v -= Dg[r][t] * xr[t];
+                    const T d = Dg[r][r];
+                    xr[r] = d != T(0) ? v / d : T(0);
+                }
             }
+#pragma unroll
+            for (int r = 0; r < 32; ++r)
+                if (r < bh) Xs[(r0 + r) * CW + tid] = xr[r];
         }
         __syncthreads();
         for (int e = tid; e < r0 * 32; e += blockDim.x) {      // stage U[0..r0, r0..r0+32)
