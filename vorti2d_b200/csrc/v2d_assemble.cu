@@ -99,68 +99,103 @@ int build_pattern(GridDev &g, const AsmParams &p, cudaStream_t s)
     return V2D_OK;
 }
 
-// One thread per node: psi row K and ome row N+K.
+// One thread per node: psi row K and ome row N+K.  A block's 128 nodes own a
+// contiguous range of the value array for their psi rows and another for
+// their ome rows; each thread places its entries at their canonical slots in
+// a shared-memory copy of the range, and the block then writes the range with
+// coalesced stores (one row per thread would scatter every warp store over
+// 32 rows).
+constexpr int kAsmNodes = 128;
+
 template <bool W32>
-__global__ void __launch_bounds__(128) assemble_newton(GlobalTopo T, Coeffs c, Fields f,
-                                                       const int *__restrict__ rowptr,
-                                                       double *__restrict__ val,
-                                                       float *__restrict__ val32,
-                                                       double *__restrict__ b,
-                                                       double *__restrict__ dinv,
-                                                       float *__restrict__ dinv32, int *flag)
+__global__ void __launch_bounds__(kAsmNodes) assemble_newton(GlobalTopo T, Coeffs c, Fields f,
+                                                             const int *__restrict__ rowptr,
+                                                             double *__restrict__ val,
+                                                             float *__restrict__ val32,
+                                                             double *__restrict__ b,
+                                                             double *__restrict__ dinv,
+                                                             float *__restrict__ dinv32, int *flag)
 {
+    __shared__ double stage[kAsmNodes * kOmeMax];
     const int N = T.N;
-    V2D_GRID_STRIDE(t, N)
-    {
-        const int K = (int)t;
+    for (int K0 = blockIdx.x * kAsmNodes; K0 < N; K0 += gridDim.x * kAsmNodes) {
+        const int K = K0 + threadIdx.x;
+        const bool live = K < N;
+        const int K1 = min(K0 + kAsmNodes, N);
         int col[kOmeMax];
         double v[kOmeMax];
-        double bk;
+        double bk = 0.0;
         double a00 = 0, a01 = 0, a10 = 0, a11 = 0;
-        // psi row
-        int n = psi_row<true>(T, c, f, K, col, v, &bk);
-        int base = rowptr[K];
-#pragma unroll
-        for (int e = 0; e < kPsiMax; ++e) {
-            if (e < n) {
-                int slot = base + col_rank<kPsiMax>(col, n, e);
-                val[slot] = v[e];
-                if (W32) val32[slot] = (float)v[e];
-                if (col[e] == K) a00 += v[e];
-                if (col[e] == N + K) a01 += v[e];
+        // psi rows
+        const int pbeg = rowptr[K0], pend = rowptr[K1];
+        if (live) {
+            int n = psi_row<true>(T, c, f, K, col, v, &bk);
+            const int base = rowptr[K] - pbeg;
+            if (n != rowptr[K + 1] - rowptr[K]) {   // pattern out of date: write nothing
+                atomicOr(flag, 4);
+                n = 0;
             }
-        }
-        b[K] = bk;
-        // ome row
-        n = ome_row<true>(T, c, f, K, col, v, &bk);
-        base = rowptr[N + K];
 #pragma unroll
-        for (int e = 0; e < kOmeMax; ++e) {
-            if (e < n) {
-                int slot = base + col_rank<kOmeMax>(col, n, e);
-                val[slot] = v[e];
-                if (W32) val32[slot] = (float)v[e];
-                if (col[e] == K) a10 += v[e];
-                if (col[e] == N + K) a11 += v[e];
+            for (int e = 0; e < kPsiMax; ++e) {
+                if (e < n) {
+                    stage[base + col_rank<kPsiMax>(col, n, e)] = v[e];
+                    if (col[e] == K) a00 += v[e];
+                    if (col[e] == N + K) a01 += v[e];
+                }
             }
+            b[K] = bk;
         }
-        b[N + K] = bk;
-        // 2x2 block inverse for block Jacobi
-        double det = a00 * a11 - a01 * a10;
-        double i00, i01, i10, i11;
-        if (det != 0.0 && isfinite(det)) {
-            double r = 1.0 / det;
-            i00 = a11 * r; i01 = -a01 * r; i10 = -a10 * r; i11 = a00 * r;
-        } else {
-            i00 = i01 = i10 = i11 = 0.0;
-            atomicOr(flag, 1);
+        __syncthreads();
+        for (int e = threadIdx.x; e < pend - pbeg; e += kAsmNodes) {
+            const double x = stage[e];
+            val[pbeg + e] = x;
+            if (W32) val32[pbeg + e] = (float)x;
         }
-        dinv[K] = i00; dinv[N + K] = i01; dinv[2 * N + K] = i10; dinv[3 * N + K] = i11;
-        if (W32) {
-            dinv32[K] = (float)i00; dinv32[N + K] = (float)i01;
-            dinv32[2 * N + K] = (float)i10; dinv32[3 * N + K] = (float)i11;
+        __syncthreads();
+        // ome rows
+        const int obeg = rowptr[N + K0], oend = rowptr[N + K1];
+        if (live) {
+            int n = ome_row<true>(T, c, f, K, col, v, &bk);
+            const int base = rowptr[N + K] - obeg;
+            if (n != rowptr[N + K + 1] - rowptr[N + K]) {
+                atomicOr(flag, 4);
+                n = 0;
+            }
+#pragma unroll
+            for (int e = 0; e < kOmeMax; ++e) {
+                if (e < n) {
+                    stage[base + col_rank<kOmeMax>(col, n, e)] = v[e];
+                    if (col[e] == K) a10 += v[e];
+                    if (col[e] == N + K) a11 += v[e];
+                }
+            }
+            b[N + K] = bk;
         }
-        if (!isfinite(bk)) atomicOr(flag, 2);
+        __syncthreads();
+        for (int e = threadIdx.x; e < oend - obeg; e += kAsmNodes) {
+            const double x = stage[e];
+            val[obeg + e] = x;
+            if (W32) val32[obeg + e] = (float)x;
+        }
+        __syncthreads();
+        if (live) {
+            // 2x2 block inverse for block Jacobi
+            double det = a00 * a11 - a01 * a10;
+            double i00, i01, i10, i11;
+            if (det != 0.0 && isfinite(det)) {
+                double r = 1.0 / det;
+                i00 = a11 * r; i01 = -a01 * r; i10 = -a10 * r; i11 = a00 * r;
+            } else {
+                i00 = i01 = i10 = i11 = 0.0;
+                atomicOr(flag, 1);
+            }
+            dinv[K] = i00; dinv[N + K] = i01; dinv[2 * N + K] = i10; dinv[3 * N + K] = i11;
+            if (W32) {
+                dinv32[K] = (float)i00; dinv32[N + K] = (float)i01;
+                dinv32[2 * N + K] = (float)i10; dinv32[3 * N + K] = (float)i11;
+            }
+            if (!isfinite(bk)) atomicOr(flag, 2);
+        }
     }
 }
 
@@ -199,13 +234,13 @@ int launch_assemble(GridDev &g, const AsmParams &p, bool want32, int *d_flag, cu
     GlobalTopo T{g.imax, g.jmax, g.N};
     Coeffs c{p.re, p.invdtau, p.inv2dt, p.urot, g.dksi, g.deta, p.ca, p.sa, p.ff_bc};
     Fields f = fields_of(g);
-    int grid = grid_for(g.N, 128);
+    int grid = grid_for(g.N, kAsmNodes);
     if (want32)
-        assemble_newton<true><<<grid, 128, 0, s>>>(T, c, f, g.rowptr, g.val, g.val32, g.b, g.dinv,
-                                                   g.dinv32, d_flag);
+        assemble_newton<true><<<grid, kAsmNodes, 0, s>>>(T, c, f, g.rowptr, g.val, g.val32, g.b,
+                                                         g.dinv, g.dinv32, d_flag);
     else
-        assemble_newton<false><<<grid, 128, 0, s>>>(T, c, f, g.rowptr, g.val, g.val32, g.b,
-                                                    g.dinv, g.dinv32, d_flag);
+        assemble_newton<false><<<grid, kAsmNodes, 0, s>>>(T, c, f, g.rowptr, g.val, g.val32, g.b,
+                                                          g.dinv, g.dinv32, d_flag);
     V2D_CUDA_TRY(cudaGetLastError());
     count_launches(1);
     return V2D_OK;

@@ -176,6 +176,10 @@ int sync_flag(v2d_solver *S, const char *what)
     int f = 0;
     V2D_CUDA_TRY(cudaMemcpyAsync(&f, S->flag, sizeof(int), cudaMemcpyDeviceToHost, S->s));
     V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    if (f & 4) {
+        set_error("%s: a Jacobian row does not match the CSR pattern", what);
+        return V2D_ECUDA;
+    }
     if (f & 2) {
         set_error("%s: non-finite right-hand side (check the state / mesh)", what);
         return V2D_ENONFINITE;
