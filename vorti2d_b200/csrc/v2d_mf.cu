@@ -1039,6 +1039,33 @@ __device__ __forceinline__ T row_dot(const T *__restrict__ row, const T *v, int 
     return warp_sum((a0 + a1) + (a2 + a3));
 }
 
+// Four rows' dot products by one warp at once: row q's entries [b_q, e_q)
+// with v (an empty range for an absent row).  The four rows' loads are in
+// flight together, so a warp that works through many short rows (one CTA
+// per front) waits for one round trip per four rows instead of per row.
+template <class T>
+__device__ __forceinline__ void dot4(const T *p0, const T *p1, const T *p2, const T *p3, int b0,
+                                     int e0, int b1, int e1, int b2, int e2, int b3, int e3,
+                                     const T *v, T &s0, T &s1, T &s2, T &s3)
+{
+    const int lane = threadIdx.x & 31;
+    const int lo = min(min(b0, b1), min(b2, b3));
+    const int hi = max(max(e0, e1), max(e2, e3));
+    T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+#pragma unroll 4
+    for (int c = lo + lane; c < hi; c += 32) {
+        const T x = v[c];
+        if (c >= b0 && c < e0) a0 += p0[c] * x;
+        if (c >= b1 && c < e1) a1 += p1[c] * x;
+        if (c >= b2 && c < e2) a2 += p2[c] * x;
+        if (c >= b3 && c < e3) a3 += p3[c] * x;
+    }
+    s0 = warp_sum(a0);
+    s1 = warp_sum(a1);
+    s2 = warp_sum(a2);
+    s3 = warp_sum(a3);
+}
+
 // Forward, part 1 (one work item = one row chunk of one front): gather the
 // front's right-hand side w = rs .* b on the fully summed rows plus the
 // children's contribution vectors, permute the fully summed part, and compute
@@ -1217,14 +1244,33 @@ __global__ void __launch_bounds__(kSolveThreads2) k_fwd_front(int q0, const MfDe
     const int *perm = D.perm + vo;
     for (int i = tid; i < S; i += blockDim.x) t2[i] = w[perm[i]];
     __syncthreads();
-    for (int r = wid; r < S; r += nw) {            // z = Linv t2 (unit diagonal)
-        const T v = row_dot(A + (long long)r * f, t2, 0, r);
-        if (lane == 0) w[r] = t2[r] + v;
+    for (int r = wid; r < S; r += 4 * nw) {        // z = Linv t2 (unit diagonal)
+        int rr[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) rr[u] = r + u * nw < S ? r + u * nw : -1;
+        T v[4];
+        dot4<T>(A + (long long)max(rr[0], 0) * f, A + (long long)max(rr[1], 0) * f,
+                A + (long long)max(rr[2], 0) * f, A + (long long)max(rr[3], 0) * f, 0,
+                max(rr[0], 0), 0, max(rr[1], 0), 0, max(rr[2], 0), 0, max(rr[3], 0), t2, v[0],
+                v[1], v[2], v[3]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (lane == 0 && rr[u] >= 0) w[rr[u]] = t2[rr[u]] + v[u];
     }
     __syncthreads();
-    for (int r = S + wid; r < f; r += nw) {        // upd = w_CB - L21 z
-        const T v = row_dot(A + (long long)r * f, w, 0, S);
-        if (lane == 0) w[r] -= v;
+    for (int r = S + wid; r < f; r += 4 * nw) {    // upd = w_CB - L21 z
+        int rr[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) rr[u] = r + u * nw < f ? r + u * nw : -1;
+        T v[4];
+        dot4<T>(A + (long long)max(rr[0], 0) * f, A + (long long)max(rr[1], 0) * f,
+                A + (long long)max(rr[2], 0) * f, A + (long long)max(rr[3], 0) * f, 0,
+                rr[0] >= 0 ? S : 0, 0, rr[1] >= 0 ? S : 0, 0, rr[2] >= 0 ? S : 0, 0,
+                rr[3] >= 0 ? S : 0, w, v[0], v[1], v[2], v[3]);
+        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (lane == 0 && rr[u] >= 0) w[rr[u]] -= v[u];
     }
     __syncthreads();
     for (int i = tid; i < S; i += blockDim.x) zbuf[vo + i] = w[i];
@@ -1248,14 +1294,33 @@ __global__ void __launch_bounds__(kSolveThreads2) k_bwd_front(int q0, const MfDe
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
     for (int i = tid; i < m; i += blockDim.x) xs[i] = x[vars[S + i]];
     __syncthreads();
-    for (int r = wid; r < S; r += nw) {
-        const T v = m > 0 ? row_dot(A + (long long)r * f + S, xs, 0, m) : T(0);
-        if (lane == 0) y[r] = zbuf[vo + r] - v;
+    for (int r = wid; r < S; r += 4 * nw) {
+        int rr[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) rr[u] = r + u * nw < S ? r + u * nw : -1;
+        T v[4];
+        dot4<T>(A + (long long)max(rr[0], 0) * f + S, A + (long long)max(rr[1], 0) * f + S,
+                A + (long long)max(rr[2], 0) * f + S, A + (long long)max(rr[3], 0) * f + S, 0,
+                rr[0] >= 0 ? m : 0, 0, rr[1] >= 0 ? m : 0, 0, rr[2] >= 0 ? m : 0, 0,
+                rr[3] >= 0 ? m : 0, xs, v[0], v[1], v[2], v[3]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (lane == 0 && rr[u] >= 0) y[rr[u]] = zbuf[vo + rr[u]] - v[u];
     }
     __syncthreads();
-    for (int r = wid; r < S; r += nw) {            // x = Uinv y (upper incl. diagonal)
-        const T v = row_dot(A + (long long)r * f, y, r, S);
-        if (lane == 0) x[vars[r]] = v;
+    for (int r = wid; r < S; r += 4 * nw) {        // x = Uinv y (upper incl. diagonal)
+        int rr[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) rr[u] = r + u * nw < S ? r + u * nw : -1;
+        T v[4];
+        dot4<T>(A + (long long)max(rr[0], 0) * f, A + (long long)max(rr[1], 0) * f,
+                A + (long long)max(rr[2], 0) * f, A + (long long)max(rr[3], 0) * f,
+                rr[0] >= 0 ? rr[0] : 0, rr[0] >= 0 ? S : 0, rr[1] >= 0 ? rr[1] : 0,
+                rr[1] >= 0 ? S : 0, rr[2] >= 0 ? rr[2] : 0, rr[2] >= 0 ? S : 0,
+                rr[3] >= 0 ? rr[3] : 0, rr[3] >= 0 ? S : 0, y, v[0], v[1], v[2], v[3]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (lane == 0 && rr[u] >= 0) x[vars[rr[u]]] = v[u];
     }
 }
 
