@@ -74,6 +74,18 @@ def test_argument_errors_before_any_device_work(v2d):
     assert L.v2d_solver_create(181, 181, None, None, ctypes.byref(prm), ctypes.byref(h)) \
         == _lib.V2D_EARG
     assert L.v2d_solver_destroy(None) == 0
+    # handle-based entry points reject a null handle before any device work
+    n = ctypes.c_int()
+    ms = (ctypes.c_double * 4)()
+    codes = (ctypes.c_int * 4)()
+    b = (ctypes.c_double * 8)()
+    x = (ctypes.c_double * 4)()
+    assert L.v2d_solver_time_lu_launches(None, 1, 0, ms, codes, 4, ctypes.byref(n)) \
+        == _lib.V2D_EARG
+    assert L.v2d_solver_time_lu_factor(None, 1, ms, codes, 4, ctypes.byref(n)) == _lib.V2D_EARG
+    assert L.v2d_solver_residual_mesh(None, x, x, 40.0, 0.0, 0.0, 0.0, 1.0, 0.0, b, 0,
+                                      None) == _lib.V2D_EARG
+    assert "null" in _lib.last_error()
 
 
 def test_no_cpu_fallback(v2d, monkeypatch, tmp_path):
