@@ -1071,6 +1071,38 @@ __device__ __forceinline__ void dot4(const T *p0, const T *p1, const T *p2, cons
 // children's contribution vectors, permute the fully summed part, and compute
 // the chunk's rows of z = L11^-1 P w (unit diagonal).  Chunk 0 also stores w
 // on the contribution rows in the front's update vector for part 2.
+// Register staging of the per-level solve items: a row of up to kRowRegs * 32
+// entries is loaded into a warp's registers before the vectors it multiplies
+// are gathered, so the two loads overlap.  kGatherRegs entries per thread
+// bound the staged gathers (fronts beyond that take the plain loads).
+constexpr int kRowRegs = 16;
+constexpr int kGatherRegs = 4;
+
+template <class T>
+__device__ __forceinline__ void row_load(T (&reg)[kRowRegs], const T *row, int c0, int c1)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < kRowRegs; ++k) {
+        const int c = lane + 32 * k;
+        reg[k] = (c >= c0 && c < c1) ? row[c] : T(0);
+    }
+}
+
+template <class T>
+__device__ __forceinline__ T row_dot_reg(const T (&reg)[kRowRegs], const T *v, int c0, int c1)
+{
+    const int lane = threadIdx.x & 31;
+    T a0 = T(0), a1 = T(0);
+#pragma unroll
+    for (int k = 0; k < kRowRegs; k += 2) {
+        const int c = lane + 32 * k;
+        if (c >= c0 && c < c1) a0 += reg[k] * v[c];
+        if (c + 32 >= c0 && c + 32 < c1) a1 += reg[k + 1] * v[c + 32];
+    }
+    return warp_sum(a0 + a1);
+}
+
 template <class T>
 __device__ __forceinline__ void fz_item(const MfDev &D, const T *F, const T *b,
                                         const double *__restrict__ rs, T *zbuf, T *upd, int q,
@@ -1079,32 +1111,87 @@ __device__ __forceinline__ void fz_item(const MfDev &D, const T *F, const T *b,
     const int S = D.S[q], f = D.f[q], vo = D.voff[q];
     const int rbeg = chunk * kSolveRows;
     if (rbeg >= S && chunk != 0) return;
+    const int ch[2] = {D.child0[q], D.child1[q]};
     const T *A = F + D.foff[q];
     const int *vars = D.vars + vo;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    for (int p = tid; p < f; p += blockDim.x) w[p] = p < S ? (T)(rs[vars[p]] * (double)b[vars[p]]) : T(0);
-    __syncthreads();
-    for (int slot = 0; slot < 2; ++slot) {
-        const int c = slot == 0 ? D.child0[q] : D.child1[q];
-        if (c >= 0) {
-            const int m = D.f[c] - D.S[c];
-            const int *map = D.cbmap + D.uoff[c];
-            const T *u = upd + D.uoff[c];
-            for (int e = tid; e < m; e += blockDim.x) w[map[e]] += __ldcg(u + e);
+    const int *perm = D.perm + vo;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nt = blockDim.x;
+    // independent loads first: the children's sizes, the front's variable
+    // and permutation indices, and this warp's row of L11^-1
+    int m[2] = {0, 0}, uof[2] = {0, 0};
+#pragma unroll
+    for (int sl = 0; sl < 2; ++sl)
+        if (ch[sl] >= 0) {
+            m[sl] = D.f[ch[sl]] - D.S[ch[sl]];
+            uof[sl] = D.uoff[ch[sl]];
+        }
+    const int r = rbeg + wid;
+    const bool rowreg = r < S && r <= kRowRegs * 32;
+    T row[kRowRegs];
+    if (rowreg) row_load(row, A + (long long)r * f, 0, r);
+    const bool staged = f <= kGatherRegs * nt && m[0] <= kGatherRegs * nt &&
+                        m[1] <= kGatherRegs * nt;
+    if (staged) {
+        int vi[kGatherRegs], pi[kGatherRegs];
+#pragma unroll
+        for (int k = 0; k < kGatherRegs; ++k) {
+            const int p = tid + k * nt;
+            vi[k] = p < S ? vars[p] : -1;
+            pi[k] = p < S ? perm[p] : 0;
+        }
+        double rv[kGatherRegs];
+        T bv[kGatherRegs];
+        int mp[2][kGatherRegs];
+        T uv[2][kGatherRegs];
+#pragma unroll
+        for (int k = 0; k < kGatherRegs; ++k) {
+            rv[k] = vi[k] >= 0 ? rs[vi[k]] : 0.0;
+            bv[k] = vi[k] >= 0 ? b[vi[k]] : T(0);
+        }
+#pragma unroll
+        for (int sl = 0; sl < 2; ++sl)
+#pragma unroll
+            for (int k = 0; k < kGatherRegs; ++k) {
+                const int e = tid + k * nt;
+                mp[sl][k] = e < m[sl] ? D.cbmap[uof[sl] + e] : 0;
+                uv[sl][k] = e < m[sl] ? __ldcg(upd + uof[sl] + e) : T(0);
+            }
+#pragma unroll
+        for (int k = 0; k < kGatherRegs; ++k) {
+            const int p = tid + k * nt;
+            if (p < f) w[p] = p < S ? (T)(rv[k] * (double)bv[k]) : T(0);
         }
         __syncthreads();
+#pragma unroll
+        for (int sl = 0; sl < 2; ++sl) {
+#pragma unroll
+            for (int k = 0; k < kGatherRegs; ++k)
+                if (tid + k * nt < m[sl]) w[mp[sl][k]] += uv[sl][k];
+            __syncthreads();
+        }
+#pragma unroll
+        for (int k = 0; k < kGatherRegs; ++k)
+            if (tid + k * nt < S) t2[tid + k * nt] = w[pi[k]];
+        __syncthreads();
+    } else {
+        for (int p = tid; p < f; p += nt) w[p] = p < S ? (T)(rs[vars[p]] * (double)b[vars[p]]) : T(0);
+        __syncthreads();
+        for (int sl = 0; sl < 2; ++sl) {
+            const int *map = D.cbmap + uof[sl];
+            const T *u = upd + uof[sl];
+            for (int e = tid; e < m[sl]; e += nt) w[map[e]] += __ldcg(u + e);
+            __syncthreads();
+        }
+        for (int i = tid; i < S; i += nt) t2[i] = w[perm[i]];
+        __syncthreads();
     }
-    const int *perm = D.perm + vo;
-    for (int i = tid; i < S; i += blockDim.x) t2[i] = w[perm[i]];
-    __syncthreads();
-    const int r = rbeg + wid;
     if (r < S) {
-        const T v = row_dot(A + (long long)r * f, t2, 0, r);
+        const T v = rowreg ? row_dot_reg(row, t2, 0, r) : row_dot(A + (long long)r * f, t2, 0, r);
         if (lane == 0) zbuf[vo + r] = t2[r] + v;
     }
     if (chunk == 0) {
         T *uo = upd + D.uoff[q];
-        for (int i = tid; i < f - S; i += blockDim.x) uo[i] = w[S + i];
+        for (int i = tid; i < f - S; i += nt) uo[i] = w[S + i];
     }
 }
 
@@ -1119,11 +1206,14 @@ __device__ __forceinline__ void fu_item(const MfDev &D, const T *F, const T *zbu
     if (rbeg >= m) return;
     const T *A = F + D.foff[q];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    for (int i = tid; i < S; i += blockDim.x) z[i] = __ldcg(zbuf + vo + i);
-    __syncthreads();
     const int i = rbeg + wid;
+    const bool rowreg = i < m && S <= kRowRegs * 32;
+    T row[kRowRegs];
+    if (rowreg) row_load(row, A + (long long)(S + i) * f, 0, S);
+    for (int j = tid; j < S; j += blockDim.x) z[j] = __ldcg(zbuf + vo + j);
+    __syncthreads();
     if (i < m) {
-        const T v = row_dot(A + (long long)(S + i) * f, z, 0, S);
+        const T v = rowreg ? row_dot_reg(row, z, 0, S) : row_dot(A + (long long)(S + i) * f, z, 0, S);
         T *u = upd + D.uoff[q] + i;
         if (lane == 0) *u = __ldcg(u) - v;
     }
@@ -1140,11 +1230,14 @@ __device__ __forceinline__ void by_item(const MfDev &D, const T *F, T *zbuf, con
     const T *A = F + D.foff[q];
     const int *vars = D.vars + vo;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int r = rbeg + wid;
+    const bool rowreg = r < S && m <= kRowRegs * 32;
+    T row[kRowRegs];
+    if (rowreg) row_load(row, A + (long long)r * f + S, 0, m);
     for (int i = tid; i < m; i += blockDim.x) xs[i] = __ldcg(x + vars[S + i]);
     __syncthreads();
-    const int r = rbeg + wid;
     if (r < S) {
-        const T v = row_dot(A + (long long)r * f + S, xs, 0, m);
+        const T v = rowreg ? row_dot_reg(row, xs, 0, m) : row_dot(A + (long long)r * f + S, xs, 0, m);
         if (lane == 0) zbuf[vo + r] = __ldcg(zbuf + vo + r) - v;
     }
 }
@@ -1159,11 +1252,14 @@ __device__ __forceinline__ void bx_item(const MfDev &D, const T *F, const T *zbu
     if (rbeg >= S) return;
     const T *A = F + D.foff[q];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int r = rbeg + wid;
+    const bool rowreg = r < S && S <= kRowRegs * 32;
+    T row[kRowRegs];
+    if (rowreg) row_load(row, A + (long long)r * f, r, S);
     for (int i = tid; i < S; i += blockDim.x) y[i] = __ldcg(zbuf + vo + i);
     __syncthreads();
-    const int r = rbeg + wid;
     if (r < S) {
-        const T v = row_dot(A + (long long)r * f, y, r, S);
+        const T v = rowreg ? row_dot_reg(row, y, r, S) : row_dot(A + (long long)r * f, y, r, S);
         if (lane == 0) x[D.vars[vo + r]] = v;
     }
 }
