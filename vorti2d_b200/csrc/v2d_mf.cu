@@ -884,9 +884,16 @@ __global__ void __launch_bounds__(kTrinvThreads) k_trinv(int q0, const int *__re
     __syncthreads();
     for (int r0 = (c0 / 32) * 32; r0 < S; r0 += 32) {
         const int bh = min(32, S - r0);
+        // the diagonal block and the L panel below it do not depend on each
+        // other: load both in one phase
+        const int rows = S - r0 - bh;
         for (int e = tid; e < 1024; e += blockDim.x) {
             const int rr = e >> 5, cc = e & 31;
             Dg[rr][cc] = (rr < bh && cc < bh) ? A[(long long)(r0 + rr) * f + r0 + cc] : T(0);
+        }
+        for (int e = tid; e < rows * 32; e += blockDim.x) {    // stage L[r0+bh.., r0..r0+32)
+            const int rr = e >> 5, t = e & 31;
+            Lp[rr * 33 + t] = t < bh ? A[(long long)(r0 + bh + rr) * f + r0 + t] : T(0);
         }
         __syncthreads();
         if (tid < CW) {   // diagonal block, one thread per column, column in registers
@@ -903,12 +910,6 @@ __global__ void __launch_bounds__(kTrinvThreads) k_trinv(int q0, const int *__re
 #pragma unroll
             for (int r = 1; r < 32; ++r)
                 if (r < bh) Xs[(r0 + r) * CW + tid] = xr[r];
-        }
-        __syncthreads();
-        const int rows = S - r0 - bh;
-        for (int e = tid; e < rows * 32; e += blockDim.x) {    // stage L[r0+bh.., r0..r0+32)
-            const int rr = e >> 5, t = e & 31;
-            Lp[rr * 33 + t] = t < bh ? A[(long long)(r0 + bh + rr) * f + r0 + t] : T(0);
         }
         __syncthreads();
         for (int e = tid; e < rows * CW; e += blockDim.x) {   // rank-bh update below
@@ -944,6 +945,10 @@ __global__ void __launch_bounds__(kTrinvThreads) k_trinv(int q0, const int *__re
             const int rr = e >> 5, cc = e & 31;
             Dg[rr][cc] = (rr < bh && cc < bh) ? A[(long long)(r0 + rr) * f + r0 + cc] : T(0);
         }
+        for (int e = tid; e < r0 * 32; e += blockDim.x) {      // stage U[0..r0, r0..r0+32)
+            const int rr = e >> 5, t = e & 31;
+            Lp[rr * 33 + t] = t < bh ? A[(long long)rr * f + r0 + t] : T(0);
+        }
         __syncthreads();
         if (tid < CW) {   // column in registers
             T xr[32];
@@ -963,11 +968,6 @@ __global__ void __launch_bounds__(kTrinvThreads) k_trinv(int q0, const int *__re
 #pragma unroll
             for (int r = 0; r < 32; ++r)
                 if (r < bh) Xs[(r0 + r) * CW + tid] = xr[r];
-        }
-        __syncthreads();
-        for (int e = tid; e < r0 * 32; e += blockDim.x) {      // stage U[0..r0, r0..r0+32)
-            const int rr = e >> 5, t = e & 31;
-            Lp[rr * 33 + t] = t < bh ? A[(long long)rr * f + r0 + t] : T(0);
         }
         __syncthreads();
         for (int e = tid; e < r0 * CW; e += blockDim.x) {   // rank update above
@@ -1076,26 +1076,28 @@ __device__ __forceinline__ void dot4(const T *p0, const T *p1, const T *p2, cons
 // are gathered, so the two loads overlap.  kGatherRegs entries per thread
 // bound the staged gathers (fronts beyond that take the plain loads).
 constexpr int kRowRegs = 16;
+constexpr int kRowRegsCB = 24;   // the contribution part of a row (U12) is longer
 constexpr int kGatherRegs = 4;
 
-template <class T>
-__device__ __forceinline__ void row_load(T (&reg)[kRowRegs], const T *row, int c0, int c1)
+template <class T, int R>
+__device__ __forceinline__ void row_load(T (&reg)[R], const T *row, int c0, int c1)
 {
     const int lane = threadIdx.x & 31;
 #pragma unroll
-    for (int k = 0; k < kRowRegs; ++k) {
+    for (int k = 0; k < R; ++k) {
         const int c = lane + 32 * k;
         reg[k] = (c >= c0 && c < c1) ? row[c] : T(0);
     }
 }
 
-template <class T>
-__device__ __forceinline__ T row_dot_reg(const T (&reg)[kRowRegs], const T *v, int c0, int c1)
+template <class T, int R>
+__device__ __forceinline__ T row_dot_reg(const T (&reg)[R], const T *v, int c0, int c1)
 {
+    static_assert(R % 2 == 0, "row registers come in pairs");
     const int lane = threadIdx.x & 31;
     T a0 = T(0), a1 = T(0);
 #pragma unroll
-    for (int k = 0; k < kRowRegs; k += 2) {
+    for (int k = 0; k < R; k += 2) {
         const int c = lane + 32 * k;
         if (c >= c0 && c < c1) a0 += reg[k] * v[c];
         if (c + 32 >= c0 && c + 32 < c1) a1 += reg[k + 1] * v[c + 32];
@@ -1231,8 +1233,8 @@ __device__ __forceinline__ void by_item(const MfDev &D, const T *F, T *zbuf, con
     const int *vars = D.vars + vo;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int r = rbeg + wid;
-    const bool rowreg = r < S && m <= kRowRegs * 32;
-    T row[kRowRegs];
+    const bool rowreg = r < S && m <= kRowRegsCB * 32;
+    T row[kRowRegsCB];
     if (rowreg) row_load(row, A + (long long)r * f + S, 0, m);
     for (int i = tid; i < m; i += blockDim.x) xs[i] = __ldcg(x + vars[S + i]);
     __syncthreads();
