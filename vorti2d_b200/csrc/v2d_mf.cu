@@ -665,21 +665,13 @@ __global__ void __launch_bounds__(kMfThreads) k_panel(int q0, int k, const int *
 // Grid: (chunks of kL21Rows rows, fronts); one thread per row.
 constexpr int kL21Rows = 64;
 
+// L21 entries of row r: x U = a, U the upper triangle of the factored w x w
+// diagonal block (in shared memory).
 template <class T>
-__device__ __forceinline__ void l21_rows(T *A, int f, int S, int k, int chunk,
-                                         T (*U)[PanelWidth<T>::v + 1])
+__device__ __forceinline__ void l21_row(T *A, int f, int k, int w, int r,
+                                        const T (*U)[PanelWidth<T>::v + 1])
 {
     constexpr int NB = PanelWidth<T>::v;
-    const int w = min(NB, S - k);
-    const int rbeg = k + w + chunk * kL21Rows;
-    if (rbeg >= f) return;
-    for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
-        const int r = e / NB, c = e - r * NB;
-        U[r][c] = (r < w && c < w) ? A[(long long)(k + r) * f + k + c] : T(0);
-    }
-    __syncthreads();
-    const int r = rbeg + threadIdx.x;
-    if (r >= f) return;
     T x[NB];
     T *row = A + (long long)r * f + k;
 #pragma unroll
@@ -697,10 +689,53 @@ __device__ __forceinline__ void l21_rows(T *A, int f, int S, int k, int chunk,
         if (c < w) row[c] = x[c];
 }
 
+template <class T>
+__device__ __forceinline__ void l21_rows(T *A, int f, int S, int k, int chunk,
+                                         T (*U)[PanelWidth<T>::v + 1])
+{
+    constexpr int NB = PanelWidth<T>::v;
+    const int w = min(NB, S - k);
+    const int rbeg = k + w + chunk * kL21Rows;
+    if (rbeg >= f) return;
+    for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+        const int r = e / NB, c = e - r * NB;
+        U[r][c] = (r < w && c < w) ? A[(long long)(k + r) * f + k + c] : T(0);
+    }
+    __syncthreads();
+    const int r = rbeg + threadIdx.x;
+    if (r >= f) return;
+    l21_row<T>(A, f, k, w, r, U);
+}
+
 // The panel's row swaps (confined to its w rows) applied to every column
 // outside the panel, then U12 = L11^-1 A12 for the panel's block row.  One
 // thread per column: the w entries are gathered through the block
 // permutation into registers, solved and written back.
+// Column col outside the panel: the panel's row swaps (new row t = old row
+// src[t]) applied to its w entries, then U12 = L11^-1 A12 for col >= k + w.
+template <class T>
+__device__ __forceinline__ void swap_trsm_col(T *A, int f, int k, int w, int col,
+                                              const T (*Ld)[PanelWidth<T>::v + 1],
+                                              const int *src)
+{
+    constexpr int NB = PanelWidth<T>::v;
+    T x[NB];
+#pragma unroll
+    for (int t = 0; t < NB; ++t) x[t] = t < w ? A[(long long)(k + src[t]) * f + col] : T(0);
+    if (col >= k + w) {
+#pragma unroll
+        for (int t = 1; t < NB; ++t) {
+            T s = x[t];
+#pragma unroll
+            for (int u = 0; u < t; ++u) s -= Ld[t][u] * x[u];
+            x[t] = s;
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < NB; ++t)
+        if (t < w) A[(long long)(k + t) * f + col] = x[t];
+}
+
 template <class T>
 __device__ __forceinline__ void swap_trsm_cols(T *A, int f, int S, int k, int vo, int chunk,
                                                const int *__restrict__ ipiv,
@@ -725,21 +760,7 @@ __device__ __forceinline__ void swap_trsm_cols(T *A, int f, int S, int k, int vo
     __syncthreads();
     const int col = chunk * blockDim.x + threadIdx.x;
     if (col >= f || (col >= k && col < k + w)) return;
-    T x[NB];
-#pragma unroll
-    for (int t = 0; t < NB; ++t) x[t] = t < w ? A[(long long)(k + src[t]) * f + col] : T(0);
-    if (col >= k + w) {
-#pragma unroll
-        for (int t = 1; t < NB; ++t) {
-            T s = x[t];
-#pragma unroll
-            for (int u = 0; u < t; ++u) s -= Ld[t][u] * x[u];
-            x[t] = s;
-        }
-    }
-#pragma unroll
-    for (int t = 0; t < NB; ++t)
-        if (t < w) A[(long long)(k + t) * f + col] = x[t];
+    swap_trsm_col<T>(A, f, k, w, col, Ld, src);
 }
 
 // Both panel steps that only read the factored diagonal block, in one launch:
@@ -768,34 +789,15 @@ __global__ void __launch_bounds__(kL21Rows) k_l21_trsm(int q0, int k, int nl,
         swap_trsm_cols<T>(A, f, S, k, voff[q], blockIdx.x - nl, ipiv, D, src);
 }
 
-// Trailing update A22 -= L21 U12 over rows/cols [k+w, f), 64x64 tiles.
-// The next panel's diagonal block, rows and columns [k+w, k+w+w'), lies in
-// tile (0, 0), and no other tile reads or writes it: so the CTA of that tile
-// factors the next panel right after its own update (panel_factor), which
-// saves the next step's panel launch.
+// Tile (tr, tc) of the trailing update A22 -= L21 U12 (rows/cols from
+// base = k + w, 64 x 64, 256 threads with 4 x 4 outputs each).
 template <class T>
-__global__ void __launch_bounds__(256) k_gemm(int q0, int k, const int *__restrict__ S_,
-                                              const int *__restrict__ f_,
-                                              const long long *__restrict__ foff,
-                                              const int *__restrict__ voff, T *F, int *ipiv,
-                                              int *perm, int *flag)
+__device__ __forceinline__ void gemm_tile(T *A, int f, int k, int w, int tr, int tc,
+                                          T (*As)[kGemmTile + 1], T (*Bs)[kGemmTile])
 {
     constexpr int NB = PanelWidth<T>::v;
-    __shared__ T As[NB][kGemmTile + 1];
-    __shared__ T Bs[NB][kGemmTile];
-    __shared__ T U[NB][NB + 1];
-    __shared__ int pv[NB];
-    const int q = q0 + blockIdx.y;
-    const int S = S_[q], f = f_[q];
-    if (S <= k) return;
-    const int w = min(NB, S - k);
-    const int base = k + w, rem = f - base;
-    if (rem <= 0) return;
-    const int nt = (rem + kGemmTile - 1) / kGemmTile;
-    if ((int)blockIdx.x >= nt * nt) return;
-    const int tr = blockIdx.x / nt, tc = blockIdx.x - tr * nt;
+    const int base = k + w;
     const int r0 = base + tr * kGemmTile, c0 = base + tc * kGemmTile;
-    T *A = F + foff[q];
     const int tid = threadIdx.x;
     for (int e = tid; e < kGemmTile * NB; e += blockDim.x) {
         const int rr = e / NB, t = e - rr * NB;   // A tile: rows r0+rr, cols k+t
@@ -836,6 +838,35 @@ __global__ void __launch_bounds__(256) k_gemm(int q0, int k, const int *__restri
             if (c < f) A[(long long)r * f + c] -= acc[a][b];
         }
     }
+}
+
+// Trailing update A22 -= L21 U12 over rows/cols [k+w, f), 64x64 tiles.
+// The next panel's diagonal block, rows and columns [k+w, k+w+w'), lies in
+// tile (0, 0), and no other tile reads or writes it: so the CTA of that tile
+// factors the next panel right after its own update (panel_factor), which
+// saves the next step's panel launch.
+template <class T>
+__global__ void __launch_bounds__(256) k_gemm(int q0, int k, const int *__restrict__ S_,
+                                              const int *__restrict__ f_,
+                                              const long long *__restrict__ foff,
+                                              const int *__restrict__ voff, T *F, int *ipiv,
+                                              int *perm, int *flag)
+{
+    constexpr int NB = PanelWidth<T>::v;
+    __shared__ T As[NB][kGemmTile + 1];
+    __shared__ T Bs[NB][kGemmTile];
+    __shared__ T U[NB][NB + 1];
+    __shared__ int pv[NB];
+    const int q = q0 + blockIdx.y;
+    const int S = S_[q], f = f_[q];
+    if (S <= k) return;
+    const int w = min(NB, S - k);
+    const int base = k + w, rem = f - base;
+    if (rem <= 0) return;
+    const int nt = (rem + kGemmTile - 1) / kGemmTile;
+    if ((int)blockIdx.x >= nt * nt) return;
+    T *A = F + foff[q];
+    gemm_tile<T>(A, f, k, w, blockIdx.x / nt, blockIdx.x % nt, As, Bs);
     if (blockIdx.x == 0 && S > base) {
         __syncthreads();   // the tile's updated entries are visible to the block
         panel_factor<T>(A, f, S, base, voff[q], ipiv, perm, flag, U, pv);
@@ -856,25 +887,15 @@ template <class T> struct InvWidth;
 template <> struct InvWidth<float> { static constexpr int v = 32; };
 template <> struct InvWidth<double> { static constexpr int v = 16; };
 
+// Columns [c0, c0 + CW) of L11^-1 (unit lower) and U11^-1 of one front's
+// factored pivot block, into X (S x S, row-major); Xs (S x CW) and Lp (S x 33)
+// in shared memory, Dg a 32 x 33 shared tile.
 template <class T>
-__global__ void __launch_bounds__(kTrinvThreads) k_trinv(int q0, const int *__restrict__ S_,
-                                                         const long long *__restrict__ foff,
-                                                         const int *__restrict__ f_,
-                                                         const long long *__restrict__ toff,
-                                                         const T *__restrict__ F, T *tmp)
+__device__ __forceinline__ void trinv_colblock(const T *A, int S, int f, T *X, int c0, T *Xs,
+                                               T *Lp, T (*Dg)[33])
 {
     constexpr int CW = InvWidth<T>::v;
-    extern __shared__ unsigned char smem_raw[];
-    T *Xs = reinterpret_cast<T *>(smem_raw);    // S x CW
-    T *Lp = Xs + (size_t)S_[q0 + blockIdx.y] * CW;   // S x 33: the 32 columns of the current step
-    __shared__ T Dg[32][33];                     // current 32 x 32 diagonal block
-    const int q = q0 + blockIdx.y;
-    const int S = S_[q], f = f_[q];
-    const int c0 = blockIdx.x * CW;
-    if (c0 >= S) return;
     const int cw = min(CW, S - c0);
-    const T *A = F + foff[q];
-    T *X = tmp + toff[q];
     const int tid = threadIdx.x;
     // ---------------- L11^-1 (unit lower): rows [c0, S)
     for (int e = tid; e < S * CW; e += blockDim.x) {
@@ -988,6 +1009,25 @@ __global__ void __launch_bounds__(kTrinvThreads) k_trinv(int q0, const int *__re
         const int r = e / CW, cc = e - r * CW;
         if (cc < cw && r <= c0 + cc) X[(long long)r * S + c0 + cc] = Xs[e];
     }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kTrinvThreads) k_trinv(int q0, const int *__restrict__ S_,
+                                                         const long long *__restrict__ foff,
+                                                         const int *__restrict__ f_,
+                                                         const long long *__restrict__ toff,
+                                                         const T *__restrict__ F, T *tmp)
+{
+    constexpr int CW = InvWidth<T>::v;
+    extern __shared__ unsigned char smem_raw[];
+    T *Xs = reinterpret_cast<T *>(smem_raw);    // S x CW
+    T *Lp = Xs + (size_t)S_[q0 + blockIdx.y] * CW;   // S x 33: the 32 columns of the current step
+    __shared__ T Dg[32][33];                     // current 32 x 32 diagonal block
+    const int q = q0 + blockIdx.y;
+    const int S = S_[q], f = f_[q];
+    const int c0 = blockIdx.x * CW;
+    if (c0 >= S) return;
+    trinv_colblock<T>(F + foff[q], S, f, tmp + toff[q], c0, Xs, Lp, Dg);
 }
 
 // Inverted S x S blocks of the level's fronts: scratch -> factor storage.
@@ -1598,9 +1638,10 @@ __global__ void __launch_bounds__(kSolveThreads2) k_apply_all(const MfDev D, con
 // ------------------------------------------------------------ host drivers
 // The dynamic shared memory limit of a kernel (cudaFuncSetAttribute) holds
 // per function and device for the whole process, so every handle shares it:
-// it is only ever raised, to the largest size any handle launches with, and
-// left at the 48 KB default below that.  Setting it to one handle's smaller
-// size would make the launches of a handle with larger fronts fail.
+// it is only ever raised, to the largest size any handle launches with.
+// Setting it to one handle's smaller size would make the launches of a
+// handle with larger fronts fail.  Until it is set, a launch may use the
+// default 48 KB less the kernel's static shared memory.
 static cudaError_t raise_dyn_smem(const void *fn, size_t bytes)
 {
     static std::mutex mu;
@@ -1608,9 +1649,13 @@ static cudaError_t raise_dyn_smem(const void *fn, size_t bytes)
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
+    cudaFuncAttributes fa;
+    e = cudaFuncGetAttributes(&fa, fn);
+    if (e != cudaSuccess) return e;
+    const size_t room = fa.sharedSizeBytes < 48 * 1024 ? 48 * 1024 - fa.sharedSizeBytes : 0;
     std::lock_guard<std::mutex> lock(mu);
     size_t &cur = limit[{fn, dev}];
-    if (bytes <= std::max<size_t>(cur, 48 * 1024)) return cudaSuccess;
+    if (bytes <= std::max(cur, room)) return cudaSuccess;
     e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e == cudaSuccess) cur = bytes;
     return e;
@@ -1739,6 +1784,12 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
     // swaps + U12, 6 trailing update + next panel, 7 trinv, 8 trcopy)
     int nev = 0;
     auto mark = [&](int code) -> int {
+        const cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess) {
+            set_error("LU factor: launch of kind %d at level %d failed: %s", code / 1000,
+                      code % 1000, cudaGetErrorString(le));
+            return V2D_ECUDA;
+        }
         if (!ev) return V2D_OK;
         if (nev >= cap) {
             set_error("LU factor timing: more than %d launches", cap);
