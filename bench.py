@@ -532,7 +532,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
     ap.add_argument("--cpu-steps", type=int, default=2)
-    ap.add_argument("--lu-reuse", type=int, default=8,
+    ap.add_argument("--lu-reuse", type=int, default=12,
                     help="keep LU factors while GMRES needs at most this many iterations "
                          "(0: factor every Newton Jacobian)")
     ap.add_argument("--kernels-grid", type=int, default=2049,
