@@ -297,6 +297,19 @@ int v2d_solver_residual(v2d_solver *s, double re, double invdtau, double inv2dt,
 int v2d_solver_residual_mesh(v2d_solver *s, const double *xg, const double *yg, double re,
                              double invdtau, double inv2dt, double urot, double ca, double sa,
                              double *b, int met_rows, double *met);
+/* Mesh sensitivities for shape gradients (no reference counterpart), on the
+ * device: for each of the P = imax-1 wall nodes i and s = +1, -1, the
+ * handle's mesh with grid line i (and the seam line with i = 0) moved by
+ * s h (nx[i], ny[i]) phi[., i] (phi: N doubles, pointer order), its metrics,
+ * the right-hand side b_s = -R at the handle's state and the wall force
+ * coefficients (the 10 values of v2d_force_coeffs, ref_length <= 0: from the
+ * wall).  dots[i] = lambda . (b_+ - b_-); forces[(2 i + (s < 0)) * 10 + c].
+ * Host arrays: nx, ny (P), phi (N), lambda (2N), dots (P), forces (20 P). */
+int v2d_solver_shape_gradient(v2d_solver *s, const double *nx, const double *ny,
+                              const double *phi, const double *lambda, double h, double re,
+                              double invdtau, double inv2dt, double urot, double ca, double sa,
+                              double ref_length, double x0, double y0, double *dots,
+                              double *forces);
 /* Current system (after the last assembly): canonical CSR of the 2N system
  * and its right-hand side.  Sizes: 2N+1, nnz, nnz, 2N. */
 int v2d_solver_nnz(const v2d_solver *s, long long *nnz);

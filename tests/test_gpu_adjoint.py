@@ -208,3 +208,45 @@ def test_torch_autograd_shape(v2d, oracle_mod):
     assert d.grad is not None and d.grad.shape == (P,)
     assert np.allclose(d.grad.numpy(), want, rtol=1e-10, atol=1e-12 * np.abs(want).max())
     assert alpha.grad is not None and re.grad is not None
+
+
+def test_device_shape_gradient_equals_host_route(v2d, oracle_mod):
+    """The device loop over the 2P displaced meshes (v2d_solver_shape_gradient)
+    gives the same components as the host route through residual_on_mesh and
+    the wall force integral, for the seam node, an interior node and the last
+    node."""
+    from vorti2d_b200.adjoint import (_wall_forces, adjoint_solve, deform_ogrid,
+                                      deformation_weights, force_gradients, gaussian_bumps,
+                                      residual_on_mesh, shape_vjp, wall_normals)
+    base = oracle_mod.generate_cylinder(33, 25)
+    P = 32
+    d0 = gaussian_bumps(P, n_bumps=3, amplitude=1e-3, seed=5)
+    X, Y = deform_ogrid(*base, d0)
+    s = v2d.Solver(steady_cfg(v2d, RE, ADEG), mesh=(X, Y))
+    s.advance(0.0)
+    w = (0.3, 1.0, -0.2)
+    h = 1e-6
+    dev, _ = shape_vjp(s, w, base, h=h)
+    nx, ny = wall_normals(*base)
+    phi = deformation_weights(*base)
+    grads = force_gradients(s.imax, s.jmax, RE, s.dksi, s.deta, s.beta, s.gama, s.detadx,
+                            s.detady, s.xphys, s.yphys)
+    g = np.zeros(2 * s.ndof)
+    g[s.ndof:] = w[0] * grads["cl"] + w[1] * grads["cd"] + w[2] * grads["cm"]
+    lam, _, _ = adjoint_solve(s, g)
+    ome3 = s.ome[:3 * s.imax]
+    for i in (0, 7, P - 1):
+        vals, bs = [], []
+        for sg in (1.0, -1.0):
+            Xs, Ys = X.copy(), Y.copy()
+            Xs[i] += sg * h * nx[i] * phi[i]
+            Ys[i] += sg * h * ny[i] * phi[i]
+            if i == 0:
+                Xs[P] += sg * h * nx[0] * phi[P]
+                Ys[P] += sg * h * ny[0] * phi[P]
+            b, met = residual_on_mesh(s, Xs, Ys, 3)
+            bs.append(b)
+            vals.append(_wall_forces(s, met, ome3, w))
+        host = (vals[0] - vals[1]) / (2 * h) + float(lam @ (bs[0] - bs[1])) / (2 * h)
+        assert abs(dev[i] - host) <= 1e-8 * max(1.0, abs(host)), (i, dev[i], host)
+    s.close()

@@ -115,6 +115,8 @@ _SIGS = {
     "v2d_solver_time_lu_launches": (_i, [_vp, _i, _ll, _dp, _ip, _i, _ip]),
     "v2d_solver_time_lu_factor": (_i, [_vp, _i, _dp, _ip, _i, _ip]),
     "v2d_solver_residual_mesh": (_i, [_vp, _dp, _dp, _d, _d, _d, _d, _d, _d, _dp, _i, _dp]),
+    "v2d_solver_shape_gradient": (_i, [_vp, _dp, _dp, _dp, _dp, _d, _d, _d, _d, _d, _d, _d, _d,
+                                       _d, _d, _dp, _dp]),
     "v2d_solver_time_lu_apply": (_i, [_vp, _i, _ll, _dp, ctypes.POINTER(_ll)]),
     "v2d_lu_plan_info": (_i, [_i, _i, _ip, _ip, _i, ctypes.POINTER(_ll)]),
 }

@@ -25,9 +25,9 @@ C(q; p) has
   by d_i, and each grid line follows with a weight that decays from 1 at the
   wall to 0 at the far field (``deform_ogrid``; linear in d).  dR/dd_i and
   dC/dd_i|_q are central differences of the residual and of the force
-  integrals on the displaced meshes at the fixed converged state
-  (``v2d_solver_residual_mesh``: metrics and residual on the device); the one
-  adjoint solve is shared by all P components.
+  integrals on the displaced meshes at the fixed converged state, all
+  evaluated on the device (``v2d_solver_shape_gradient``); the one adjoint
+  solve is shared by all P components.
 """
 from __future__ import annotations
 
@@ -229,10 +229,12 @@ def shape_vjp(solver, weights, base_mesh, h=None):
     state, for wall displacements d along the normals of ``base_mesh`` (the
     undeformed (xg, yg) that ``deform_ogrid`` displaced to the solver's
     mesh).  Central differences of step h (default 1e-6 of the wall's
-    extent) on the residual and the force integrals, one adjoint solve."""
+    extent) on the residual and the force integrals, all 2P displaced meshes
+    evaluated on the device (``v2d_solver_shape_gradient``), one adjoint
+    solve."""
     xg0, yg0 = (np.asarray(a, dtype=np.float64) for a in base_mesh)
     nx, ny = wall_normals(xg0, yg0)
-    phi = deformation_weights(xg0, yg0)
+    phi = np.asfortranarray(deformation_weights(xg0, yg0))
     X = np.asarray(solver.xg, dtype=np.float64)
     Y = np.asarray(solver.yg, dtype=np.float64)
     P = solver.imax - 1
@@ -247,21 +249,22 @@ def shape_vjp(solver, weights, base_mesh, h=None):
     g = np.zeros(2 * N)
     g[N:] = w_cl * grads["cl"] + w_cd * grads["cd"] + w_cm * grads["cm"]
     lam, its, rel = adjoint_solve(solver, g)
-    ome3 = np.asarray(solver.ome, dtype=np.float64).reshape(-1)[:3 * solver.imax]
-    out = np.empty(P)
-    for i in range(P):
-        vals, bs = [], []
-        for sg in (1.0, -1.0):
-            Xs, Ys = X.copy(), Y.copy()
-            Xs[i] += sg * h * nx[i] * phi[i]
-            Ys[i] += sg * h * ny[i] * phi[i]
-            if i == 0:
-                Xs[P] += sg * h * nx[0] * phi[P]
-                Ys[P] += sg * h * ny[0] * phi[P]
-            b, met = residual_on_mesh(solver, Xs, Ys, 3)
-            bs.append(b)
-            vals.append(_wall_forces(solver, met, ome3, weights))
-        out[i] = (vals[0] - vals[1]) / (2.0 * h) + float(lam @ (bs[0] - bs[1])) / (2.0 * h)
+    nx = np.ascontiguousarray(nx)
+    ny = np.ascontiguousarray(ny)
+    dots = np.empty(P)
+    forces = np.empty((P, 2, 10))
+    a = math.radians(cfg.alpha_deg)
+    rl = -1.0 if cfg.ref_length is None else float(cfg.ref_length)
+    mc = cfg.moment_center
+    check(lib().v2d_solver_shape_gradient(solver.dev.h, dptr(nx), dptr(ny), dptr(phi), dptr(lam),
+                                          float(h), float(cfg.re), cfg.inv_dtau(), cfg.inv_2dt(),
+                                          float(cfg.u_rot(solver.t)), math.cos(a), math.sin(a),
+                                          rl, float(mc[0]), float(mc[1]), dptr(dots),
+                                          dptr(forces)),
+          "shape_gradient")
+    # v2d_force_coeffs order: cd, cl, cm, ...
+    c = w_cd * forces[:, :, 0] + w_cl * forces[:, :, 1] + w_cm * forces[:, :, 2]
+    out = (c[:, 0] - c[:, 1]) / (2.0 * h) + dots / (2.0 * h)
     return out, dict(refinements=its, rel_res=rel, h=h)
 
 

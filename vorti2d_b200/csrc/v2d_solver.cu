@@ -636,6 +636,93 @@ extern "C" int v2d_solver_residual_mesh(v2d_solver *S, const double *xg, const d
     return V2D_OK;
 }
 
+namespace v2d {
+
+// Column i of the mesh (and the seam column imax-1 with i = 0) set to the base
+// coordinates plus (ax, ay) * phi, or back to the base with restore; the
+// product and the sum are rounded separately, as on the host.
+static __global__ void k_shape_column(int imax, int jmax, int i, double ax, double ay, int restore,
+                               const double *__restrict__ phi, const double *__restrict__ x0,
+                               const double *__restrict__ y0, double *x, double *y)
+{
+    const int cols = i == 0 ? 2 : 1;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cols * jmax;
+         t += gridDim.x * blockDim.x) {
+        const int j = t % jmax;
+        const int c = t < jmax ? i : imax - 1;
+        const int k = c + imax * j;
+        x[k] = restore ? x0[k] : __dadd_rn(x0[k], __dmul_rn(ax, phi[k]));
+        y[k] = restore ? y0[k] : __dadd_rn(y0[k], __dmul_rn(ay, phi[k]));
+    }
+}
+
+// out[i] = lambda . (bp - bm), one block, fixed summation order.
+static __global__ void __launch_bounds__(1024) k_lambda_diff(int n, const double *__restrict__ lam,
+                                                      const double *__restrict__ bp,
+                                                      const double *__restrict__ bm, double *out,
+                                                      int i)
+{
+    __shared__ double red[32];
+    double a = 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) a += lam[k] * (bp[k] - bm[k]);
+    a = block_sum(a, red);
+    if (threadIdx.x == 0) out[i] = a;
+}
+
+}  // namespace v2d
+
+extern "C" int v2d_solver_shape_gradient(v2d_solver *S, const double *nx, const double *ny,
+                                         const double *phi, const double *lambda, double h,
+                                         double re, double invdtau, double inv2dt, double urot,
+                                         double ca, double sa, double ref_length, double x0,
+                                         double y0, double *dots, double *forces)
+{
+    V2D_ARG_CHECK(S && nx && ny && phi && lambda && dots && forces,
+                  "solver_shape_gradient: null pointer");
+    V2D_ARG_CHECK(re > 0.0 && h > 0.0, "solver_shape_gradient: re and h must be positive");
+    const GridDev &g0 = S->g;
+    const int P = g0.imax - 1;
+    const size_t N = (size_t)g0.N, n = (size_t)g0.n;
+    DevBuf<double> buf;
+    V2D_TRY(buf.alloc(12 * N + 2 * n + n + N + 2 * P + (size_t)P * 20 + P, S->s));
+    GridDev g = g0;   // the state is the handle's; mesh and metrics point to scratch
+    g.x = buf.p;
+    g.y = buf.p + N;
+    for (int q = 0; q < 10; ++q) g.met[q] = buf.p + (2 + q) * N;
+    double *bp = buf.p + 12 * N, *bm = bp + n, *dlam = bm + n, *dphi = dlam + n;
+    double *dnx = dphi + N, *dny = dnx + P, *dforce = dny + P, *ddot = dforce + (size_t)P * 20;
+    V2D_CUDA_TRY(cudaMemcpyAsync(g.x, g0.x, N * sizeof(double), cudaMemcpyDeviceToDevice, S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(g.y, g0.y, N * sizeof(double), cudaMemcpyDeviceToDevice, S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(dlam, lambda, n * sizeof(double), cudaMemcpyHostToDevice, S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(dphi, phi, N * sizeof(double), cudaMemcpyHostToDevice, S->s));
+    AsmParams ap{re, invdtau, inv2dt, urot, ca, sa, S->prm.ff_bc};
+    const int gcol = std::max(1, (2 * g.jmax + 255) / 256);
+    for (int i = 0; i < P; ++i) {
+        for (int sg = 0; sg < 2; ++sg) {
+            const double sgn = sg == 0 ? 1.0 : -1.0;
+            k_shape_column<<<gcol, 256, 0, S->s>>>(g.imax, g.jmax, i, sgn * h * nx[i],
+                                                   sgn * h * ny[i], 0, dphi, g0.x, g0.y, g.x,
+                                                   g.y);
+            V2D_CUDA_TRY(cudaGetLastError());
+            V2D_TRY(launch_metrics(g, S->s));
+            V2D_TRY(launch_residual(g, ap, sg == 0 ? bp : bm, S->s));
+            V2D_TRY(launch_forces(g, re, ref_length, x0, y0, dforce + ((size_t)i * 2 + sg) * 10,
+                                  S->s));
+            count_launches(2);
+        }
+        k_lambda_diff<<<1, 1024, 0, S->s>>>((int)n, dlam, bp, bm, ddot, i);
+        k_shape_column<<<gcol, 256, 0, S->s>>>(g.imax, g.jmax, i, 0.0, 0.0, 1, dphi, g0.x, g0.y,
+                                               g.x, g.y);
+        V2D_CUDA_TRY(cudaGetLastError());
+        count_launches(2);
+    }
+    V2D_CUDA_TRY(cudaMemcpyAsync(dots, ddot, P * sizeof(double), cudaMemcpyDeviceToHost, S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(forces, dforce, (size_t)P * 20 * sizeof(double),
+                                 cudaMemcpyDeviceToHost, S->s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    return V2D_OK;
+}
+
 extern "C" int v2d_solver_adjoint(v2d_solver *S, double urot, const double *g_host, double *lam_host,
                                   double rtol, int max_refine, int *refinements, double *rel_res)
 {
