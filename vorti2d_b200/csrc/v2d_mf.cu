@@ -1062,6 +1062,11 @@ constexpr int kSolveRows = kSolveRowsHost;
 // levels with at least this many fronts are solved with one CTA per front
 constexpr int kFrontPerCta = 64;
 constexpr int kSolveThreads2 = 32 * kSolveRows;
+// the one-CTA-per-front solve kernels: more warps share a front's rows when
+// a level's CTAs of that size all fit on the GPU at once (2 per SM), else
+// kSolveThreads2 per front
+constexpr int kFrontThreads = 512;
+inline int front_threads(int nq) { return nq <= 2 * kSMs ? kFrontThreads : kSolveThreads2; }
 
 template <class T>
 __device__ __forceinline__ T row_dot(const T *__restrict__ row, const T *v, int c0, int c1)
@@ -1352,7 +1357,7 @@ __global__ void __launch_bounds__(kSolveThreads2) k_bwd_x(int q0, const MfDev D,
 // (gather, z, contribution vector) or backward (y, x) step, so the right-hand
 // side is gathered once per front instead of once per row chunk.
 template <class T>
-__global__ void __launch_bounds__(kSolveThreads2) k_fwd_front(int q0, const MfDev D, const T *F,
+__global__ void __launch_bounds__(kFrontThreads) k_fwd_front(int q0, const MfDev D, const T *F,
                                                               const T *b,
                                                               const double *__restrict__ rs,
                                                               T *zbuf, T *upd, const int *stop_a,
@@ -1417,7 +1422,7 @@ __global__ void __launch_bounds__(kSolveThreads2) k_fwd_front(int q0, const MfDe
 }
 
 template <class T>
-__global__ void __launch_bounds__(kSolveThreads2) k_bwd_front(int q0, const MfDev D, const T *F,
+__global__ void __launch_bounds__(kFrontThreads) k_bwd_front(int q0, const MfDev D, const T *F,
                                                               const T *zbuf, T *x,
                                                               const int *stop_a, const int *stop_b)
 {
@@ -1960,7 +1965,7 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
     for (int L = 0; L < P->nlevel; ++L) {
         const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
         if (nq >= kFrontPerCta) {
-            k_fwd_front<T><<<nq, kSolveThreads2, smf, s>>>(q0, D, F, b, M->rs, z, upd, stop_a,
+            k_fwd_front<T><<<nq, front_threads(nq), smf, s>>>(q0, D, F, b, M->rs, z, upd, stop_a,
                                                            stop_b);
             V2D_TRY(solve_launch("k_fwd_front", L));
             V2D_TRY(mark(kCodeFwdFront * 1000 + L));
@@ -1984,7 +1989,7 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
     for (int L = P->nlevel - 1; L >= 0; --L) {
         const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
         if (nq >= kFrontPerCta) {
-            k_bwd_front<T><<<nq, kSolveThreads2, smf, s>>>(q0, D, F, z, x, stop_a, stop_b);
+            k_bwd_front<T><<<nq, front_threads(nq), smf, s>>>(q0, D, F, z, x, stop_a, stop_b);
             V2D_TRY(solve_launch("k_bwd_front", L));
             V2D_TRY(mark(kCodeBwdFront * 1000 + L));
             ++launches;
