@@ -329,6 +329,71 @@ def run_adjoint_workload(args):
     s.close()
 
 
+def run_large_workload(args):
+    """Large unsteady run: cylinder O-grid N x N (default 2049, 8.4M
+    unknowns), Re 200, dt 0.05, outflow far field, BDF2 with at most 5 Newton
+    iterations per step, FP32 LU + Krylov inside FP64 defect correction.
+    One warm-up step (plan, factors and graphs), then --large-steps timed
+    steps with CUDA events; the LU solve of one GMRES iteration is timed
+    after an L2 flush against the HBM roofline (at this size the factors do
+    not fit in L2)."""
+    import ctypes
+    import torch
+    import vorti2d_b200 as v
+    from vorti2d_b200 import _lib
+    torch.cuda.set_device(0)
+    n = args.large_grid
+    xg, yg = v.generate_cylinder(n, n)
+    cfg = v.Config(verbose=False, write_csv=False, write_xdmf=False, compute_forces=False,
+                   re=200.0, steady=False, dt_phys=0.05, farfield_bc="outflow",
+                   raise_on_linear_failure=False, precision="mixed",
+                   lu_reuse_its=args.lu_reuse, **SOLVER)
+    t0 = time.perf_counter()
+    s = v.Solver(cfg, mesh=(xg, yg))
+    setup_s = time.perf_counter() - t0
+    times = s.times()
+    t0 = time.perf_counter()
+    s.advance(times[0])
+    torch.cuda.synchronize()
+    first_s = time.perf_counter() - t0
+    phase_times(_lib, s, reset=True)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    K = args.large_steps
+    ms, newton, krylov = timed_steps(torch, s, times, 1, K, flush)
+    ph = phase_times(_lib, s)
+    lu_ms = ctypes.c_double()
+    fb = ctypes.c_longlong()
+    _lib.check(_lib.lib().v2d_solver_time_lu_apply(s.dev.h, 3, L2_FLUSH_BYTES,
+                                                  ctypes.byref(lu_ms), ctypes.byref(fb)))
+    hbm = 6650.0
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            hbm = json.load(fh)["hbm_gbs"]
+    except (OSError, ValueError, KeyError):
+        pass
+    gbs = fb.value / (lu_ms.value * 1e-3) / 1e9
+    step_ms = float(np.mean(ms))
+    line = {"metric": f"BDF2 steps/s, {n}x{n} cylinder O-grid Re=200 dt=0.05 (<=5 Newton, "
+                      "GMRES(30))",
+            "value": 1e3 / step_ms, "unit": "steps/s", "n_gpus": 1, "steps": K, "warmup": 1,
+            "ms_per_step": step_ms, "higher_is_better": True, "dtype": "f32-krylov/f64",
+            "data": "synthetic",
+            "config": {"workload": f"large unsteady BDF2 cylinder {n}x{n} Re=200 dt=0.05 outflow",
+                       "unknowns": 2 * n * n, "lu_reuse_its": args.lu_reuse,
+                       "l2": "flushed (256 MiB write) before every timed step"},
+            "setup_s": setup_s, "first_step_s": first_s, "newton_per_step": newton / K,
+            "krylov_per_step": krylov / K,
+            "ms_per_newton": {"assembly": ph[0] / max(ph[4], 1), "factor": ph[1] / max(ph[4], 1),
+                              "krylov": ph[2] / max(ph[4], 1), "update": ph[3] / max(ph[4], 1)},
+            "factorizations_per_step": ph[5] / K,
+            "roofline": {"bound": "hbm", "kernel": "lu_apply_fp32", "achieved": gbs,
+                         "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                         "bytes_per_launch": fb.value, "ms_per_launch": lu_ms.value},
+            "cd": s.force_coeffs().cd}
+    print(json.dumps(line), flush=True)
+    s.close()
+
+
 def phase_times(_lib, s, reset=False):
     """(assembly, factorization, Krylov, update) device ms summed over Newton
     iterations, and the iteration count."""
@@ -537,10 +602,14 @@ def main():
                          "(0: factor every Newton Jacobian)")
     ap.add_argument("--kernels-grid", type=int, default=2049,
                     help="grid side of the HBM-bound kernel roofline table (0: skip)")
-    ap.add_argument("--workload", default="unsteady", choices=["unsteady", "sweep", "adjoint"],
+    ap.add_argument("--workload", default="unsteady", choices=["unsteady", "sweep", "adjoint", "large"],
                     help="unsteady: the BDF2 benchmark; sweep: the batched steady sweep; "
-                         "adjoint: steady adjoint gradients")
+                         "adjoint: steady adjoint gradients; large: the large unsteady grid")
     ap.add_argument("--sweep-workers", type=int, default=16)
+    ap.add_argument("--large-grid", type=int, default=2049,
+                    help="grid side of the large unsteady workload (--workload large)")
+    ap.add_argument("--large-steps", type=int, default=3,
+                    help="timed BDF2 steps of the large unsteady workload")
     ap.add_argument("--adjoint-re", type=float, default=500.0,
                     help="Reynolds number of the adjoint workload (--workload adjoint)")
     ap.add_argument("--kernels-only", action="store_true",
@@ -562,6 +631,9 @@ def main():
         return
     if args.workload == "adjoint" and args.impl == "ours":
         run_adjoint_workload(args)
+        return
+    if args.workload == "large" and args.impl == "ours":
+        run_large_workload(args)
         return
     if args.kernels_only:
         import torch

@@ -86,6 +86,8 @@ struct MfFactor {
     int fp32 = 0;
     void *F = nullptr, *upd = nullptr, *z = nullptr;
     void *tmp = nullptr;        // triangular inverses of one level before they replace L11 / U11
+    void *inv_g = nullptr;      // inversion work space in global memory for separators too
+                                // wide for shared memory (per CTA: S x (CW + 33))
     void *wb = nullptr;         // transposed solve: per-front adjoint right-hand sides (vtotal)
     double *rs = nullptr;       // row scaling 1 / max |a_r.|
     int *ipiv = nullptr, *perm = nullptr, *flag = nullptr;

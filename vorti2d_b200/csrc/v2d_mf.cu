@@ -1030,6 +1030,34 @@ __global__ void __launch_bounds__(kTrinvThreads) k_trinv(int q0, const int *__re
     trinv_colblock<T>(F + foff[q], S, f, tmp + toff[q], c0, Xs, Lp, Dg);
 }
 
+// The same inversion for separators whose column block does not fit in
+// shared memory: the S x CW block and the S x 33 panel live in a global work
+// space, one slice of S x (CW + 33) per CTA (sstride elements apart).
+constexpr size_t kInvSmemMax = 200 * 1024;
+// grids with one y index per front take at most this many fronts per launch
+// (the grid's y dimension is limited to 65535)
+constexpr int kMaxFrontsY = 65535;
+constexpr int kTrinvThreadsG = 256;
+
+template <class T>
+__global__ void __launch_bounds__(kTrinvThreadsG) k_trinv_g(int q0, const int *__restrict__ S_,
+                                                           const long long *__restrict__ foff,
+                                                           const int *__restrict__ f_,
+                                                           const long long *__restrict__ toff,
+                                                           const T *__restrict__ F, T *tmp,
+                                                           T *work, long long sstride)
+{
+    constexpr int CW = InvWidth<T>::v;
+    __shared__ T Dg[32][33];
+    const int q = q0 + blockIdx.y;
+    const int S = S_[q], f = f_[q];
+    const int c0 = blockIdx.x * CW;
+    if (c0 >= S) return;
+    T *Xs = work + ((long long)blockIdx.y * gridDim.x + blockIdx.x) * sstride;
+    T *Lp = Xs + (size_t)S * CW;
+    trinv_colblock<T>(F + foff[q], S, f, tmp + toff[q], c0, Xs, Lp, Dg);
+}
+
 // Inverted S x S blocks of the level's fronts: scratch -> factor storage.
 template <class T>
 __global__ void k_trcopy(int q0, const int *__restrict__ S_, const int *__restrict__ f_,
@@ -1696,13 +1724,33 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
     // dynamic shared memory of the solve and inversion kernels (set once,
     // outside any stream capture)
     const size_t solve = (size_t)(P->maxf + P->maxS) * es;
-    const size_t inv = (size_t)P->maxS * (fp32 ? (InvWidth<float>::v + 33) * sizeof(float)
-                                               : (InvWidth<double>::v + 33) * sizeof(double));
-    if (solve > 227 * 1024 || inv > 227 * 1024) {
+    const int cw = fp32 ? InvWidth<float>::v : InvWidth<double>::v;
+    // shared-memory inversion where its column block fits, the global work
+    // space elsewhere (sized for the largest such level)
+    size_t inv = 0, inv_g = 0;
+    for (int L = 0; L < P->nlevel; ++L) {
+        const size_t sl = (size_t)P->lvl_maxS[L] * (cw + 33);
+        if (sl * es <= kInvSmemMax) {
+            inv = std::max(inv, sl * es);
+        } else {
+            const size_t nbc = (P->lvl_maxS[L] + cw - 1) / cw;
+            inv_g = std::max(inv_g, nbc * (size_t)(P->lvl_off[L + 1] - P->lvl_off[L]) * sl);
+        }
+    }
+    if (solve > 227 * 1024) {
         set_error("mf_factor: front of %d unknowns (separator %d) exceeds shared memory",
                   P->maxf, P->maxS);
         mf_factor_destroy(M);
         return V2D_EARG;
+    }
+    if (inv_g > 0) {
+        cudaError_t ge = cudaMalloc(&M->inv_g, inv_g * es);
+        if (ge != cudaSuccess) {
+            set_error("mf_factor: inversion work space of %.1f MB: %s", inv_g * es / 1e6,
+                      cudaGetErrorString(ge));
+            mf_factor_destroy(M);
+            return V2D_ENOMEM;
+        }
     }
     auto attr = [&](const void *fn, size_t bytes) {
         if (e == cudaSuccess) e = raise_dyn_smem(fn, bytes);
@@ -1760,7 +1808,8 @@ void mf_factor_destroy(MfFactor *M)
 {
     if (!M) return;
     if (M->graph) cudaGraphExecDestroy(M->graph);
-    void *ptrs[] = {M->F, M->upd, M->z, M->tmp, M->wb, M->rs, M->ipiv, M->perm, M->flag, M->bar};
+    void *ptrs[] = {M->F,  M->upd,  M->z,    M->tmp,  M->wb, M->rs,
+                    M->ipiv, M->perm, M->flag, M->bar, M->inv_g};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     delete M;
@@ -1824,11 +1873,13 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
             const long long mm = (long long)P->lvl_maxm_child[L] * P->lvl_maxm_child[L];
             const int gx = (int)std::max(1LL, std::min<long long>((mm + 255) / 256, 64));
             for (int slot = 0; slot < 2; ++slot) {
-                k_extend_add<T><<<dim3(gx, nq), 256, 0, s>>>(q0, slot, P->d_S, P->d_f, P->d_foff,
-                                                             P->d_uoff, P->d_child0, P->d_child1,
-                                                             P->d_cbmap, F);
+                for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
+                    k_extend_add<T><<<dim3(gx, std::min(nq - qb, kMaxFrontsY)), 256, 0, s>>>(
+                        q0 + qb, slot, P->d_S, P->d_f, P->d_foff, P->d_uoff, P->d_child0,
+                        P->d_child1, P->d_cbmap, F);
+                    ++launches;
+                }
                 V2D_TRY(mark(2000 + L));
-                ++launches;
             }
         }
         const int maxf = P->lvl_maxf[L];
@@ -1842,27 +1893,45 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
             const int below = std::max(1, maxf - k - 1);
             const int nl = (below + kL21Rows - 1) / kL21Rows;
             const int ncol = (maxf + kL21Rows - 1) / kL21Rows;
-            k_l21_trsm<T><<<dim3(nl + ncol, nq), kL21Rows, 0, s>>>(q0, k, nl, P->d_S, P->d_f,
-                                                                   P->d_foff, P->d_voff, F,
-                                                                   M->ipiv);
+            for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
+                k_l21_trsm<T><<<dim3(nl + ncol, std::min(nq - qb, kMaxFrontsY)), kL21Rows, 0,
+                                s>>>(q0 + qb, k, nl, P->d_S, P->d_f, P->d_foff, P->d_voff, F,
+                                     M->ipiv);
+                if (qb > 0) ++launches;
+            }
             V2D_TRY(mark(4000 + L));
             const int rem = std::max(1, maxf - k - 1);
             const int nt = (rem + kGemmTile - 1) / kGemmTile;
-            k_gemm<T><<<dim3(nt * nt, nq), 256, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff,
-                                                        P->d_voff, F, M->ipiv, M->perm,
-                                                        M->flag);
+            for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
+                k_gemm<T><<<dim3(nt * nt, std::min(nq - qb, kMaxFrontsY)), 256, 0, s>>>(
+                    q0 + qb, k, P->d_S, P->d_f, P->d_foff, P->d_voff, F, M->ipiv, M->perm,
+                    M->flag);
+                if (qb > 0) ++launches;
+            }
             V2D_TRY(mark(6000 + L));
             launches += 2;
         }
         const int nbc = (P->lvl_maxS[L] + InvWidth<T>::v - 1) / InvWidth<T>::v;
-        k_trinv<T><<<dim3(nbc, nq), kTrinvThreads,
-                     (size_t)P->lvl_maxS[L] * (InvWidth<T>::v + 33) * sizeof(T), s>>>(
-            q0, P->d_S, P->d_foff, P->d_f, P->d_toff, F, (T *)M->tmp);
+        const size_t inv_bytes = (size_t)P->lvl_maxS[L] * (InvWidth<T>::v + 33) * sizeof(T);
+        for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
+            const int nb = std::min(nq - qb, kMaxFrontsY);
+            if (inv_bytes <= kInvSmemMax)
+                k_trinv<T><<<dim3(nbc, nb), kTrinvThreads, inv_bytes, s>>>(
+                    q0 + qb, P->d_S, P->d_foff, P->d_f, P->d_toff, F, (T *)M->tmp);
+            else
+                k_trinv_g<T><<<dim3(nbc, nb), kTrinvThreadsG, 0, s>>>(
+                    q0 + qb, P->d_S, P->d_foff, P->d_f, P->d_toff, F, (T *)M->tmp,
+                    (T *)M->inv_g, (long long)P->lvl_maxS[L] * (InvWidth<T>::v + 33));
+            if (qb > 0) ++launches;
+        }
         V2D_TRY(mark(7000 + L));
         const long long ss = (long long)P->lvl_maxS[L] * P->lvl_maxS[L];
         const int gcp = (int)std::max(1LL, std::min<long long>((ss + 255) / 256, 256));
-        k_trcopy<T><<<dim3(gcp, nq), 256, 0, s>>>(q0, P->d_S, P->d_f, P->d_foff, P->d_toff,
-                                                  (const T *)M->tmp, F);
+        for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
+            k_trcopy<T><<<dim3(gcp, std::min(nq - qb, kMaxFrontsY)), 256, 0, s>>>(
+                q0 + qb, P->d_S, P->d_f, P->d_foff, P->d_toff, (const T *)M->tmp, F);
+            if (qb > 0) ++launches;
+        }
         V2D_TRY(mark(8000 + L));
         launches += 2;
     }
@@ -1972,16 +2041,23 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
             ++launches;
             continue;
         }
-        k_fwd_z<T><<<dim3(chunks(P->lvl_maxS[L]), nq), kSolveThreads2,
-                     (size_t)(P->maxf + P->maxS) * sizeof(T), s>>>(q0, D, F, b, M->rs, z, upd,
-                                                                   stop_a, stop_b);
-        V2D_TRY(solve_launch("k_fwd_z", L));
+        for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
+            k_fwd_z<T><<<dim3(chunks(P->lvl_maxS[L]), std::min(nq - qb, kMaxFrontsY)),
+                         kSolveThreads2, smf, s>>>(q0 + qb, D, F, b, M->rs, z, upd, stop_a,
+                                                   stop_b);
+            V2D_TRY(solve_launch("k_fwd_z", L));
+            if (qb > 0) ++launches;
+        }
         V2D_TRY(mark(kCodeFwdZ * 1000 + L));
         ++launches;
         if (P->lvl_maxm[L] > 0) {
-            k_fwd_u<T><<<dim3(chunks(P->lvl_maxm[L]), nq), kSolveThreads2,
-                         (size_t)P->maxS * sizeof(T), s>>>(q0, D, F, z, upd, stop_a, stop_b);
-            V2D_TRY(solve_launch("k_fwd_u", L));
+            for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
+                k_fwd_u<T><<<dim3(chunks(P->lvl_maxm[L]), std::min(nq - qb, kMaxFrontsY)),
+                             kSolveThreads2, (size_t)P->maxS * sizeof(T), s>>>(
+                    q0 + qb, D, F, z, upd, stop_a, stop_b);
+                V2D_TRY(solve_launch("k_fwd_u", L));
+                if (qb > 0) ++launches;
+            }
             V2D_TRY(mark(kCodeFwdU * 1000 + L));
             ++launches;
         }
@@ -1996,15 +2072,23 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
             continue;
         }
         if (P->lvl_maxm[L] > 0) {
-            k_bwd_y<T><<<dim3(chunks(P->lvl_maxS[L]), nq), kSolveThreads2,
-                         (size_t)P->maxf * sizeof(T), s>>>(q0, D, F, z, x, stop_a, stop_b);
-            V2D_TRY(solve_launch("k_bwd_y", L));
+            for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
+                k_bwd_y<T><<<dim3(chunks(P->lvl_maxS[L]), std::min(nq - qb, kMaxFrontsY)),
+                             kSolveThreads2, (size_t)P->maxf * sizeof(T), s>>>(
+                    q0 + qb, D, F, z, x, stop_a, stop_b);
+                V2D_TRY(solve_launch("k_bwd_y", L));
+                if (qb > 0) ++launches;
+            }
             V2D_TRY(mark(kCodeBwdY * 1000 + L));
             ++launches;
         }
-        k_bwd_x<T><<<dim3(chunks(P->lvl_maxS[L]), nq), kSolveThreads2,
-                     (size_t)P->maxS * sizeof(T), s>>>(q0, D, F, z, x, stop_a, stop_b);
-        V2D_TRY(solve_launch("k_bwd_x", L));
+        for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
+            k_bwd_x<T><<<dim3(chunks(P->lvl_maxS[L]), std::min(nq - qb, kMaxFrontsY)),
+                         kSolveThreads2, (size_t)P->maxS * sizeof(T), s>>>(
+                q0 + qb, D, F, z, x, stop_a, stop_b);
+            V2D_TRY(solve_launch("k_bwd_x", L));
+            if (qb > 0) ++launches;
+        }
         V2D_TRY(mark(kCodeBwdX * 1000 + L));
         ++launches;
     }
