@@ -398,6 +398,46 @@ def run_large_workload(args):
     s.close()
 
 
+def run_unsteady_adjoint_workload(args):
+    """Unsteady discrete adjoint: time-mean Cd over --ua-steps BDF2 steps of
+    the cylinder N x N (default 181), Re 200, dt 0.05, outflow far field,
+    every step converged to 1e-12, and its gradient with respect to (alpha,
+    Re) with a checkpoint every --ua-checkpoint steps (forward run, then per
+    segment: recomputation from the checkpoint and a backward sweep of FP64
+    transposed solves).  value = gradients per second (wall clock of the
+    whole forward + backward computation)."""
+    import torch
+    import vorti2d_b200 as v
+    from vorti2d_b200.unsteady_adjoint import unsteady_mean_force_vjp
+    torch.cuda.set_device(0)
+    n = args.ua_grid
+    mesh = v.generate_cylinder(n, n)
+
+    def make():
+        cfg = v.Config(verbose=False, write_csv=False, write_xdmf=False, compute_forces=False,
+                       re=200.0, steady=False, dt_phys=0.05, farfield_bc="outflow",
+                       pseudo_tol=1e-12, max_pseudo_iter=20, ksp_rtol=1e-12,
+                       precision="fp64", raise_on_linear_failure=False)
+        return v.Solver(cfg, mesh=mesh)
+
+    unsteady_mean_force_vjp(make, 2, (0.0, 1.0, 0.0), checkpoint_every=1)   # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    J, d_alpha, d_re, info = unsteady_mean_force_vjp(make, args.ua_steps, (0.0, 1.0, 0.0),
+                                                     checkpoint_every=args.ua_checkpoint)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    line = {"metric": f"unsteady adjoint gradients/s (mean Cd over {args.ua_steps} BDF2 steps, "
+                      f"d/dalpha and d/dRe), {n}x{n} cylinder Re=200 dt=0.05",
+            "value": 1.0 / dt, "unit": "gradients/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"unsteady discrete adjoint, cylinder {n}x{n}, "
+                                   f"{args.ua_steps} steps, checkpoint every "
+                                   f"{args.ua_checkpoint}"},
+            "seconds": dt, "mean_cd": J, "dJ_dalpha": d_alpha, "dJ_dRe": d_re, **info}
+    print(json.dumps(line), flush=True)
+
+
 def phase_times(_lib, s, reset=False):
     """(assembly, factorization, Krylov, update) device ms summed over Newton
     iterations, and the iteration count."""
@@ -606,9 +646,11 @@ def main():
                          "(0: factor every Newton Jacobian)")
     ap.add_argument("--kernels-grid", type=int, default=2049,
                     help="grid side of the HBM-bound kernel roofline table (0: skip)")
-    ap.add_argument("--workload", default="unsteady", choices=["unsteady", "sweep", "adjoint", "large"],
+    ap.add_argument("--workload", default="unsteady", choices=["unsteady", "sweep", "adjoint", "large",
+                                                    "unsteady_adjoint"],
                     help="unsteady: the BDF2 benchmark; sweep: the batched steady sweep; "
-                         "adjoint: steady adjoint gradients; large: the large unsteady grid")
+                         "adjoint: steady adjoint gradients; large: the large unsteady grid; "
+                         "unsteady_adjoint: the checkpointed unsteady adjoint")
     ap.add_argument("--sweep-workers", type=int, default=16)
     ap.add_argument("--large-grid", type=int, default=2049,
                     help="grid side of the large unsteady workload (--workload large)")
@@ -616,6 +658,12 @@ def main():
                     help="timed BDF2 steps of the large unsteady workload")
     ap.add_argument("--large-precision", default="fp64", choices=["mixed", "fp64"],
                     help="LU factors and Krylov vectors of the large unsteady workload")
+    ap.add_argument("--ua-grid", type=int, default=181,
+                    help="grid side of the unsteady adjoint workload")
+    ap.add_argument("--ua-steps", type=int, default=20,
+                    help="BDF2 steps of the unsteady adjoint workload")
+    ap.add_argument("--ua-checkpoint", type=int, default=5,
+                    help="checkpoint spacing of the unsteady adjoint workload")
     ap.add_argument("--adjoint-re", type=float, default=500.0,
                     help="Reynolds number of the adjoint workload (--workload adjoint)")
     ap.add_argument("--kernels-only", action="store_true",
@@ -640,6 +688,9 @@ def main():
         return
     if args.workload == "large" and args.impl == "ours":
         run_large_workload(args)
+        return
+    if args.workload == "unsteady_adjoint" and args.impl == "ours":
+        run_unsteady_adjoint_workload(args)
         return
     if args.kernels_only:
         import torch

@@ -77,3 +77,10 @@ def test_steady_forces_needs_base_mesh_with_displacement():
     from vorti2d_b200.adjoint import SteadyForces
     with pytest.raises(ValueError):
         SteadyForces.apply(torch.tensor(0.0), torch.tensor(40.0), None, torch.zeros(4))
+
+
+def test_unsteady_adjoint_history_rows():
+    from vorti2d_b200.unsteady_adjoint import _interior_ome_rows
+    rows = _interior_ome_rows(5, 4)
+    # 2N = 40 unknowns; the BDF2 history sits on the vorticity rows of j = 1, 2
+    assert list(rows) == list(range(20 + 5, 20 + 15))
