@@ -78,7 +78,7 @@ def test_handles_with_different_front_sizes_coexist(v2d, oracle_mod, precision):
     small.close()
 
 
-def test_config1_steady_129_matches_oracle(v2d, oracle_mod):
+def test_steady_cylinder_129_matches_oracle(v2d, oracle_mod):
     """Plain FP64 steady Newton, 129x129 cylinder, Re=40, Dirichlet far field,
     pure Newton (dtau = inf) to ||dq||/(2N) < 1e-12: psi/omega within 1e-9,
     Cl/Cd/Cm within 1e-8 of the oracle; the reference's BC and symmetry checks
@@ -106,7 +106,7 @@ def test_config1_steady_129_matches_oracle(v2d, oracle_mod):
 
 @pytest.mark.parametrize("precision,reuse", [("fp64", 0), ("mixed", 0), ("mixed", 20),
                                               ("fp64", 20)])
-def test_config2_unsteady_181_matches_oracle(v2d, oracle_mod, precision, reuse):
+def test_unsteady_cylinder_181_matches_oracle(v2d, oracle_mod, precision, reuse):
     """The benchmark case (181x181, Re=100, dt=0.2, rotational kick 0.5 until
     t=2, outflow far field, at most 5 Newton iterations per step): the first
     three BDF2 steps equal the oracle's to 1e-9 with |dCd| < 1e-8, with the
