@@ -58,3 +58,22 @@ def test_checkpoint_spacing_does_not_change_the_gradient(v2d, oracle_mod):
         assert abs(J - out[0][0]) <= 1e-12 * max(1.0, abs(J))
         assert abs(da - out[0][1]) <= 1e-8 * max(1.0, abs(da))
         assert abs(dr - out[0][2]) <= 1e-8 * max(1.0, abs(dr))
+
+
+def test_torch_autograd_unsteady(v2d, oracle_mod):
+    import torch
+    from vorti2d_b200.unsteady_adjoint import UnsteadyMeanForces, unsteady_mean_force_vjp
+    mesh = oracle_mod.generate_cylinder(33, 25)
+
+    def make(adeg, re):
+        return v2d.Solver(_cfg(v2d, re, adeg), mesh=mesh)
+
+    alpha = torch.tensor(ADEG, dtype=torch.float64, requires_grad=True)
+    re = torch.tensor(RE, dtype=torch.float64, requires_grad=True)
+    out = UnsteadyMeanForces.apply(alpha, re, make, STEPS, 3)
+    loss = W[0] * out[0] + W[1] * out[1] + W[2] * out[2]
+    assert abs(loss.item() - _mean(v2d, mesh, RE, ADEG)) <= 1e-12 * max(1.0, abs(loss.item()))
+    loss.backward()
+    J, da, dr, _ = unsteady_mean_force_vjp(lambda: make(ADEG, RE), STEPS, W, checkpoint_every=3)
+    assert abs(alpha.grad.item() - da) <= 1e-10 * max(1.0, abs(da))
+    assert abs(re.grad.item() - dr) <= 1e-10 * max(1.0, abs(dr))

@@ -126,3 +126,54 @@ def unsteady_mean_force_vjp(make_solver, n_steps, weights, checkpoint_every=20, 
             lam2, lam1 = lam1, lam
     s.close()
     return Jval, d_alpha, d_re, dict(steps=M, checkpoints=len(ckpt), adjoint_solves=solves)
+
+
+class UnsteadyMeanForces:
+    """(alpha_deg, Re) -> time-mean (Cl, Cd, Cm) over the first n_steps BDF2
+    steps, as a torch.autograd.Function whose backward is the checkpointed
+    discrete adjoint (one backward sweep per output weight vector).
+
+    Usage::
+
+        out = UnsteadyMeanForces.apply(alpha, re, make_solver, n_steps, checkpoint_every)
+
+    ``make_solver(alpha_deg, re)`` returns a fresh unsteady
+    ``vorti2d_b200.Solver`` at its initial state.
+    """
+
+    _fn = None
+
+    @classmethod
+    def function(cls):
+        if cls._fn is None:
+            import torch
+
+            class _Fn(torch.autograd.Function):
+                @staticmethod
+                def forward(ctx, alpha, re, make_solver, n_steps, checkpoint_every):
+                    a, r = float(alpha), float(re)
+                    s = make_solver(a, r)
+                    acc = np.zeros(3)
+                    times = s.times()[:n_steps]
+                    for t in times:
+                        s.advance(t)
+                        acc += _coeffs(s.force_coeffs())
+                    s.close()
+                    ctx.args = (a, r, make_solver, n_steps, checkpoint_every)
+                    return torch.tensor(acc / max(len(times), 1), dtype=torch.float64)
+
+                @staticmethod
+                def backward(ctx, grad):
+                    a, r, make_solver, n_steps, every = ctx.args
+                    w = grad.detach().cpu().numpy().astype(np.float64)
+                    _, d_alpha, d_re, _ = unsteady_mean_force_vjp(
+                        lambda: make_solver(a, r), n_steps, w, checkpoint_every=every)
+                    return (torch.tensor(d_alpha, dtype=torch.float64),
+                            torch.tensor(d_re, dtype=torch.float64), None, None, None)
+
+            cls._fn = _Fn
+        return cls._fn
+
+    @classmethod
+    def apply(cls, alpha, re, make_solver, n_steps, checkpoint_every=20):
+        return cls.function().apply(alpha, re, make_solver, int(n_steps), int(checkpoint_every))
