@@ -595,20 +595,16 @@ def _e2e(torch, v, s, times, k0, K, flush_buf):
     Solver.set_state / advance / state readback with pinned host buffers; the
     copies are inside the timed region, the L2 flush before each step is not."""
     N = s.ndof
-    host = [torch.empty(N, dtype=torch.float64, pin_memory=True) for _ in range(4)]
-    st = s.dev.get_state()
-    for h, a in zip(host, st):
-        h.numpy()[:] = a
+    host = [torch.empty(N, dtype=torch.float64, pin_memory=True).numpy() for _ in range(4)]
+    s.get_state(out=host)
     dt = 0.0
     for m in range(K):
         flush_l2(torch, flush_buf)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        s.set_state(*[h.numpy() for h in host])
+        s.set_state(*host)
         s.advance(times[k0 + m])
-        out = s.dev.get_state()
-        for h, a in zip(host, out):
-            h.numpy()[:] = a
+        s.get_state(out=host)
         dt += time.perf_counter() - t0
     return dict(steps_per_s=K / dt, h2d=4 * N * 8, d2h=4 * N * 8, steps=K)
 

@@ -189,3 +189,33 @@ def test_linsys_seam_canonical_csr_and_solve(v2d, oracle_mod):
     with pytest.raises(ValueError):
         lin.assemble(cj, ci, cv, b)    # different pattern
     lin.destroy()
+
+
+def test_state_round_trip_through_pinned_buffers(v2d, oracle_mod):
+    """Solver.set_state -> get_state(out=...) into pinned host buffers returns
+    the arrays bit for bit, matches get_state(), and rejects bad buffers."""
+    import torch
+    imax, jmax = 33, 25
+    xg, yg = oracle_mod.generate_cylinder(imax, jmax)
+    cfg = v2d.Config(re=100.0, steady=False, dt_phys=0.2, verbose=False)
+    s = v2d.Solver(cfg, mesh=(xg, yg))
+    N = imax * jmax
+    rng = np.random.default_rng(7)
+    st = [rng.standard_normal(N) for _ in range(4)]
+    s.set_state(*st)
+    host = [torch.empty(N, dtype=torch.float64, pin_memory=True).numpy() for _ in range(4)]
+    got = s.get_state(out=host)
+    assert all(g is h for g, h in zip(got, host))
+    for h, a, b in zip(host, st, s.get_state()):
+        assert np.array_equal(h, a)
+        assert np.array_equal(b, a)
+    assert np.array_equal(s.psi, st[0]) and np.array_equal(s.omeoldold, st[3])
+    with pytest.raises(ValueError):
+        s.get_state(out=host[:3])
+    with pytest.raises(ValueError):
+        s.get_state(out=[np.zeros(N, dtype=np.float32)] + host[1:])
+    with pytest.raises(ValueError):
+        s.get_state(out=[np.zeros(N + 1)] + host[1:])
+    with pytest.raises(ValueError):
+        s.get_state(out=[np.zeros((N, 2))[:, 0]] + host[1:])
+    s.close()

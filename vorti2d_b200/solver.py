@@ -67,8 +67,21 @@ class DeviceState:
         check(lib().v2d_solver_get_metrics(self.h, arr), "get_metrics")
         return outs
 
-    def get_state(self):
-        outs = [np.zeros(self.N) for _ in range(4)]
+    def get_state(self, out=None):
+        """psi, ome, omeold, omeoldold as flat float64 arrays.  ``out``: four
+        caller-owned C-contiguous float64 arrays of imax*jmax entries (e.g.
+        views of pinned host buffers) to copy into instead of new arrays."""
+        if out is None:
+            outs = [np.zeros(self.N) for _ in range(4)]
+        else:
+            outs = list(out)
+            if len(outs) != 4:
+                raise ValueError("get_state: out needs four arrays (psi, ome, omeold, omeoldold)")
+            for o in outs:
+                if (not isinstance(o, np.ndarray) or o.dtype != np.float64 or o.size != self.N
+                        or not o.flags.c_contiguous or not o.flags.writeable):
+                    raise ValueError(f"get_state: each out array must be a writable C-contiguous "
+                                     f"float64 array of imax*jmax = {self.N} entries")
         check(lib().v2d_solver_get_state(self.h, *[dptr(o) for o in outs]), "get_state")
         return outs
 
@@ -214,6 +227,13 @@ class Solver:
     @property
     def omeoldold(self):
         return self._state()[3]
+
+    def get_state(self, out=None):
+        """Copy the device state (psi, ome, omeold, omeoldold; flat, i fastest)
+        to the host; ``out`` names four caller-owned float64 arrays to fill."""
+        if out is None:
+            return [a.copy() for a in self._state()]
+        return self.dev.get_state(out)
 
     def set_state(self, psi, ome, omeold, omeoldold):
         self.dev.set_state(psi, ome, omeold, omeoldold)
