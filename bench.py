@@ -232,7 +232,8 @@ def run_sweep_workload(args):
     from vorti2d_b200.batch import run_sweep, sweep_cases
     torch.cuda.set_device(0)
     cases = sweep_cases(seed=0)
-    res = run_sweep(cases, workers=args.sweep_workers, precision="mixed")
+    cont = args.sweep_continuation if args.sweep_continuation > 1.0 else None
+    res = run_sweep(cases, workers=args.sweep_workers, precision="mixed", continuation=cont)
     kinds = {}
     for r in res.results:
         k = r.name.rsplit("_", 1)[0]
@@ -266,7 +267,11 @@ def run_sweep_workload(args):
             "config": {"workload": "batched steady sweep, seed 0", "workers": res.workers,
                        "precond": "multifrontal LU per Newton iteration",
                        "newton": "<=20 iterations, stop when ||dq|| > 1e3 x the first",
-                       "krylov_max_it": 300},
+                       "krylov_max_it": 300,
+                       "continuation": (f"Re from 80 x{cont} per rung, rungs to ||dq||/(2N) <= 1e-7"
+                                        if cont else "none (free stream at the case's Re)")},
+            "max_re_converged": max([r.re for r in res.results if r.converged], default=None),
+            "min_re_failed": min([r.re for r in res.results if not r.converged], default=None),
             "krylov_iters": res.krylov_iters,
             "errors": sorted({r.error for r in res.results if r.error})[:4],
             "converged": res.converged, "instances": len(cases), "solve_s": res.solve_s,
@@ -648,6 +653,9 @@ def main():
                          "adjoint: steady adjoint gradients; large: the large unsteady grid; "
                          "unsteady_adjoint: the checkpointed unsteady adjoint")
     ap.add_argument("--sweep-workers", type=int, default=16)
+    ap.add_argument("--sweep-continuation", type=float, default=0.0,
+                    help="sweep: Reynolds continuation factor per rung from Re 80 (0: none, "
+                         "plain Newton from the free stream as the reference)")
     ap.add_argument("--large-grid", type=int, default=2049,
                     help="grid side of the large unsteady workload (--workload large)")
     ap.add_argument("--large-steps", type=int, default=3,

@@ -68,3 +68,25 @@ def test_sweep_matches_oracle_forces(v2d, oracle_mod):
         for key in ("cd", "cl"):
             want = getattr(fc, key)
             assert abs(getattr(r, key) - want) <= 1e-8 * max(1.0, abs(want)), (c.name, key)
+
+
+@pytest.mark.gpu
+def test_reynolds_continuation_reaches_the_oracle_state(v2d, oracle_mod):
+    """A sweep instance solved along Re 80 -> 120 -> 150 (set_re on one
+    handle, each Reynolds number from the previous state) ends on the steady
+    state the oracle's plain Newton finds at Re 150 (65x49 cylinder, alpha
+    0, where plain Newton converges too)."""
+    from vorti2d_b200.batch import Case, run_sweep
+    xg, yg = v2d.generate_cylinder(65, 49)
+    case = Case("cyl_cont", xg, yg, 150.0, 0.0)
+    out = run_sweep([case], workers=1, precision="fp64", pseudo_tol=1e-11, continuation=1.5,
+                    re_start=80.0)
+    r = out.results[0]
+    assert r.converged and r.rungs == 3 and r.re_reached == 150.0, r
+    o = oracle_mod.OracleSolver(xg, yg, re=150.0, alpha_deg=0.0, steady=True, pseudo_tol=1e-11,
+                                max_pseudo_iter=30)
+    o.advance(0.0)
+    fc = oracle_mod.compute_force_coeffs(o.imax, o.jmax, o.re, o.dksi, o.deta, o.beta, o.gama,
+                                         o.detadx, o.detady, o.xphys, o.yphys, o.ome)
+    assert abs(r.cd - fc.cd) <= 1e-8 * max(1.0, abs(fc.cd)), (r.cd, fc.cd)
+    assert abs(r.cl - fc.cl) <= 1e-8, (r.cl, fc.cl)

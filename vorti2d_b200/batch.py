@@ -49,6 +49,8 @@ class CaseResult:
     res: float
     krylov_iters: int = 0
     diverged: bool = False
+    re_reached: float = math.nan   # last Reynolds number solved (continuation)
+    rungs: int = 0                 # Reynolds numbers attempted (1 without continuation)
     cd: float = math.nan
     cl: float = math.nan
     cm: float = math.nan
@@ -112,9 +114,70 @@ class SweepResult:
         return self.newton_iters / self.solve_s if self.solve_s > 0 else 0.0
 
 
+def re_ladder(re_target: float, re_start: float, factor: float | None) -> list:
+    """Reynolds numbers of a natural-parameter continuation: re_start,
+    re_start*factor, ... while below re_target, then re_target itself.  No
+    continuation (``factor`` None or 0, or re_target <= re_start): the
+    target alone."""
+    if not (math.isfinite(re_target) and re_target > 0):
+        raise ValueError(f"re_ladder: target Re must be finite and positive, got {re_target}")
+    if not factor or re_target <= re_start:
+        return [float(re_target)]
+    if not (factor > 1.0 and math.isfinite(factor)):
+        raise ValueError(f"re_ladder: factor must be > 1, got {factor}")
+    if not re_start > 0:
+        raise ValueError(f"re_ladder: start Re must be positive, got {re_start}")
+    out, re = [], float(re_start)
+    while re < re_target:
+        out.append(re)
+        re *= factor
+    out.append(float(re_target))
+    return out
+
+
+def solve_case(s, r: CaseResult, ladder, max_newton: int, pseudo_tol: float,
+               rung_tol: float, diverge_factor: float) -> float:
+    """Steady Newton solves of one instance along ``ladder`` (its Reynolds
+    numbers, last = the case's own).  ``s`` is a Solver; ``r`` accumulates
+    iterations, the last update norm and the last Reynolds number reached.
+    Each Reynolds number gets at most ``max_newton`` iterations; an update
+    norm above ``diverge_factor`` times the first of its Reynolds number, or
+    a non-finite one, marks the instance diverged.  ``r.converged`` is set
+    when the last Reynolds number reaches ``pseudo_tol``.  Returns the last
+    update norm ||dq||/(2N)."""
+    cfg = s.cfg
+    urot = cfg.u_rot(cfg.t_start)
+    res = math.inf
+    for k, re in enumerate(ladder):
+        last = k == len(ladder) - 1
+        tol = pseudo_tol if last else max(pseudo_tol, rung_tol)
+        if len(ladder) > 1:
+            s.dev.set_re(re)
+        r.rungs += 1
+        res, first, n = math.inf, None, 0
+        while n < max_newton:
+            res = s._assemble_and_solve_once(cfg.inv_dtau(), cfg.inv_2dt(), urot)
+            n += 1
+            r.newton_iters += 1
+            r.krylov_iters += s._last_lin.iterations
+            r.res = res
+            first = res if first is None else first
+            if not np.isfinite(res) or res > diverge_factor * first:
+                r.diverged = True
+                return res
+            if res <= tol:
+                break
+        if not res <= tol:
+            return res
+        r.re_reached = re
+    r.converged = True
+    return res
+
+
 def run_sweep(cases, workers: int = 16, precision: str = "mixed", max_newton: int = 20,
               pseudo_tol: float = 1e-10, krylov_max_it: int = 300,
-              diverge_factor: float = 1e3, **cfg_kw) -> SweepResult:
+              diverge_factor: float = 1e3, continuation: float | None = None,
+              re_start: float = 80.0, rung_tol: float = 1e-7, **cfg_kw) -> SweepResult:
     """Solve every case to a steady state, ``workers`` instances at a time.
 
     Each instance runs the steady Newton loop (vorti2d/solver.py:136-145:
@@ -124,7 +187,13 @@ def run_sweep(cases, workers: int = 16, precision: str = "mixed", max_newton: in
     ``krylov_max_it`` iterations per Newton step.  Handles are created first
     (device allocation synchronises the device, so it is kept out of the
     timed solve phase); ``solve_s`` is the wall time of the concurrent
-    solves."""
+    solves.
+
+    ``continuation`` (a factor > 1) solves each case above ``re_start`` along
+    ``re_ladder``: every Reynolds number but the last to ||dq||/(2N) <=
+    ``rung_tol``, starting from the previous one's state, the last to
+    ``pseudo_tol``.  Without it every case starts from the free stream at
+    its own Re, the reference's steady method."""
     from .solver import Solver
     out = SweepResult(workers=workers)
     t0 = time.perf_counter()
@@ -135,30 +204,13 @@ def run_sweep(cases, workers: int = 16, precision: str = "mixed", max_newton: in
     results = [None] * len(cases)
     lock = threading.Lock()
 
-    def newton_loop(s, r):
-        cfg = s.cfg
-        urot = cfg.u_rot(cfg.t_start)
-        res, first = math.inf, None
-        while r.newton_iters < max_newton:
-            res = s._assemble_and_solve_once(cfg.inv_dtau(), cfg.inv_2dt(), urot)
-            r.newton_iters += 1
-            r.krylov_iters += s._last_lin.iterations
-            r.res = res
-            first = res if first is None else first
-            if not np.isfinite(res) or res > diverge_factor * first:
-                r.diverged = True
-                break
-            if res <= pseudo_tol:
-                break
-        return res
-
     def work(i):
         c, s = cases[i], solvers[i]
         t = time.perf_counter()
         r = CaseResult(c.name, c.re, c.alpha_deg, s.ndof, False, 0, math.inf)
         try:
-            res = newton_loop(s, r)
-            r.converged = bool(np.isfinite(res) and res <= pseudo_tol)
+            solve_case(s, r, re_ladder(c.re, re_start, continuation), max_newton, pseudo_tol,
+                       rung_tol, diverge_factor)
             if r.converged:
                 fc = s.force_coeffs()
                 r.cd, r.cl, r.cm = fc.cd, fc.cl, fc.cm

@@ -85,6 +85,14 @@ class DeviceState:
         check(lib().v2d_solver_get_state(self.h, *[dptr(o) for o in outs]), "get_state")
         return outs
 
+    def set_re(self, re: float):
+        """Change the Reynolds number of the handle's Newton system (the
+        state, pattern and workspaces stay; old LU factors are not reused)."""
+        if not (np.isfinite(re) and re > 0):
+            raise ValueError(f"set_re: Re must be finite and positive, got {re}")
+        self.params.re = float(re)
+        check(lib().v2d_solver_set_params(self.h, ctypes.byref(self.params)), "set_params")
+
     def set_state(self, psi, ome, omeold, omeoldold):
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (psi, ome, omeold, omeoldold)]
         for a in arrs:
