@@ -139,10 +139,10 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------- our arm
-def make_solver(v, xg, yg, precision, lu_reuse=0):
+def make_solver(v, xg, yg, precision, lu_reuse=0, lu_steps=0):
     cfg = v.Config(verbose=False, write_csv=False, write_xdmf=False, compute_forces=False,
                    raise_on_linear_failure=False, precision=precision, lu_reuse_its=lu_reuse,
-                   **WORKLOAD, **SOLVER)
+                   lu_reuse_steps=bool(lu_steps), **WORKLOAD, **SOLVER)
     return v.Solver(cfg, mesh=(xg, yg))
 
 
@@ -485,7 +485,7 @@ def profile_lu_launches(args):
     torch.cuda.set_device(0)
     xg, yg = v.generate_cylinder(IMAX, JMAX)
     prec = "mixed" if args.precision == "both" else args.precision
-    s = make_solver(v, xg, yg, prec, args.lu_reuse)
+    s = make_solver(v, xg, yg, prec, args.lu_reuse, args.lu_reuse_steps)
     times = s.times()
     for m in range(2):
         s.advance(times[m])
@@ -535,7 +535,7 @@ def run_ours(args, rank, world, local_rank):
     legs = ["mixed", "fp64"] if args.precision == "both" else [args.precision]
     launches = {}
     for prec in legs:
-        s = make_solver(v, xg, yg, prec, args.lu_reuse)
+        s = make_solver(v, xg, yg, prec, args.lu_reuse, args.lu_reuse_steps)
         times = s.times()
         for m in range(W):
             s.advance(times[m])
@@ -578,7 +578,7 @@ def run_ours(args, rank, world, local_rank):
             results["nnz"] = nnz.value
             # e2e: the same steps again through the public API, with the
             # state copied host->device and back every step
-            s2 = make_solver(v, xg, yg, prec, args.lu_reuse)
+            s2 = make_solver(v, xg, yg, prec, args.lu_reuse, args.lu_reuse_steps)
             for m in range(W):
                 s2.advance(times[m])
             results["e2e"] = _e2e(torch, v, s2, times, W, K, flush_buf)
@@ -645,6 +645,9 @@ def main():
     ap.add_argument("--lu-reuse", type=int, default=12,
                     help="keep LU factors while GMRES needs at most this many iterations "
                          "(0: factor every Newton Jacobian)")
+    ap.add_argument("--lu-reuse-steps", type=int, default=1, choices=[0, 1],
+                    help="1: keep the LU factors across time steps (and the e2e leg's "
+                         "set_state) under the same rule; 0: refactor at every step")
     ap.add_argument("--kernels-grid", type=int, default=2049,
                     help="grid side of the HBM-bound kernel roofline table (0: skip)")
     ap.add_argument("--workload", default="unsteady", choices=["unsteady", "sweep", "adjoint", "large",
@@ -766,7 +769,7 @@ def main():
         "config": {"workload": "unsteady BDF2 cylinder 181x181 Re=100 dt=0.2 kick 0.5<=2 outflow",
                    "precision": head, "newton_max": 5,
                    "krylov": "GMRES(30), multifrontal LU preconditioner (FP32 factors in mixed)",
-                   "lu_reuse_its": args.lu_reuse,
+                   "lu_reuse_its": args.lu_reuse, "lu_reuse_steps": args.lu_reuse_steps,
                    "l2": "flushed (256 MiB write) before every timed step",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": world * res["e2e"]["steps_per_s"], "unit": "steps/s",

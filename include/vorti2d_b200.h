@@ -183,6 +183,12 @@ typedef struct {
                              with kept factors that needs more than k+5
                              iterations refactors and solves again.  Newton
                              steps are still solved to rtol.                */
+    int lu_reuse_steps;   /* LU, with lu_reuse_its > 0: 1 keeps the factors
+                             across the BDF2 history shift and
+                             v2d_solver_set_state too, under the same
+                             iteration rule; 0 refreshes them at the first
+                             Newton iteration of every time step and after
+                             every set_state (0)                            */
 } v2d_krylov_params;
 
 void v2d_krylov_defaults(v2d_krylov_params *p);

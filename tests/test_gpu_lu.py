@@ -104,21 +104,24 @@ def test_steady_cylinder_129_matches_oracle(v2d, oracle_mod):
     s.close()
 
 
-@pytest.mark.parametrize("precision,reuse", [("fp64", 0), ("mixed", 0), ("mixed", 20),
-                                              ("fp64", 20)])
-def test_unsteady_cylinder_181_matches_oracle(v2d, oracle_mod, precision, reuse):
+@pytest.mark.parametrize("precision,reuse,steps", [("fp64", 0, False), ("mixed", 0, False),
+                                                    ("mixed", 20, False), ("fp64", 20, False),
+                                                    ("mixed", 12, True)])
+def test_unsteady_cylinder_181_matches_oracle(v2d, oracle_mod, precision, reuse, steps):
     """The benchmark case (181x181, Re=100, dt=0.2, rotational kick 0.5 until
     t=2, outflow far field, at most 5 Newton iterations per step): the first
     three BDF2 steps equal the oracle's to 1e-9 with |dCd| < 1e-8, with the
-    LU factors refreshed every Newton iteration or reused while GMRES stays
-    within 20 iterations."""
+    LU factors refreshed every Newton iteration, reused within a time step
+    while GMRES stays within 20 iterations, or reused across time steps
+    while it stays within 12."""
     imax = jmax = 181
     xg, yg = oracle_mod.generate_cylinder(imax, jmax)
     kw = dict(re=100.0, steady=False, dt_phys=0.2, rot_speed=0.5, rot_until=2.0,
               farfield_bc="outflow")
     ref = oracle_mod.OracleSolver(xg, yg, pseudo_tol=1e-10, max_pseudo_iter=5, **kw)
     s = v2d.Solver(cfg(v2d, ksp_rtol=1e-10, pseudo_tol=1e-10, max_pseudo_iter=5,
-                       precision=precision, lu_reuse_its=reuse, **kw), mesh=(xg, yg))
+                       precision=precision, lu_reuse_its=reuse, lu_reuse_steps=steps, **kw),
+                     mesh=(xg, yg))
     for t in ref.times()[:3]:
         _, it_ref = ref.advance(t)
         _, it, _ = s.advance(t)

@@ -219,3 +219,28 @@ def test_state_round_trip_through_pinned_buffers(v2d, oracle_mod):
     with pytest.raises(ValueError):
         s.get_state(out=[np.zeros((N, 2))[:, 0]] + host[1:])
     s.close()
+
+
+def test_set_state_keeps_factors_when_reused_across_steps(v2d, oracle_mod):
+    """With LU factors kept across steps, copying the state out and back in
+    between steps (set_state) changes nothing: the next step equals that of
+    a twin solver that kept its state on the device, and no extra
+    factorization is needed for it."""
+    xg, yg = oracle_mod.generate_cylinder(65, 49)
+    kw = dict(re=100.0, steady=False, dt_phys=0.2, rot_speed=0.5, rot_until=2.0,
+              farfield_bc="outflow", verbose=False, precision="mixed", precond="lu",
+              lu_reuse_its=12, lu_reuse_steps=True, max_pseudo_iter=5)
+    a = v2d.Solver(v2d.Config(**kw), mesh=(xg, yg))
+    b = v2d.Solver(v2d.Config(**kw), mesh=(xg, yg))
+    times = a.times()
+    for t in times[:3]:
+        a.advance(t)
+        b.advance(t)
+    b.set_state(*b.get_state())
+    a.advance(times[3])
+    b.advance(times[3])
+    for x, y in zip(a.get_state(), b.get_state()):
+        assert np.max(np.abs(x - y)) <= 1e-12 * max(1.0, np.max(np.abs(x)))
+    assert a.newton_log[-1][1:3] == b.newton_log[-1][1:3]
+    a.close()
+    b.close()

@@ -38,7 +38,7 @@ _ll = ctypes.c_longlong
 class KrylovParams(ctypes.Structure):
     _fields_ = [("restart", _i), ("max_it", _i), ("rtol", _d), ("atol", _d),
                 ("precond", _i), ("precision", _i), ("inner_rtol", _d), ("dc_max_it", _i),
-                ("lu_leaf", _i), ("lu_reuse_its", _i)]
+                ("lu_leaf", _i), ("lu_reuse_its", _i), ("lu_reuse_steps", _i)]
 
 
 class LinStats(ctypes.Structure):

@@ -77,6 +77,10 @@ class Config:
     factors across the Newton iterations of one time step while the last
     solve with them needed at most k Krylov iterations (each Newton step is
     still solved to ``ksp_rtol``)."""
+    lu_reuse_steps: bool = False
+    """LU preconditioner with ``lu_reuse_its > 0``: keep the factors across
+    time steps and ``set_state`` too (the same iteration rule decides when to
+    refactor)."""
     raise_on_linear_failure: bool = True
     """Raise if a Krylov solve misses ``ksp_rtol`` (the reference raises on a
     failed PETSc solve, vorti2d/petsc_solver.py:103-105)."""

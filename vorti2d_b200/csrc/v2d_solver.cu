@@ -206,6 +206,7 @@ extern "C" void v2d_krylov_defaults(v2d_krylov_params *p)
     p->dc_max_it = 20;
     p->lu_leaf = 64;
     p->lu_reuse_its = 0;
+    p->lu_reuse_steps = 0;
 }
 
 extern "C" int v2d_solver_destroy(v2d_solver *S)
@@ -323,7 +324,10 @@ extern "C" int v2d_solver_set_state(v2d_solver *S, const double *psi, const doub
         if (src[q]) V2D_CUDA_TRY(cudaMemcpyAsync(dst[q], src[q], bytes, cudaMemcpyHostToDevice, S->s));
     V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
     S->assembled = false;
-    S->lu_valid = false;   // a new state: do not precondition with old factors
+    // a new state: old factors precondition it only when the caller keeps
+    // factors across steps (a solve that needs more than lu_reuse_its + 5
+    // iterations with them refactors and solves again)
+    if (!S->prm.krylov.lu_reuse_steps) S->lu_valid = false;
     return V2D_OK;
 }
 
@@ -481,7 +485,9 @@ extern "C" int v2d_solver_shift_history(v2d_solver *S)
     const size_t bytes = (size_t)S->g.N * sizeof(double);
     V2D_CUDA_TRY(cudaMemcpyAsync(S->g.omeoldold, S->g.omeold, bytes, cudaMemcpyDeviceToDevice, S->s));
     V2D_CUDA_TRY(cudaMemcpyAsync(S->g.omeold, S->g.ome, bytes, cudaMemcpyDeviceToDevice, S->s));
-    S->lu_valid = false;   // factors are reused within a time step, refreshed at the next
+    // factors are reused within a time step and refreshed at the next, unless
+    // the caller keeps them across steps under the same iteration rule
+    if (!S->prm.krylov.lu_reuse_steps) S->lu_valid = false;
     return V2D_OK;
 }
 

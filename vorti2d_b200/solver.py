@@ -43,6 +43,7 @@ def solver_params(cfg: Config) -> _lib.SolverParams:
     k.precond = cfg.precond_code()
     k.inner_rtol = float(cfg.inner_rtol)
     k.lu_reuse_its = int(cfg.lu_reuse_its)
+    k.lu_reuse_steps = int(bool(cfg.lu_reuse_steps))
     p.krylov = k
     return p
 
