@@ -353,7 +353,8 @@ def run_large_workload(args):
     cfg = v.Config(verbose=False, write_csv=False, write_xdmf=False, compute_forces=False,
                    re=200.0, steady=False, dt_phys=0.05, farfield_bc="outflow",
                    raise_on_linear_failure=False, precision=args.large_precision,
-                   lu_reuse_its=args.lu_reuse, **SOLVER)
+                   lu_reuse_its=args.lu_reuse, lu_reuse_steps=bool(args.lu_reuse_steps),
+                   **SOLVER)
     t0 = time.perf_counter()
     s = v.Solver(cfg, mesh=(xg, yg))
     setup_s = time.perf_counter() - t0
@@ -387,6 +388,7 @@ def run_large_workload(args):
             "data": "synthetic",
             "config": {"workload": f"large unsteady BDF2 cylinder {n}x{n} Re=200 dt=0.05 outflow",
                        "unknowns": 2 * n * n, "lu_reuse_its": args.lu_reuse,
+                       "lu_reuse_steps": args.lu_reuse_steps,
                        "l2": "flushed (256 MiB write) before every timed step"},
             "setup_s": setup_s, "first_step_s": first_s, "newton_per_step": newton / K,
             "krylov_per_step": krylov / K,
