@@ -49,7 +49,7 @@ def load_mesh(xg_path: str, yg_path: str):
 
 def load_cgns_ogrid(cgns_path: str, plane: int = 0, block: int = 0, verbose: bool = False):
     """pyHyp CGNS reader (vorti2d/mesh.py:93-140).  Needs ``cgnsutilities``,
-    which this build does not ship; convert the grid to xg/yg CSV instead."""
+    which vorti2d_b200 does not depend on; convert the grid to xg/yg CSV instead."""
     try:
         import cgnsutilities  # noqa: F401
     except ImportError as exc:

@@ -296,11 +296,12 @@ class Solver:
 
     # ------------------------------------------------------------------- run
     def run(self):
-        """vorti2d/solver.py:148-224 (XDMF/HDF5 output needs h5py, which this
-        build does not ship: ``write_xdmf`` is ignored with a notice)."""
+        """vorti2d/solver.py:148-224 (XDMF/HDF5 output needs h5py, which
+        vorti2d_b200 does not depend on: ``write_xdmf`` is ignored with a
+        notice)."""
         cfg = self.cfg
         if cfg.write_xdmf and cfg.verbose:
-            self._log("  note: write_xdmf ignored (XDMF/HDF5 output is not part of this build)")
+            self._log("  note: write_xdmf ignored (XDMF/HDF5 output is not part of vorti2d_b200)")
         needs_dir = cfg.write_csv or cfg.compute_forces or True
         if needs_dir:
             fields_io.ensure_dirs(cfg.out_dir)
