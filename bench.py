@@ -39,6 +39,7 @@ WORKLOAD = dict(re=100.0, steady=False, dt_phys=0.2, rot_speed=0.5, rot_until=2.
 SOLVER = dict(ksp_restart=30, ksp_rtol=1e-10, krylov_max_it=3000, pseudo_tol=1e-10,
               max_pseudo_iter=5, precond="lu")
 METRIC = "BDF2 steps/s, 181x181 cylinder O-grid Re=100 dt=0.2 (<=5 Newton, GMRES(30))"
+WORKLOAD_NAME = "unsteady BDF2 cylinder 181x181 Re=100 dt=0.2 kick 0.5<=2 outflow"
 L2_FLUSH_BYTES = 256 << 20
 SPMV_BYTES_PER_NNZ = {"fp64": 8 + 4, "fp32": 4 + 4}
 # DRAM bytes (read + write) of one mixed-precision LU apply at 181x181: the
@@ -727,7 +728,7 @@ def main():
             "steps": n, "warmup": W, "ms_per_step": 1e3 * dt / n, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "unsteady BDF2 cylinder 181x181 Re=100 dt=0.2 kick 0.5<=2 outflow",
+            "config": {"workload": WORKLOAD_NAME,
                        "solver": "C restatement of vorti2d_core.f90 + scipy SuperLU (MUMPS stand-in)"},
             "cpu_baseline": {"value": val, "unit": "steps/s", "cores": 1, "kind": "port",
                              "sample": f"{n} BDF2 steps after {W} warm-up step(s) from t=0 "
@@ -768,7 +769,7 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_head,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32-krylov/f64" if head == "mixed" else "f64", "data": "synthetic",
-        "config": {"workload": "unsteady BDF2 cylinder 181x181 Re=100 dt=0.2 kick 0.5<=2 outflow",
+        "config": {"workload": WORKLOAD_NAME,
                    "precision": head, "newton_max": 5,
                    "krylov": "GMRES(30), multifrontal LU preconditioner (FP32 factors in mixed)",
                    "lu_reuse_its": args.lu_reuse, "lu_reuse_steps": args.lu_reuse_steps,

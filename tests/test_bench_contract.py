@@ -1,0 +1,36 @@
+"""The reference arm of bench.py on the CPU: one JSON line on the same
+metric, unit and workload as the GPU arm, with the keys the benchmark
+contract asks for (a bounded sample of the CPU restatement)."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _last_json(out: str) -> dict:
+    lines = [ln for ln in out.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, out[-2000:]
+    return json.loads(lines[0])
+
+
+def test_reference_arm_prints_one_contract_line():
+    sys.path.insert(0, ROOT)
+    import bench
+    p = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1",
+                        "--warmup", "3"], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr[-2000:]
+    d = _last_json(p.stdout)
+    assert d["impl"] == "reference"
+    assert d["metric"] == bench.METRIC and d["unit"] == "steps/s"
+    assert d["higher_is_better"] is True and d["n_gpus"] == 1
+    assert d["config"]["workload"] == bench.WORKLOAD_NAME
+    assert d["value"] > 0 and d["steps"] == 1 and d["warmup"] == 1
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] == 1 and cb["value"] == d["value"]
+    assert cb["sample"]
+    e = d["e2e"]
+    assert e["value"] == d["value"] and e["unit"] == d["unit"]
+    assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+    assert d["vs_baseline"] is None
