@@ -189,7 +189,15 @@ __global__ void __launch_bounds__(256) k_scale_precond(const Desc *d, Ctl *ctl, 
     V2D_GRID_STRIDE(q, units) { precond_block<T>(d, (int)q, vj, z); }
 }
 
-// y = A x, kTPR threads per row, FP32 or FP64 values/vectors.
+// Entries of a row one lane takes with all its loads issued together: the
+// 9-point stencil's rows hold at most 13 entries, kTPR * kSpmvRowRegs = 16.
+constexpr int kSpmvRowRegs = 4;
+
+// y = A x, kTPR threads per row, FP32 or FP64 values/vectors.  A lane's
+// first kSpmvRowRegs entries load their column indices and values first and
+// then the gathered x, so a row's loads overlap instead of chaining index ->
+// gather per entry; longer rows finish in a plain loop.  The sum runs over
+// the lane's entries in column-position order either way.
 template <class T>
 __device__ __forceinline__ void spmv_rows(const int *__restrict__ rowptr, const int *__restrict__ colind,
                                           const T *__restrict__ val, const T *__restrict__ x,
@@ -207,8 +215,22 @@ __device__ __forceinline__ void spmv_rows(const int *__restrict__ rowptr, const 
         int row = valid ? (int)(t / kTPR) : 0;
         T acc = 0;
         if (valid) {
-            int p0 = rowptr[row], p1 = rowptr[row + 1];
-            for (int p = p0 + lane; p < p1; p += kTPR) acc += val[p] * x[colind[p]];
+            const int p0 = rowptr[row], p1 = rowptr[row + 1];
+            int c[kSpmvRowRegs];
+            T v[kSpmvRowRegs], xv[kSpmvRowRegs];
+#pragma unroll
+            for (int k = 0; k < kSpmvRowRegs; ++k) {
+                const int p = p0 + lane + k * kTPR;
+                c[k] = p < p1 ? colind[p] : -1;
+                v[k] = p < p1 ? val[p] : T(0);
+            }
+#pragma unroll
+            for (int k = 0; k < kSpmvRowRegs; ++k) xv[k] = c[k] >= 0 ? x[c[k]] : T(0);
+#pragma unroll
+            for (int k = 0; k < kSpmvRowRegs; ++k)
+                if (c[k] >= 0) acc += v[k] * xv[k];
+            for (int p = p0 + lane + kSpmvRowRegs * kTPR; p < p1; p += kTPR)
+                acc += val[p] * x[colind[p]];
         }
 #pragma unroll
         for (int o = kTPR / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, kTPR);
