@@ -66,6 +66,22 @@ def test_host_only_entry_points(v2d):
     assert b"node_neighbors" in L.v2d_last_error()
 
 
+def test_krylov_defaults_and_config_mapping(v2d):
+    """The C defaults factor every Newton Jacobian (as MUMPS does) and keep
+    no factors across steps; Config's GPU knobs reach the C structure."""
+    from vorti2d_b200 import _lib
+    from vorti2d_b200.solver import solver_params
+    d = _lib.krylov_defaults()
+    assert d.lu_reuse_its == 0 and d.lu_reuse_steps == 0 and d.lu_leaf == 64
+    p = solver_params(v2d.Config(re=150.0, precision="mixed", precond="lu", lu_reuse_its=12,
+                                 lu_reuse_steps=True, krylov_max_it=300))
+    assert p.re == 150.0 and p.krylov.lu_reuse_its == 12 and p.krylov.lu_reuse_steps == 1
+    assert p.krylov.precond == _lib.PC_LU and p.krylov.precision == _lib.PREC_MIXED
+    assert p.krylov.max_it == 300
+    q = solver_params(v2d.Config())
+    assert q.krylov.lu_reuse_its == 0 and q.krylov.lu_reuse_steps == 0
+
+
 def test_argument_errors_before_any_device_work(v2d):
     from vorti2d_b200 import _lib
     L = _lib.lib()
