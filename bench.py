@@ -505,7 +505,7 @@ def profile_lu_launches(args):
     times = s.times()
     for m in range(2):
         s.advance(times[m])
-    kinds = ["fwd_front", "fwd_z", "fwd_u", "bwd_front", "bwd_y", "bwd_x"]
+    kinds = ["fwd_front", "fwd_z", "fwd_u", "bwd_front", "bwd_y", "bwd_x", "flow"]
     out = {"profile": "LU solve launches", "precision": prec}
     for label, flush in (("warm", 0), ("cold", L2_FLUSH_BYTES)):
         cap = 256

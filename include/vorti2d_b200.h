@@ -340,6 +340,15 @@ int v2d_solver_time_spmv(v2d_solver *s, int fp32, int reps, long long flush_byte
  * entries. */
 int v2d_lu_plan_info(int imax, int jmax, const int *indptr, const int *indices, int leaf,
                      long long *out8);
+/* Planning aid for the dataflow solve of the upper levels (host only):
+ * info4 = {first level of the one-launch dataflow solve, work items, 1 if the
+ * item order passed its check, fronts}; when cap_items >= items, items gets
+ * 4 ints per item (kind 0 z rows, 1 contribution rows, 2 backward y rows,
+ * 3 backward x rows, 4 x rows of a front without contribution rows; front;
+ * row chunk; the count its dependency counter must reach), and when
+ * cap_fronts >= fronts, parent gets each front's parent (-1 at the root). */
+int v2d_lu_flow_plan(int imax, int jmax, const int *indptr, const int *indices, int leaf,
+                     int *info4, int *items, int cap_items, int *parent, int cap_fronts);
 
 /* Measurement aid (no reference counterpart): device time in ms, summed over
  * the Newton iterations since the last reset, of the four phases of a Newton

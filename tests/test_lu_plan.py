@@ -76,3 +76,143 @@ def test_plan_rejects_bad_input(v2d, oracle_mod):
     assert code == _lib.V2D_EARG
     out = (ctypes.c_longlong * 8)()
     assert _lib.lib().v2d_lu_plan_info(9, 7, None, None, 64, out) == _lib.V2D_EARG
+
+
+def flow_plan(v2d, imax, jmax, ip, ix, leaf=64):
+    from vorti2d_b200 import _lib
+    info = np.zeros(4, dtype=np.intc)
+    code = _lib.lib().v2d_lu_flow_plan(imax, jmax, _lib.iptr(ip), _lib.iptr(ix), leaf,
+                                       _lib.iptr(info), None, 0, None, 0)
+    assert code == 0, v2d._lib.last_error()
+    items = np.zeros(4 * max(int(info[1]), 1), dtype=np.intc)
+    parent = np.zeros(max(int(info[3]), 1), dtype=np.intc)
+    code = _lib.lib().v2d_lu_flow_plan(imax, jmax, _lib.iptr(ip), _lib.iptr(ix), leaf,
+                                       _lib.iptr(info), _lib.iptr(items), int(info[1]),
+                                       _lib.iptr(parent), int(info[3]))
+    assert code == 0, v2d._lib.last_error()
+    return info, items[:4 * int(info[1])].reshape(-1, 4), parent[:int(info[3])]
+
+
+FZ, FU, BY, BX, BXROOT = range(5)
+
+
+def _wait_ctr(kind, q, parent, nf):
+    # the counter each kind waits on (4 per front: z, children's contribution, y, x)
+    return {FZ: nf + q, FU: q, BY: 3 * nf + parent[q] if parent[q] >= 0 else -1,
+            BX: 2 * nf + q, BXROOT: q}[kind]
+
+
+def _done_ctr(kind, q, parent, nf):
+    return {FZ: q, FU: nf + parent[q] if parent[q] >= 0 else -1, BY: 2 * nf + q,
+            BX: 3 * nf + q, BXROOT: 3 * nf + q}[kind]
+
+
+def _producers(items, parent):
+    """What each item reads, from the algorithm alone (not from the
+    counters): z rows need every contribution chunk of the front's children,
+    contribution rows every z chunk of the front, backward y rows every x
+    chunk of the parent, x rows every y chunk of the front (or, without
+    contribution rows, every z chunk)."""
+    by_kind = {}
+    for k, (kind, q, c, t) in enumerate(items):
+        by_kind.setdefault((kind, q), []).append(k)
+    kids = {}
+    for k, (kind, q, c, t) in enumerate(items):
+        if kind == FU:
+            kids.setdefault(parent[q], set()).add(q)
+    prod = []
+    for kind, q, c, t in items:
+        if kind == FZ:
+            p = [k for ch in kids.get(q, ()) for k in by_kind[(FU, ch)]]
+        elif kind == FU:
+            p = by_kind[(FZ, q)]
+        elif kind == BY:
+            p = by_kind.get((BX, parent[q]), []) + by_kind.get((BXROOT, parent[q]), [])
+        elif kind == BX:
+            p = by_kind[(BY, q)]
+        else:
+            p = by_kind[(FZ, q)]
+        prod.append(p)
+    return prod
+
+
+def _simulate(items, parent, nf, ctas, rng):
+    """The kernel's schedule: CTAs take items in ticket order, wait on one
+    counter, finish after a random time, count the item.  Returns the finish
+    order; fails on a deadlock or on an item starting before what it reads."""
+    n = len(items)
+    ctr = np.zeros(4 * nf, dtype=np.int64)
+    prod = _producers(items, parent)
+    done = np.zeros(n, dtype=bool)
+    ticket = 0
+    held = {}            # cta -> [item, finish time or None while waiting]
+    now, order = 0.0, []
+    for cta in range(ctas):
+        if ticket < n:
+            held[cta] = [ticket, None]
+            ticket += 1
+    while held:
+        progressed = False
+        for cta, slot in list(held.items()):
+            k = slot[0]
+            kind, q, c, t = items[k]
+            if slot[1] is None:
+                w = _wait_ctr(kind, q, parent, nf)
+                if t <= 0 or ctr[w] >= t:
+                    assert all(done[p] for p in prod[k]), (k, items[k])
+                    slot[1] = now + rng.uniform(0.5, 2.0)
+                    progressed = True
+        running = [(s[1], cta) for cta, s in held.items() if s[1] is not None]
+        assert running or progressed, "deadlock"
+        if not running:
+            continue
+        tfin, cta = min(running)
+        now = tfin
+        k = held[cta][0]
+        kind, q, c, t = items[k]
+        d = _done_ctr(kind, q, parent, nf)
+        if d >= 0:
+            ctr[d] += 1
+        done[k] = True
+        order.append(k)
+        if ticket < n:
+            held[cta] = [ticket, None]
+            ticket += 1
+        else:
+            del held[cta]
+    assert done.all()
+    return order
+
+
+@pytest.mark.parametrize("imax,jmax,leaf", [(33, 21, 16), (65, 49, 64), (129, 129, 64),
+                                            (181, 181, 64), (257, 129, 64)])
+def test_flow_plan_order_is_safe(v2d, oracle_mod, imax, jmax, leaf):
+    """The dataflow solve's work items: validated by the plan, every front
+    above the one-CTA-per-front levels appears with the chunk counts of its
+    rows, and a simulated schedule (1 to 300 CTAs, random item times) never
+    deadlocks and never starts an item before the items it reads."""
+    ip, ix = pattern(oracle_mod, imax, jmax, 1)
+    info, items, parent = flow_plan(v2d, imax, jmax, ip, ix, leaf)
+    L0, nflow, valid, nf = (int(v) for v in info)
+    assert valid == 1 and nflow == len(items) > 0
+    kinds = set(items[:, 0].tolist())
+    assert {FZ, FU, BX} <= kinds and BXROOT in kinds
+    # forward items precede backward ones
+    fwd = np.isin(items[:, 0], [FZ, FU])
+    assert fwd[:fwd.sum()].all()
+    rng = np.random.default_rng(imax * 7 + jmax)
+    for ctas in (1, 2, 5, 37, 300):
+        order = _simulate(items, parent, nf, ctas, rng)
+        assert len(order) == nflow
+
+
+def test_flow_plan_181_levels(v2d, oracle_mod):
+    """181x181, 64-node leaves: levels 0-3 (512, 256, 128, 64 fronts) keep
+    the one-CTA-per-front launches; the other 65 fronts (levels 4-10) form
+    the dataflow, the root last."""
+    ip, ix = pattern(oracle_mod, 181, 181, 1)
+    info, items, parent = flow_plan(v2d, 181, 181, ip, ix)
+    assert int(info[0]) == 4 and int(info[3]) == 1025
+    fronts = sorted(set(items[:, 1].tolist()))
+    assert fronts == list(range(960, 1025))
+    assert parent[1024] == -1 and (parent[960:1024] >= 960).all()

@@ -70,6 +70,12 @@ struct MfPlan {
     int *d_lvl4 = nullptr;         // per level: first front, fronts, row chunks (S, CB)
     int *d_vars = nullptr, *d_cbmap = nullptr, *d_asm_csr = nullptr, *d_asm_row = nullptr;
     long long *d_asm_pos = nullptr;
+    // dataflow solve of the levels from flow_level up (one launch; opt-in):
+    // work items {kind, front, chunk, wait target}, forward then backward,
+    // validated on the host (flow_valid) when the plan is built
+    int flow_level = 0, nflow = 0, flow_valid = 0;
+    std::vector<int> h_flow;
+    int *d_flow = nullptr;
     // host copies, kept only between the build and the upload
     std::vector<int> h_vars, h_cbmap, h_asm_csr, h_asm_row;
     std::vector<long long> h_asm_pos;
@@ -93,6 +99,8 @@ struct MfFactor {
     int *ipiv = nullptr, *perm = nullptr, *flag = nullptr;
     MfBarrier *bar = nullptr;
     int coop_grid = 0;          // CTAs of the one-launch persistent solve (0: per-phase launches)
+    int *flow_ctr = nullptr;    // dataflow solve: 4 counters per front + the work ticket
+    int flow_grid = 0;          // CTAs of the dataflow solve (0: per-phase launches)
     cudaGraphExec_t graph = nullptr;
     const double *graph_val = nullptr;
     const int *graph_rowptr = nullptr;
@@ -129,7 +137,7 @@ int mf_apply(const MfPlan *P, const MfFactor *M, const void *b, void *x, const i
 int mf_apply_transpose(const MfPlan *P, MfFactor *M, const void *g, void *lambda, cudaStream_t s);
 int mf_flag(const MfFactor *M, int *flag, cudaStream_t s);
 // V2D_ETIMEOUT (and a reset barrier) if a grid barrier of the persistent solve
-// timed out since the last check.
+// or a dependency wait of the dataflow solve timed out since the last check.
 int mf_check_barrier(MfFactor *M, cudaStream_t s);
 // Average device time (ms) of `reps` LU applies to a zero vector, each after a
 // write of flush_bytes (evicts L2); CUDA events on stream s.

@@ -61,6 +61,46 @@ namespace v2d {
 
 // rows per work item of the solve (kSolveRows below; also the level table's unit)
 constexpr int kSolveRowsHost = 8;
+// levels with at least this many fronts are solved with one CTA per front
+constexpr int kFrontPerCtaHost = 64;
+
+// Dataflow solve of the upper levels: one launch runs the work items of the
+// levels from the plan's flow_level up, forward then backward, in a fixed
+// order.  A CTA takes the next item by ticket, waits until one counter
+// reaches the item's target, runs it and counts it on one counter.  Item
+// kinds and the counters (4 per front: z chunks done, the children's
+// contribution chunks done, y chunks done, x chunks done):
+//   kFlowZ      z rows of a front        waits: children's contribution rows  done: z[q]
+//   kFlowU      contribution rows        waits: z[q] (all z chunks)           done: cu[parent]
+//   kFlowY      backward y rows          waits: x[parent] (all x chunks)      done: y[q]
+//   kFlowX      backward x rows          waits: y[q] (all y chunks)           done: x[q]
+//   kFlowXRoot  x rows, no contribution  waits: z[q]                          done: x[q]
+// Every counter an item waits on is advanced only by items earlier in the
+// order, which the plan checks: a ticket-ordered CTA then only ever waits
+// for items that running CTAs already hold, so the launch needs no
+// co-resident grid.
+enum { kFlowZ = 0, kFlowU = 1, kFlowY = 2, kFlowX = 3, kFlowXRoot = 4 };
+
+__host__ __device__ inline int flow_wait_ctr(int kind, int q, int parent, int nf)
+{
+    switch (kind) {
+    case kFlowZ: return nf + q;
+    case kFlowU: return q;
+    case kFlowY: return parent >= 0 ? 3 * nf + parent : -1;
+    case kFlowX: return 2 * nf + q;
+    default: return q;
+    }
+}
+
+__host__ __device__ inline int flow_done_ctr(int kind, int q, int parent, int nf)
+{
+    switch (kind) {
+    case kFlowZ: return q;
+    case kFlowU: return parent >= 0 ? nf + parent : -1;
+    case kFlowY: return 2 * nf + q;
+    default: return 3 * nf + q;
+    }
+}
 
 // ================================================================ symbolic
 namespace {
@@ -178,10 +218,99 @@ void mf_plan_destroy(MfPlan *p)
     if (!p) return;
     void *ptrs[] = {p->d_S, p->d_f, p->d_voff, p->d_uoff, p->d_child0, p->d_child1, p->d_parent,
                     p->d_foff, p->d_toff, p->d_lvl4,
-                    p->d_vars, p->d_cbmap, p->d_asm_csr, p->d_asm_row, p->d_asm_pos};
+                    p->d_vars, p->d_cbmap, p->d_asm_csr, p->d_asm_row, p->d_asm_pos,
+                    p->d_flow};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     delete p;
+}
+
+// Work items of the dataflow solve (kinds and counters at flow_wait_ctr) for
+// the levels from the first one above which every level has fewer than
+// kFrontPerCtaHost fronts, then the check that makes the order safe: the
+// counter each item waits on reaches exactly the item's target, and only
+// through items before it.  A plan that fails the check (or has no such
+// levels) keeps nflow = 0 and the per-phase launches.
+static void flow_build(MfPlan *P)
+{
+    const int nf = P->nfront, nl = P->nlevel;
+    P->h_flow.clear();
+    P->nflow = 0;
+    P->flow_valid = 0;
+    int L0 = nl;
+    while (L0 > 0 && P->lvl_off[L0] - P->lvl_off[L0 - 1] < kFrontPerCtaHost) --L0;
+    P->flow_level = L0;
+    if (L0 >= nl) return;
+    auto chunks = [](int rows) { return (rows + kSolveRowsHost - 1) / kSolveRowsHost; };
+    std::vector<int> lvl(nf, 0);
+    for (int L = 0; L < nl; ++L)
+        for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q) lvl[q] = L;
+    auto nz = [&](int q) { return std::max(1, chunks(P->S[q])); };
+    std::vector<int> &it = P->h_flow;
+    auto push = [&](int kind, int q, int c, int target) {
+        it.push_back(kind);
+        it.push_back(q);
+        it.push_back(c);
+        it.push_back(target);
+    };
+    for (int L = L0; L < nl; ++L) {
+        for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q) {
+            int target = 0;
+            for (int c : {P->child0[q], P->child1[q]})
+                if (c >= 0 && lvl[c] >= L0) target += chunks(P->f[c] - P->S[c]);
+            for (int c = 0; c < nz(q); ++c) push(kFlowZ, q, c, target);
+        }
+        for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q)
+            for (int c = 0; c < chunks(P->f[q] - P->S[q]); ++c) push(kFlowU, q, c, nz(q));
+    }
+    for (int L = nl - 1; L >= L0; --L) {
+        for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q) {
+            if (P->f[q] == P->S[q]) continue;
+            const int par = P->parent[q];
+            const int target = par >= 0 ? chunks(P->S[par]) : 0;
+            for (int c = 0; c < chunks(P->S[q]); ++c) push(kFlowY, q, c, target);
+        }
+        for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q) {
+            const bool cb = P->f[q] > P->S[q];
+            for (int c = 0; c < chunks(P->S[q]); ++c)
+                push(cb ? kFlowX : kFlowXRoot, q, c, cb ? chunks(P->S[q]) : nz(q));
+        }
+    }
+    // the check: totals per counter, then each wait against the items before it
+    const int nitems = (int)it.size() / 4;
+    std::vector<int> total(4 * nf, 0), seen(4 * nf, 0);
+    bool ok = true;
+    for (int k = 0; k < nitems && ok; ++k) {
+        const int kind = it[4 * k], q = it[4 * k + 1];
+        if (q < 0 || q >= nf || lvl[q] < L0 || kind < kFlowZ || kind > kFlowXRoot) {
+            ok = false;
+            break;
+        }
+        const int c = it[4 * k + 2];
+        const int rows = kind == kFlowU ? P->f[q] - P->S[q] : P->S[q];
+        const int nc = kind == kFlowZ ? nz(q) : chunks(rows);
+        if (c < 0 || c >= nc) {
+            ok = false;
+            break;
+        }
+        const int d = flow_done_ctr(kind, q, P->parent[q], nf);
+        if (d >= 0) ++total[d];
+    }
+    for (int k = 0; k < nitems && ok; ++k) {
+        const int kind = it[4 * k], q = it[4 * k + 1], target = it[4 * k + 3];
+        if (kind == kFlowY && P->parent[q] < 0) ok = false;
+        const int w = flow_wait_ctr(kind, q, P->parent[q], nf);
+        if (target > 0 && (w < 0 || seen[w] != target || total[w] != target)) ok = false;
+        if (target == 0 && w >= 0 && total[w] != 0) ok = false;
+        const int d = flow_done_ctr(kind, q, P->parent[q], nf);
+        if (d >= 0) ++seen[d];
+    }
+    if (!ok) {
+        it.clear();
+        return;
+    }
+    P->nflow = nitems;
+    P->flow_valid = 1;
 }
 
 int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_colind,
@@ -440,6 +569,7 @@ int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_c
     P->h_asm_csr = std::move(asm_csr);
     P->h_asm_row = std::move(asm_row);
     P->h_asm_pos = std::move(asm_pos);
+    flow_build(P);
     *out = P;
     return V2D_OK;
 }
@@ -475,6 +605,7 @@ int mf_plan_create(int imax, int jmax, int n, const int *h_rowptr, const int *h_
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_asm_csr, P->h_asm_csr);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_asm_row, P->h_asm_row);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_asm_pos, P->h_asm_pos);
+    if (st_up == V2D_OK && P->nflow > 0) st_up = upload_vec(&P->d_flow, P->h_flow);
     if (st_up != V2D_OK) {
         mf_plan_destroy(P);
         return st_up;
@@ -507,6 +638,29 @@ extern "C" int v2d_lu_plan_info(int imax, int jmax, const int *indptr, const int
     out8[5] = (long long)P->flops;
     out8[6] = P->vtotal;
     out8[7] = P->utotal;
+    mf_plan_destroy(P);
+    return V2D_OK;
+}
+
+// Planning aid for the dataflow solve (host only): info4 = {first level of
+// the dataflow launch, work items, 1 if the order passed its check, fronts};
+// items (4 ints each: kind, front, chunk, wait target) and each front's
+// parent are copied out when the caller's arrays are large enough.
+extern "C" int v2d_lu_flow_plan(int imax, int jmax, const int *indptr, const int *indices,
+                                int leaf, int *info4, int *items, int cap_items, int *parent,
+                                int cap_fronts)
+{
+    using namespace v2d;
+    V2D_ARG_CHECK(indptr && indices && info4, "lu_flow_plan: null pointer");
+    MfPlan *P = nullptr;
+    V2D_TRY(mf_plan_build(imax, jmax, 2 * imax * jmax, indptr, indices, leaf, &P));
+    info4[0] = P->flow_level;
+    info4[1] = P->nflow;
+    info4[2] = P->flow_valid;
+    info4[3] = P->nfront;
+    if (items && cap_items >= P->nflow)
+        std::copy(P->h_flow.begin(), P->h_flow.end(), items);
+    if (parent && cap_fronts >= P->nfront) std::copy(P->parent.begin(), P->parent.end(), parent);
     mf_plan_destroy(P);
     return V2D_OK;
 }
@@ -1088,7 +1242,7 @@ __device__ __forceinline__ bool stopped(const int *a, const int *b)
 // independent partial sums), so the large top fronts use many SMs.
 constexpr int kSolveRows = kSolveRowsHost;
 // levels with at least this many fronts are solved with one CTA per front
-constexpr int kFrontPerCta = 64;
+constexpr int kFrontPerCta = kFrontPerCtaHost;
 constexpr int kSolveThreads2 = 32 * kSolveRows;
 // the one-CTA-per-front solve kernels: more warps share a front's rows when
 // a level's CTAs of that size all fit on the GPU at once (2 per SM), else
@@ -1666,6 +1820,84 @@ __global__ void __launch_bounds__(kSolveThreads2) k_apply_all(const MfDev D, con
     }
 }
 
+// Polls of one dependency counter before a dataflow CTA gives up (each poll
+// sleeps ~40 ns: well under a second), records the timeout and returns.
+constexpr long long kFlowSpins = 1LL << 22;
+
+__device__ __forceinline__ int ld_acquire_gpu(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// The upper levels' forward and backward solve as one launch of work items
+// (flow_build): a CTA takes items by ticket (ctr[4 nf]), thread 0 waits with
+// acquire loads until the item's counter reaches its target, the CTA runs
+// the item (the same item functions as the per-phase launches; data from
+// other CTAs is read through L2), and after a fence thread 0 counts it.  A
+// wait that runs out, or an error seen while waiting, sets bar->err (bit 2)
+// and ends the CTA; the host reads it with mf_check_barrier.  ctr is zeroed
+// before each launch.
+template <class T>
+__global__ void __launch_bounds__(kSolveThreads2, 2) k_apply_flow(const MfDev D, const T *F, const T *b,
+                                                               const double *__restrict__ rs,
+                                                               T *zbuf, T *upd, T *x,
+                                                               const int4 *__restrict__ items,
+                                                               int nitems, int *ctr, int nf,
+                                                               MfBarrier *bar, const int *stop_a,
+                                                               const int *stop_b)
+{
+    if (stopped(stop_a, stop_b)) return;   // the flags are the same for every CTA
+    extern __shared__ unsigned char smem_raw[];
+    T *w = reinterpret_cast<T *>(smem_raw);
+    T *t2 = w + D.maxf;
+    __shared__ int item_s, ok_s;
+    volatile int *err = &bar->err;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int it = atomicAdd(ctr + 4 * nf, 1);
+            int ok = 1;
+            if (it < nitems) {
+                const int4 v = items[it];
+                if (v.w > 0) {
+                    const int par = v.x == kFlowY ? D.parent[v.y] : -1;
+                    const int wc = flow_wait_ctr(v.x, v.y, par, nf);
+                    long long spins = 0;
+                    while (ld_acquire_gpu(ctr + wc) < v.w) {
+                        if (*err || ++spins > kFlowSpins) {
+                            atomicOr(&bar->err, 2);
+                            ok = 0;
+                            break;
+                        }
+                        __nanosleep(40);
+                    }
+                }
+            }
+            item_s = it;
+            ok_s = ok;
+        }
+        __syncthreads();
+        const int it = item_s;
+        if (it >= nitems || !ok_s) return;
+        const int4 v = items[it];
+        switch (v.x) {
+        case kFlowZ: fz_item<T>(D, F, b, rs, zbuf, upd, v.y, v.z, w, t2); break;
+        case kFlowU: fu_item<T>(D, F, zbuf, upd, v.y, v.z, w); break;
+        case kFlowY: by_item<T>(D, F, zbuf, x, v.y, v.z, w); break;
+        default: bx_item<T>(D, F, zbuf, x, v.y, v.z, w); break;
+        }
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int par = v.x == kFlowU ? D.parent[v.y] : -1;
+            const int dc = flow_done_ctr(v.x, v.y, par, nf);
+            __threadfence();
+            if (dc >= 0) atomicAdd(ctr + dc, 1);
+        }
+    }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------ host drivers
@@ -1757,6 +1989,7 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
     };
     if (fp32) {
         attr((const void *)k_apply_all<float>, solve);
+        attr((const void *)k_apply_flow<float>, solve);
         attr((const void *)k_fwd_front<float>, solve);
         attr((const void *)k_tup_front<float>, solve);
         attr((const void *)k_tdown_front<float>, solve);
@@ -1768,6 +2001,7 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
         attr((const void *)k_trinv<float>, inv);
     } else {
         attr((const void *)k_apply_all<double>, solve);
+        attr((const void *)k_apply_flow<double>, solve);
         attr((const void *)k_fwd_front<double>, solve);
         attr((const void *)k_tup_front<double>, solve);
         attr((const void *)k_tdown_front<double>, solve);
@@ -1799,6 +2033,22 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
                                     &per_sm, k_apply_all<double>, kSolveThreads2, solve);
         if (oe == cudaSuccess && per_sm > 0) M->coop_grid = nsm * std::min(per_sm, 2);
     }
+    // dataflow solve of the upper levels (opt-in, V2D_LU_FLOW=1): one launch
+    // instead of two per level and sweep above the one-CTA-per-front levels
+    const char *fenv = getenv("V2D_LU_FLOW");
+    if (fenv && fenv[0] == '1' && P->nflow > 0 && P->d_flow && M->coop_grid == 0 &&
+        cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess) {
+        int fper = 0;
+        cudaError_t oe = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                    &fper, k_apply_flow<float>, kSolveThreads2, solve)
+                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                    &fper, k_apply_flow<double>, kSolveThreads2, solve);
+        if (oe == cudaSuccess && fper > 0 &&
+            cudaMalloc((void **)&M->flow_ctr, (size_t)(4 * P->nfront + 1) * sizeof(int)) ==
+                cudaSuccess)
+            M->flow_grid = std::min(P->nflow, nsm * fper);
+    }
     cudaGetLastError();
     *out = M;
     return V2D_OK;
@@ -1809,7 +2059,7 @@ void mf_factor_destroy(MfFactor *M)
     if (!M) return;
     if (M->graph) cudaGraphExecDestroy(M->graph);
     void *ptrs[] = {M->F,  M->upd,  M->z,    M->tmp,  M->wb, M->rs,
-                    M->ipiv, M->perm, M->flag, M->bar, M->inv_g};
+                    M->ipiv, M->perm, M->flag, M->bar, M->inv_g, M->flow_ctr};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     delete M;
@@ -1987,7 +2237,7 @@ static int solve_launch(const char *what, int L)
 
 // Launch codes of the solve's kernels for per-launch timing (kind * 1000 + level).
 enum { kCodeFwdFront = 0, kCodeFwdZ = 1, kCodeFwdU = 2, kCodeBwdFront = 3, kCodeBwdY = 4,
-       kCodeBwdX = 5 };
+       kCodeBwdX = 5, kCodeFlow = 6 };
 
 template <class T>
 static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, const int *stop_a,
@@ -2031,7 +2281,10 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
     }
     auto chunks = [](int rows) { return std::max(1, (rows + kSolveRows - 1) / kSolveRows); };
     const size_t smf = (size_t)(P->maxf + P->maxS) * sizeof(T);
-    for (int L = 0; L < P->nlevel; ++L) {
+    // levels from Lf up run as one dataflow launch when the factor has one
+    const bool flow = M->flow_grid > 0 && M->flow_ctr && P->nflow > 0;
+    const int Lf = flow ? P->flow_level : P->nlevel;
+    for (int L = 0; L < Lf; ++L) {
         const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
         if (nq >= kFrontPerCta) {
             k_fwd_front<T><<<nq, front_threads(nq), smf, s>>>(q0, D, F, b, M->rs, z, upd, stop_a,
@@ -2062,7 +2315,16 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
             ++launches;
         }
     }
-    for (int L = P->nlevel - 1; L >= 0; --L) {
+    if (flow) {
+        V2D_CUDA_TRY(cudaMemsetAsync(M->flow_ctr, 0, (size_t)(4 * P->nfront + 1) * sizeof(int), s));
+        k_apply_flow<T><<<M->flow_grid, kSolveThreads2, smf, s>>>(
+            D, F, b, M->rs, z, upd, x, (const int4 *)P->d_flow, P->nflow, M->flow_ctr, P->nfront,
+            M->bar, stop_a, stop_b);
+        V2D_TRY(solve_launch("k_apply_flow", Lf));
+        V2D_TRY(mark(kCodeFlow * 1000 + Lf));
+        ++launches;
+    }
+    for (int L = Lf - 1; L >= 0; --L) {
         const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
         if (nq >= kFrontPerCta) {
             k_bwd_front<T><<<nq, front_threads(nq), smf, s>>>(q0, D, F, z, x, stop_a, stop_b);
@@ -2260,7 +2522,7 @@ int mf_check_barrier(MfFactor *M, cudaStream_t s)
     V2D_CUDA_TRY(cudaStreamSynchronize(s));
     if (err) {
         V2D_CUDA_TRY(cudaMemsetAsync(M->bar, 0, sizeof(MfBarrier), s));
-        set_error("LU solve: a grid barrier of the persistent solve timed out");
+        set_error("LU solve: a wait of the persistent or dataflow solve timed out");
         return V2D_ETIMEOUT;
     }
     return V2D_OK;
