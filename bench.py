@@ -661,6 +661,9 @@ def main():
     ap.add_argument("--lu-reuse", type=int, default=12,
                     help="keep LU factors while GMRES needs at most this many iterations "
                          "(0: factor every Newton Jacobian)")
+    ap.add_argument("--lu-flow", action="store_true",
+                    help="solve the LU preconditioner's upper levels as one dataflow launch "
+                         "(opt-in kernel; sets V2D_LU_FLOW=1 before any factors exist)")
     ap.add_argument("--lu-reuse-steps", type=int, default=1, choices=[0, 1],
                     help="1: keep the LU factors across time steps (and the e2e leg's "
                          "set_state) under the same rule; 0: refactor at every step")
@@ -696,6 +699,8 @@ def main():
     ap.add_argument("--profile-newton", action="store_true",
                     help="one warm-up step, then one Newton iteration in NVTX range v2d_newton")
     args = ap.parse_args()
+    if args.lu_flow:
+        os.environ["V2D_LU_FLOW"] = "1"
     rank, world, local_rank = dist_env()
     if args.profile_newton:
         profile_newton(args)
@@ -786,6 +791,7 @@ def main():
                    "precision": head, "newton_max": 5,
                    "krylov": "GMRES(30), multifrontal LU preconditioner (FP32 factors in mixed)",
                    "lu_reuse_its": args.lu_reuse, "lu_reuse_steps": args.lu_reuse_steps,
+                   "lu_solve": "dataflow upper levels" if args.lu_flow else "per-level launches",
                    "l2": "flushed (256 MiB write) before every timed step",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": world * res["e2e"]["steps_per_s"], "unit": "steps/s",
