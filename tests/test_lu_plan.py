@@ -109,10 +109,10 @@ def _done_ctr(kind, q, parent, nf):
 
 def _producers(items, parent):
     """What each item reads, from the algorithm alone (not from the
-    counters): z rows need every contribution chunk of the front's children,
-    contribution rows every z chunk of the front, backward y rows every x
-    chunk of the parent, x rows every y chunk of the front (or, without
-    contribution rows, every z chunk)."""
+    counters): z rows need every contribution chunk of the front's children;
+    contribution rows every z chunk of the front; backward y rows the
+    front's z and the x chunks of every ancestor (its contribution variables
+    are pivots of ancestors); x rows the front's z and y chunks."""
     by_kind = {}
     for k, (kind, q, c, t) in enumerate(items):
         by_kind.setdefault((kind, q), []).append(k)
@@ -120,6 +120,10 @@ def _producers(items, parent):
     for k, (kind, q, c, t) in enumerate(items):
         if kind == FU:
             kids.setdefault(parent[q], set()).add(q)
+
+    def xs(a):
+        return by_kind.get((BX, a), []) + by_kind.get((BXROOT, a), [])
+
     prod = []
     for kind, q, c, t in items:
         if kind == FZ:
@@ -127,11 +131,13 @@ def _producers(items, parent):
         elif kind == FU:
             p = by_kind[(FZ, q)]
         elif kind == BY:
-            p = by_kind.get((BX, parent[q]), []) + by_kind.get((BXROOT, parent[q]), [])
-        elif kind == BX:
-            p = by_kind[(BY, q)]
+            p = list(by_kind[(FZ, q)])
+            a = parent[q]
+            while a >= 0:
+                p += xs(a)
+                a = parent[a]
         else:
-            p = by_kind[(FZ, q)]
+            p = by_kind[(FZ, q)] + by_kind.get((BY, q), [])
         prod.append(p)
     return prod
 

@@ -276,10 +276,14 @@ static void flow_build(MfPlan *P)
                 push(cb ? kFlowX : kFlowXRoot, q, c, cb ? chunks(P->S[q]) : nz(q));
         }
     }
-    // the check: totals per counter, then each wait against the items before it
+    // the check: every front of the dataflow has pivots (a backward wait on a
+    // parent's x chunks must stand for all its ancestors), totals per
+    // counter, then each wait against the items before it
     const int nitems = (int)it.size() / 4;
     std::vector<int> total(4 * nf, 0), seen(4 * nf, 0);
     bool ok = true;
+    for (int q = P->lvl_off[L0]; q < nf; ++q)
+        if (P->S[q] <= 0) ok = false;
     for (int k = 0; k < nitems && ok; ++k) {
         const int kind = it[4 * k], q = it[4 * k + 1];
         if (q < 0 || q >= nf || lvl[q] < L0 || kind < kFlowZ || kind > kFlowXRoot) {
