@@ -190,8 +190,9 @@ def _simulate(items, parent, nf, ctas, rng):
     return order
 
 
-@pytest.mark.parametrize("imax,jmax,leaf", [(33, 21, 16), (65, 49, 64), (129, 129, 64),
-                                            (181, 181, 64), (257, 129, 64)])
+@pytest.mark.parametrize("imax,jmax,leaf", [(5, 4, 64), (9, 7, 4), (24, 13, 16), (33, 21, 16),
+                                            (65, 49, 64), (129, 129, 64), (181, 181, 64),
+                                            (257, 129, 64)])
 def test_flow_plan_order_is_safe(v2d, oracle_mod, imax, jmax, leaf):
     """The dataflow solve's work items: validated by the plan, every front
     above the one-CTA-per-front levels appears with the chunk counts of its
