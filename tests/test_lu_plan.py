@@ -223,3 +223,22 @@ def test_flow_plan_181_levels(v2d, oracle_mod):
     fronts = sorted(set(items[:, 1].tolist()))
     assert fronts == list(range(960, 1025))
     assert parent[1024] == -1 and (parent[960:1024] >= 960).all()
+
+
+def test_plan_rejects_malformed_csr(v2d, oracle_mod):
+    """Column indices outside [0, n) and decreasing row pointers are argument
+    errors, found before any index is used."""
+    from vorti2d_b200 import _lib
+    ip, ix = pattern(oracle_mod, 33, 21, 1)
+    bad = ix.copy()
+    bad[len(bad) // 2] = 2 * 33 * 21
+    code, _ = plan_info(v2d, 33, 21, ip, bad)
+    assert code == _lib.V2D_EARG and b"outside" in _lib.lib().v2d_last_error()
+    bad = ix.copy()
+    bad[3] = -1
+    code, _ = plan_info(v2d, 33, 21, ip, bad)
+    assert code == _lib.V2D_EARG
+    bip = ip.copy()
+    bip[10] = bip[12] + 1
+    code, _ = plan_info(v2d, 33, 21, bip, ix)
+    assert code == _lib.V2D_EARG and b"decreases" in _lib.lib().v2d_last_error()

@@ -201,6 +201,17 @@ struct TreeBuilder {
     }
 };
 
+// Node adjacency in CSR form: node v's neighbours are nb[off[v], off[v] + len[v]).
+struct NodeGraph {
+    std::vector<int> off, len, nb;
+    struct Range {
+        const int *b, *e;
+        const int *begin() const { return b; }
+        const int *end() const { return e; }
+    };
+    Range of(int v) const { return {nb.data() + off[v], nb.data() + off[v] + len[v]}; }
+};
+
 template <class T>
 int upload_vec(T **d, const std::vector<T> &h)
 {
@@ -324,22 +335,53 @@ int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_c
     const int N = imax * jmax;
     V2D_ARG_CHECK(n == 2 * N, "mf_plan: system size %d != 2 * %d nodes", n, N);
     V2D_ARG_CHECK(imax >= 5 && jmax >= 4, "mf_plan: grid %d x %d too small", imax, jmax);
+    // the CSR pattern: row pointers from 0, non-decreasing; columns in [0, n)
+    V2D_ARG_CHECK(h_rowptr[0] == 0, "mf_plan: indptr[0] = %d, not 0", h_rowptr[0]);
+    for (int r = 0; r < n; ++r)
+        V2D_ARG_CHECK(h_rowptr[r + 1] >= h_rowptr[r], "mf_plan: indptr decreases at row %d", r);
+    for (int p = 0; p < h_rowptr[n]; ++p)
+        V2D_ARG_CHECK(h_colind[p] >= 0 && h_colind[p] < n,
+                      "mf_plan: column index %d at entry %d outside [0, %d)", h_colind[p], p, n);
     TreeBuilder tb{imax, jmax, std::max(4, leaf), {}};
     tb.build();
     const int nf = (int)tb.t.size();
-    // --- symmetrised node graph (CSR)
-    std::vector<std::vector<int>> adj(N);
-    for (int r = 0; r < n; ++r)
-        for (int p = h_rowptr[r]; p < h_rowptr[r + 1]; ++p) {
-            int a = r % N, b = h_colind[p] % N;
-            if (a != b) {
-                adj[a].push_back(b);
-                adj[b].push_back(a);
-            }
+    // --- symmetrised node graph (CSR): the distinct other nodes of each
+    // node's two rows, then every such edge in both directions
+    NodeGraph adj;
+    {
+        std::vector<int> foff(N + 1, 0), fwd, mark(N, -1);
+        fwd.reserve((size_t)h_rowptr[n] / 2 + 16);
+        for (int a = 0; a < N; ++a) {
+            for (int r : {a, N + a})
+                for (int p = h_rowptr[r]; p < h_rowptr[r + 1]; ++p) {
+                    const int c = h_colind[p], b = c < N ? c : c - N;
+                    if (b != a && mark[b] != a) {
+                        mark[b] = a;
+                        fwd.push_back(b);
+                    }
+                }
+            foff[a + 1] = (int)fwd.size();
         }
-    for (auto &v : adj) {
-        std::sort(v.begin(), v.end());
-        v.erase(std::unique(v.begin(), v.end()), v.end());
+        adj.off.assign(N + 1, 0);
+        for (int a = 0; a < N; ++a)
+            for (int p = foff[a]; p < foff[a + 1]; ++p) {
+                ++adj.off[a + 1];
+                ++adj.off[fwd[p] + 1];
+            }
+        for (int a = 0; a < N; ++a) adj.off[a + 1] += adj.off[a];
+        adj.nb.resize(adj.off[N]);
+        std::vector<int> fill(adj.off.begin(), adj.off.end() - 1);
+        for (int a = 0; a < N; ++a)
+            for (int p = foff[a]; p < foff[a + 1]; ++p) {
+                adj.nb[fill[a]++] = fwd[p];
+                adj.nb[fill[fwd[p]]++] = a;
+            }
+        adj.len.resize(N);
+        for (int a = 0; a < N; ++a) {
+            int *b = adj.nb.data() + adj.off[a], *e = adj.nb.data() + adj.off[a + 1];
+            std::sort(b, e);
+            adj.len[a] = (int)(std::unique(b, e) - b);
+        }
     }
     // --- elimination order (postorder of the tree)
     std::vector<int> elim(N, -1), owner(N, -1), last_elim(nf);
@@ -374,7 +416,7 @@ int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_c
             if (c >= 0)
                 for (int u : st[c]) take(u);
         for (int v : tb.t[q].sep)
-            for (int u : adj[v]) take(u);
+            for (int u : adj.of(v)) take(u);
         std::sort(s.begin(), s.end(), [&](int a, int b) { return elim[a] < elim[b]; });
         st[q] = std::move(s);
     }
@@ -388,7 +430,7 @@ int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_c
     }
     for (int q = 0; q < nf; ++q)
         for (int v : tb.t[q].sep)
-            for (int u : adj[v])
+            for (int u : adj.of(v))
                 if (elim[u] < first_elim[q]) {
                     set_error("mf_plan: node %d couples to node %d of a sibling subtree", v, u);
                     return V2D_EARG;
@@ -495,7 +537,8 @@ int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_c
     std::vector<int> cnt(nf + 1, 0), entry_front(h_rowptr[n]);
     for (int r = 0; r < n; ++r)
         for (int p = h_rowptr[r]; p < h_rowptr[r + 1]; ++p) {
-            const int a = r % N, b = h_colind[p] % N;
+            const int c = h_colind[p];
+            const int a = r < N ? r : r - N, b = c < N ? c : c - N;
             const int fr = newid[elim[a] < elim[b] ? owner[a] : owner[b]];
             entry_front[p] = fr;
             cnt[fr + 1]++;
@@ -505,31 +548,27 @@ int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_c
     std::vector<int> asm_csr(nnz), asm_row(nnz);
     std::vector<long long> asm_pos(nnz);
     {
+        // entries of each front in row order (a counting sort by front),
+        // then each front's local positions from its variables' lookup
         std::vector<int> fill(cnt.begin(), cnt.end() - 1);
-        std::vector<std::vector<int>> rows_of_front;  // unused; positions computed below
-        // local index lookup per front: scan fronts, mark their vars
-        std::vector<std::vector<int>> ent(nf);
         for (int r = 0; r < n; ++r)
-            for (int p = h_rowptr[r]; p < h_rowptr[r + 1]; ++p) ent[entry_front[p]].push_back(p);
-        std::vector<int> row_of(nnz);
-        for (int r = 0; r < n; ++r)
-            for (int p = h_rowptr[r]; p < h_rowptr[r + 1]; ++p) row_of[p] = r;
+            for (int p = h_rowptr[r]; p < h_rowptr[r + 1]; ++p) {
+                const int o = fill[entry_front[p]]++;
+                asm_csr[o] = p;
+                asm_row[o] = r;
+            }
         for (int id = 0; id < nf; ++id) {
             const int f = P->f[id];
             for (int t = 0; t < f; ++t) loc[vars[P->voff[id] + t]] = t;
-            int o = cnt[id];
-            for (int p : ent[id]) {
-                const int r = row_of[p], c = h_colind[p];
+            for (int o = cnt[id]; o < cnt[id + 1]; ++o) {
+                const int r = asm_row[o], c = h_colind[asm_csr[o]];
                 const int lr = loc[r], lc = loc[c];
                 if (lr < 0 || lc < 0) {
                     set_error("mf_plan: entry (%d, %d) outside its front", r, c);
                     mf_plan_destroy(P);
                     return V2D_EARG;
                 }
-                asm_csr[o] = p;
-                asm_row[o] = r;
                 asm_pos[o] = P->foff[id] + (long long)lr * f + lc;
-                ++o;
             }
             for (int t = 0; t < f; ++t) loc[vars[P->voff[id] + t]] = -1;
         }
