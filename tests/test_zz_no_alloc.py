@@ -7,8 +7,9 @@ loop that must avoid cudaMalloc/cudaFree); its scratch is a fixed array inside
 the library.  Two calls in a row with different rows, states and boundary
 conditions must both equal the allocating entry point bit for bit (the
 tolerance the other assembly parity tests use), so nothing the first call
-leaves in the shared scratch leaks into the second.  This file is collected
-last on purpose."""
+leaves in the shared scratch leaks into the second, and neither call may take
+device memory (checked with the default memory pool's high watermark and the
+free device memory).  This file is collected last on purpose."""
 import ctypes
 
 import numpy as np
@@ -19,7 +20,48 @@ from cases import smooth_state
 pytestmark = pytest.mark.gpu
 
 
-def _call_noalloc(v2d, torch, imax, jmax, args_scalars, fields, r0, r1, maxnnz, ff_bc, ca, sa):
+class _PoolWatch:
+    """Allocation probe: the library's stream-ordered allocations come from the
+    device's default memory pool, so the pool's used-memory high watermark,
+    reset just before the call, stays at the memory in use before it.  With
+    check_free, the free device memory must not drop either (a plain
+    cudaMalloc still held); that check is left out of a process's first call,
+    where loading the library's device code maps its static data, the
+    scratch array included."""
+
+    def __init__(self, torch, check_free):
+        self.check_free = check_free
+        from cuda.bindings import driver as drv
+        self.drv, self.torch = drv, torch
+        err, self.pool = drv.cuDeviceGetDefaultMemPool(torch.cuda.current_device())
+        assert err == drv.CUresult.CUDA_SUCCESS, err
+
+    def _attr(self, a):
+        err, v = self.drv.cuMemPoolGetAttribute(self.pool, a)
+        assert err == self.drv.CUresult.CUDA_SUCCESS, err
+        return int(v)
+
+    def __enter__(self):
+        A = self.drv.CUmemPool_attribute
+        self.used0 = self._attr(A.CU_MEMPOOL_ATTR_USED_MEM_CURRENT)
+        err, = self.drv.cuMemPoolSetAttribute(self.pool, A.CU_MEMPOOL_ATTR_USED_MEM_HIGH,
+                                              self.drv.cuuint64_t(0))
+        assert err == self.drv.CUresult.CUDA_SUCCESS, err
+        self.free0 = self.torch.cuda.mem_get_info()[0]
+        return self
+
+    def __exit__(self, *exc):
+        A = self.drv.CUmemPool_attribute
+        self.high = self._attr(A.CU_MEMPOOL_ATTR_USED_MEM_HIGH)
+        self.free1 = self.torch.cuda.mem_get_info()[0]
+        return False
+
+    def allocated_nothing(self):
+        return self.high <= self.used0 and (not self.check_free or self.free1 >= self.free0)
+
+
+def _call_noalloc(v2d, torch, imax, jmax, args_scalars, fields, r0, r1, maxnnz, ff_bc, ca, sa,
+                  watch=False):
     from vorti2d_b200 import _lib
     dev = [torch.from_numpy(np.ascontiguousarray(f)).cuda() for f in fields]
     ptrs = (ctypes.c_void_p * 14)(*[t.data_ptr() for t in dev])
@@ -29,9 +71,15 @@ def _call_noalloc(v2d, torch, imax, jmax, args_scalars, fields, r0, r1, maxnnz, 
     b = torch.zeros(max(r1 - r0, 1), dtype=torch.float64, device="cuda")
     nnz = ctypes.c_int(-1)
     torch.cuda.synchronize()
+    w = _PoolWatch(torch, watch == 2) if watch else None
+    if w:
+        w.__enter__()
     code = _lib.lib().v2d_assemble_coo_noalloc(
         imax, jmax, *args_scalars, ptrs, r0, r1, maxnnz, ff_bc, ca, sa, ci.data_ptr(),
         cj.data_ptr(), cv.data_ptr(), ctypes.byref(nnz), b.data_ptr(), None)
+    if w:
+        w.__exit__(None, None, None)
+        assert w.allocated_nothing(), (w.used0, w.high, w.free0, w.free1)
     return code, nnz.value, ci.cpu().numpy(), cj.cpu().numpy(), cv.cpu().numpy(), \
         b.cpu().numpy()[:r1 - r0]
 
@@ -59,7 +107,8 @@ def test_noalloc_matches_allocating_entry_point_twice(v2d, oracle_mod):
                                      r0, r1, maxnnz, ff_bc, ca, sa)
         code, n, ci, cj, cv, b = _call_noalloc(v2d, torch, imax, jmax,
                                               (re, invdtau, inv2dt, urot, dk, de), fields,
-                                              r0, r1, maxnnz, ff_bc, ca, sa)
+                                              r0, r1, maxnnz, ff_bc, ca, sa,
+                                              watch=1 if k == 0 else 2)
         assert code == 0, _lib.last_error()
         assert n == want[3]
         assert np.array_equal(ci[:n], want[0][:n]) and np.array_equal(cj[:n], want[1][:n])

@@ -8,6 +8,7 @@ restatement; the Krylov units keep FMA contraction.
 """
 from __future__ import annotations
 
+import hashlib
 import os
 import shutil
 import subprocess
@@ -44,11 +45,34 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found: the CUDA toolkit is required to build vorti2d_b200")
 
 
-def _stale(target: str, deps: list[str]) -> bool:
-    if not os.path.exists(target):
+def _digest(paths: list[str], flags: list[str]) -> str:
+    """Content hash of the inputs of one build step (file contents and flags,
+    not modification times: a prebuilt file copied next to changed sources
+    with a newer time stamp must still be rebuilt)."""
+    h = hashlib.sha256()
+    root = os.path.dirname(HERE)
+    for f in flags:   # paths relative to the checkout, which moves between machines
+        f = os.path.relpath(f, root) if os.path.isabs(f) else f
+        h.update(f.encode() + b"\0")
+    for p in sorted(paths):
+        h.update(os.path.basename(p).encode() + b"\0")
+        with open(p, "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()
+
+
+def _stale(target: str, digest: str) -> bool:
+    """True unless target exists and its stamp file records this digest."""
+    stamp = target + ".sha256"
+    if not (os.path.exists(target) and os.path.exists(stamp)):
         return True
-    t = os.path.getmtime(target)
-    return any(os.path.getmtime(d) > t for d in deps)
+    with open(stamp) as fh:
+        return fh.read().strip() != digest
+
+
+def _stamp(target: str, digest: str) -> None:
+    with open(target + ".sha256", "w") as fh:
+        fh.write(digest + "\n")
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
@@ -63,16 +87,20 @@ def build(force: bool = False, verbose: bool = False) -> str:
             continue
         obj = os.path.join(OUT_DIR, src.replace(".cu", ".o"))
         objs.append(obj)
-        if force or _stale(obj, [path, __file__] + headers):
-            cmd = [nv, *ARCH, *COMMON, *extra, "-c", path, "-o", obj]
+        cmd = [nv, *ARCH, *COMMON, *extra, "-c", path, "-o", obj]
+        dg = _digest([path] + headers, cmd[1:])
+        if force or _stale(obj, dg):
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.check_call(cmd)
-    if force or _stale(LIB, objs):
-        cmd = [nv, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+            _stamp(obj, dg)
+    cmd = [nv, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+    dg = _digest(objs, cmd[1:])
+    if force or _stale(LIB, dg):
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)
+        _stamp(LIB, dg)
     return LIB
 
 

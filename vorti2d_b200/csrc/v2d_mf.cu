@@ -1879,9 +1879,10 @@ __device__ __forceinline__ int ld_acquire_gpu(const int *p)
 // acquire loads until the item's counter reaches its target, the CTA runs
 // the item (the same item functions as the per-phase launches; data from
 // other CTAs is read through L2), and after a fence thread 0 counts it.  A
-// wait that runs out, or an error seen while waiting, sets bar->err (bit 2)
-// and ends the CTA; the host reads it with mf_check_barrier.  ctr is zeroed
-// before each launch.
+// wait that runs out, or an error seen while waiting, sets bar->err (bit 2),
+// sets *stop_a (the Krylov solve's stop flag, so GMRES ends instead of
+// iterating with an unfinished preconditioner) and ends the CTA; the host
+// reads bar->err with mf_check_barrier.  ctr is zeroed before each launch.
 template <class T>
 __global__ void __launch_bounds__(kSolveThreads2, 2) k_apply_flow(const MfDev D, const T *F, const T *b,
                                                                const double *__restrict__ rs,
@@ -1910,6 +1911,9 @@ __global__ void __launch_bounds__(kSolveThreads2, 2) k_apply_flow(const MfDev D,
                     while (ld_acquire_gpu(ctr + wc) < v.w) {
                         if (*err || ++spins > kFlowSpins) {
                             atomicOr(&bar->err, 2);
+                            // end the Krylov solve at once: with a CTA gone the
+                            // preconditioner output is unfinished
+                            if (stop_a) atomicExch(const_cast<int *>(stop_a), 1);
                             ok = 0;
                             break;
                         }
@@ -2472,6 +2476,7 @@ int mf_time_apply(const MfPlan *P, const MfFactor *M, int reps, size_t flush_byt
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (st != V2D_OK) return st;
+    V2D_TRY(mf_check_barrier(const_cast<MfFactor *>(M), s));   // a solve that gave up is no time
     *ms_avg = total / reps;
     return V2D_OK;
 }
@@ -2522,6 +2527,7 @@ int mf_time_apply_launches(const MfPlan *P, const MfFactor *M, int reps, size_t 
     for (auto &e : ev)
         if (e) cudaEventDestroy(e);
     if (st != V2D_OK) return st;
+    V2D_TRY(mf_check_barrier(const_cast<MfFactor *>(M), s));
     for (long long k = 0; k < nl; ++k) ms[k] = acc[k] / reps;
     *n = (int)nl;
     return V2D_OK;

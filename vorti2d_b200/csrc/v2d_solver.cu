@@ -408,6 +408,7 @@ extern "C" int v2d_solver_newton(v2d_solver *S, double urot, double *res, v2d_li
         v2d_krylov_params k2 = kp;
         k2.max_it = std::min(kp.max_it, kp.lu_reuse_its + 5);
         V2D_TRY(krylov_solve(S->kw, A, g.b, S->delta, k2, &ls, S->s));
+        V2D_TRY(mf_check_barrier(S->lu[mixed], S->s));   // a timed-out solve is no retry case
         if (!ls.converged) {
             const int its0 = ls.iterations;
             V2D_TRY(mf_factor(S->plan, S->lu[mixed], g.rowptr, g.val, S->s));
