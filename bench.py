@@ -42,10 +42,6 @@ METRIC = "BDF2 steps/s, 181x181 cylinder O-grid Re=100 dt=0.2 (<=5 Newton, GMRES
 WORKLOAD_NAME = "unsteady BDF2 cylinder 181x181 Re=100 dt=0.2 kick 0.5<=2 outflow"
 L2_FLUSH_BYTES = 256 << 20
 SPMV_BYTES_PER_NNZ = {"fp64": 8 + 4, "fp32": 4 + 4}
-# DRAM bytes (read + write) of one mixed-precision LU apply at 181x181: the
-# solve kernels' dram__bytes_read.sum + dram__bytes_write.sum of one Newton
-# iteration (4 applies) captured with ncu, divided by 4 (cold caches)
-TRAFFIC_LU = 114.8e6
 
 
 # ------------------------------------------------------------------ ranks
@@ -505,7 +501,7 @@ def profile_lu_launches(args):
     times = s.times()
     for m in range(2):
         s.advance(times[m])
-    kinds = ["fwd_front", "fwd_z", "fwd_u", "bwd_front", "bwd_y", "bwd_x", "flow"]
+    kinds = ["forward_level", "backward_level", "dataflow"]
     out = {"profile": "LU solve launches", "precision": prec}
     for label, flush in (("warm", 0), ("cold", L2_FLUSH_BYTES)):
         cap = 256
@@ -521,8 +517,8 @@ def profile_lu_launches(args):
         out[label] = {"total_ms": sum(t for _, _, t in rows), "launches": len(rows),
                       "by_kind_ms": by_kind,
                       "per_launch_us": [[kind, lvl, round(1e3 * t, 2)] for kind, lvl, t in rows]}
-    fkinds = ["rowscale", "scatter", "extend_add", "panel", "l21", "swap_trsm", "gemm", "trinv",
-              "trcopy"]
+    fkinds = ["rowscale", "scatter", "extend_add", "panel", "l21_swap_trsm", "-", "gemm", "trinv",
+              "trcopy", "gh", "ghcopy"]
     cap = 1024
     ms = (ctypes.c_double * cap)()
     codes = (ctypes.c_int * cap)()
@@ -661,9 +657,9 @@ def main():
     ap.add_argument("--lu-reuse", type=int, default=12,
                     help="keep LU factors while GMRES needs at most this many iterations "
                          "(0: factor every Newton Jacobian)")
-    ap.add_argument("--lu-flow", action="store_true",
-                    help="solve the LU preconditioner's upper levels as one dataflow launch "
-                         "(opt-in kernel; sets V2D_LU_FLOW=1 before any factors exist)")
+    ap.add_argument("--lu-solve", default="flow", choices=["flow", "levels"],
+                    help="LU preconditioner solve: one dataflow launch over the front tree "
+                         "(flow) or one launch per level and sweep (levels)")
     ap.add_argument("--lu-reuse-steps", type=int, default=1, choices=[0, 1],
                     help="1: keep the LU factors across time steps (and the e2e leg's "
                          "set_state) under the same rule; 0: refactor at every step")
@@ -699,8 +695,7 @@ def main():
     ap.add_argument("--profile-newton", action="store_true",
                     help="one warm-up step, then one Newton iteration in NVTX range v2d_newton")
     args = ap.parse_args()
-    if args.lu_flow:
-        os.environ["V2D_LU_FLOW"] = "1"
+    SOLVER["lu_solve"] = args.lu_solve
     rank, world, local_rank = dist_env()
     if args.profile_newton:
         profile_newton(args)
@@ -791,15 +786,17 @@ def main():
                    "precision": head, "newton_max": 5,
                    "krylov": "GMRES(30), multifrontal LU preconditioner (FP32 factors in mixed)",
                    "lu_reuse_its": args.lu_reuse, "lu_reuse_steps": args.lu_reuse_steps,
-                   "lu_solve": "dataflow upper levels" if args.lu_flow else "per-level launches",
+                   "lu_solve": {"flow": "one dataflow launch", "levels": "one launch per level and sweep"}[args.lu_solve],
                    "l2": "flushed (256 MiB write) before every timed step",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": world * res["e2e"]["steps_per_s"], "unit": "steps/s",
                 "h2d_bytes_per_step": res["e2e"]["h2d"], "d2h_bytes_per_step": res["e2e"]["d2h"]},
-        "roofline": {"bound": "hbm", "kernel": f"lu_apply_{prec_key} (forward + backward "
-                     "sweep over all levels: k_fwd_z, k_fwd_u, k_bwd_y, k_bwd_x)",
+        "roofline": {"bound": "hbm", "kernel": f"lu_apply_{prec_key} (the preconditioner "
+                     "solve: k_solve_flow, or k_solve_level per level and sweep)",
                      "achieved": achieved_lu, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved_lu / peaks["hbm_gbs"], "traffic": TRAFFIC_LU,
+                     "frac": achieved_lu / peaks["hbm_gbs"], "traffic": None,
+                     "traffic_note": "not measured in this run: ncu DRAM bytes of the same "
+                                     "launch are in profiles/",
                      "bytes_per_launch": lu_bytes, "ms_per_launch": res["lu_apply_ms"],
                      "peak_note": peak_src},
         "roofline_spmv": {"bound": "hbm", "kernel": f"spmv_csr_{prec_key}",

@@ -189,6 +189,9 @@ typedef struct {
                              iteration rule; 0 refreshes them at the first
                              Newton iteration of every time step and after
                              every set_state (0)                            */
+    int lu_solve;         /* LU: 0 the preconditioner solve is one dataflow
+                             launch over the whole front tree (default);
+                             1 one launch per tree level and sweep          */
 } v2d_krylov_params;
 
 void v2d_krylov_defaults(v2d_krylov_params *p);
@@ -207,9 +210,18 @@ typedef struct v2d_linsys v2d_linsys;
 
 /* Replaces MumpsSolver(n) (vorti2d/petsc_solver.py:38-70).  block_layout:
  * 0 point diagonal, 1 field-blocked 2x2 pairs (r, r+n/2), 2 interleaved
- * 2x2 pairs (2q, 2q+1). */
+ * 2x2 pairs (2q, 2q+1).  With p->precond = V2D_PC_LU (block_layout 1 only)
+ * every solve factors the assembled matrix (multifrontal LU, nested
+ * dissection of the O-grid) and refines with GMRES to rtol, like the
+ * reference's MUMPS direct solve (petsc_solver.py:55-61); lu_reuse_its > 0
+ * keeps factors across solves under the rule of v2d_krylov_params. */
 int v2d_linsys_create(int n, int block_layout, const v2d_krylov_params *p,
                       v2d_linsys **out);
+/* The O-grid shape (n = 2 imax jmax) for the LU preconditioner; call before
+ * the first assemble.  Without it the shape is recognised from the pattern at
+ * the first assemble.  No reference counterpart (MUMPS orders the matrix
+ * itself). */
+int v2d_linsys_set_grid(v2d_linsys *s, int imax, int jmax);
 /* Replaces MumpsSolver.assemble (vorti2d/petsc_solver.py:76-95): the first
  * call fixes the canonical CSR pattern (rows sorted, columns sorted,
  * duplicates summed); later calls must repeat the same (i, j) sequence and
@@ -340,15 +352,16 @@ int v2d_solver_time_spmv(v2d_solver *s, int fp32, int reps, long long flush_byte
  * entries. */
 int v2d_lu_plan_info(int imax, int jmax, const int *indptr, const int *indices, int leaf,
                      long long *out8);
-/* Planning aid for the dataflow solve of the upper levels (host only):
- * info4 = {first level of the one-launch dataflow solve, work items, 1 if the
- * item order passed its check, fronts}; when cap_items >= items, items gets
- * 4 ints per item (kind 0 z rows, 1 contribution rows, 2 backward y rows,
- * 3 backward x rows, 4 x rows of a front without contribution rows; front;
- * row chunk; the count its dependency counter must reach), and when
- * cap_fronts >= fronts, parent gets each front's parent (-1 at the root). */
-int v2d_lu_flow_plan(int imax, int jmax, const int *indptr, const int *indices, int leaf,
-                     int *info4, int *items, int cap_items, int *parent, int cap_fronts);
+/* Planning aid for the preconditioner solve's work items (host only; no
+ * reference counterpart): info4 = {work items, dependency counters, fronts,
+ * levels}; when cap_items >= items, items gets 12 ints per item (kind 0
+ * forward / 1 backward, front, first row, end row, wait counter and target,
+ * second wait counter and target, two done counters, 0, 0; -1 for none);
+ * when cap_fronts >= fronts, fronts3 gets each front's pivots S, size f and
+ * parent (-1 at the root).  Items run in this order in the one-launch
+ * dataflow solve; the plan checks that every wait is met by earlier items. */
+int v2d_lu_solve_plan(int imax, int jmax, const int *indptr, const int *indices, int leaf,
+                      int *info4, int *items, int cap_items, int *fronts3, int cap_fronts);
 
 /* Measurement aid (no reference counterpart): device time in ms, summed over
  * the Newton iterations since the last reset, of the four phases of a Newton
@@ -361,23 +374,24 @@ int v2d_solver_phase_times(v2d_solver *s, double *out6, int reset);
  * `reps` applications of the current LU factors (the preconditioner solve of
  * one GMRES iteration), each preceded by a write of flush_bytes to evict L2;
  * *factor_bytes receives the bytes of factor entries one application reads
- * (per front the pivot-block inverses and the L21 / U12 blocks). */
+ * (per front the pivot-block inverses and the blocks G = L21 L11^-1 and
+ * H = U11^-1 U12, which hold as many entries as L21 and U12). */
 int v2d_solver_time_lu_apply(v2d_solver *s, int reps, long long flush_bytes, double *ms_avg,
                              long long *factor_bytes);
 
 /* Measurement aid (no reference counterpart): the device time of each
  * launch of one LU preconditioner solve, averaged over `reps` solves (each
  * after a write of flush_bytes; 0 keeps the factors warm in L2).  ms[k] and
- * codes[k] (kind * 1000 + level; kinds 0 forward per-front, 1 forward pivot
- * rows, 2 forward contribution rows, 3 backward per-front, 4 backward
- * contribution part, 5 backward pivot rows) for k < *n <= cap. */
+ * codes[k] (kind * 1000 + level; kinds 0 forward level, 1 backward level,
+ * 2 the one-launch dataflow solve) for k < *n <= cap. */
 int v2d_solver_time_lu_launches(v2d_solver *s, int reps, long long flush_bytes, double *ms,
                                 int *codes, int cap, int *n);
 /* Measurement aid (no reference counterpart): the device time of each kernel
  * of one LU factorization of the last assembled Jacobian, launched directly,
  * averaged over `reps` (codes kind * 1000 + level; kinds 0 row scaling,
- * 1 scatter, 2 extend-add, 3 panel, 4 L21, 5 row swaps + U12, 6 Schur update,
- * 7 pivot-block inversion, 8 inverse copy). */
+ * 1 scatter, 2 extend-add, 3 first panel, 4 L21 + row swaps + U12, 6 Schur
+ * update + next panel, 7 pivot-block inversion, 8 inverse copy, 9 products
+ * G = L21 L11^-1 and H = U11^-1 U12, 10 their copy). */
 int v2d_solver_time_lu_factor(v2d_solver *s, int reps, double *ms, int *codes, int cap, int *n);
 
 /* Measurement aid (no reference counterpart): average ms of `reps` launches

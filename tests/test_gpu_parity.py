@@ -174,7 +174,7 @@ def test_linsys_seam_canonical_csr_and_solve(v2d, oracle_mod):
     perm = rng.permutation(len(rows))
     ci = np.array(rows)[perm]; cj = np.array(cols)[perm]; cv = np.array(vals)[perm]
     b = rng.standard_normal(n)
-    lin = v2d.MumpsSolver(n, block_layout=2, restart=30, rtol=1e-12)
+    lin = v2d.MumpsSolver(n, block_layout=2, restart=30, rtol=1e-12, precond="bjacobi")
     lin.assemble(ci, cj, cv, b)
     A = sp.csr_matrix((cv, (ci, cj)), shape=(n, n))
     ip, ix, dv = lin.csr()

@@ -78,77 +78,69 @@ def test_plan_rejects_bad_input(v2d, oracle_mod):
     assert _lib.lib().v2d_lu_plan_info(9, 7, None, None, 64, out) == _lib.V2D_EARG
 
 
-def flow_plan(v2d, imax, jmax, ip, ix, leaf=64):
+def solve_plan(v2d, imax, jmax, ip, ix, leaf=64):
+    """The solve's work items (12 ints each) and (S, f, parent) per front."""
     from vorti2d_b200 import _lib
     info = np.zeros(4, dtype=np.intc)
-    code = _lib.lib().v2d_lu_flow_plan(imax, jmax, _lib.iptr(ip), _lib.iptr(ix), leaf,
-                                       _lib.iptr(info), None, 0, None, 0)
+    code = _lib.lib().v2d_lu_solve_plan(imax, jmax, _lib.iptr(ip), _lib.iptr(ix), leaf,
+                                        _lib.iptr(info), None, 0, None, 0)
     assert code == 0, v2d._lib.last_error()
-    items = np.zeros(4 * max(int(info[1]), 1), dtype=np.intc)
-    parent = np.zeros(max(int(info[3]), 1), dtype=np.intc)
-    code = _lib.lib().v2d_lu_flow_plan(imax, jmax, _lib.iptr(ip), _lib.iptr(ix), leaf,
-                                       _lib.iptr(info), _lib.iptr(items), int(info[1]),
-                                       _lib.iptr(parent), int(info[3]))
+    ni, nc, nf, nl = (int(v) for v in info)
+    items = np.zeros(12 * max(ni, 1), dtype=np.intc)
+    fronts = np.zeros(3 * max(nf, 1), dtype=np.intc)
+    code = _lib.lib().v2d_lu_solve_plan(imax, jmax, _lib.iptr(ip), _lib.iptr(ix), leaf,
+                                        _lib.iptr(info), _lib.iptr(items), ni,
+                                        _lib.iptr(fronts), nf)
     assert code == 0, v2d._lib.last_error()
-    return info, items[:4 * int(info[1])].reshape(-1, 4), parent[:int(info[3])]
+    return (ni, nc, nf, nl), items[:12 * ni].reshape(-1, 12), fronts[:3 * nf].reshape(-1, 3)
 
 
-FZ, FU, BY, BX, BXROOT = range(5)
+FWD, BWD = 0, 1
 
 
-def _wait_ctr(kind, q, parent, nf):
-    # the counter each kind waits on (4 per front: z, children's contribution, y, x)
-    return {FZ: nf + q, FU: q, BY: 3 * nf + parent[q] if parent[q] >= 0 else -1,
-            BX: 2 * nf + q, BXROOT: q}[kind]
-
-
-def _done_ctr(kind, q, parent, nf):
-    return {FZ: q, FU: nf + parent[q] if parent[q] >= 0 else -1, BY: 2 * nf + q,
-            BX: 3 * nf + q, BXROOT: 3 * nf + q}[kind]
-
-
-def _producers(items, parent):
+def _producers(items, fronts):
     """What each item reads, from the algorithm alone (not from the
-    counters): z rows need every contribution chunk of the front's children;
-    contribution rows every z chunk of the front; backward y rows the
-    front's z and the x chunks of every ancestor (its contribution variables
-    are pivots of ancestors); x rows the front's z and y chunks."""
-    by_kind = {}
-    for k, (kind, q, c, t) in enumerate(items):
-        by_kind.setdefault((kind, q), []).append(k)
+    counters): a forward item gathers its children's contribution rows; a
+    backward item multiplies its front's z rows and the x of every ancestor
+    (the front's contribution variables are pivots of ancestors)."""
+    S, f, parent = fronts[:, 0], fronts[:, 1], fronts[:, 2]
     kids = {}
-    for k, (kind, q, c, t) in enumerate(items):
-        if kind == FU:
-            kids.setdefault(parent[q], set()).add(q)
-
-    def xs(a):
-        return by_kind.get((BX, a), []) + by_kind.get((BXROOT, a), [])
-
+    for q, pa in enumerate(parent):
+        if pa >= 0:
+            kids.setdefault(int(pa), []).append(q)
+    fwd_cb, fwd_z, bwd = {}, {}, {}
+    for k, it in enumerate(items):
+        kind, q, rb, re = (int(v) for v in it[:4])
+        if kind == FWD:
+            if re > S[q]:
+                fwd_cb.setdefault(q, []).append(k)
+            if rb < S[q]:
+                fwd_z.setdefault(q, []).append(k)
+        else:
+            bwd.setdefault(q, []).append(k)
     prod = []
-    for kind, q, c, t in items:
-        if kind == FZ:
-            p = [k for ch in kids.get(q, ()) for k in by_kind[(FU, ch)]]
-        elif kind == FU:
-            p = by_kind[(FZ, q)]
-        elif kind == BY:
-            p = list(by_kind[(FZ, q)])
+    for it in items:
+        kind, q = int(it[0]), int(it[1])
+        if kind == FWD:
+            prod.append([k for c in kids.get(q, ()) for k in fwd_cb.get(c, [])])
+        else:
+            p = list(fwd_z.get(q, []))
             a = parent[q]
             while a >= 0:
-                p += xs(a)
+                p += bwd.get(int(a), [])
                 a = parent[a]
-        else:
-            p = by_kind[(FZ, q)] + by_kind.get((BY, q), [])
-        prod.append(p)
+            prod.append(p)
     return prod
 
 
-def _simulate(items, parent, nf, ctas, rng):
-    """The kernel's schedule: CTAs take items in ticket order, wait on one
-    counter, finish after a random time, count the item.  Returns the finish
-    order; fails on a deadlock or on an item starting before what it reads."""
+def _simulate(items, fronts, nc, ctas, rng):
+    """The kernel's schedule: CTAs take items in ticket order, wait until both
+    of the item's counters reach their targets, finish after a random time
+    and add one to the item's done counters.  Fails on a deadlock or on an
+    item starting before what it reads; returns the finish order."""
     n = len(items)
-    ctr = np.zeros(4 * nf, dtype=np.int64)
-    prod = _producers(items, parent)
+    ctr = np.zeros(nc, dtype=np.int64)
+    prod = _producers(items, fronts)
     done = np.zeros(n, dtype=bool)
     ticket = 0
     held = {}            # cta -> [item, finish time or None while waiting]
@@ -161,11 +153,12 @@ def _simulate(items, parent, nf, ctas, rng):
         progressed = False
         for cta, slot in list(held.items()):
             k = slot[0]
-            kind, q, c, t = items[k]
+            it = items[k]
             if slot[1] is None:
-                w = _wait_ctr(kind, q, parent, nf)
-                if t <= 0 or ctr[w] >= t:
-                    assert all(done[p] for p in prod[k]), (k, items[k])
+                ready = all(c < 0 or t <= 0 or ctr[c] >= t for c, t in ((it[4], it[5]),
+                                                                         (it[6], it[7])))
+                if ready:
+                    assert all(done[p] for p in prod[k]), (k, it)
                     slot[1] = now + rng.uniform(0.5, 2.0)
                     progressed = True
         running = [(s[1], cta) for cta, s in held.items() if s[1] is not None]
@@ -175,10 +168,9 @@ def _simulate(items, parent, nf, ctas, rng):
         tfin, cta = min(running)
         now = tfin
         k = held[cta][0]
-        kind, q, c, t = items[k]
-        d = _done_ctr(kind, q, parent, nf)
-        if d >= 0:
-            ctr[d] += 1
+        for d in items[k][8:10]:
+            if d >= 0:
+                ctr[d] += 1
         done[k] = True
         order.append(k)
         if ticket < n:
@@ -193,36 +185,50 @@ def _simulate(items, parent, nf, ctas, rng):
 @pytest.mark.parametrize("imax,jmax,leaf", [(5, 4, 64), (9, 7, 4), (24, 13, 16), (33, 21, 16),
                                             (65, 49, 64), (129, 129, 64), (181, 181, 64),
                                             (257, 129, 64)])
-def test_flow_plan_order_is_safe(v2d, oracle_mod, imax, jmax, leaf):
-    """The dataflow solve's work items: validated by the plan, every front
-    above the one-CTA-per-front levels appears with the chunk counts of its
-    rows, and a simulated schedule (1 to 300 CTAs, random item times) never
-    deadlocks and never starts an item before the items it reads."""
+def test_solve_plan_order_is_safe(v2d, oracle_mod, imax, jmax, leaf):
+    """The solve's work items: every front's forward rows [0, f) and backward
+    rows [0, S) are covered exactly once, forward items precede backward
+    ones, and a simulated dataflow schedule (1 to 300 CTAs, random item
+    times) never deadlocks and never starts an item before the items it
+    reads."""
     ip, ix = pattern(oracle_mod, imax, jmax, 1)
-    info, items, parent = flow_plan(v2d, imax, jmax, ip, ix, leaf)
-    L0, nflow, valid, nf = (int(v) for v in info)
-    assert valid == 1 and nflow == len(items) > 0
-    kinds = set(items[:, 0].tolist())
-    assert {FZ, FU, BX} <= kinds and BXROOT in kinds
-    # forward items precede backward ones
-    fwd = np.isin(items[:, 0], [FZ, FU])
+    (ni, nc, nf, nl), items, fronts = solve_plan(v2d, imax, jmax, ip, ix, leaf)
+    assert ni == len(items) > 0 and nc == 3 * nf
+    S, f = fronts[:, 0], fronts[:, 1]
+    cover = {}
+    for it in items:
+        cover.setdefault((int(it[0]), int(it[1])), []).append((int(it[2]), int(it[3])))
+    for q in range(nf):
+        for kind, end in ((FWD, f[q]), (BWD, S[q])):
+            rows = sorted(cover[(kind, q)])
+            assert rows[0][0] == 0 and rows[-1][1] == end
+            assert all(a[1] == b[0] for a, b in zip(rows, rows[1:]))
+    fwd = items[:, 0] == FWD
     assert fwd[:fwd.sum()].all()
     rng = np.random.default_rng(imax * 7 + jmax)
     for ctas in (1, 2, 5, 37, 300):
-        order = _simulate(items, parent, nf, ctas, rng)
-        assert len(order) == nflow
+        order = _simulate(items, fronts, nc, ctas, rng)
+        assert len(order) == ni
 
 
-def test_flow_plan_181_levels(v2d, oracle_mod):
-    """181x181, 64-node leaves: levels 0-3 (512, 256, 128, 64 fronts) keep
-    the one-CTA-per-front launches; the other 65 fronts (levels 4-10) form
-    the dataflow, the root last."""
+def test_solve_plan_181_items(v2d, oracle_mod):
+    """181x181, 64-node leaves: levels 0-3 (512, 256, 128, 64 fronts) take
+    whole fronts as items; the 65 fronts above split into 8-row items; the
+    root (362 pivots, no contribution rows) is the last forward front and the
+    first backward one."""
     ip, ix = pattern(oracle_mod, 181, 181, 1)
-    info, items, parent = flow_plan(v2d, 181, 181, ip, ix)
-    assert int(info[0]) == 4 and int(info[3]) == 1025
-    fronts = sorted(set(items[:, 1].tolist()))
-    assert fronts == list(range(960, 1025))
-    assert parent[1024] == -1 and (parent[960:1024] >= 960).all()
+    (ni, nc, nf, nl), items, fronts = solve_plan(v2d, 181, 181, ip, ix)
+    assert (nf, nl) == (1025, 11)
+    whole = items[items[:, 1] < 960]
+    assert (whole[:, 2] == 0).all()
+    assert (whole[:, 3] == np.where(whole[:, 0] == FWD, fronts[whole[:, 1], 1],
+                                    fronts[whole[:, 1], 0])).all()
+    upper = items[items[:, 1] >= 960]
+    assert (upper[:, 3] - upper[:, 2] <= 8).all()
+    fwd = items[items[:, 0] == FWD]
+    bwd = items[items[:, 0] == BWD]
+    assert fwd[-1, 1] == 1024 and bwd[0, 1] == 1024 and fronts[1024, 2] == -1
+    assert fronts[1024, 0] == fronts[1024, 1] == 362
 
 
 def test_plan_rejects_malformed_csr(v2d, oracle_mod):

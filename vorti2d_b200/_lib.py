@@ -38,7 +38,8 @@ _ll = ctypes.c_longlong
 class KrylovParams(ctypes.Structure):
     _fields_ = [("restart", _i), ("max_it", _i), ("rtol", _d), ("atol", _d),
                 ("precond", _i), ("precision", _i), ("inner_rtol", _d), ("dc_max_it", _i),
-                ("lu_leaf", _i), ("lu_reuse_its", _i), ("lu_reuse_steps", _i)]
+                ("lu_leaf", _i), ("lu_reuse_its", _i), ("lu_reuse_steps", _i),
+                ("lu_solve", _i)]
 
 
 class LinStats(ctypes.Structure):
@@ -88,6 +89,7 @@ _SIGS = {
     "v2d_krylov_defaults": (None, [ctypes.POINTER(KrylovParams)]),
     "v2d_linsys_create": (_i, [_i, _i, ctypes.POINTER(KrylovParams), ctypes.POINTER(_vp)]),
     "v2d_linsys_assemble": (_i, [_vp, _ip, _ip, _dp, _ll, _dp]),
+    "v2d_linsys_set_grid": (_i, [_vp, _i, _i]),
     "v2d_linsys_solve": (_i, [_vp, _dp, ctypes.POINTER(LinStats)]),
     "v2d_linsys_nnz": (_i, [_vp, ctypes.POINTER(_ll)]),
     "v2d_linsys_csr": (_i, [_vp, _ip, _ip, _dp]),
@@ -119,7 +121,7 @@ _SIGS = {
                                        _d, _d, _dp, _dp]),
     "v2d_solver_time_lu_apply": (_i, [_vp, _i, _ll, _dp, ctypes.POINTER(_ll)]),
     "v2d_lu_plan_info": (_i, [_i, _i, _ip, _ip, _i, ctypes.POINTER(_ll)]),
-    "v2d_lu_flow_plan": (_i, [_i, _i, _ip, _ip, _i, _ip, _ip, _i, _ip, _i]),
+    "v2d_lu_solve_plan": (_i, [_i, _i, _ip, _ip, _i, _ip, _ip, _i, _ip, _i]),
 }
 
 _LIB = None

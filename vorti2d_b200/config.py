@@ -81,6 +81,10 @@ class Config:
     """LU preconditioner with ``lu_reuse_its > 0``: keep the factors across
     time steps and ``set_state`` too (the same iteration rule decides when to
     refactor)."""
+    lu_solve: str = "flow"
+    """LU preconditioner solve: ``"flow"`` runs each application as one
+    dataflow launch over the whole front tree; ``"levels"`` as one launch per
+    tree level and sweep (same arithmetic, same results)."""
     raise_on_linear_failure: bool = True
     """Raise if a Krylov solve misses ``ksp_rtol`` (the reference raises on a
     failed PETSc solve, vorti2d/petsc_solver.py:103-105)."""

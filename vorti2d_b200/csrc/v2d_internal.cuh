@@ -62,26 +62,31 @@ struct MfPlan {
     std::vector<long long> foff;
     std::vector<long long> toff;   // offset of the front's S x S block in the level's scratch
     long long tmax = 0;            // largest sum of S^2 over the fronts of one level
+    std::vector<long long> goff;   // offset of the front's G and H in the level's scratch
+    long long gmax = 0;            // largest sum of 2 m S over the fronts of one level
     std::vector<int> lvl_off, lvl_maxS, lvl_maxf, lvl_maxm, lvl_maxm_child;
     std::vector<long long> lvl_fbeg, lvl_fend, lvl_abeg, lvl_aend;
     int *d_S = nullptr, *d_f = nullptr, *d_voff = nullptr, *d_uoff = nullptr;
     int *d_child0 = nullptr, *d_child1 = nullptr, *d_parent = nullptr;
-    long long *d_foff = nullptr, *d_toff = nullptr;
-    int *d_lvl4 = nullptr;         // per level: first front, fronts, row chunks (S, CB)
+    long long *d_foff = nullptr, *d_toff = nullptr, *d_goff = nullptr;
     int *d_vars = nullptr, *d_cbmap = nullptr, *d_asm_csr = nullptr, *d_asm_row = nullptr;
     long long *d_asm_pos = nullptr;
-    // dataflow solve of the levels from flow_level up (one launch; opt-in):
-    // work items {kind, front, chunk, wait target}, forward then backward,
-    // validated on the host (flow_valid) when the plan is built
-    int flow_level = 0, nflow = 0, flow_valid = 0;
-    std::vector<int> h_flow;
-    int *d_flow = nullptr;
+    // work items of the solve (12 ints each: kind, front, rows [beg, end),
+    // two (counter, target) waits, two done counters), forward items level by
+    // level bottom-up, then backward items top-down; the items of level L's
+    // forward sweep are [lvl_fwd[L], lvl_fwd[L + 1]), of its backward sweep
+    // [lvl_bwd[L], lvl_bwd[L + 1]) (lvl_bwd descends with L).  The order is
+    // checked when the plan is built (see items_build).
+    int nitems = 0, nctr = 0;
+    std::vector<int> h_items, lvl_fwd, lvl_bwd;
+    int *d_items = nullptr;
     // host copies, kept only between the build and the upload
     std::vector<int> h_vars, h_cbmap, h_asm_csr, h_asm_row;
     std::vector<long long> h_asm_pos;
 };
 
-// Grid barrier state of the persistent solve (cooperative launch).
+// Error state of the dataflow solve: err is set when a dependency wait ran
+// out (read and reset by mf_check_barrier).
 struct MfBarrier {
     unsigned int count, gen;
     int err, pad;
@@ -92,15 +97,18 @@ struct MfFactor {
     int fp32 = 0;
     void *F = nullptr, *upd = nullptr, *z = nullptr;
     void *tmp = nullptr;        // triangular inverses of one level before they replace L11 / U11
+    void *gh = nullptr;         // G = L21 L11^-1 and H = U11^-1 U12 of one level before they
+                                // replace L21 / U12
     void *inv_g = nullptr;      // inversion work space in global memory for separators too
                                 // wide for shared memory (per CTA: S x (CW + 33))
     void *wb = nullptr;         // transposed solve: per-front adjoint right-hand sides (vtotal)
     double *rs = nullptr;       // row scaling 1 / max |a_r.|
     int *ipiv = nullptr, *perm = nullptr, *flag = nullptr;
     MfBarrier *bar = nullptr;
-    int coop_grid = 0;          // CTAs of the one-launch persistent solve (0: per-phase launches)
-    int *flow_ctr = nullptr;    // dataflow solve: 4 counters per front + the work ticket
-    int flow_grid = 0;          // CTAs of the dataflow solve (0: per-phase launches)
+    int *sctr = nullptr;        // dataflow solve: 3 counters per front + the work ticket
+    int flow_grid = 0;          // CTAs of the dataflow solve
+    int flow = 1;               // 1: the solve is one dataflow launch; 0: one launch per level
+                                // and sweep
     cudaGraphExec_t graph = nullptr;
     const double *graph_val = nullptr;
     const int *graph_rowptr = nullptr;
@@ -127,31 +135,32 @@ void mf_factor_destroy(MfFactor *M);
 MfDev mf_dev(const MfPlan *P, const MfFactor *M);
 // Factor the CSR values (FP64, row-scaled and rounded to the factor's precision).
 int mf_factor(const MfPlan *P, MfFactor *M, const int *rowptr, const double *val, cudaStream_t s);
-// x = A^-1 b with the factors (vectors in the factor's precision).  The
-// kernels exit at once while *stop_a or *stop_b is non-zero (either may be
-// null).  *n_launches (if given) receives the number of kernels launched.
+// x = A^-1 b with the factors (vectors in the factor's precision): one
+// dataflow launch (M->flow) or one launch per level and sweep.  The kernels
+// exit at once while *stop_a or *stop_b is non-zero (either may be null).
+// *n_launches (if given) receives the number of kernels launched.
 int mf_apply(const MfPlan *P, const MfFactor *M, const void *b, void *x, const int *stop_a,
              const int *stop_b, cudaStream_t s, long long *n_launches);
 // lambda = A^-T g with the factors (the transposed solve: a bottom-up sweep
-// with U11^-T / U12^T, then a top-down sweep with L21^T / L11^-T).
+// with U11^-T / H^T, then a top-down sweep with L11^-T / G^T).
 int mf_apply_transpose(const MfPlan *P, MfFactor *M, const void *g, void *lambda, cudaStream_t s);
 int mf_flag(const MfFactor *M, int *flag, cudaStream_t s);
-// V2D_ETIMEOUT (and a reset barrier) if a grid barrier of the persistent solve
-// or a dependency wait of the dataflow solve timed out since the last check.
+// V2D_ETIMEOUT (and a reset error state) if a dependency wait of the
+// dataflow solve timed out since the last check.
 int mf_check_barrier(MfFactor *M, cudaStream_t s);
 // Average device time (ms) of `reps` LU applies to a zero vector, each after a
 // write of flush_bytes (evicts L2); CUDA events on stream s.
 int mf_time_apply(const MfPlan *P, const MfFactor *M, int reps, size_t flush_bytes, cudaStream_t s,
                   double *ms_avg);
 // Per-launch device time of one solve (average of reps), with the launch
-// codes (kind * 1000 + level; kinds: 0 fwd_front, 1 fwd_z, 2 fwd_u,
-// 3 bwd_front, 4 bwd_y, 5 bwd_x); *n receives the number of launches.
+// codes (kind * 1000 + level; kinds: 0 forward level, 1 backward level,
+// 2 the dataflow launch); *n receives the number of launches.
 int mf_time_apply_launches(const MfPlan *P, const MfFactor *M, int reps, size_t flush_bytes,
                            cudaStream_t s, double *ms, int *codes, int cap, int *n);
 // Per-kernel device time of one factorization launched directly (not from
 // its graph), average of reps; codes kind * 1000 + level (kinds 0 rowscale,
-// 1 scatter, 2 extend_add, 3 panel, 4 l21, 5 swap_trsm, 6 gemm, 7 trinv,
-// 8 trcopy).  The factors are recomputed from the same values.
+// 1 scatter, 2 extend_add, 3 panel, 4 L21 + row swaps + U12, 6 gemm,
+// 7 trinv, 8 trcopy, 9 G/H products, 10 G/H copy).  The factors are recomputed from the same values.
 int mf_time_factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, const double *val,
                             int reps, cudaStream_t s, double *ms, int *codes, int cap, int *n);
 

@@ -93,6 +93,7 @@ struct KrylovWork {
     int graph_m[2] = {0, 0};
     int graph_pc[2] = {-1, -1};
     const void *graph_lu[2] = {nullptr, nullptr};
+    int graph_lu_flow[2] = {-1, -1};   // the LU solve form the graph was captured with
 };
 
 // ---------------------------------------------------------------- helpers
@@ -665,6 +666,7 @@ static int capture_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, doub
     w->graph_m[which] = w->m;
     w->graph_pc[which] = precond;
     w->graph_lu[which] = lu ? (const void *)A.lu : nullptr;
+    w->graph_lu_flow[which] = lu ? A.lu->flow : -1;
     return V2D_OK;
 }
 
@@ -676,7 +678,8 @@ static int run_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, double *
     const bool lu = precond == V2D_PC_LU;
     if (w->seg[which].empty() || !w->fin[which] || w->graph_m[which] != w->m ||
         w->graph_pc[which] != precond ||
-        w->graph_lu[which] != (lu ? (const void *)A.lu : nullptr))
+        w->graph_lu[which] != (lu ? (const void *)A.lu : nullptr) ||
+        w->graph_lu_flow[which] != (lu ? A.lu->flow : -1))
         V2D_TRY(capture_cycle<T>(w, which, V, wv, z, Z, x, A, precond, s));
     for (size_t q = 0; q < w->seg[which].size(); ++q) {
         V2D_CUDA_TRY(cudaGraphLaunch(w->seg[which][q], s));

@@ -6,13 +6,22 @@
 // -- what scipy's csr_matrix produces at vorti2d/petsc_solver.py:81-84) and
 // keeps the COO->slot structure; later calls only gather the new values
 // (the cached-permutation refresh of vorti2d/dist_solver.py:327-366).
-// solve(): GMRES(m) with block Jacobi on the device, full solution returned.
+// solve(): GMRES(m) on the device, full solution returned.  The default
+// preconditioner is the multifrontal LU of the assembled matrix (V2D_PC_LU),
+// refreshed at every solve, so each solve is a direct solve refined by GMRES
+// to rtol -- the role of the reference's MUMPS LU (petsc_solver.py:55-61).
+// Its nested-dissection ordering needs the O-grid shape (imax, jmax): given by
+// v2d_linsys_set_grid, or recognised from the pattern at the first assemble
+// (the only imax that divides n/2 whose interior rows have the 9-point
+// psi/omega stencil); block Jacobi and no preconditioner need no grid.
 //
 // Pattern build: row histogram (integer atomics), scan, scatter of COO
 // indices into row buckets, then one thread per row sorts its bucket by
 // (column, COO index) -- the result does not depend on the atomic order, so
 // the pattern and the duplicate summation order are deterministic.
+#include <algorithm>
 #include <cstring>
+#include <vector>
 
 #include "v2d_internal.cuh"
 
@@ -36,6 +45,12 @@ struct v2d_linsys {
     int *flag = nullptr;
     KrylovWork *kw = nullptr;
     bool has_pattern = false, has_values = false;
+    // LU preconditioner (field-blocked O-grid systems)
+    int imax = 0, jmax = 0;
+    MfPlan *plan = nullptr;
+    MfFactor *lu = nullptr;
+    bool lu_fresh = false;      // factors of the current values
+    int lu_last_its = 0;
 };
 
 namespace {
@@ -164,8 +179,101 @@ extern "C" int v2d_linsys_destroy(v2d_linsys *L)
     for (void *p : ptrs)
         if (p) cudaFree(p);
     krylov_destroy(L->kw);
+    mf_factor_destroy(L->lu);
+    mf_plan_destroy(L->plan);
     if (L->s) cudaStreamDestroy(L->s);
     delete L;
+    return V2D_OK;
+}
+
+// The O-grid shape of a field-blocked 2N system (psi rows [0, N), omega rows
+// [N, 2N), node K = imax*j + i) from its pattern: a candidate imax (a divisor
+// of N) is accepted when three interior nodes away from the seam, the wall
+// and the far field have exactly the interior columns of
+// vorti2d_core.f90:276-293 (psi: the 9 psi neighbours and omega_K) and
+// :341-378 (omega: the 9 omega neighbours and psi n, s, e, w).
+static bool interior_rows_match(int imax, int N, const int *rp, const int *ci, int i, int j)
+{
+    const int K = imax * j + i;
+    int want_psi[10], want_ome[13], a = 0;
+    for (int dj = -1; dj <= 1; ++dj)
+        for (int di = -1; di <= 1; ++di) want_psi[a++] = K + dj * imax + di;
+    want_psi[a++] = N + K;
+    a = 0;
+    for (int dj = -1; dj <= 1; ++dj)
+        for (int di = -1; di <= 1; ++di) want_ome[a++] = N + K + dj * imax + di;
+    want_ome[a++] = K - imax;
+    want_ome[a++] = K - 1;
+    want_ome[a++] = K + 1;
+    want_ome[a++] = K + imax;
+    std::sort(want_psi, want_psi + 10);
+    std::sort(want_ome, want_ome + 13);
+    auto same = [&](int r, const int *w, int nw) {
+        std::vector<int> c(ci + rp[r], ci + rp[r + 1]);
+        std::sort(c.begin(), c.end());
+        c.erase(std::unique(c.begin(), c.end()), c.end());
+        return (int)c.size() == nw && std::equal(c.begin(), c.end(), w);
+    };
+    return same(K, want_psi, 10) && same(N + K, want_ome, 13);
+}
+
+static int infer_grid(int n, const std::vector<int> &rp, const std::vector<int> &ci, int *imax,
+                      int *jmax)
+{
+    const int N = n / 2;
+    int found = 0, fi = 0;
+    for (int im = 5; im <= N / 6; ++im) {
+        if (N % im) continue;
+        const int jm = N / im;
+        if (jm < 6) continue;
+        const int probes[3][2] = {{im / 2, jm / 2}, {1, 2}, {im - 2, jm - 3}};
+        bool ok = true;
+        for (auto &pr : probes)
+            ok = ok && interior_rows_match(im, N, rp.data(), ci.data(), pr[0], pr[1]);
+        if (ok) {
+            ++found;
+            fi = im;
+        }
+    }
+    if (found != 1) {
+        set_error("linsys: the LU preconditioner needs the O-grid shape; %s (call "
+                  "v2d_linsys_set_grid, or use block Jacobi)",
+                  found ? "several grid shapes fit the pattern" : "the pattern is not a "
+                  "field-blocked psi-omega O-grid system with at least 6 rows");
+        return V2D_EARG;
+    }
+    *imax = fi;
+    *jmax = N / fi;
+    return V2D_OK;
+}
+
+extern "C" int v2d_linsys_set_grid(v2d_linsys *L, int imax, int jmax)
+{
+    V2D_ARG_CHECK(L, "linsys_set_grid: null handle");
+    V2D_ARG_CHECK(!L->has_pattern, "linsys_set_grid: the pattern is already fixed");
+    V2D_ARG_CHECK(imax >= 5 && jmax >= 4 && (long long)imax * jmax * 2 == L->n,
+                  "linsys_set_grid: 2 * %d * %d != n = %d", imax, jmax, L->n);
+    L->imax = imax;
+    L->jmax = jmax;
+    return V2D_OK;
+}
+
+// Symbolic LU plan and factor storage for the fixed pattern.
+static int setup_lu(v2d_linsys *L)
+{
+    V2D_ARG_CHECK(L->layout == 1, "linsys: the LU preconditioner needs the field-blocked "
+                  "layout (block_layout 1)");
+    std::vector<int> rp(L->n + 1), ci(L->nnz);
+    V2D_CUDA_TRY(cudaMemcpyAsync(rp.data(), L->indptr, (L->n + 1) * sizeof(int),
+                                 cudaMemcpyDeviceToHost, L->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(ci.data(), L->indices, L->nnz * sizeof(int),
+                                 cudaMemcpyDeviceToHost, L->s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(L->s));
+    if (!L->imax) V2D_TRY(infer_grid(L->n, rp, ci, &L->imax, &L->jmax));
+    const int leaf = L->prm.lu_leaf > 0 ? L->prm.lu_leaf : 64;
+    V2D_TRY(mf_plan_create(L->imax, L->jmax, L->n, rp.data(), ci.data(), leaf, &L->plan));
+    V2D_TRY(mf_factor_create(L->plan, L->prm.precision == V2D_PREC_MIXED ? 1 : 0, &L->lu));
+    L->lu->flow = L->prm.lu_solve == 0 ? 1 : 0;
     return V2D_OK;
 }
 
@@ -177,7 +285,9 @@ extern "C" int v2d_linsys_create(int n, int block_layout, const v2d_krylov_param
     V2D_ARG_CHECK(n > 0, "linsys_create: n must be positive (got %d)", n);
     V2D_ARG_CHECK(block_layout >= 0 && block_layout <= 2, "linsys_create: layout %d", block_layout);
     V2D_ARG_CHECK(block_layout == 0 || n % 2 == 0, "linsys_create: 2x2 layouts need an even n");
-    V2D_ARG_CHECK(p->precond != V2D_PC_LU, "linsys_create: the LU preconditioner needs the grid (use the solver API)");
+    V2D_ARG_CHECK(p->precond != V2D_PC_LU || block_layout == 1,
+                  "linsys_create: the LU preconditioner needs the field-blocked layout "
+                  "(block_layout 1)");
     v2d_linsys *L = new v2d_linsys();
     L->n = n;
     L->layout = block_layout;
@@ -252,6 +362,7 @@ extern "C" int v2d_linsys_assemble(v2d_linsys *L, const int *coo_i, const int *c
         k_row_indices<<<grid_for(n, 128), 128, 0, s>>>(n, L->coo_j, L->bucket_ptr, L->bucket,
                                                         L->indptr, L->indices);
         V2D_CUDA_TRY(cudaGetLastError());
+        if (L->prm.precond == V2D_PC_LU) V2D_TRY(setup_lu(L));
         L->has_pattern = true;
     } else {
         V2D_ARG_CHECK(nnz == L->nnz_coo,
@@ -285,6 +396,7 @@ extern "C" int v2d_linsys_assemble(v2d_linsys *L, const int *coo_i, const int *c
         return V2D_EBREAKDOWN;
     }
     L->has_values = true;
+    L->lu_fresh = false;
     return V2D_OK;
 }
 
@@ -297,7 +409,43 @@ extern "C" int v2d_linsys_solve(v2d_linsys *L, double *x, v2d_lin_stats *st)
     A.val32 = L->data32; A.dinv = L->dinv; A.dinv32 = L->dinv32; A.layout = L->layout;
     A.nblk = L->layout == 0 ? L->n : L->n / 2;
     v2d_lin_stats ls{};
-    V2D_TRY(krylov_solve(L->kw, A, L->b, L->x, L->prm, &ls, L->s));
+    if (L->prm.precond == V2D_PC_LU) {
+        // factors of the current values, or (lu_reuse_its > 0) the last
+        // factors while the solves with them stay within that many
+        // iterations: a bounded attempt, then refactor and solve again
+        const v2d_krylov_params &kp = L->prm;
+        A.lu_plan = L->plan;
+        A.lu = L->lu;
+        bool fresh = L->lu_fresh;
+        const bool reuse = !fresh && kp.lu_reuse_its > 0 && L->lu_last_its >= 0 &&
+                           L->lu_last_its <= kp.lu_reuse_its;
+        if (!fresh && !reuse) {
+            V2D_TRY(mf_factor(L->plan, L->lu, L->indptr, L->data, L->s));
+            fresh = true;
+        }
+        int its0 = 0;
+        if (!fresh) {
+            v2d_krylov_params k2 = kp;
+            k2.max_it = std::min(kp.max_it, kp.lu_reuse_its + 5);
+            V2D_TRY(krylov_solve(L->kw, A, L->b, L->x, k2, &ls, L->s));
+            V2D_TRY(mf_check_barrier(L->lu, L->s));
+            if (!ls.converged) {
+                its0 = ls.iterations;
+                V2D_TRY(mf_factor(L->plan, L->lu, L->indptr, L->data, L->s));
+                fresh = true;
+            }
+        }
+        if (fresh) {
+            V2D_TRY(krylov_solve(L->kw, A, L->b, L->x, kp, &ls, L->s));
+            V2D_TRY(mf_check_barrier(L->lu, L->s));
+            ls.iterations += its0;
+        }
+        const bool refactored = fresh && !L->lu_fresh;
+        if (fresh) L->lu_fresh = true;
+        L->lu_last_its = refactored ? 0 : ls.iterations;
+    } else {
+        V2D_TRY(krylov_solve(L->kw, A, L->b, L->x, L->prm, &ls, L->s));
+    }
     V2D_CUDA_TRY(cudaMemcpyAsync(x, L->x, (size_t)L->n * sizeof(double), cudaMemcpyDeviceToHost, L->s));
     V2D_CUDA_TRY(cudaStreamSynchronize(L->s));
     if (st) *st = ls;

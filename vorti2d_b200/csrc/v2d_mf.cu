@@ -46,6 +46,7 @@
 // x = U11^-1 y, scatter).  Every step is a row-parallel product split over
 // CTAs of 8 rows, so the large top fronts spread over many SMs.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -59,48 +60,20 @@
 
 namespace v2d {
 
-// rows per work item of the solve (kSolveRows below; also the level table's unit)
+// rows per work item of the solve on levels with few fronts
 constexpr int kSolveRowsHost = 8;
-// levels with at least this many fronts are solved with one CTA per front
+// threads of a solve work item (8 warps)
+constexpr int kSolveThreadsHost = 256;
+// levels with at least this many fronts take whole fronts as work items
 constexpr int kFrontPerCtaHost = 64;
 
-// Dataflow solve of the upper levels: one launch runs the work items of the
-// levels from the plan's flow_level up, forward then backward, in a fixed
-// order.  A CTA takes the next item by ticket, waits until one counter
-// reaches the item's target, runs it and counts it on one counter.  Item
-// kinds and the counters (4 per front: z chunks done, the children's
-// contribution chunks done, y chunks done, x chunks done):
-//   kFlowZ      z rows of a front        waits: children's contribution rows  done: z[q]
-//   kFlowU      contribution rows        waits: z[q] (all z chunks)           done: cu[parent]
-//   kFlowY      backward y rows          waits: x[parent] (all x chunks)      done: y[q]
-//   kFlowX      backward x rows          waits: y[q] (all y chunks)           done: x[q]
-//   kFlowXRoot  x rows, no contribution  waits: z[q]                          done: x[q]
-// Every counter an item waits on is advanced only by items earlier in the
-// order, which the plan checks: a ticket-ordered CTA then only ever waits
-// for items that running CTAs already hold, so the launch needs no
-// co-resident grid.
-enum { kFlowZ = 0, kFlowU = 1, kFlowY = 2, kFlowX = 3, kFlowXRoot = 4 };
-
-__host__ __device__ inline int flow_wait_ctr(int kind, int q, int parent, int nf)
-{
-    switch (kind) {
-    case kFlowZ: return nf + q;
-    case kFlowU: return q;
-    case kFlowY: return parent >= 0 ? 3 * nf + parent : -1;
-    case kFlowX: return 2 * nf + q;
-    default: return q;
-    }
-}
-
-__host__ __device__ inline int flow_done_ctr(int kind, int q, int parent, int nf)
-{
-    switch (kind) {
-    case kFlowZ: return q;
-    case kFlowU: return parent >= 0 ? nf + parent : -1;
-    case kFlowY: return 2 * nf + q;
-    default: return 3 * nf + q;
-    }
-}
+// Counters of the dataflow solve, three per front q: forward items of q
+// that wrote z rows (fz), the children's forward items that wrote
+// contribution rows (fin), backward items of q (bx); the work ticket after
+// them.
+__host__ __device__ inline int ctr_fz(int q, int nf) { return q; }
+__host__ __device__ inline int ctr_fin(int q, int nf) { return nf + q; }
+__host__ __device__ inline int ctr_bx(int q, int nf) { return 2 * nf + q; }
 
 // ================================================================ symbolic
 namespace {
@@ -228,104 +201,123 @@ void mf_plan_destroy(MfPlan *p)
 {
     if (!p) return;
     void *ptrs[] = {p->d_S, p->d_f, p->d_voff, p->d_uoff, p->d_child0, p->d_child1, p->d_parent,
-                    p->d_foff, p->d_toff, p->d_lvl4,
-                    p->d_vars, p->d_cbmap, p->d_asm_csr, p->d_asm_row, p->d_asm_pos,
-                    p->d_flow};
+                    p->d_foff, p->d_toff, p->d_goff, p->d_vars, p->d_cbmap, p->d_asm_csr,
+                    p->d_asm_row, p->d_asm_pos, p->d_items};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     delete p;
 }
 
-// Work items of the dataflow solve (kinds and counters at flow_wait_ctr) for
-// the levels from the first one above which every level has fewer than
-// kFrontPerCtaHost fronts, then the check that makes the order safe: the
-// counter each item waits on reaches exactly the item's target, and only
-// through items before it.  A plan that fails the check (or has no such
-// levels) keeps nflow = 0 and the per-phase launches.
-static void flow_build(MfPlan *P)
+// Work items of the solve.  Forward: per level bottom-up, per front, rows
+// [0, f) -- whole fronts on levels with at least kFrontPerCtaHost fronts,
+// chunks of kSolveRowsHost rows above.  Backward: per level top-down, rows
+// [0, S) in the same granularity.  Waits and done counters:
+//   forward item of q   waits fin[q] = all children's items with contribution
+//                       rows; done: fz[q] if it has z rows, fin[parent] if
+//                       it has contribution rows
+//   backward item of q  waits fz[q] = all of q's forward items with z rows,
+//                       and bx[parent] = all of the parent's backward items
+//                       (which waited for theirs: all ancestors' x);
+//                       done: bx[q]
+// The check: every wait's counter reaches exactly its target in all, and
+// only through items earlier in the order; so the items an item reads have
+// all finished before it starts, and a CTA that takes items in order only
+// waits for items that running CTAs hold.
+static int items_build(MfPlan *P)
 {
     const int nf = P->nfront, nl = P->nlevel;
-    P->h_flow.clear();
-    P->nflow = 0;
-    P->flow_valid = 0;
-    int L0 = nl;
-    while (L0 > 0 && P->lvl_off[L0] - P->lvl_off[L0 - 1] < kFrontPerCtaHost) --L0;
-    P->flow_level = L0;
-    if (L0 >= nl) return;
-    auto chunks = [](int rows) { return (rows + kSolveRowsHost - 1) / kSolveRowsHost; };
-    std::vector<int> lvl(nf, 0);
-    for (int L = 0; L < nl; ++L)
-        for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q) lvl[q] = L;
-    auto nz = [&](int q) { return std::max(1, chunks(P->S[q])); };
-    std::vector<int> &it = P->h_flow;
-    auto push = [&](int kind, int q, int c, int target) {
-        it.push_back(kind);
-        it.push_back(q);
-        it.push_back(c);
-        it.push_back(target);
+    std::vector<int> &it = P->h_items;
+    it.clear();
+    P->lvl_fwd.assign(nl + 1, 0);
+    P->lvl_bwd.assign(nl + 1, 0);
+    auto per = [&](int L) {
+        return P->lvl_off[L + 1] - P->lvl_off[L] >= kFrontPerCtaHost ? INT_MAX : kSolveRowsHost;
     };
-    for (int L = L0; L < nl; ++L) {
-        for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q) {
-            int target = 0;
-            for (int c : {P->child0[q], P->child1[q]})
-                if (c >= 0 && lvl[c] >= L0) target += chunks(P->f[c] - P->S[c]);
-            for (int c = 0; c < nz(q); ++c) push(kFlowZ, q, c, target);
-        }
+    auto push = [&](int kind, int q, int rb, int re) {
+        const int v[12] = {kind, q, rb, re, -1, 0, -1, 0, -1, -1, 0, 0};
+        it.insert(it.end(), v, v + 12);
+    };
+    for (int L = 0; L < nl; ++L) {
+        P->lvl_fwd[L] = (int)it.size() / 12;
+        const int R = per(L);
         for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q)
-            for (int c = 0; c < chunks(P->f[q] - P->S[q]); ++c) push(kFlowU, q, c, nz(q));
+            for (int rb = 0; rb < P->f[q]; rb += std::min(R, P->f[q]))
+                push(0, q, rb, (int)std::min<long long>((long long)rb + R, P->f[q]));
     }
-    for (int L = nl - 1; L >= L0; --L) {
-        for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q) {
-            if (P->f[q] == P->S[q]) continue;
-            const int par = P->parent[q];
-            const int target = par >= 0 ? chunks(P->S[par]) : 0;
-            for (int c = 0; c < chunks(P->S[q]); ++c) push(kFlowY, q, c, target);
-        }
-        for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q) {
-            const bool cb = P->f[q] > P->S[q];
-            for (int c = 0; c < chunks(P->S[q]); ++c)
-                push(cb ? kFlowX : kFlowXRoot, q, c, cb ? chunks(P->S[q]) : nz(q));
+    P->lvl_fwd[nl] = (int)it.size() / 12;
+    for (int L = nl - 1; L >= 0; --L) {
+        P->lvl_bwd[L + 1] = (int)it.size() / 12;
+        const int R = per(L);
+        for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q)
+            for (int rb = 0; rb < P->S[q]; rb += std::min(R, P->S[q]))
+                push(1, q, rb, (int)std::min<long long>((long long)rb + R, P->S[q]));
+    }
+    P->lvl_bwd[0] = (int)it.size() / 12;
+    const int ni = (int)it.size() / 12;
+    // totals per front
+    std::vector<int> nfz(nf, 0), nfin(nf, 0), nbx(nf, 0);
+    for (int k = 0; k < ni; ++k) {
+        const int *v = &it[12 * k];
+        const int q = v[1];
+        if (v[0] == 0) {
+            if (v[2] < P->S[q]) ++nfz[q];
+            if (v[3] > P->S[q] && P->parent[q] >= 0) ++nfin[P->parent[q]];
+        } else {
+            ++nbx[q];
         }
     }
-    // the check: every front of the dataflow has pivots (a backward wait on a
-    // parent's x chunks must stand for all its ancestors), totals per
-    // counter, then each wait against the items before it
-    const int nitems = (int)it.size() / 4;
-    std::vector<int> total(4 * nf, 0), seen(4 * nf, 0);
+    for (int k = 0; k < ni; ++k) {
+        int *v = &it[12 * k];
+        const int q = v[1], pa = P->parent[q];
+        if (v[0] == 0) {
+            if (nfin[q] > 0) { v[4] = ctr_fin(q, nf); v[5] = nfin[q]; }
+            if (v[2] < P->S[q]) v[8] = ctr_fz(q, nf);
+            if (v[3] > P->S[q] && pa >= 0) v[9] = ctr_fin(pa, nf);
+        } else {
+            v[4] = ctr_fz(q, nf);
+            v[5] = nfz[q];
+            if (pa >= 0) { v[6] = ctr_bx(pa, nf); v[7] = nbx[pa]; }
+            v[8] = ctr_bx(q, nf);
+        }
+    }
+    // the check
+    const int nc = 3 * nf;
+    std::vector<int> total(nc, 0), seen(nc, 0);
     bool ok = true;
-    for (int q = P->lvl_off[L0]; q < nf; ++q)
-        if (P->S[q] <= 0) ok = false;
-    for (int k = 0; k < nitems && ok; ++k) {
-        const int kind = it[4 * k], q = it[4 * k + 1];
-        if (q < 0 || q >= nf || lvl[q] < L0 || kind < kFlowZ || kind > kFlowXRoot) {
-            ok = false;
-            break;
+    for (int q = 0; q < nf; ++q)
+        ok = ok && P->S[q] > 0 && (P->f[q] == P->S[q] || P->parent[q] >= 0);
+    for (int k = 0; k < ni && ok; ++k) {
+        const int *v = &it[12 * k];
+        const int q = v[1];
+        ok = ok && (v[0] == 0 || v[0] == 1) && q >= 0 && q < nf && v[2] >= 0 && v[3] > v[2] &&
+             v[3] <= (v[0] == 0 ? P->f[q] : P->S[q]);
+        for (int d : {v[8], v[9]}) {
+            ok = ok && d >= -1 && d < nc;
+            if (ok && d >= 0) ++total[d];
         }
-        const int c = it[4 * k + 2];
-        const int rows = kind == kFlowU ? P->f[q] - P->S[q] : P->S[q];
-        const int nc = kind == kFlowZ ? nz(q) : chunks(rows);
-        if (c < 0 || c >= nc) {
-            ok = false;
-            break;
-        }
-        const int d = flow_done_ctr(kind, q, P->parent[q], nf);
-        if (d >= 0) ++total[d];
     }
-    for (int k = 0; k < nitems && ok; ++k) {
-        const int kind = it[4 * k], q = it[4 * k + 1], target = it[4 * k + 3];
-        if (kind == kFlowY && P->parent[q] < 0) ok = false;
-        const int w = flow_wait_ctr(kind, q, P->parent[q], nf);
-        if (target > 0 && (w < 0 || seen[w] != target || total[w] != target)) ok = false;
-        if (target == 0 && w >= 0 && total[w] != 0) ok = false;
-        const int d = flow_done_ctr(kind, q, P->parent[q], nf);
-        if (d >= 0) ++seen[d];
+    for (int k = 0; k < ni && ok; ++k) {
+        const int *v = &it[12 * k];
+        for (int w : {0, 1}) {
+            const int c = v[4 + 2 * w], t = v[5 + 2 * w];
+            if (c < 0) continue;
+            ok = ok && c < nc && t > 0 && total[c] == t && seen[c] == t;
+        }
+        // a backward item needs its own z and, below the root, its parent's x
+        if (v[0] == 1)
+            ok = ok && v[4] == ctr_fz(v[1], nf) && v[5] == nfz[v[1]] &&
+                 (P->parent[v[1]] < 0 || v[6] == ctr_bx(P->parent[v[1]], nf));
+        for (int d : {v[8], v[9]})
+            if (d >= 0) ++seen[d];
     }
     if (!ok) {
+        set_error("mf_plan: solve work items failed their order check");
         it.clear();
-        return;
+        return V2D_EARG;
     }
-    P->nflow = nitems;
-    P->flow_valid = 1;
+    P->nitems = ni;
+    P->nctr = nc;
+    return V2D_OK;
 }
 
 int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_colind,
@@ -507,6 +499,15 @@ int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_c
         }
         P->tmax = std::max(P->tmax, t);
     }
+    P->goff.assign(nf, 0);
+    for (int L = 0; L < nlevel; ++L) {
+        long long t = 0;
+        for (int id = P->lvl_off[L]; id < P->lvl_off[L + 1]; ++id) {
+            P->goff[id] = t;
+            t += 2LL * P->S[id] * (P->f[id] - P->S[id]);
+        }
+        P->gmax = std::max(P->gmax, t);
+    }
     for (int L = 0; L < nlevel; ++L) {
         const int a = P->lvl_off[L], b = P->lvl_off[L + 1];
         P->lvl_fbeg[L] = P->foff[a];
@@ -612,7 +613,10 @@ int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_c
     P->h_asm_csr = std::move(asm_csr);
     P->h_asm_row = std::move(asm_row);
     P->h_asm_pos = std::move(asm_pos);
-    flow_build(P);
+    if (items_build(P) != V2D_OK) {
+        mf_plan_destroy(P);
+        return V2D_EARG;
+    }
     *out = P;
     return V2D_OK;
 }
@@ -633,22 +637,13 @@ int mf_plan_create(int imax, int jmax, int n, const int *h_rowptr, const int *h_
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_parent, P->parent);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_foff, P->foff);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_toff, P->toff);
-    if (st_up == V2D_OK) {
-        std::vector<int> l4(4 * P->nlevel);
-        for (int L = 0; L < P->nlevel; ++L) {
-            l4[4 * L] = P->lvl_off[L];
-            l4[4 * L + 1] = P->lvl_off[L + 1] - P->lvl_off[L];
-            l4[4 * L + 2] = std::max(1, (P->lvl_maxS[L] + kSolveRowsHost - 1) / kSolveRowsHost);
-            l4[4 * L + 3] = (P->lvl_maxm[L] + kSolveRowsHost - 1) / kSolveRowsHost;
-        }
-        st_up = upload_vec(&P->d_lvl4, l4);
-    }
+    if (st_up == V2D_OK) st_up = upload_vec(&P->d_goff, P->goff);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_vars, P->h_vars);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_cbmap, P->h_cbmap);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_asm_csr, P->h_asm_csr);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_asm_row, P->h_asm_row);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_asm_pos, P->h_asm_pos);
-    if (st_up == V2D_OK && P->nflow > 0) st_up = upload_vec(&P->d_flow, P->h_flow);
+    if (st_up == V2D_OK) st_up = upload_vec(&P->d_items, P->h_items);
     if (st_up != V2D_OK) {
         mf_plan_destroy(P);
         return st_up;
@@ -685,25 +680,31 @@ extern "C" int v2d_lu_plan_info(int imax, int jmax, const int *indptr, const int
     return V2D_OK;
 }
 
-// Planning aid for the dataflow solve (host only): info4 = {first level of
-// the dataflow launch, work items, 1 if the order passed its check, fronts};
-// items (4 ints each: kind, front, chunk, wait target) and each front's
-// parent are copied out when the caller's arrays are large enough.
-extern "C" int v2d_lu_flow_plan(int imax, int jmax, const int *indptr, const int *indices,
-                                int leaf, int *info4, int *items, int cap_items, int *parent,
-                                int cap_fronts)
+// Planning aid for the solve's work items (host only): info4 = {work items,
+// counters, fronts, levels}; when cap_items >= items, items gets 12 ints per
+// item (kind 0 forward / 1 backward, front, first row, end row, wait counter
+// and target, second wait counter and target, two done counters, 0, 0; -1
+// for none); when cap_fronts >= fronts, fronts3 gets S, f and the parent of
+// each front.
+extern "C" int v2d_lu_solve_plan(int imax, int jmax, const int *indptr, const int *indices,
+                                 int leaf, int *info4, int *items, int cap_items, int *fronts3,
+                                 int cap_fronts)
 {
     using namespace v2d;
-    V2D_ARG_CHECK(indptr && indices && info4, "lu_flow_plan: null pointer");
+    V2D_ARG_CHECK(indptr && indices && info4, "lu_solve_plan: null pointer");
     MfPlan *P = nullptr;
     V2D_TRY(mf_plan_build(imax, jmax, 2 * imax * jmax, indptr, indices, leaf, &P));
-    info4[0] = P->flow_level;
-    info4[1] = P->nflow;
-    info4[2] = P->flow_valid;
-    info4[3] = P->nfront;
-    if (items && cap_items >= P->nflow)
-        std::copy(P->h_flow.begin(), P->h_flow.end(), items);
-    if (parent && cap_fronts >= P->nfront) std::copy(P->parent.begin(), P->parent.end(), parent);
+    info4[0] = P->nitems;
+    info4[1] = P->nctr;
+    info4[2] = P->nfront;
+    info4[3] = P->nlevel;
+    if (items && cap_items >= P->nitems) std::copy(P->h_items.begin(), P->h_items.end(), items);
+    if (fronts3 && cap_fronts >= P->nfront)
+        for (int q = 0; q < P->nfront; ++q) {
+            fronts3[3 * q] = P->S[q];
+            fronts3[3 * q + 1] = P->f[q];
+            fronts3[3 * q + 2] = P->parent[q];
+        }
     mf_plan_destroy(P);
     return V2D_OK;
 }
@@ -1273,422 +1274,528 @@ __global__ void k_trcopy(int q0, const int *__restrict__ S_, const int *__restri
     }
 }
 
+// G = L21 L11^-1 (rows [S, f) x columns [0, S)) and H = U11^-1 U12 (rows
+// [0, S) x columns [S, f)) of every front of a level, from the inverted pivot
+// block, into the level's scratch (G row-major m x S, then H S x m; copied over
+// L21 and U12 by k_ghcopy: each tile of G reads L21 entries that other tiles
+// overwrite).  One CTA per 64 x 64 output tile, 256 threads with 4 x 4
+// outputs each; the triangular factor bounds the inner range (G: k >= c0,
+// with L11^-1's unit diagonal; H: k >= r0).  Grid: (tiles of G then of H for
+// the level's largest front, fronts).
+template <class T>
+__global__ void __launch_bounds__(256) k_gh(int q0, const int *__restrict__ S_,
+                                            const int *__restrict__ f_,
+                                            const long long *__restrict__ foff,
+                                            const long long *__restrict__ goff, const T *F, T *gh)
+{
+    constexpr int NB = PanelWidth<T>::v;
+    constexpr int TL = kGemmTile;
+    __shared__ T As[NB][TL + 1];
+    __shared__ T Bs[NB][TL];
+    const int q = q0 + blockIdx.y;
+    const int S = S_[q], f = f_[q], m = f - S;
+    if (m <= 0) return;
+    const int ts = (S + TL - 1) / TL, tm = (m + TL - 1) / TL;
+    int t = blockIdx.x;
+    const bool isG = t < tm * ts;
+    if (!isG) t -= tm * ts;
+    if (t >= tm * ts) return;
+    const T *A = F + foff[q];
+    T *out = gh + goff[q];
+    int r0, c0, kb;
+    if (isG) {
+        r0 = S + (t / ts) * TL;
+        c0 = (t % ts) * TL;
+        kb = c0;
+    } else {
+        r0 = (t / tm) * TL;
+        c0 = S + (t % tm) * TL;
+        kb = r0;
+    }
+    const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
+    T acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[a][c] = T(0);
+    for (int k = kb; k < S; k += NB) {
+        for (int e = tid; e < TL * NB; e += blockDim.x) {
+            const int rr = e / NB, tt = e - rr * NB;
+            const int r = r0 + rr, kk = k + tt;
+            T a = T(0);
+            if (kk < S && (isG ? r < f : (r < S && kk >= r))) a = A[(long long)r * f + kk];
+            As[tt][rr] = a;
+        }
+        for (int e = tid; e < NB * TL; e += blockDim.x) {
+            const int tt = e / TL, cc = e - tt * TL;
+            const int c = c0 + cc, kk = k + tt;
+            T bv = T(0);
+            if (kk < S) {
+                if (isG) {
+                    if (c < S) bv = kk > c ? A[(long long)kk * f + c] : (kk == c ? T(1) : T(0));
+                } else if (c < f) {
+                    bv = A[(long long)kk * f + c];
+                }
+            }
+            Bs[tt][cc] = bv;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int tt = 0; tt < NB; ++tt) {
+            T av[4], bv[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) av[a] = As[tt][ty + 16 * a];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) bv[c] = Bs[tt][tx + 16 * c];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[a][c] += av[a] * bv[c];
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int r = r0 + ty + 16 * a;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int col = c0 + tx + 16 * c;
+            if (isG) {
+                if (r < f && col < S) out[(long long)(r - S) * S + col] = acc[a][c];
+            } else if (r < S && col < f) {
+                out[(long long)m * S + (long long)r * m + (col - S)] = acc[a][c];
+            }
+        }
+    }
+}
+
+// G and H of the level's fronts: scratch -> factor storage.
+template <class T>
+__global__ void k_ghcopy(int q0, const int *__restrict__ S_, const int *__restrict__ f_,
+                         const long long *__restrict__ foff, const long long *__restrict__ goff,
+                         const T *__restrict__ gh, T *F)
+{
+    const int q = q0 + blockIdx.y;
+    const int S = S_[q], f = f_[q], m = f - S;
+    const T *src = gh + goff[q];
+    T *dst = F + foff[q];
+    const long long ng = (long long)m * S, tot = 2 * ng;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+         e += (long long)gridDim.x * blockDim.x) {
+        long long r, c;
+        if (e < ng) {
+            r = S + e / S;
+            c = e % S;
+        } else {
+            r = (e - ng) / m;
+            c = S + (e - ng) % m;
+        }
+        dst[r * f + c] = src[e];
+    }
+}
+
 // ------------------------------------------------------------------ solve
+// After the factorization each front's storage holds, row-major f x f:
+//   [0,S) x [0,S)   L11^-1 strictly below the diagonal (unit diagonal implied)
+//                   and U11^-1 on and above it,
+//   [S,f) x [0,S)   G = L21 L11^-1,
+//   [0,S) x [S,f)   H = U11^-1 U12,
+// so every row of the solve is one contiguous dot product with a vector
+// gathered once per work item:
+//   forward,  r <  S:  z_r = t_r + F[r, 0:r] . t[0:r]      t = P w_FS (permuted)
+//             r >= S:  u_r = w_r - F[r, 0:S] . t[0:S]      contribution to the parent
+//   backward, r <  S:  x_r = F[r, r:f] . v[r:f]            v = (z, -x_struct)
+// A front's forward rows need only its children's contributions and its
+// backward rows only its own z and its ancestors' x: one dependent step per
+// level and sweep.  G and H hold as many entries as L21 and U12, so a solve
+// still reads sum S (2f - S) factor entries.
 
 __device__ __forceinline__ bool stopped(const int *a, const int *b)
 {
     return (a && *a) || (b && *b);
 }
 
-// The solve runs every step of a front as row-parallel products split over
-// CTAs of kSolveRows rows (one warp per row, lanes across the columns, four
-// independent partial sums), so the large top fronts use many SMs.
-constexpr int kSolveRows = kSolveRowsHost;
-// levels with at least this many fronts are solved with one CTA per front
-constexpr int kFrontPerCta = kFrontPerCtaHost;
-constexpr int kSolveThreads2 = 32 * kSolveRows;
-// the one-CTA-per-front solve kernels: more warps share a front's rows when
-// a level's CTAs of that size all fit on the GPU at once (2 per SM), else
-// kSolveThreads2 per front
-constexpr int kFrontThreads = 512;
-inline int front_threads(int nq) { return nq <= 2 * kSMs ? kFrontThreads : kSolveThreads2; }
+constexpr int kSolveThreads = kSolveThreadsHost;   // 8 warps per work item
+constexpr int kGatherRegs = 4;   // staged gather entries per thread (fronts up to 4 x 256)
 
-template <class T>
-__device__ __forceinline__ T row_dot(const T *__restrict__ row, const T *v, int c0, int c1)
-{
-    const int lane = threadIdx.x & 31;
-    T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
-    int c = c0 + lane;
-    for (; c + 96 < c1; c += 128) {
-        a0 += row[c] * v[c];
-        a1 += row[c + 32] * v[c + 32];
-        a2 += row[c + 64] * v[c + 64];
-        a3 += row[c + 96] * v[c + 96];
-    }
-    for (; c < c1; c += 32) a0 += row[c] * v[c];
-    return warp_sum((a0 + a1) + (a2 + a3));
-}
-
-// Four rows' dot products by one warp at once: row q's entries [b_q, e_q)
-// with v (an empty range for an absent row).  The four rows' loads are in
-// flight together, so a warp that works through many short rows (one CTA
-// per front) waits for one round trip per four rows instead of per row.
-template <class T>
-__device__ __forceinline__ void dot4(const T *p0, const T *p1, const T *p2, const T *p3, int b0,
-                                     int e0, int b1, int e1, int b2, int e2, int b3, int e3,
-                                     const T *v, T &s0, T &s1, T &s2, T &s3)
-{
-    const int lane = threadIdx.x & 31;
-    const int lo = min(min(b0, b1), min(b2, b3));
-    const int hi = max(max(e0, e1), max(e2, e3));
-    T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
-#pragma unroll 4
-    for (int c = lo + lane; c < hi; c += 32) {
-        const T x = v[c];
-        if (c >= b0 && c < e0) a0 += p0[c] * x;
-        if (c >= b1 && c < e1) a1 += p1[c] * x;
-        if (c >= b2 && c < e2) a2 += p2[c] * x;
-        if (c >= b3 && c < e3) a3 += p3[c] * x;
-    }
-    s0 = warp_sum(a0);
-    s1 = warp_sum(a1);
-    s2 = warp_sum(a2);
-    s3 = warp_sum(a3);
-}
-
-// Forward, part 1 (one work item = one row chunk of one front): gather the
-// front's right-hand side w = rs .* b on the fully summed rows plus the
-// children's contribution vectors, permute the fully summed part, and compute
-// the chunk's rows of z = L11^-1 P w (unit diagonal).  Chunk 0 also stores w
-// on the contribution rows in the front's update vector for part 2.
-// Register staging of the per-level solve items: a row of up to kRowRegs * 32
-// entries is loaded into a warp's registers before the vectors it multiplies
-// are gathered, so the two loads overlap.  kGatherRegs entries per thread
-// bound the staged gathers (fronts beyond that take the plain loads).
-constexpr int kRowRegs = 16;
-constexpr int kRowRegsCB = 24;   // the contribution part of a row (U12) is longer
-constexpr int kGatherRegs = 4;
+// Row registers: a warp that computes a single row of an item loads it into
+// registers before the item's dependency wait; rows up to kRowRegs<T> x 32
+// entries (from a 32-aligned start).
+template <class T> struct RowRegs;
+template <> struct RowRegs<float> { static constexpr int v = 32; };
+template <> struct RowRegs<double> { static constexpr int v = 16; };
 
 template <class T, int R>
-__device__ __forceinline__ void row_load(T (&reg)[R], const T *row, int c0, int c1)
+__device__ __forceinline__ void row_load(T (&reg)[R], const T *row, int base, int lo, int hi)
 {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int k = 0; k < R; ++k) {
-        const int c = lane + 32 * k;
-        reg[k] = (c >= c0 && c < c1) ? row[c] : T(0);
+        const int c = base + lane + 32 * k;
+        reg[k] = (c >= lo && c < hi) ? row[c] : T(0);
     }
 }
 
 template <class T, int R>
-__device__ __forceinline__ T row_dot_reg(const T (&reg)[R], const T *v, int c0, int c1)
+__device__ __forceinline__ T row_dot_reg(const T (&reg)[R], const T *v, int base, int lo, int hi)
 {
-    static_assert(R % 2 == 0, "row registers come in pairs");
     const int lane = threadIdx.x & 31;
     T a0 = T(0), a1 = T(0);
 #pragma unroll
     for (int k = 0; k < R; k += 2) {
-        const int c = lane + 32 * k;
-        if (c >= c0 && c < c1) a0 += reg[k] * v[c];
-        if (c + 32 >= c0 && c + 32 < c1) a1 += reg[k + 1] * v[c + 32];
+        const int c = base + lane + 32 * k;
+        if (c >= lo && c < hi) a0 += reg[k] * v[c];
+        if (c + 32 >= lo && c + 32 < hi) a1 += reg[k + 1] * v[c + 32];
     }
     return warp_sum(a0 + a1);
 }
 
+// Four rows' dot products by one warp at once: row u's entries [b_u, e_u)
+// with v (an empty range for an absent row), all loads in flight together.
 template <class T>
-__device__ __forceinline__ void fz_item(const MfDev &D, const T *F, const T *b,
-                                        const double *__restrict__ rs, T *zbuf, T *upd, int q,
-                                        int chunk, T *w, T *t2)
+__device__ __forceinline__ void dot4(const T *const (&p)[4], const int (&b)[4], const int (&e)[4],
+                                     const T *v, T (&s)[4])
 {
-    const int S = D.S[q], f = D.f[q], vo = D.voff[q];
-    const int rbeg = chunk * kSolveRows;
-    if (rbeg >= S && chunk != 0) return;
-    const int ch[2] = {D.child0[q], D.child1[q]};
-    const T *A = F + D.foff[q];
-    const int *vars = D.vars + vo;
-    const int *perm = D.perm + vo;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nt = blockDim.x;
-    // independent loads first: the children's sizes, the front's variable
-    // and permutation indices, and this warp's row of L11^-1
-    int m[2] = {0, 0}, uof[2] = {0, 0};
-#pragma unroll
-    for (int sl = 0; sl < 2; ++sl)
-        if (ch[sl] >= 0) {
-            m[sl] = D.f[ch[sl]] - D.S[ch[sl]];
-            uof[sl] = D.uoff[ch[sl]];
+    const int lane = threadIdx.x & 31;
+    const int lo = min(min(b[0], b[1]), min(b[2], b[3]));
+    const int hi = max(max(e[0], e[1]), max(e[2], e[3]));
+    T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+#pragma unroll 4
+    for (int c = (lo & ~31) + lane; c < hi; c += 32) {
+        const T x = v[c];
+        if (c >= b[0] && c < e[0]) a0 += p[0][c] * x;
+        if (c >= b[1] && c < e[1]) a1 += p[1][c] * x;
+        if (c >= b[2] && c < e[2]) a2 += p[2][c] * x;
+        if (c >= b[3] && c < e[3]) a3 += p[3][c] * x;
+    }
+    s[0] = warp_sum(a0);
+    s[1] = warp_sum(a1);
+    s[2] = warp_sum(a2);
+    s[3] = warp_sum(a3);
+}
+
+// Column range of row r of front (S, f) in the forward (fwd) or backward sweep.
+__device__ __forceinline__ void row_range(bool fwd, int r, int S, int f, int &lo, int &hi)
+{
+    if (fwd) {
+        lo = 0;
+        hi = r < S ? r : S;
+    } else {
+        lo = r;
+        hi = f;
+    }
+}
+
+// A work item: rows [rbeg, rend) of front q in one sweep.  The parts that
+// depend on no other item (indices, scaled right-hand side, the single row a
+// warp owns) are loaded by pre(); run() then gathers the vector the rows
+// multiply (after the item's dependencies are met) and computes the rows.
+template <class T>
+struct SolveItemCtx {
+    static constexpr int R = RowRegs<T>::v;
+    bool fwd;
+    int q, S, f, vo, rbeg, rend;
+    const T *A;
+    // staged gather (forward: vars/perm/child maps; backward: struct vars)
+    bool staged;
+    int ch[2], m[2], uof[2];
+    int pi[kGatherRegs], mp[2][kGatherRegs], xi[kGatherRegs];
+    T rsb[kGatherRegs];
+    // this warp's single row, if the item has at most one row per warp
+    bool onerow;
+    int base;
+    T reg[R];
+
+    __device__ __forceinline__ void pre(const MfDev &D, const T *F, const T *b,
+                                        const double *__restrict__ rs, bool fwd_, int q_,
+                                        int rbeg_, int rend_)
+    {
+        fwd = fwd_;
+        q = q_;
+        rbeg = rbeg_;
+        rend = rend_;
+        S = D.S[q];
+        f = D.f[q];
+        vo = D.voff[q];
+        A = F + D.foff[q];
+        const int tid = threadIdx.x, nt = blockDim.x, wid = tid >> 5, nw = nt >> 5;
+        const int *vars = D.vars + vo;
+        onerow = rend - rbeg <= nw;
+        const int r = rbeg + wid;
+        if (onerow && r < rend) {
+            int lo, hi;
+            row_range(fwd, r, S, f, lo, hi);
+            base = lo & ~31;
+            if (hi - base <= 32 * R) row_load<T, R>(reg, A + (long long)r * f, base, lo, hi);
+            else onerow = false;
+        } else {
+            onerow = false;
         }
-    const int r = rbeg + wid;
-    const bool rowreg = r < S && r <= kRowRegs * 32;
-    T row[kRowRegs];
-    if (rowreg) row_load(row, A + (long long)r * f, 0, r);
-    const bool staged = f <= kGatherRegs * nt && m[0] <= kGatherRegs * nt &&
-                        m[1] <= kGatherRegs * nt;
-    if (staged) {
-        int vi[kGatherRegs], pi[kGatherRegs];
+        if (fwd) {
+            ch[0] = D.child0[q];
+            ch[1] = D.child1[q];
+            for (int sl = 0; sl < 2; ++sl) {
+                m[sl] = ch[sl] >= 0 ? D.f[ch[sl]] - D.S[ch[sl]] : 0;
+                uof[sl] = ch[sl] >= 0 ? D.uoff[ch[sl]] : 0;
+            }
+            staged = f <= kGatherRegs * nt && m[0] <= kGatherRegs * nt &&
+                     m[1] <= kGatherRegs * nt;
+            if (staged) {
+                int vi[kGatherRegs];
 #pragma unroll
-        for (int k = 0; k < kGatherRegs; ++k) {
-            const int p = tid + k * nt;
-            vi[k] = p < S ? vars[p] : -1;
-            pi[k] = p < S ? perm[p] : 0;
+                for (int k = 0; k < kGatherRegs; ++k) {
+                    const int p = tid + k * nt;
+                    vi[k] = p < S ? vars[p] : -1;
+                    pi[k] = p < S ? D.perm[vo + p] : 0;
+#pragma unroll
+                    for (int sl = 0; sl < 2; ++sl) mp[sl][k] = p < m[sl] ? D.cbmap[uof[sl] + p] : 0;
+                }
+#pragma unroll
+                for (int k = 0; k < kGatherRegs; ++k)
+                    rsb[k] = vi[k] >= 0 ? (T)(rs[vi[k]] * (double)b[vi[k]]) : T(0);
+            }
+        } else {
+            staged = f - S <= kGatherRegs * nt;
+            if (staged) {
+#pragma unroll
+                for (int k = 0; k < kGatherRegs; ++k) {
+                    const int e = tid + k * nt;
+                    xi[k] = e < f - S ? vars[S + e] : 0;
+                }
+            }
         }
-        double rv[kGatherRegs];
-        T bv[kGatherRegs];
-        int mp[2][kGatherRegs];
-        T uv[2][kGatherRegs];
+    }
+
+    // Forward: w (f entries: scaled b on the fully summed rows plus the
+    // children's contributions), t = P w_FS; then the item's rows.
+    __device__ __forceinline__ void run_fwd(const MfDev &D, const T *b,
+                                            const double *__restrict__ rs, T *zbuf, T *upd, T *w,
+                                            T *t)
+    {
+        const int tid = threadIdx.x, nt = blockDim.x;
+        if (staged) {
+            T uv[2][kGatherRegs];
 #pragma unroll
-        for (int k = 0; k < kGatherRegs; ++k) {
-            rv[k] = vi[k] >= 0 ? rs[vi[k]] : 0.0;
-            bv[k] = vi[k] >= 0 ? b[vi[k]] : T(0);
+            for (int sl = 0; sl < 2; ++sl)
+#pragma unroll
+                for (int k = 0; k < kGatherRegs; ++k) {
+                    const int e = tid + k * nt;
+                    uv[sl][k] = e < m[sl] ? __ldcg(upd + uof[sl] + e) : T(0);
+                }
+#pragma unroll
+            for (int k = 0; k < kGatherRegs; ++k) {
+                const int p = tid + k * nt;
+                if (p < f) w[p] = rsb[k];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int sl = 0; sl < 2; ++sl) {
+#pragma unroll
+                for (int k = 0; k < kGatherRegs; ++k)
+                    if (tid + k * nt < m[sl]) w[mp[sl][k]] += uv[sl][k];
+                __syncthreads();
+            }
+#pragma unroll
+            for (int k = 0; k < kGatherRegs; ++k)
+                if (tid + k * nt < S) t[tid + k * nt] = w[pi[k]];
+        } else {
+            const int *vars = D.vars + vo;
+            for (int p = tid; p < f; p += nt)
+                w[p] = p < S ? (T)(rs[vars[p]] * (double)b[vars[p]]) : T(0);
+            __syncthreads();
+            for (int sl = 0; sl < 2; ++sl) {
+                const int *map = D.cbmap + uof[sl];
+                const T *u = upd + uof[sl];
+                for (int e = tid; e < m[sl]; e += nt) w[map[e]] += __ldcg(u + e);
+                __syncthreads();
+            }
+            for (int i = tid; i < S; i += nt) t[i] = w[D.perm[vo + i]];
         }
-#pragma unroll
-        for (int sl = 0; sl < 2; ++sl)
+        __syncthreads();
+        T *uo = upd + D.uoff[q] - S;   // row r >= S -> uo[r]
+        rows(t, [&](int r, T v) {
+            if (r < S) zbuf[vo + r] = t[r] + v;
+            else uo[r] = w[r] - v;
+        });
+    }
+
+    // Backward: v = (z, -x on the front's struct variables); then the rows.
+    __device__ __forceinline__ void run_bwd(const MfDev &D, const T *zbuf, T *x, T *v)
+    {
+        const int tid = threadIdx.x, nt = blockDim.x, mm = f - S;
+        const int *vars = D.vars + vo;
+        for (int i = tid; i < S; i += nt) v[i] = __ldcg(zbuf + vo + i);
+        if (staged) {
 #pragma unroll
             for (int k = 0; k < kGatherRegs; ++k) {
                 const int e = tid + k * nt;
-                mp[sl][k] = e < m[sl] ? D.cbmap[uof[sl] + e] : 0;
-                uv[sl][k] = e < m[sl] ? __ldcg(upd + uof[sl] + e) : T(0);
+                if (e < mm) v[S + e] = -__ldcg(x + xi[k]);
             }
-#pragma unroll
-        for (int k = 0; k < kGatherRegs; ++k) {
-            const int p = tid + k * nt;
-            if (p < f) w[p] = p < S ? (T)(rv[k] * (double)bv[k]) : T(0);
+        } else {
+            for (int e = tid; e < mm; e += nt) v[S + e] = -__ldcg(x + vars[S + e]);
         }
         __syncthreads();
-#pragma unroll
-        for (int sl = 0; sl < 2; ++sl) {
-#pragma unroll
-            for (int k = 0; k < kGatherRegs; ++k)
-                if (tid + k * nt < m[sl]) w[mp[sl][k]] += uv[sl][k];
-            __syncthreads();
+        rows(v, [&](int r, T val) { x[vars[r]] = val; });
+    }
+
+    // The item's rows: one per warp from registers, or four per warp at a
+    // time (dot4) when the item has more rows than warps.
+    template <class Out>
+    __device__ __forceinline__ void rows(const T *vec, Out out)
+    {
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        if (rend - rbeg <= nw) {
+            const int r = rbeg + wid;
+            if (r < rend) {
+                int lo, hi;
+                row_range(fwd, r, S, f, lo, hi);
+                T s = T(0);
+                if (onerow) {
+                    s = row_dot_reg<T, R>(reg, vec, base, lo, hi);
+                } else {
+                    const T *p[4] = {A + (long long)r * f, A, A, A};
+                    const int bb[4] = {lo, 0, 0, 0}, ee[4] = {hi, 0, 0, 0};
+                    T s4[4];
+                    dot4<T>(p, bb, ee, vec, s4);
+                    s = s4[0];
+                }
+                if (lane == 0) out(r, s);
+            }
+            return;
         }
+        for (int r = rbeg + wid; r < rend; r += 4 * nw) {
+            const T *p[4];
+            int bb[4], ee[4], rr[4];
 #pragma unroll
-        for (int k = 0; k < kGatherRegs; ++k)
-            if (tid + k * nt < S) t2[tid + k * nt] = w[pi[k]];
-        __syncthreads();
-    } else {
-        for (int p = tid; p < f; p += nt) w[p] = p < S ? (T)(rs[vars[p]] * (double)b[vars[p]]) : T(0);
-        __syncthreads();
-        for (int sl = 0; sl < 2; ++sl) {
-            const int *map = D.cbmap + uof[sl];
-            const T *u = upd + uof[sl];
-            for (int e = tid; e < m[sl]; e += nt) w[map[e]] += __ldcg(u + e);
-            __syncthreads();
+            for (int u = 0; u < 4; ++u) {
+                rr[u] = r + u * nw;
+                if (rr[u] < rend) {
+                    row_range(fwd, rr[u], S, f, bb[u], ee[u]);
+                    p[u] = A + (long long)rr[u] * f;
+                } else {
+                    bb[u] = ee[u] = 0;
+                    p[u] = A;
+                }
+            }
+            T s4[4];
+            dot4<T>(p, bb, ee, vec, s4);
+            if (lane == 0) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (rr[u] < rend) out(rr[u], s4[u]);
+            }
         }
-        for (int i = tid; i < S; i += nt) t2[i] = w[perm[i]];
+    }
+};
+
+// Work item table entry: 12 ints.
+//   x: kind (0 forward, 1 backward), front, first row, end row
+//   y: wait counter 0, its target, wait counter 1, its target (-1 / 0: none)
+//   z: done counters 0 and 1 (-1: none), unused, unused
+struct SolveItemDev {
+    int4 x, y, z;
+};
+
+template <class T>
+__device__ __forceinline__ void run_item(SolveItemCtx<T> &c, const MfDev &D, const T *b,
+                                         const double *__restrict__ rs, T *zbuf, T *upd, T *x,
+                                         T *smem)
+{
+    if (c.fwd) c.run_fwd(D, b, rs, zbuf, upd, smem, smem + D.maxf);
+    else c.run_bwd(D, zbuf, x, smem);
+}
+
+// One launch per level and sweep: block i runs item i0 + i (its
+// dependencies are the previous launches).
+template <class T>
+__global__ void __launch_bounds__(kSolveThreads, 2) k_solve_level(
+    const MfDev D, const T *F, const T *b, const double *__restrict__ rs, T *zbuf, T *upd, T *x,
+    const SolveItemDev *__restrict__ items, int i0, const int *stop_a, const int *stop_b)
+{
+    if (stopped(stop_a, stop_b)) return;
+    extern __shared__ unsigned char smem_raw[];
+    T *smem = reinterpret_cast<T *>(smem_raw);
+    const int4 it = items[i0 + blockIdx.x].x;
+    SolveItemCtx<T> c;
+    c.pre(D, F, b, rs, it.x == 0, it.y, it.z, it.w);
+    run_item<T>(c, D, b, rs, zbuf, upd, x, smem);
+}
+
+// Polls of one dependency counter before a CTA of the dataflow solve gives
+// up (each poll sleeps ~40 ns: well under a second in all).
+constexpr long long kFlowSpins = 1LL << 22;
+
+__device__ __forceinline__ int ld_acquire_gpu(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Bounded wait until *ctr >= target; false if it ran out or another CTA
+// reported an error meanwhile.
+__device__ __forceinline__ bool wait_count(const int *ctr, int target, volatile int *err)
+{
+    long long spins = 0;
+    while (ld_acquire_gpu(ctr) < target) {
+        if (*err || ++spins > kFlowSpins) return false;
+        __nanosleep(40);
+    }
+    return true;
+}
+
+// The whole solve as one launch of work items in the plan's order (forward
+// bottom-up, then backward top-down).  A CTA takes items by ticket
+// (ctr[nctr]), loads what needs no other item, waits (thread 0, acquire
+// loads) until the item's counters reach their targets, runs the item and,
+// after a fence, adds one to the item's done counters.  The plan checks that
+// every counter an item waits on is advanced only by items before it, so a
+// CTA only ever waits for items held by running CTAs: no co-resident grid is
+// needed.  A wait that runs out (or an error seen while waiting) sets
+// bar->err (bit 2) and *stop_a (so GMRES stops instead of using an
+// unfinished preconditioner) and ends the CTA.  ctr is zeroed before each
+// launch.
+template <class T>
+__global__ void __launch_bounds__(kSolveThreads, 2) k_solve_flow(
+    const MfDev D, const T *F, const T *b, const double *__restrict__ rs, T *zbuf, T *upd, T *x,
+    const SolveItemDev *__restrict__ items, int nitems, int *ctr, int nctr, MfBarrier *bar,
+    const int *stop_a, const int *stop_b)
+{
+    if (stopped(stop_a, stop_b)) return;   // the flags are the same for every CTA
+    extern __shared__ unsigned char smem_raw[];
+    T *smem = reinterpret_cast<T *>(smem_raw);
+    __shared__ int item_s, ok_s;
+    volatile int *err = &bar->err;
+    int next = threadIdx.x == 0 ? atomicAdd(ctr + nctr, 1) : 0;
+    for (;;) {
+        if (threadIdx.x == 0) item_s = next;
         __syncthreads();
-    }
-    if (r < S) {
-        const T v = rowreg ? row_dot_reg(row, t2, 0, r) : row_dot(A + (long long)r * f, t2, 0, r);
-        if (lane == 0) zbuf[vo + r] = t2[r] + v;
-    }
-    if (chunk == 0) {
-        T *uo = upd + D.uoff[q];
-        for (int i = tid; i < f - S; i += nt) uo[i] = w[S + i];
-    }
-}
-
-// Forward, part 2 (item = contribution-row chunk): upd = w_CB - L21 z, in
-// place in the front's update vector.
-template <class T>
-__device__ __forceinline__ void fu_item(const MfDev &D, const T *F, const T *zbuf, T *upd, int q,
-                                        int chunk, T *z)
-{
-    const int S = D.S[q], f = D.f[q], vo = D.voff[q], m = f - S;
-    const int rbeg = chunk * kSolveRows;
-    if (rbeg >= m) return;
-    const T *A = F + D.foff[q];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int i = rbeg + wid;
-    const bool rowreg = i < m && S <= kRowRegs * 32;
-    T row[kRowRegs];
-    if (rowreg) row_load(row, A + (long long)(S + i) * f, 0, S);
-    for (int j = tid; j < S; j += blockDim.x) z[j] = __ldcg(zbuf + vo + j);
-    __syncthreads();
-    if (i < m) {
-        const T v = rowreg ? row_dot_reg(row, z, 0, S) : row_dot(A + (long long)(S + i) * f, z, 0, S);
-        T *u = upd + D.uoff[q] + i;
-        if (lane == 0) *u = __ldcg(u) - v;
-    }
-}
-
-// Backward, part 1 (item = row chunk): y = z - U12 x_struct, in place in zbuf.
-template <class T>
-__device__ __forceinline__ void by_item(const MfDev &D, const T *F, T *zbuf, const T *x, int q,
-                                        int chunk, T *xs)
-{
-    const int S = D.S[q], f = D.f[q], vo = D.voff[q], m = f - S;
-    const int rbeg = chunk * kSolveRows;
-    if (rbeg >= S || m == 0) return;
-    const T *A = F + D.foff[q];
-    const int *vars = D.vars + vo;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int r = rbeg + wid;
-    const bool rowreg = r < S && m <= kRowRegsCB * 32;
-    T row[kRowRegsCB];
-    if (rowreg) row_load(row, A + (long long)r * f + S, 0, m);
-    for (int i = tid; i < m; i += blockDim.x) xs[i] = __ldcg(x + vars[S + i]);
-    __syncthreads();
-    if (r < S) {
-        const T v = rowreg ? row_dot_reg(row, xs, 0, m) : row_dot(A + (long long)r * f + S, xs, 0, m);
-        if (lane == 0) zbuf[vo + r] = __ldcg(zbuf + vo + r) - v;
-    }
-}
-
-// Backward, part 2 (item = row chunk): x_FS = U11^-1 y, scattered to x.
-template <class T>
-__device__ __forceinline__ void bx_item(const MfDev &D, const T *F, const T *zbuf, T *x, int q,
-                                        int chunk, T *y)
-{
-    const int S = D.S[q], f = D.f[q], vo = D.voff[q];
-    const int rbeg = chunk * kSolveRows;
-    if (rbeg >= S) return;
-    const T *A = F + D.foff[q];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int r = rbeg + wid;
-    const bool rowreg = r < S && S <= kRowRegs * 32;
-    T row[kRowRegs];
-    if (rowreg) row_load(row, A + (long long)r * f, r, S);
-    for (int i = tid; i < S; i += blockDim.x) y[i] = __ldcg(zbuf + vo + i);
-    __syncthreads();
-    if (r < S) {
-        const T v = rowreg ? row_dot_reg(row, y, r, S) : row_dot(A + (long long)r * f, y, r, S);
-        if (lane == 0) x[D.vars[vo + r]] = v;
-    }
-}
-
-// One launch per phase and level (grid: chunks x fronts).
-template <class T>
-__global__ void __launch_bounds__(kSolveThreads2) k_fwd_z(int q0, const MfDev D, const T *F, const T *b,
-                                                          const double *__restrict__ rs, T *zbuf,
-                                                          T *upd, const int *stop_a, const int *stop_b)
-{
-    if (stopped(stop_a, stop_b)) return;
-    extern __shared__ unsigned char smem_raw[];
-    T *w = reinterpret_cast<T *>(smem_raw);
-    fz_item<T>(D, F, b, rs, zbuf, upd, q0 + blockIdx.y, blockIdx.x, w, w + D.maxf);
-}
-
-template <class T>
-__global__ void __launch_bounds__(kSolveThreads2) k_fwd_u(int q0, const MfDev D, const T *F,
-                                                          const T *zbuf, T *upd, const int *stop_a,
-                                                          const int *stop_b)
-{
-    if (stopped(stop_a, stop_b)) return;
-    extern __shared__ unsigned char smem_raw[];
-    fu_item<T>(D, F, zbuf, upd, q0 + blockIdx.y, blockIdx.x, reinterpret_cast<T *>(smem_raw));
-}
-
-template <class T>
-__global__ void __launch_bounds__(kSolveThreads2) k_bwd_y(int q0, const MfDev D, const T *F, T *zbuf,
-                                                          const T *x, const int *stop_a,
-                                                          const int *stop_b)
-{
-    if (stopped(stop_a, stop_b)) return;
-    extern __shared__ unsigned char smem_raw[];
-    by_item<T>(D, F, zbuf, x, q0 + blockIdx.y, blockIdx.x, reinterpret_cast<T *>(smem_raw));
-}
-
-template <class T>
-__global__ void __launch_bounds__(kSolveThreads2) k_bwd_x(int q0, const MfDev D, const T *F,
-                                                          const T *zbuf, T *x, const int *stop_a,
-                                                          const int *stop_b)
-{
-    if (stopped(stop_a, stop_b)) return;
-    extern __shared__ unsigned char smem_raw[];
-    bx_item<T>(D, F, zbuf, x, q0 + blockIdx.y, blockIdx.x, reinterpret_cast<T *>(smem_raw));
-}
-
-// Levels with many small fronts: one CTA per front does the whole forward
-// (gather, z, contribution vector) or backward (y, x) step, so the right-hand
-// side is gathered once per front instead of once per row chunk.
-template <class T>
-__global__ void __launch_bounds__(kFrontThreads) k_fwd_front(int q0, const MfDev D, const T *F,
-                                                              const T *b,
-                                                              const double *__restrict__ rs,
-                                                              T *zbuf, T *upd, const int *stop_a,
-                                                              const int *stop_b)
-{
-    if (stopped(stop_a, stop_b)) return;
-    extern __shared__ unsigned char smem_raw[];
-    T *w = reinterpret_cast<T *>(smem_raw);   // f
-    T *t2 = w + D.maxf;                         // S
-    const int q = q0 + blockIdx.x;
-    const int S = D.S[q], f = D.f[q], vo = D.voff[q];
-    const T *A = F + D.foff[q];
-    const int *vars = D.vars + vo;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
-    for (int p = tid; p < f; p += blockDim.x) w[p] = p < S ? (T)(rs[vars[p]] * (double)b[vars[p]]) : T(0);
-    __syncthreads();
-    for (int slot = 0; slot < 2; ++slot) {
-        const int c = slot == 0 ? D.child0[q] : D.child1[q];
-        if (c >= 0) {
-            const int m = D.f[c] - D.S[c];
-            const int *map = D.cbmap + D.uoff[c];
-            const T *u = upd + D.uoff[c];
-            for (int e = tid; e < m; e += blockDim.x) w[map[e]] += u[e];
+        const int i = item_s;
+        if (i >= nitems) return;
+        const SolveItemDev it = items[i];
+        SolveItemCtx<T> c;
+        c.pre(D, F, b, rs, it.x.x == 0, it.x.y, it.x.z, it.x.w);
+        if (threadIdx.x == 0) {
+            next = atomicAdd(ctr + nctr, 1);   // in flight during the wait
+            bool ok = true;
+            if (it.y.x >= 0 && it.y.y > 0) ok = wait_count(ctr + it.y.x, it.y.y, err);
+            if (ok && it.y.z >= 0 && it.y.w > 0) ok = wait_count(ctr + it.y.z, it.y.w, err);
+            if (!ok) {
+                atomicOr(&bar->err, 2);
+                if (stop_a) atomicExch(const_cast<int *>(stop_a), 1);
+            }
+            ok_s = ok;
         }
         __syncthreads();
-    }
-    const int *perm = D.perm + vo;
-    for (int i = tid; i < S; i += blockDim.x) t2[i] = w[perm[i]];
-    __syncthreads();
-    for (int r = wid; r < S; r += 4 * nw) {        // z = Linv t2 (unit diagonal)
-        int rr[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) rr[u] = r + u * nw < S ? r + u * nw : -1;
-        T v[4];
-        dot4<T>(A + (long long)max(rr[0], 0) * f, A + (long long)max(rr[1], 0) * f,
-                A + (long long)max(rr[2], 0) * f, A + (long long)max(rr[3], 0) * f, 0,
-                max(rr[0], 0), 0, max(rr[1], 0), 0, max(rr[2], 0), 0, max(rr[3], 0), t2, v[0],
-                v[1], v[2], v[3]);
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-            if (lane == 0 && rr[u] >= 0) w[rr[u]] = t2[rr[u]] + v[u];
-    }
-    __syncthreads();
-    for (int r = S + wid; r < f; r += 4 * nw) {    // upd = w_CB - L21 z
-        int rr[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) rr[u] = r + u * nw < f ? r + u * nw : -1;
-        T v[4];
-        dot4<T>(A + (long long)max(rr[0], 0) * f, A + (long long)max(rr[1], 0) * f,
-                A + (long long)max(rr[2], 0) * f, A + (long long)max(rr[3], 0) * f, 0,
-                rr[0] >= 0 ? S : 0, 0, rr[1] >= 0 ? S : 0, 0, rr[2] >= 0 ? S : 0, 0,
-                rr[3] >= 0 ? S : 0, w, v[0], v[1], v[2], v[3]);
-        __syncwarp();
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-            if (lane == 0 && rr[u] >= 0) w[rr[u]] -= v[u];
-    }
-    __syncthreads();
-    for (int i = tid; i < S; i += blockDim.x) zbuf[vo + i] = w[i];
-    T *uo = upd + D.uoff[q];
-    for (int i = tid; i < f - S; i += blockDim.x) uo[i] = w[S + i];
-}
-
-template <class T>
-__global__ void __launch_bounds__(kFrontThreads) k_bwd_front(int q0, const MfDev D, const T *F,
-                                                              const T *zbuf, T *x,
-                                                              const int *stop_a, const int *stop_b)
-{
-    if (stopped(stop_a, stop_b)) return;
-    extern __shared__ unsigned char smem_raw[];
-    T *y = reinterpret_cast<T *>(smem_raw);   // S
-    T *xs = y + D.maxS;                         // f - S
-    const int q = q0 + blockIdx.x;
-    const int S = D.S[q], f = D.f[q], vo = D.voff[q], m = f - S;
-    const T *A = F + D.foff[q];
-    const int *vars = D.vars + vo;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
-    for (int i = tid; i < m; i += blockDim.x) xs[i] = x[vars[S + i]];
-    __syncthreads();
-    for (int r = wid; r < S; r += 4 * nw) {
-        int rr[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) rr[u] = r + u * nw < S ? r + u * nw : -1;
-        T v[4];
-        dot4<T>(A + (long long)max(rr[0], 0) * f + S, A + (long long)max(rr[1], 0) * f + S,
-                A + (long long)max(rr[2], 0) * f + S, A + (long long)max(rr[3], 0) * f + S, 0,
-                rr[0] >= 0 ? m : 0, 0, rr[1] >= 0 ? m : 0, 0, rr[2] >= 0 ? m : 0, 0,
-                rr[3] >= 0 ? m : 0, xs, v[0], v[1], v[2], v[3]);
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-            if (lane == 0 && rr[u] >= 0) y[rr[u]] = zbuf[vo + rr[u]] - v[u];
-    }
-    __syncthreads();
-    for (int r = wid; r < S; r += 4 * nw) {        // x = Uinv y (upper incl. diagonal)
-        int rr[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) rr[u] = r + u * nw < S ? r + u * nw : -1;
-        T v[4];
-        dot4<T>(A + (long long)max(rr[0], 0) * f, A + (long long)max(rr[1], 0) * f,
-                A + (long long)max(rr[2], 0) * f, A + (long long)max(rr[3], 0) * f,
-                rr[0] >= 0 ? rr[0] : 0, rr[0] >= 0 ? S : 0, rr[1] >= 0 ? rr[1] : 0,
-                rr[1] >= 0 ? S : 0, rr[2] >= 0 ? rr[2] : 0, rr[2] >= 0 ? S : 0,
-                rr[3] >= 0 ? rr[3] : 0, rr[3] >= 0 ? S : 0, y, v[0], v[1], v[2], v[3]);
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-            if (lane == 0 && rr[u] >= 0) x[vars[rr[u]]] = v[u];
+        if (!ok_s) return;
+        run_item<T>(c, D, b, rs, zbuf, upd, x, smem);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            if (it.z.x >= 0) atomicAdd(ctr + it.z.x, 1);
+            if (it.z.y >= 0) atomicAdd(ctr + it.z.y, 1);
+        }
     }
 }
 
@@ -1697,15 +1804,15 @@ __global__ void __launch_bounds__(kFrontThreads) k_bwd_front(int q0, const MfDev
 // order.  Bottom-up (adjoint of the backward sweep): the front gathers g on
 // its fully summed variables plus its children's contributions (the same
 // contribution-block maps as the forward sweep), forms ybar = U11^-T acc_FS
-// (kept in zbuf) and passes acc_CB - U12^T ybar up.  Top-down (adjoint of the
-// forward sweep): the front takes its parent's adjoint right-hand side on its
-// contribution rows, zbar = ybar - L21^T upd_bar, t = L11^-T zbar (unit
+// (kept in zbuf) and passes acc_CB - H^T acc_FS up.  Top-down (adjoint of the
+// forward sweep): the front takes its parent's adjoint right-hand side
+// upd_bar on its contribution rows, t = L11^-T ybar - G^T upd_bar (unit
 // diagonal), scatters t through the row permutation and writes
 // lambda = rs .* w_bar on its fully summed variables.  One CTA per front; the
 // transposed products read the factor rows column-wise (one thread per
 // column, coalesced across the warp).
 template <class T>
-__global__ void __launch_bounds__(kSolveThreads2) k_tup_front(int q0, const MfDev D, const T *F,
+__global__ void __launch_bounds__(kSolveThreads) k_tup_front(int q0, const MfDev D, const T *F,
                                                               const T *g, T *zbuf, T *upd)
 {
     extern __shared__ unsigned char smem_raw[];
@@ -1736,213 +1843,44 @@ __global__ void __launch_bounds__(kSolveThreads2) k_tup_front(int q0, const MfDe
     __syncthreads();
     for (int j = tid; j < S; j += blockDim.x) zbuf[vo + j] = yb[j];
     T *uo = upd + D.uoff[q];
-    for (int k = tid; k < m; k += blockDim.x) {     // acc_CB - U12^T ybar
+    for (int k = tid; k < m; k += blockDim.x) {     // acc_CB - H^T acc_FS
         T v = T(0);
-        for (int i = 0; i < S; ++i) v += A[(long long)i * f + S + k] * yb[i];
+        for (int i = 0; i < S; ++i) v += A[(long long)i * f + S + k] * acc[i];
         uo[k] = acc[S + k] - v;
     }
 }
 
 template <class T>
-__global__ void __launch_bounds__(kSolveThreads2) k_tdown_front(int q0, const MfDev D, const T *F,
-                                                                const double *__restrict__ rs,
-                                                                const T *zbuf, T *wb, T *lam)
+__global__ void __launch_bounds__(kSolveThreads) k_tdown_front(int q0, const MfDev D, const T *F,
+                                                               const double *__restrict__ rs,
+                                                               const T *zbuf, T *wb, T *lam)
 {
     extern __shared__ unsigned char smem_raw[];
     T *wbar = reinterpret_cast<T *>(smem_raw);  // f
-    T *zb = wbar + D.maxf;                        // S
+    T *v = wbar + D.maxf;                         // f: (ybar, -upd_bar)
     const int q = q0 + blockIdx.x;
     const int S = D.S[q], f = D.f[q], vo = D.voff[q], m = f - S;
     const T *A = F + D.foff[q];
     const int *vars = D.vars + vo;
     const int tid = threadIdx.x;
     const int pa = D.parent[q];
-    for (int k = tid; k < m; k += blockDim.x)       // upd_bar from the parent
-        wbar[S + k] = pa >= 0 ? wb[D.voff[pa] + D.cbmap[D.uoff[q] + k]] : T(0);
-    __syncthreads();
-    for (int j = tid; j < S; j += blockDim.x) {     // zbar = ybar - L21^T upd_bar
-        T v = T(0);
-        for (int k = 0; k < m; ++k) v += A[(long long)(S + k) * f + j] * wbar[S + k];
-        zb[j] = zbuf[vo + j] - v;
+    for (int k = tid; k < m; k += blockDim.x) {     // upd_bar from the parent
+        const T u = pa >= 0 ? wb[D.voff[pa] + D.cbmap[D.uoff[q] + k]] : T(0);
+        wbar[S + k] = u;
+        v[S + k] = -u;
     }
+    for (int j = tid; j < S; j += blockDim.x) v[j] = zbuf[vo + j];
     __syncthreads();
     const int *perm = D.perm + vo;
-    for (int i = tid; i < S; i += blockDim.x) {     // t = Linv^T zbar; w_bar[perm[i]] = t
-        T v = zb[i];
-        for (int j = i + 1; j < S; ++j) v += A[(long long)j * f + i] * zb[j];
-        wbar[perm[i]] = v;
+    // t = Linv^T ybar - G^T upd_bar: column i of rows (i, f); w_bar[perm[i]] = t
+    for (int i = tid; i < S; i += blockDim.x) {
+        T t = v[i];
+        for (int j = i + 1; j < f; ++j) t += A[(long long)j * f + i] * v[j];
+        wbar[perm[i]] = t;
     }
     __syncthreads();
     for (int p = tid; p < f; p += blockDim.x) wb[vo + p] = wbar[p];
     for (int p = tid; p < S; p += blockDim.x) lam[vars[p]] = (T)(rs[vars[p]] * (double)wbar[p]);
-}
-
-// Grid-wide barrier of a cooperative launch (all CTAs resident): a
-// generation counter in global memory.  The wait is bounded: after
-// kBarrierSpins polls the CTA records a timeout in bar->err and reports
-// failure, and the kernel returns; the host checks bar->err after the solve.
-constexpr long long kBarrierSpins = 1LL << 24;
-
-__device__ __forceinline__ bool grid_barrier(MfBarrier *bar)
-{
-    __shared__ int ok_s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        volatile unsigned int *gen = &bar->gen;
-        const unsigned int g = *gen;
-        __threadfence();
-        const unsigned int arrived = atomicAdd(&bar->count, 1u) + 1u;
-        if (arrived == gridDim.x) {
-            atomicExch(&bar->count, 0u);
-            __threadfence();
-            atomicAdd(&bar->gen, 1u);
-        } else {
-            long long spins = 0;
-            while (*gen == g) {
-                if (++spins > kBarrierSpins) {
-                    atomicOr(&bar->err, 1);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-        ok_s = ok;
-    }
-    __syncthreads();
-    return ok_s != 0;
-}
-
-// The whole solve in one cooperative launch: each phase of each level is a
-// loop over its (front, chunk) work items, separated by grid barriers.  Data
-// written by other CTAs in earlier phases (contribution vectors, z, x) is
-// read with L1-bypassing loads in the item functions.
-template <class T>
-__global__ void __launch_bounds__(kSolveThreads2) k_apply_all(const MfDev D, const T *F, const T *b,
-                                                              const double *__restrict__ rs,
-                                                              T *zbuf, T *upd, T *x,
-                                                              const int4 *__restrict__ lvl, int nlevel,
-                                                              MfBarrier *bar, const int *stop_a,
-                                                              const int *stop_b)
-{
-    if (stopped(stop_a, stop_b)) return;   // the flags are the same for every CTA
-    extern __shared__ unsigned char smem_raw[];
-    T *w = reinterpret_cast<T *>(smem_raw);
-    T *t2 = w + D.maxf;
-    for (int L = 0; L < nlevel; ++L) {
-        const int4 v = lvl[L];   // q0, fronts, chunks over S, chunks over the contribution rows
-        for (int it = blockIdx.x; it < v.y * v.z; it += gridDim.x) {
-            fz_item<T>(D, F, b, rs, zbuf, upd, v.x + it / v.z, it % v.z, w, t2);
-            __syncthreads();
-        }
-        if (!grid_barrier(bar)) return;
-        if (v.w > 0) {
-            for (int it = blockIdx.x; it < v.y * v.w; it += gridDim.x) {
-                fu_item<T>(D, F, zbuf, upd, v.x + it / v.w, it % v.w, w);
-                __syncthreads();
-            }
-            if (!grid_barrier(bar)) return;
-        }
-    }
-    for (int L = nlevel - 1; L >= 0; --L) {
-        const int4 v = lvl[L];
-        if (v.w > 0) {
-            for (int it = blockIdx.x; it < v.y * v.z; it += gridDim.x) {
-                by_item<T>(D, F, zbuf, x, v.x + it / v.z, it % v.z, w);
-                __syncthreads();
-            }
-            if (!grid_barrier(bar)) return;
-        }
-        for (int it = blockIdx.x; it < v.y * v.z; it += gridDim.x) {
-            bx_item<T>(D, F, zbuf, x, v.x + it / v.z, it % v.z, w);
-            __syncthreads();
-        }
-        if (L > 0 && !grid_barrier(bar)) return;
-    }
-}
-
-// Polls of one dependency counter before a dataflow CTA gives up (each poll
-// sleeps ~40 ns: well under a second), records the timeout and returns.
-constexpr long long kFlowSpins = 1LL << 22;
-
-__device__ __forceinline__ int ld_acquire_gpu(const int *p)
-{
-    int v;
-    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-// The upper levels' forward and backward solve as one launch of work items
-// (flow_build): a CTA takes items by ticket (ctr[4 nf]), thread 0 waits with
-// acquire loads until the item's counter reaches its target, the CTA runs
-// the item (the same item functions as the per-phase launches; data from
-// other CTAs is read through L2), and after a fence thread 0 counts it.  A
-// wait that runs out, or an error seen while waiting, sets bar->err (bit 2),
-// sets *stop_a (the Krylov solve's stop flag, so GMRES ends instead of
-// iterating with an unfinished preconditioner) and ends the CTA; the host
-// reads bar->err with mf_check_barrier.  ctr is zeroed before each launch.
-template <class T>
-__global__ void __launch_bounds__(kSolveThreads2, 2) k_apply_flow(const MfDev D, const T *F, const T *b,
-                                                               const double *__restrict__ rs,
-                                                               T *zbuf, T *upd, T *x,
-                                                               const int4 *__restrict__ items,
-                                                               int nitems, int *ctr, int nf,
-                                                               MfBarrier *bar, const int *stop_a,
-                                                               const int *stop_b)
-{
-    if (stopped(stop_a, stop_b)) return;   // the flags are the same for every CTA
-    extern __shared__ unsigned char smem_raw[];
-    T *w = reinterpret_cast<T *>(smem_raw);
-    T *t2 = w + D.maxf;
-    __shared__ int item_s, ok_s;
-    volatile int *err = &bar->err;
-    for (;;) {
-        if (threadIdx.x == 0) {
-            const int it = atomicAdd(ctr + 4 * nf, 1);
-            int ok = 1;
-            if (it < nitems) {
-                const int4 v = items[it];
-                if (v.w > 0) {
-                    const int par = v.x == kFlowY ? D.parent[v.y] : -1;
-                    const int wc = flow_wait_ctr(v.x, v.y, par, nf);
-                    long long spins = 0;
-                    while (ld_acquire_gpu(ctr + wc) < v.w) {
-                        if (*err || ++spins > kFlowSpins) {
-                            atomicOr(&bar->err, 2);
-                            // end the Krylov solve at once: with a CTA gone the
-                            // preconditioner output is unfinished
-                            if (stop_a) atomicExch(const_cast<int *>(stop_a), 1);
-                            ok = 0;
-                            break;
-                        }
-                        __nanosleep(40);
-                    }
-                }
-            }
-            item_s = it;
-            ok_s = ok;
-        }
-        __syncthreads();
-        const int it = item_s;
-        if (it >= nitems || !ok_s) return;
-        const int4 v = items[it];
-        switch (v.x) {
-        case kFlowZ: fz_item<T>(D, F, b, rs, zbuf, upd, v.y, v.z, w, t2); break;
-        case kFlowU: fu_item<T>(D, F, zbuf, upd, v.y, v.z, w); break;
-        case kFlowY: by_item<T>(D, F, zbuf, x, v.y, v.z, w); break;
-        default: bx_item<T>(D, F, zbuf, x, v.y, v.z, w); break;
-        }
-        __threadfence();
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const int par = v.x == kFlowU ? D.parent[v.y] : -1;
-            const int dc = flow_done_ctr(v.x, v.y, par, nf);
-            __threadfence();
-            if (dc >= 0) atomicAdd(ctr + dc, 1);
-        }
-    }
 }
 
 }  // namespace
@@ -1987,6 +1925,8 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
     grab(&M->upd, (size_t)P->utotal * es);
     grab(&M->z, (size_t)P->vtotal * es);
     grab(&M->tmp, (size_t)P->tmax * es);
+    grab(&M->gh, (size_t)P->gmax * es);
+    grab((void **)&M->sctr, (size_t)(P->nctr + 1) * sizeof(int));
     grab(&M->wb, (size_t)P->vtotal * es);
     grab((void **)&M->rs, (size_t)P->n * sizeof(double));
     grab((void **)&M->ipiv, (size_t)P->vtotal * sizeof(int));
@@ -2034,29 +1974,24 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
     auto attr = [&](const void *fn, size_t bytes) {
         if (e == cudaSuccess) e = raise_dyn_smem(fn, bytes);
     };
+    const size_t tsolve = (size_t)2 * P->maxf * es;   // transposed solve: two f vectors
+    if (tsolve > 227 * 1024) {
+        set_error("mf_factor: front of %d unknowns exceeds shared memory (transposed solve)",
+                  P->maxf);
+        mf_factor_destroy(M);
+        return V2D_EARG;
+    }
     if (fp32) {
-        attr((const void *)k_apply_all<float>, solve);
-        attr((const void *)k_apply_flow<float>, solve);
-        attr((const void *)k_fwd_front<float>, solve);
-        attr((const void *)k_tup_front<float>, solve);
-        attr((const void *)k_tdown_front<float>, solve);
-        attr((const void *)k_bwd_front<float>, solve);
-        attr((const void *)k_fwd_z<float>, solve);
-        attr((const void *)k_fwd_u<float>, solve);
-        attr((const void *)k_bwd_y<float>, solve);
-        attr((const void *)k_bwd_x<float>, solve);
+        attr((const void *)k_solve_level<float>, solve);
+        attr((const void *)k_solve_flow<float>, solve);
+        attr((const void *)k_tup_front<float>, tsolve);
+        attr((const void *)k_tdown_front<float>, tsolve);
         attr((const void *)k_trinv<float>, inv);
     } else {
-        attr((const void *)k_apply_all<double>, solve);
-        attr((const void *)k_apply_flow<double>, solve);
-        attr((const void *)k_fwd_front<double>, solve);
-        attr((const void *)k_tup_front<double>, solve);
-        attr((const void *)k_tdown_front<double>, solve);
-        attr((const void *)k_bwd_front<double>, solve);
-        attr((const void *)k_fwd_z<double>, solve);
-        attr((const void *)k_fwd_u<double>, solve);
-        attr((const void *)k_bwd_y<double>, solve);
-        attr((const void *)k_bwd_x<double>, solve);
+        attr((const void *)k_solve_level<double>, solve);
+        attr((const void *)k_solve_flow<double>, solve);
+        attr((const void *)k_tup_front<double>, tsolve);
+        attr((const void *)k_tdown_front<double>, tsolve);
         attr((const void *)k_trinv<double>, inv);
     }
     if (e != cudaSuccess) {
@@ -2064,38 +1999,23 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
         mf_factor_destroy(M);
         return V2D_ECUDA;
     }
-    // persistent solve: as many CTAs as can be resident at once (at most 2 per
-    // SM); 0 keeps the one-launch-per-phase path (the default)
-    int dev = 0, coop = 0, nsm = 0, per_sm = 0;
-    // opt-in (V2D_LU_PERSISTENT=1): on 181x181 the per-phase launches were
-    // faster than one cooperative launch with a grid barrier per phase
-    const char *env = getenv("V2D_LU_PERSISTENT");
-    const bool allow = env && env[0] == '1';
-    if (allow && cudaGetDevice(&dev) == cudaSuccess &&
-        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess &&
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && coop) {
-        cudaError_t oe = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                                    &per_sm, k_apply_all<float>, kSolveThreads2, solve)
-                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                                    &per_sm, k_apply_all<double>, kSolveThreads2, solve);
-        if (oe == cudaSuccess && per_sm > 0) M->coop_grid = nsm * std::min(per_sm, 2);
+    // dataflow solve: as many CTAs as can be resident at once (two per SM at
+    // most), never more than there are work items
+    int dev = 0, nsm = 0, per_sm = 0;
+    cudaError_t oe = cudaGetDevice(&dev);
+    if (oe == cudaSuccess) oe = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (oe == cudaSuccess)
+        oe = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_flow<float>,
+                                                                  kSolveThreads, solve)
+                  : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_flow<double>,
+                                                                  kSolveThreads, solve);
+    if (oe != cudaSuccess || per_sm <= 0) {
+        set_error("mf_factor: occupancy of the dataflow solve: %s",
+                  oe != cudaSuccess ? cudaGetErrorString(oe) : "no CTA fits on an SM");
+        mf_factor_destroy(M);
+        return V2D_ECUDA;
     }
-    // dataflow solve of the upper levels (opt-in, V2D_LU_FLOW=1): one launch
-    // instead of two per level and sweep above the one-CTA-per-front levels
-    const char *fenv = getenv("V2D_LU_FLOW");
-    if (fenv && fenv[0] == '1' && P->nflow > 0 && P->d_flow && M->coop_grid == 0 &&
-        cudaGetDevice(&dev) == cudaSuccess &&
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess) {
-        int fper = 0;
-        cudaError_t oe = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                                    &fper, k_apply_flow<float>, kSolveThreads2, solve)
-                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                                    &fper, k_apply_flow<double>, kSolveThreads2, solve);
-        if (oe == cudaSuccess && fper > 0 &&
-            cudaMalloc((void **)&M->flow_ctr, (size_t)(4 * P->nfront + 1) * sizeof(int)) ==
-                cudaSuccess)
-            M->flow_grid = std::min(P->nflow, nsm * fper);
-    }
+    M->flow_grid = std::max(1, std::min(P->nitems, nsm * std::min(per_sm, 2)));
     cudaGetLastError();
     *out = M;
     return V2D_OK;
@@ -2105,8 +2025,8 @@ void mf_factor_destroy(MfFactor *M)
 {
     if (!M) return;
     if (M->graph) cudaGraphExecDestroy(M->graph);
-    void *ptrs[] = {M->F,  M->upd,  M->z,    M->tmp,  M->wb, M->rs,
-                    M->ipiv, M->perm, M->flag, M->bar, M->inv_g, M->flow_ctr};
+    void *ptrs[] = {M->F,    M->upd,  M->z,    M->tmp,  M->gh,    M->wb,  M->rs,
+                    M->ipiv, M->perm, M->flag, M->bar, M->inv_g, M->sctr};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     delete M;
@@ -2132,7 +2052,8 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
     long long launches = 0;
     // with ev: an event is recorded after each kernel (kind * 1000 + level;
     // kinds 0 rowscale, 1 scatter, 2 extend_add, 3 first panel, 4 L21 + row
-    // swaps + U12, 6 trailing update + next panel, 7 trinv, 8 trcopy)
+    // swaps + U12, 6 trailing update + next panel, 7 trinv, 8 trcopy, 9 G/H
+    // products, 10 G/H copy)
     int nev = 0;
     auto mark = [&](int code) -> int {
         const cudaError_t le = cudaGetLastError();
@@ -2231,6 +2152,26 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
         }
         V2D_TRY(mark(8000 + L));
         launches += 2;
+        // G = L21 L11^-1, H = U11^-1 U12 (the solve's row products)
+        if (P->lvl_maxm[L] > 0) {
+            const int ts = (P->lvl_maxS[L] + kGemmTile - 1) / kGemmTile;
+            const int tm = (P->lvl_maxm[L] + kGemmTile - 1) / kGemmTile;
+            const long long sm = 2LL * P->lvl_maxS[L] * P->lvl_maxm[L];
+            const int gcg = (int)std::max(1LL, std::min<long long>((sm + 255) / 256, 256));
+            for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
+                k_gh<T><<<dim3(2 * ts * tm, std::min(nq - qb, kMaxFrontsY)), 256, 0, s>>>(
+                    q0 + qb, P->d_S, P->d_f, P->d_foff, P->d_goff, F, (T *)M->gh);
+                if (qb > 0) ++launches;
+            }
+            V2D_TRY(mark(9000 + L));
+            for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
+                k_ghcopy<T><<<dim3(gcg, std::min(nq - qb, kMaxFrontsY)), 256, 0, s>>>(
+                    q0 + qb, P->d_S, P->d_f, P->d_foff, P->d_goff, (const T *)M->gh, F);
+                if (qb > 0) ++launches;
+            }
+            V2D_TRY(mark(10000 + L));
+            launches += 2;
+        }
     }
     V2D_CUDA_TRY(cudaGetLastError());
     if (nev_out) *nev_out = nev;
@@ -2283,8 +2224,7 @@ static int solve_launch(const char *what, int L)
 }
 
 // Launch codes of the solve's kernels for per-launch timing (kind * 1000 + level).
-enum { kCodeFwdFront = 0, kCodeFwdZ = 1, kCodeFwdU = 2, kCodeBwdFront = 3, kCodeBwdY = 4,
-       kCodeBwdX = 5, kCodeFlow = 6 };
+enum { kCodeFwdLevel = 0, kCodeBwdLevel = 1, kCodeFlow = 2 };
 
 template <class T>
 static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, const int *stop_a,
@@ -2307,99 +2247,34 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
     const MfDev D = mf_dev(P, M);
     const T *F = (const T *)M->F;
     T *z = (T *)M->z, *upd = (T *)M->upd;
-    long long launches = 0;
-    if (M->coop_grid > 0) {
-        // the whole solve as one cooperative launch (graph-capturable)
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(M->coop_grid);
-        cfg.blockDim = dim3(kSolveThreads2);
-        cfg.dynamicSmemBytes = (size_t)(P->maxf + P->maxS) * sizeof(T);
-        cfg.stream = s;
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeCooperative;
-        at[0].val.cooperative = 1;
-        cfg.attrs = at;
-        cfg.numAttrs = 1;
-        V2D_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_apply_all<T>, D, F, b, (const double *)M->rs, z,
-                                        upd, x, (const int4 *)P->d_lvl4, P->nlevel, M->bar,
-                                        stop_a, stop_b));
-        if (n_launches) *n_launches = 1;
-        return V2D_OK;
-    }
-    auto chunks = [](int rows) { return std::max(1, (rows + kSolveRows - 1) / kSolveRows); };
+    const SolveItemDev *items = (const SolveItemDev *)P->d_items;
     const size_t smf = (size_t)(P->maxf + P->maxS) * sizeof(T);
-    // levels from Lf up run as one dataflow launch when the factor has one
-    const bool flow = M->flow_grid > 0 && M->flow_ctr && P->nflow > 0;
-    const int Lf = flow ? P->flow_level : P->nlevel;
-    for (int L = 0; L < Lf; ++L) {
-        const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
-        if (nq >= kFrontPerCta) {
-            k_fwd_front<T><<<nq, front_threads(nq), smf, s>>>(q0, D, F, b, M->rs, z, upd, stop_a,
-                                                           stop_b);
-            V2D_TRY(solve_launch("k_fwd_front", L));
-            V2D_TRY(mark(kCodeFwdFront * 1000 + L));
-            ++launches;
-            continue;
-        }
-        for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
-            k_fwd_z<T><<<dim3(chunks(P->lvl_maxS[L]), std::min(nq - qb, kMaxFrontsY)),
-                         kSolveThreads2, smf, s>>>(q0 + qb, D, F, b, M->rs, z, upd, stop_a,
-                                                   stop_b);
-            V2D_TRY(solve_launch("k_fwd_z", L));
-            if (qb > 0) ++launches;
-        }
-        V2D_TRY(mark(kCodeFwdZ * 1000 + L));
-        ++launches;
-        if (P->lvl_maxm[L] > 0) {
-            for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
-                k_fwd_u<T><<<dim3(chunks(P->lvl_maxm[L]), std::min(nq - qb, kMaxFrontsY)),
-                             kSolveThreads2, (size_t)P->maxS * sizeof(T), s>>>(
-                    q0 + qb, D, F, z, upd, stop_a, stop_b);
-                V2D_TRY(solve_launch("k_fwd_u", L));
-                if (qb > 0) ++launches;
-            }
-            V2D_TRY(mark(kCodeFwdU * 1000 + L));
+    long long launches = 0;
+    if (M->flow) {
+        V2D_CUDA_TRY(cudaMemsetAsync(M->sctr, 0, (size_t)(P->nctr + 1) * sizeof(int), s));
+        k_solve_flow<T><<<M->flow_grid, kSolveThreads, smf, s>>>(
+            D, F, b, M->rs, z, upd, x, items, P->nitems, M->sctr, P->nctr, M->bar, stop_a,
+            stop_b);
+        V2D_TRY(solve_launch("k_solve_flow", 0));
+        V2D_TRY(mark(kCodeFlow * 1000));
+        launches = 1;
+    } else {
+        for (int L = 0; L < P->nlevel; ++L) {
+            const int i0 = P->lvl_fwd[L], ni = P->lvl_fwd[L + 1] - i0;
+            k_solve_level<T><<<ni, kSolveThreads, smf, s>>>(D, F, b, M->rs, z, upd, x, items, i0,
+                                                           stop_a, stop_b);
+            V2D_TRY(solve_launch("k_solve_level (forward)", L));
+            V2D_TRY(mark(kCodeFwdLevel * 1000 + L));
             ++launches;
         }
-    }
-    if (flow) {
-        V2D_CUDA_TRY(cudaMemsetAsync(M->flow_ctr, 0, (size_t)(4 * P->nfront + 1) * sizeof(int), s));
-        k_apply_flow<T><<<M->flow_grid, kSolveThreads2, smf, s>>>(
-            D, F, b, M->rs, z, upd, x, (const int4 *)P->d_flow, P->nflow, M->flow_ctr, P->nfront,
-            M->bar, stop_a, stop_b);
-        V2D_TRY(solve_launch("k_apply_flow", Lf));
-        V2D_TRY(mark(kCodeFlow * 1000 + Lf));
-        ++launches;
-    }
-    for (int L = Lf - 1; L >= 0; --L) {
-        const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
-        if (nq >= kFrontPerCta) {
-            k_bwd_front<T><<<nq, front_threads(nq), smf, s>>>(q0, D, F, z, x, stop_a, stop_b);
-            V2D_TRY(solve_launch("k_bwd_front", L));
-            V2D_TRY(mark(kCodeBwdFront * 1000 + L));
-            ++launches;
-            continue;
-        }
-        if (P->lvl_maxm[L] > 0) {
-            for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
-                k_bwd_y<T><<<dim3(chunks(P->lvl_maxS[L]), std::min(nq - qb, kMaxFrontsY)),
-                             kSolveThreads2, (size_t)P->maxf * sizeof(T), s>>>(
-                    q0 + qb, D, F, z, x, stop_a, stop_b);
-                V2D_TRY(solve_launch("k_bwd_y", L));
-                if (qb > 0) ++launches;
-            }
-            V2D_TRY(mark(kCodeBwdY * 1000 + L));
+        for (int L = P->nlevel - 1; L >= 0; --L) {
+            const int i0 = P->lvl_bwd[L + 1], ni = P->lvl_bwd[L] - i0;
+            k_solve_level<T><<<ni, kSolveThreads, smf, s>>>(D, F, b, M->rs, z, upd, x, items, i0,
+                                                           stop_a, stop_b);
+            V2D_TRY(solve_launch("k_solve_level (backward)", L));
+            V2D_TRY(mark(kCodeBwdLevel * 1000 + L));
             ++launches;
         }
-        for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
-            k_bwd_x<T><<<dim3(chunks(P->lvl_maxS[L]), std::min(nq - qb, kMaxFrontsY)),
-                         kSolveThreads2, (size_t)P->maxS * sizeof(T), s>>>(
-                q0 + qb, D, F, z, x, stop_a, stop_b);
-            V2D_TRY(solve_launch("k_bwd_x", L));
-            if (qb > 0) ++launches;
-        }
-        V2D_TRY(mark(kCodeBwdX * 1000 + L));
-        ++launches;
     }
     V2D_CUDA_TRY(cudaGetLastError());
     if (n_launches) *n_launches = ev ? nev : launches;
@@ -2422,15 +2297,15 @@ static int apply_transpose_launches(const MfPlan *P, MfFactor *M, const T *g, T 
 {
     const MfDev D = mf_dev(P, M);
     const T *F = (const T *)M->F;
-    const size_t smf = (size_t)(P->maxf + P->maxS) * sizeof(T);
+    const size_t smf = (size_t)2 * P->maxf * sizeof(T);
     for (int L = 0; L < P->nlevel; ++L) {
         const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
-        k_tup_front<T><<<nq, kSolveThreads2, smf, s>>>(q0, D, F, g, (T *)M->z, (T *)M->upd);
+        k_tup_front<T><<<nq, kSolveThreads, smf, s>>>(q0, D, F, g, (T *)M->z, (T *)M->upd);
     }
     for (int L = P->nlevel - 1; L >= 0; --L) {
         const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
-        k_tdown_front<T><<<nq, kSolveThreads2, smf, s>>>(q0, D, F, M->rs, (const T *)M->z,
-                                                         (T *)M->wb, lam);
+        k_tdown_front<T><<<nq, kSolveThreads, smf, s>>>(q0, D, F, M->rs, (const T *)M->z,
+                                                        (T *)M->wb, lam);
     }
     V2D_CUDA_TRY(cudaGetLastError());
     count_launches(2LL * P->nlevel);
@@ -2492,10 +2367,6 @@ __global__ void k_delay(int us)
 int mf_time_apply_launches(const MfPlan *P, const MfFactor *M, int reps, size_t flush_bytes,
                            cudaStream_t s, double *ms, int *codes, int cap, int *n)
 {
-    if (M->coop_grid > 0) {
-        set_error("LU solve timing: per-launch timing needs the per-level launches");
-        return V2D_EARG;
-    }
     const size_t es = M->fp32 ? sizeof(float) : sizeof(double);
     DevBuf<char> buf;
     V2D_TRY(buf.alloc(2 * P->n * es + flush_bytes + 256, s));
@@ -2571,7 +2442,7 @@ int mf_check_barrier(MfFactor *M, cudaStream_t s)
     V2D_CUDA_TRY(cudaStreamSynchronize(s));
     if (err) {
         V2D_CUDA_TRY(cudaMemsetAsync(M->bar, 0, sizeof(MfBarrier), s));
-        set_error("LU solve: a wait of the persistent or dataflow solve timed out");
+        set_error("LU solve: a dependency wait of the dataflow solve timed out");
         return V2D_ETIMEOUT;
     }
     return V2D_OK;

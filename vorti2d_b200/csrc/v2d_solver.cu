@@ -168,6 +168,7 @@ int ensure_lu(v2d_solver *S)
     }
     const int q = k.precision == V2D_PREC_MIXED ? 1 : 0;
     if (!S->lu[q]) V2D_TRY(mf_factor_create(S->plan, q, &S->lu[q]));
+    S->lu[q]->flow = k.lu_solve == 0 ? 1 : 0;
     return V2D_OK;
 }
 
@@ -207,6 +208,7 @@ extern "C" void v2d_krylov_defaults(v2d_krylov_params *p)
     p->lu_leaf = 64;
     p->lu_reuse_its = 0;
     p->lu_reuse_steps = 0;
+    p->lu_solve = 0;
 }
 
 extern "C" int v2d_solver_destroy(v2d_solver *S)

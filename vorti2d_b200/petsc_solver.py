@@ -1,10 +1,17 @@
 """Linear-solver seam: drop-in for ``vorti2d.petsc_solver.MumpsSolver``
-(vorti2d/petsc_solver.py:37-132), solved by GMRES(m) on the GPU.
+(vorti2d/petsc_solver.py:37-132), solved on the GPU.
 
 Same five methods: ``row_range``, ``assemble``, ``solve``, ``timings``,
 ``destroy``.  One process owns the whole system (r0 = 0, r1 = n); the first
 ``assemble`` fixes the canonical CSR pattern on the device, later calls only
 refresh values (as the reference's preallocated pattern does).
+
+The default preconditioner is "lu": every solve factors the assembled matrix
+with the device multifrontal LU and refines with GMRES to ``rtol``, which is
+what the reference's MUMPS direct solve (petsc_solver.py:55-61) delivers.  The
+LU's ordering needs the O-grid shape: pass ``grid=(imax, jmax)``, or let the
+first ``assemble`` recognise it from the pattern.  "bjacobi" and "none" need
+no grid but converge slowly or not at all on pure-Newton systems.
 """
 from __future__ import annotations
 
@@ -28,9 +35,10 @@ class GpuLinearSolver:
     ordering), 0 point Jacobi.
     """
 
-    def __init__(self, n: int, comm=None, block_layout: int = 1, restart: int = 200,
+    def __init__(self, n: int, comm=None, block_layout: int = 1, restart: int = 30,
                  rtol: float = 1e-10, max_it: int = 5000, precision: str = "fp64",
-                 precond: str = "bjacobi", inner_rtol: float = 1e-5):
+                 precond: str = "lu", inner_rtol: float = 1e-5, grid=None,
+                 lu_reuse_its: int = 0):
         self.comm = comm
         self.n = int(n)
         self.r0, self.r1 = 0, self.n
@@ -40,13 +48,16 @@ class GpuLinearSolver:
         p.rtol = float(rtol)
         p.max_it = int(max_it)
         p.precision = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}[precision]
-        p.precond = {"none": _lib.PC_NONE, "bjacobi": _lib.PC_BJACOBI}[precond]
+        p.precond = {"none": _lib.PC_NONE, "bjacobi": _lib.PC_BJACOBI, "lu": _lib.PC_LU}[precond]
         p.inner_rtol = float(inner_rtol)
+        p.lu_reuse_its = int(lu_reuse_its)
         self._params = p
         h = ctypes.c_void_p()
         check(lib().v2d_linsys_create(self.n, int(block_layout), ctypes.byref(p), ctypes.byref(h)),
               "MumpsSolver")
         self._h = h
+        if grid is not None:
+            check(lib().v2d_linsys_set_grid(h, int(grid[0]), int(grid[1])), "MumpsSolver(grid)")
         self.t_csr = self.t_solve = self.t_gather = 0.0
         self.n_solves = 0
         self.last_stats = None

@@ -44,6 +44,7 @@ def solver_params(cfg: Config) -> _lib.SolverParams:
     k.inner_rtol = float(cfg.inner_rtol)
     k.lu_reuse_its = int(cfg.lu_reuse_its)
     k.lu_reuse_steps = int(bool(cfg.lu_reuse_steps))
+    k.lu_solve = {"flow": 0, "levels": 1}[cfg.lu_solve]
     p.krylov = k
     return p
 
