@@ -627,23 +627,99 @@ def _e2e(torch, v, s, times, k0, K, flush_buf):
 
 
 # ------------------------------------------------------------ CPU arm
-def run_cpu_reference(steps, warmup=0):
-    """CPU restatement of the reference path (C assembly restating
-    vorti2d_core.f90 + SuperLU direct solve standing in for MUMPS),
-    single-threaded like one reference rank: `warmup` untimed steps, then
-    `steps` timed ones."""
+def _oracle_solver():
     from oracle import oracle as O
     xg, yg = O.generate_cylinder(IMAX, JMAX)
-    s = O.OracleSolver(xg, yg, pseudo_tol=SOLVER["pseudo_tol"],
-                       max_pseudo_iter=SOLVER["max_pseudo_iter"], **WORKLOAD)
+    return O, O.OracleSolver(xg, yg, pseudo_tol=SOLVER["pseudo_tol"],
+                             max_pseudo_iter=SOLVER["max_pseudo_iter"], **WORKLOAD)
+
+
+def _cpu_replica(warmup, steps, barrier, queue):
+    """One replica of the CPU restatement: `warmup` untimed steps from t=0,
+    then `steps` timed ones (the same window as the device's timed steps)."""
+    _, s = _oracle_solver()
     times = s.times()
     for m in range(warmup):
         s.advance(times[m])
+    if barrier is not None:
+        barrier.wait()
     t0 = time.perf_counter()
     for m in range(warmup, warmup + steps):
         s.advance(times[m])
     dt = time.perf_counter() - t0
-    return steps / dt, dt, steps
+    if queue is not None:
+        queue.put(dt)
+    return dt
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_cpu_reference(steps, warmup=0, procs=1):
+    """CPU restatement of the reference path (C assembly restating
+    vorti2d_core.f90 + SuperLU direct solves standing in for MUMPS), one
+    single-threaded replica per process like one reference rank each.
+    `procs` replicas (spawned processes, one BLAS thread each) run the same
+    steps at once, timed over the same window; returns (whole-job steps/s,
+    mean steps/s of one replica, slowest replica's seconds)."""
+    if procs <= 1:
+        dt = _cpu_replica(warmup, steps, None, None)
+        return steps / dt, steps / dt, dt
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    barrier, queue = ctx.Barrier(procs), ctx.Queue()
+    saved = {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS",
+                                             "MKL_NUM_THREADS")}
+    for k in saved:
+        os.environ[k] = "1"
+    try:
+        ps = [ctx.Process(target=_cpu_replica, args=(warmup, steps, barrier, queue))
+              for _ in range(procs)]
+        for p in ps:
+            p.start()
+        dts = [queue.get() for _ in ps]
+        for p in ps:
+            p.join()
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    slow = max(dts)
+    return procs * steps / slow, float(np.mean([steps / d for d in dts])), slow
+
+
+def cpu_iterative_sample(warmup):
+    """The reference's iterative CPU solve (gmres_asm) against its direct one
+    on the same system: after `warmup` steps from t=0, the first Newton
+    Jacobian of the next step solved by SuperLU and by GMRES(200) with a
+    threshold ILU (scipy), one core each."""
+    import scipy.sparse.linalg as spla
+    O, s = _oracle_solver()
+    times = s.times()
+    for m in range(warmup):
+        s.advance(times[m])
+    t = times[warmup]
+    ci, cj, cv, nnz, b = s.assemble(O.u_rot(t, s.steady, s.rot_speed, s.rot_until))
+    A = O.canonical_csr(ci[:nnz], cj[:nnz], cv[:nnz], 2 * s.ndof, 2 * s.ndof)
+    t0 = time.perf_counter()
+    x = spla.spsolve(A.tocsc(), b)
+    t_lu = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    _, its, conv, rel = O.gmres_ilu_solve(A, b, rtol=SOLVER["ksp_rtol"])
+    t_it = time.perf_counter() - t0
+    return {"system": f"first Newton Jacobian of step {warmup} (t={t:.1f})",
+            "superlu_s": t_lu,
+            "gmres_ilu": {"s": t_it, "iterations": its, "converged": bool(conv),
+                          "rel_residual": rel,
+                          "solver": "GMRES(200), rtol 1e-10, at most 2000 iterations, "
+                                    "scipy spilu (ILUTP, drop 1e-3, fill 10, diagonal "
+                                    "pivots) standing in for PETSc ASM/ILU(1)"}}
 
 
 def main():
@@ -653,10 +729,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-steps", type=int, default=2,
+                    help="timed steps of the one-core CPU sample in the device arm's line")
+    ap.add_argument("--cpu-procs", type=int, default=128,
+                    help="--impl reference: at most this many CPU replicas (one per core)")
     ap.add_argument("--lu-reuse", type=int, default=12,
                     help="keep LU factors while GMRES needs at most this many iterations "
                          "(0: factor every Newton Jacobian)")
+    ap.add_argument("--lu-factors", default="fp32", choices=["fp32", "fp64"],
+                    help="mixed leg: LU factorization in FP32, or in FP64 rounded to FP32 "
+                         "for the FP32 solve")
     ap.add_argument("--lu-solve", default="flow", choices=["flow", "levels"],
                     help="LU preconditioner solve: one dataflow launch over the front tree "
                          "(flow) or one launch per level and sweep (levels)")
@@ -696,6 +778,7 @@ def main():
                     help="one warm-up step, then one Newton iteration in NVTX range v2d_newton")
     args = ap.parse_args()
     SOLVER["lu_solve"] = args.lu_solve
+    SOLVER["lu_factors"] = args.lu_factors
     rank, world, local_rank = dist_env()
     if args.profile_newton:
         profile_newton(args)
@@ -731,21 +814,30 @@ def main():
         # CPU restatement on rank 0 only; other ranks exit without work
         if rank != 0:
             return
-        # a bounded sample: a CPU step takes seconds, so at most 3 timed and
-        # 1 warm-up step of the workload
-        K = max(1, min(args.steps, 3))
-        W = min(args.warmup, 1)
-        val, dt, n = run_cpu_reference(K, W)
+        # the device arm's window (W untimed steps from t=0, then K timed
+        # ones), on one replica per host core; a CPU step takes seconds, so K
+        # is capped to keep the run within a few minutes
+        K = max(1, min(args.steps, 20))
+        W = args.warmup
+        P = max(1, min(host_cores(), args.cpu_procs))
+        val, per_rep, dt = run_cpu_reference(K, W, P)
+        it_sample = cpu_iterative_sample(W)
         line = {
             "metric": METRIC, "value": val, "unit": "steps/s", "n_gpus": args.gpus,
-            "steps": n, "warmup": W, "ms_per_step": 1e3 * dt / n, "higher_is_better": True,
+            "steps": K, "warmup": W, "ms_per_step": 1e3 * dt / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": WORKLOAD_NAME,
-                       "solver": "C restatement of vorti2d_core.f90 + scipy SuperLU (MUMPS stand-in)"},
-            "cpu_baseline": {"value": val, "unit": "steps/s", "cores": 1, "kind": "port",
-                             "sample": f"{n} BDF2 steps after {W} warm-up step(s) from t=0 "
-                                       "(bounded sample)"},
+                       "solver": "C restatement of vorti2d_core.f90 + scipy SuperLU "
+                                 "(MUMPS stand-in), one replica per core",
+                       "replicas": P},
+            "cpu_baseline": {"value": val, "unit": "steps/s", "cores": P, "kind": "port",
+                             "sample": f"steps {W}..{W + K - 1} (t={0.2 * W:.1f}..."
+                                       f"{0.2 * (W + K - 1):.1f}) of the workload, the "
+                                       f"device arm's timed window, on {P} independent "
+                                       "replicas at once (whole-job steps/s)",
+                             "per_replica_steps_per_s": per_rep,
+                             "linear_solve_sample": it_sample},
             "e2e": {"value": val, "unit": "steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
         }
@@ -761,9 +853,12 @@ def main():
         return
     cpu = None
     if world == 1 and args.cpu_steps > 0:
-        cval, cdt, cn = run_cpu_reference(args.cpu_steps)
+        W = args.warmup
+        cval, _, _ = run_cpu_reference(args.cpu_steps, W, 1)
         cpu = {"value": cval, "unit": "steps/s", "cores": 1, "kind": "port",
-               "sample": f"{cn} BDF2 steps from t=0 of the same workload (C assembly + SuperLU)"}
+               "sample": f"steps {W}..{W + args.cpu_steps - 1} of the same workload (the "
+                         "first of the device's timed steps; C assembly + SuperLU, one core); "
+                         "bench.py --impl reference runs the whole window on every core"}
     nnz = res["nnz"]
     n = 2 * IMAX * JMAX
     prec_key = "fp32" if head == "mixed" else "fp64"
@@ -784,7 +879,9 @@ def main():
         "dtype": "f32-krylov/f64" if head == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD_NAME,
                    "precision": head, "newton_max": 5,
-                   "krylov": "GMRES(30), multifrontal LU preconditioner (FP32 factors in mixed)",
+                   "krylov": "GMRES(30), multifrontal LU preconditioner (mixed: "
+                             + ("FP32 factors" if args.lu_factors == "fp32"
+                                else "FP64 factors rounded to FP32") + ")",
                    "lu_reuse_its": args.lu_reuse, "lu_reuse_steps": args.lu_reuse_steps,
                    "lu_solve": {"flow": "one dataflow launch", "levels": "one launch per level and sweep"}[args.lu_solve],
                    "l2": "flushed (256 MiB write) before every timed step",

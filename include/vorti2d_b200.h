@@ -192,6 +192,9 @@ typedef struct {
     int lu_solve;         /* LU: 0 the preconditioner solve is one dataflow
                              launch over the whole front tree (default);
                              1 one launch per tree level and sweep          */
+    int lu_factor64;      /* LU in the mixed form: 0 factors in FP32 (0);
+                             1 factors in FP64 and rounds them to FP32 for
+                             the FP32 solve (better pivots, same solve bytes)*/
 } v2d_krylov_params;
 
 void v2d_krylov_defaults(v2d_krylov_params *p);
@@ -328,6 +331,21 @@ int v2d_solver_shape_gradient(v2d_solver *s, const double *nx, const double *ny,
                               double invdtau, double inv2dt, double urot, double ca, double sa,
                               double ref_length, double x0, double y0, double *dots,
                               double *forces);
+/* Exact mesh sensitivities for shape gradients (no reference counterpart):
+ * the same directions as v2d_solver_shape_gradient (grid line i, and the seam
+ * line with i = 0, moved by (nx[i], ny[i]) phi[.]), differentiated by
+ * forward-mode (tangent) derivatives through the metric computation
+ * (vorti2d_core.f90:66-189), the residual rows (:219-381) and the wall force
+ * integrals (vorti2d/forces.py:82-194) on the device -- no step size, no
+ * displaced meshes.  dots[i] = lambda . db/dd_i (b = -R at the handle's state
+ * with the given scalar parameters), dforces[10 i + c] = d(force value c)/dd_i
+ * in the order of v2d_force_coeffs (ref_length <= 0: from the wall).
+ * Host arrays: nx, ny (P = imax-1), phi (N), lambda (2N), dots (P),
+ * dforces (10 P). */
+int v2d_solver_shape_tangent(v2d_solver *s, const double *nx, const double *ny,
+                             const double *phi, const double *lambda, double re, double invdtau,
+                             double inv2dt, double urot, double ca, double sa, double ref_length,
+                             double x0, double y0, double *dots, double *dforces);
 /* Current system (after the last assembly): canonical CSR of the 2N system
  * and its right-hand side.  Sizes: 2N+1, nnz, nnz, 2N. */
 int v2d_solver_nnz(const v2d_solver *s, long long *nnz);

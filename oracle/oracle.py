@@ -299,6 +299,32 @@ def canonical_csr(ci, cj, cv, nrows, ncols):
                          shape=(nrows, ncols))
 
 
+def gmres_ilu_solve(A, b, rtol=1e-10, restart=200, max_it=2000, drop_tol=1e-3, fill_factor=10.0):
+    """Stand-in for the reference's iterative CPU solve ``gmres_asm``
+    (vorti2d/dist_solver.py:138-158: GMRES(ksp_restart = 200), rtol, at most
+    2000 iterations, ASM with ILU(1) subdomain solves -- on one rank the ASM
+    subdomain is the whole matrix).  scipy has no level-of-fill ILU, so the
+    preconditioner is scipy's threshold ILU (spilu, SuperLU's ILUTP) with the
+    given drop tolerance and fill factor and the diagonal as pivot (with
+    partial pivoting the incomplete factors of these systems hit exact zero
+    pivots).  Returns (x, iterations, converged, relative residual)."""
+    import scipy.sparse.linalg as spla
+    Ac = A.tocsc()
+    ilu = spla.spilu(Ac, drop_tol=drop_tol, fill_factor=fill_factor, diag_pivot_thresh=0.0)
+    M = spla.LinearOperator(A.shape, ilu.solve)
+    count = [0]
+
+    def cb(_):
+        count[0] += 1
+
+    x, info = spla.gmres(A, b, M=M, rtol=rtol, atol=0.0, restart=restart,
+                         maxiter=max(1, -(-max_it // restart)), callback=cb,
+                         callback_type="pr_norm")
+    bn = float(np.linalg.norm(b))
+    rel = float(np.linalg.norm(A @ x - b) / bn) if bn > 0 else 0.0
+    return x, count[0], info == 0, rel
+
+
 class OracleSolver:
     """Replicated-path driver restated from vorti2d/solver.py:48-224 (one
     process; MUMPS replaced by scipy SuperLU).  The state arrays and the

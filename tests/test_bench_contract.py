@@ -1,6 +1,8 @@
 """The reference arm of bench.py on the CPU: one JSON line on the same
 metric, unit and workload as the GPU arm, with the keys the benchmark
-contract asks for (a bounded sample of the CPU restatement)."""
+contract asks for: the CPU restatement on the device arm's step window, one
+replica per core (two here), and the direct-vs-iterative linear solve
+sample."""
 import json
 import os
 import subprocess
@@ -19,7 +21,8 @@ def test_reference_arm_prints_one_contract_line():
     sys.path.insert(0, ROOT)
     import bench
     p = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1",
-                        "--warmup", "3"], cwd=ROOT, capture_output=True, text=True, timeout=300)
+                        "--warmup", "1", "--cpu-procs", "2"], cwd=ROOT, capture_output=True,
+                       text=True, timeout=600)
     assert p.returncode == 0, p.stderr[-2000:]
     d = _last_json(p.stdout)
     assert d["impl"] == "reference"
@@ -28,8 +31,12 @@ def test_reference_arm_prints_one_contract_line():
     assert d["config"]["workload"] == bench.WORKLOAD_NAME
     assert d["value"] > 0 and d["steps"] == 1 and d["warmup"] == 1
     cb = d["cpu_baseline"]
-    assert cb["kind"] == "port" and cb["cores"] == 1 and cb["value"] == d["value"]
-    assert cb["sample"]
+    cores = min(2, len(os.sched_getaffinity(0)))
+    assert cb["kind"] == "port" and cb["cores"] == cores and cb["value"] == d["value"]
+    assert d["config"]["replicas"] == cores and cb["sample"]
+    assert 0 < cb["per_replica_steps_per_s"] <= d["value"]
+    ls = cb["linear_solve_sample"]
+    assert ls["superlu_s"] > 0 and ls["gmres_ilu"]["iterations"] > 0
     e = d["e2e"]
     assert e["value"] == d["value"] and e["unit"] == d["unit"]
     assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0

@@ -226,7 +226,7 @@ def test_device_shape_gradient_equals_host_route(v2d, oracle_mod):
     s.advance(0.0)
     w = (0.3, 1.0, -0.2)
     h = 1e-6
-    dev, _ = shape_vjp(s, w, base, h=h)
+    dev, _ = shape_vjp(s, w, base, h=h, method="fd")
     nx, ny = wall_normals(*base)
     phi = deformation_weights(*base)
     grads = force_gradients(s.imax, s.jmax, RE, s.dksi, s.deta, s.beta, s.gama, s.detadx,
@@ -249,4 +249,32 @@ def test_device_shape_gradient_equals_host_route(v2d, oracle_mod):
             vals.append(_wall_forces(s, met, ome3, w))
         host = (vals[0] - vals[1]) / (2 * h) + float(lam @ (bs[0] - bs[1])) / (2 * h)
         assert abs(dev[i] - host) <= 1e-8 * max(1.0, abs(host)), (i, dev[i], host)
+    s.close()
+
+
+@pytest.mark.parametrize("kind,im,jm,re,adeg,ref_length", SHAPE_CASES)
+def test_shape_tangent_equals_extrapolated_differences(v2d, oracle_mod, kind, im, jm, re, adeg,
+                                                       ref_length):
+    """The exact tangent shape gradient (dual numbers through metrics,
+    residual and wall integrals) against the displaced-mesh central
+    differences extrapolated in the step (Richardson, h and h/2: error
+    O(h^4)), for every wall node at once, within 1e-7 relative to the
+    gradient's largest component."""
+    from vorti2d_b200.adjoint import deform_ogrid, gaussian_bumps, shape_vjp
+    base = _base_mesh(v2d, oracle_mod, kind, im, jm)
+    P = im - 1
+    d0 = gaussian_bumps(P, n_bumps=4, amplitude=1e-3, seed=3)
+    s = _shape_solve(v2d, base, d0, re, adeg, ref_length)
+    w = (0.7, 1.0, -0.4)
+    tan, info = shape_vjp(s, w, base)
+    assert info["method"] == "tangent"
+    h = 1e-4 * max(np.ptp(base[0][:P, 0]), np.ptp(base[1][:P, 0]))
+    f1, _ = shape_vjp(s, w, base, h=h, method="fd")
+    f2, _ = shape_vjp(s, w, base, h=h / 2, method="fd")
+    rich = (4.0 * f2 - f1) / 3.0
+    scale = np.abs(tan).max()
+    err = np.abs(tan - rich).max() / scale
+    print(f"{kind}: tangent vs extrapolated differences, max rel {err:.2e} "
+          f"(plain h={h:.1e}: {np.abs(tan - f1).max() / scale:.2e})")
+    assert err <= 1e-7, err
     s.close()

@@ -39,7 +39,7 @@ class KrylovParams(ctypes.Structure):
     _fields_ = [("restart", _i), ("max_it", _i), ("rtol", _d), ("atol", _d),
                 ("precond", _i), ("precision", _i), ("inner_rtol", _d), ("dc_max_it", _i),
                 ("lu_leaf", _i), ("lu_reuse_its", _i), ("lu_reuse_steps", _i),
-                ("lu_solve", _i)]
+                ("lu_solve", _i), ("lu_factor64", _i)]
 
 
 class LinStats(ctypes.Structure):
@@ -117,6 +117,8 @@ _SIGS = {
     "v2d_solver_time_lu_launches": (_i, [_vp, _i, _ll, _dp, _ip, _i, _ip]),
     "v2d_solver_time_lu_factor": (_i, [_vp, _i, _dp, _ip, _i, _ip]),
     "v2d_solver_residual_mesh": (_i, [_vp, _dp, _dp, _d, _d, _d, _d, _d, _d, _dp, _i, _dp]),
+    "v2d_solver_shape_tangent": (_i, [_vp, _dp, _dp, _dp, _dp, _d, _d, _d, _d, _d, _d, _d, _d,
+                                      _d, _dp, _dp]),
     "v2d_solver_shape_gradient": (_i, [_vp, _dp, _dp, _dp, _dp, _d, _d, _d, _d, _d, _d, _d, _d,
                                        _d, _d, _dp, _dp]),
     "v2d_solver_time_lu_apply": (_i, [_vp, _i, _ll, _dp, ctypes.POINTER(_ll)]),

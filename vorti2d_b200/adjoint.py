@@ -24,10 +24,13 @@ C(q; p) has
 * Shape: the P = imax-1 distinct wall nodes move along their outward normals
   by d_i, and each grid line follows with a weight that decays from 1 at the
   wall to 0 at the far field (``deform_ogrid``; linear in d).  dR/dd_i and
-  dC/dd_i|_q are central differences of the residual and of the force
-  integrals on the displaced meshes at the fixed converged state, all
-  evaluated on the device (``v2d_solver_shape_gradient``); the one adjoint
-  solve is shared by all P components.
+  dC/dd_i|_q are forward-mode (tangent) derivatives through the metric
+  computation, the residual rows and the wall force integrals on the device
+  (``v2d_solver_shape_tangent``: dual numbers, one CTA per direction, only
+  the four grid lines a direction touches): exact, with no step size.  The
+  one adjoint solve is shared by all P components.  Central differences on
+  displaced meshes (``v2d_solver_shape_gradient``) remain available as a
+  check (``method="fd"``).
 """
 from __future__ import annotations
 
@@ -224,21 +227,24 @@ def _wall_forces(solver, met3, ome3, weights):
     return w_cl * fc.cl + w_cd * fc.cd + w_cm * fc.cm
 
 
-def shape_vjp(solver, weights, base_mesh, h=None):
+def shape_vjp(solver, weights, base_mesh, h=None, method="tangent"):
     """d(w . (Cl, Cd, Cm))/d(d_i), i < P, at the solver's converged steady
     state, for wall displacements d along the normals of ``base_mesh`` (the
     undeformed (xg, yg) that ``deform_ogrid`` displaced to the solver's
-    mesh).  Central differences of step h (default 1e-6 of the wall's
-    extent) on the residual and the force integrals, all 2P displaced meshes
-    evaluated on the device (``v2d_solver_shape_gradient``), one adjoint
-    solve."""
+    mesh), with one adjoint solve.  method "tangent": exact tangent
+    derivatives of the residual and the force integrals on the device
+    (``v2d_solver_shape_tangent``); "fd": central differences of step h
+    (default 1e-6 of the wall's extent) on the 2P displaced meshes
+    (``v2d_solver_shape_gradient``)."""
+    if method not in ("tangent", "fd"):
+        raise ValueError(f"unknown method {method!r}")
     xg0, yg0 = (np.asarray(a, dtype=np.float64) for a in base_mesh)
     nx, ny = wall_normals(xg0, yg0)
     phi = np.asfortranarray(deformation_weights(xg0, yg0))
     X = np.asarray(solver.xg, dtype=np.float64)
     Y = np.asarray(solver.yg, dtype=np.float64)
     P = solver.imax - 1
-    if h is None:
+    if h is None and method == "fd":
         h = 1e-6 * max(np.ptp(X[:P, 0]), np.ptp(Y[:P, 0]))
     cfg = solver.cfg
     grads = force_gradients(solver.imax, solver.jmax, float(cfg.re), solver.dksi, solver.deta,
@@ -252,10 +258,21 @@ def shape_vjp(solver, weights, base_mesh, h=None):
     nx = np.ascontiguousarray(nx)
     ny = np.ascontiguousarray(ny)
     dots = np.empty(P)
-    forces = np.empty((P, 2, 10))
     a = math.radians(cfg.alpha_deg)
     rl = -1.0 if cfg.ref_length is None else float(cfg.ref_length)
     mc = cfg.moment_center
+    if method == "tangent":
+        dforces = np.empty((P, 10))
+        check(lib().v2d_solver_shape_tangent(solver.dev.h, dptr(nx), dptr(ny), dptr(phi),
+                                             dptr(lam), float(cfg.re), cfg.inv_dtau(),
+                                             cfg.inv_2dt(), float(cfg.u_rot(solver.t)),
+                                             math.cos(a), math.sin(a), rl, float(mc[0]),
+                                             float(mc[1]), dptr(dots), dptr(dforces)),
+              "shape_tangent")
+        # v2d_force_coeffs order: cd, cl, cm, ...
+        dc = w_cd * dforces[:, 0] + w_cl * dforces[:, 1] + w_cm * dforces[:, 2]
+        return dc + dots, dict(refinements=its, rel_res=rel, method="tangent")
+    forces = np.empty((P, 2, 10))
     check(lib().v2d_solver_shape_gradient(solver.dev.h, dptr(nx), dptr(ny), dptr(phi), dptr(lam),
                                           float(h), float(cfg.re), cfg.inv_dtau(), cfg.inv_2dt(),
                                           float(cfg.u_rot(solver.t)), math.cos(a), math.sin(a),
@@ -265,7 +282,7 @@ def shape_vjp(solver, weights, base_mesh, h=None):
     # v2d_force_coeffs order: cd, cl, cm, ...
     c = w_cd * forces[:, :, 0] + w_cl * forces[:, :, 1] + w_cm * forces[:, :, 2]
     out = (c[:, 0] - c[:, 1]) / (2.0 * h) + dots / (2.0 * h)
-    return out, dict(refinements=its, rel_res=rel, h=h)
+    return out, dict(refinements=its, rel_res=rel, h=h, method="fd")
 
 
 def _torch():

@@ -81,6 +81,11 @@ class Config:
     """LU preconditioner with ``lu_reuse_its > 0``: keep the factors across
     time steps and ``set_state`` too (the same iteration rule decides when to
     refactor)."""
+    lu_factors: str = "fp32"
+    """LU preconditioner in the mixed form: ``"fp32"`` factors in FP32;
+    ``"fp64"`` factors in FP64 and rounds the factors to FP32 for the FP32
+    solve (more accurate pivots and updates, the same bytes per solve).  The
+    FP64 form always factors in FP64."""
     lu_solve: str = "flow"
     """LU preconditioner solve: ``"flow"`` runs each application as one
     dataflow launch over the whole front tree; ``"levels"`` as one launch per

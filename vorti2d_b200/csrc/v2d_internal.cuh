@@ -43,6 +43,14 @@ int launch_velocity(int imax, int jmax, double dksi, double deta, const double *
                     const double *detady, const double *psi, double *u, double *v, double *vmag,
                     cudaStream_t s);
 
+// v2d_shape.cu: tangent derivatives along the P wall-normal displacement
+// directions (grid line i moved by (nx[i], ny[i]) * phi): dots[i] =
+// lambda . db/dd_i and dforces[10 i + c] = d(force value c)/dd_i.  phi, nx, ny,
+// lam, dots, dforces are device arrays.
+int launch_shape_tangent(const GridDev &g, const AsmParams &p, const double *phi,
+                         const double *nx, const double *ny, const double *lam, double ref_length,
+                         double x0, double y0, double *dots, double *dforces, cudaStream_t s);
+
 // v2d_forces.cu
 int launch_forces(const GridDev &g, double re, double ref_length, double x0, double y0,
                   double *d_out10, cudaStream_t s);
@@ -94,8 +102,11 @@ struct MfBarrier {
 
 // Numeric factors of one plan in one precision.
 struct MfFactor {
-    int fp32 = 0;
+    int fp32 = 0;               // precision of the solve (Krylov vectors, applied factors)
+    int fact64 = 0;             // with fp32: the factorization runs in FP64 and the factors
+                                // are rounded to FP32 for the solve (F32)
     void *F = nullptr, *upd = nullptr, *z = nullptr;
+    void *F32 = nullptr;        // fact64: FP32 copy of F that the solve reads
     void *tmp = nullptr;        // triangular inverses of one level before they replace L11 / U11
     void *gh = nullptr;         // G = L21 L11^-1 and H = U11^-1 U12 of one level before they
                                 // replace L21 / U12
@@ -130,7 +141,8 @@ int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_c
 int mf_plan_create(int imax, int jmax, int n, const int *h_rowptr, const int *h_colind, int leaf,
                    MfPlan **out);
 void mf_plan_destroy(MfPlan *p);
-int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out);
+// fp32: FP32 solve; fact64 (with fp32): FP64 factorization rounded to FP32.
+int mf_factor_create(const MfPlan *P, int fp32, int fact64, MfFactor **out);
 void mf_factor_destroy(MfFactor *M);
 MfDev mf_dev(const MfPlan *P, const MfFactor *M);
 // Factor the CSR values (FP64, row-scaled and rounded to the factor's precision).

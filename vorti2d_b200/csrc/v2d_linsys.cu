@@ -272,7 +272,8 @@ static int setup_lu(v2d_linsys *L)
     if (!L->imax) V2D_TRY(infer_grid(L->n, rp, ci, &L->imax, &L->jmax));
     const int leaf = L->prm.lu_leaf > 0 ? L->prm.lu_leaf : 64;
     V2D_TRY(mf_plan_create(L->imax, L->jmax, L->n, rp.data(), ci.data(), leaf, &L->plan));
-    V2D_TRY(mf_factor_create(L->plan, L->prm.precision == V2D_PREC_MIXED ? 1 : 0, &L->lu));
+    V2D_TRY(mf_factor_create(L->plan, L->prm.precision == V2D_PREC_MIXED ? 1 : 0,
+                             L->prm.lu_factor64, &L->lu));
     L->lu->flow = L->prm.lu_solve == 0 ? 1 : 0;
     return V2D_OK;
 }

@@ -1274,6 +1274,13 @@ __global__ void k_trcopy(int q0, const int *__restrict__ S_, const int *__restri
     }
 }
 
+// FP64 factors rounded to FP32 (the solve of the mixed form with FP64
+// factorization).
+__global__ void k_round_f32(const double *__restrict__ a, float *__restrict__ b, long long n)
+{
+    V2D_GRID_STRIDE(i, n) { b[i] = (float)a[i]; }
+}
+
 // G = L21 L11^-1 (rows [S, f) x columns [0, S)) and H = U11^-1 U12 (rows
 // [0, S) x columns [S, f)) of every front of a level, from the inverted pivot
 // block, into the level's scratch (G row-major m x S, then H S x m; copied over
@@ -1911,21 +1918,24 @@ static cudaError_t raise_dyn_smem(const void *fn, size_t bytes)
     return e;
 }
 
-int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
+int mf_factor_create(const MfPlan *P, int fp32, int fact64, MfFactor **out)
 {
     *out = nullptr;
     MfFactor *M = new MfFactor();
     M->fp32 = fp32;
-    const size_t es = fp32 ? sizeof(float) : sizeof(double);
+    M->fact64 = fp32 && fact64 ? 1 : 0;
+    const size_t es = fp32 ? sizeof(float) : sizeof(double);          // solve
+    const size_t esf = fp32 && !M->fact64 ? sizeof(float) : sizeof(double);   // factorization
     cudaError_t e = cudaSuccess;
     auto grab = [&](void **p, size_t bytes) {
         if (e == cudaSuccess) e = cudaMalloc(p, std::max<size_t>(bytes, 16));
     };
-    grab(&M->F, (size_t)P->ftotal * es);
+    grab(&M->F, (size_t)P->ftotal * esf);
+    if (M->fact64) grab(&M->F32, (size_t)P->ftotal * sizeof(float));
     grab(&M->upd, (size_t)P->utotal * es);
     grab(&M->z, (size_t)P->vtotal * es);
-    grab(&M->tmp, (size_t)P->tmax * es);
-    grab(&M->gh, (size_t)P->gmax * es);
+    grab(&M->tmp, (size_t)P->tmax * esf);
+    grab(&M->gh, (size_t)P->gmax * esf);
     grab((void **)&M->sctr, (size_t)(P->nctr + 1) * sizeof(int));
     grab(&M->wb, (size_t)P->vtotal * es);
     grab((void **)&M->rs, (size_t)P->n * sizeof(double));
@@ -1936,21 +1946,21 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
     if (e == cudaSuccess) e = cudaMemset(M->bar, 0, sizeof(MfBarrier));
     if (e != cudaSuccess) {
         set_error("mf_factor: allocation of %.1f MB failed: %s",
-                  ((double)P->ftotal * es) / 1e6, cudaGetErrorString(e));
+                  ((double)P->ftotal * (esf + (M->fact64 ? 4 : 0))) / 1e6, cudaGetErrorString(e));
         mf_factor_destroy(M);
         return V2D_ENOMEM;
     }
     // dynamic shared memory of the solve and inversion kernels (set once,
     // outside any stream capture)
     const size_t solve = (size_t)(P->maxf + P->maxS) * es;
-    const int cw = fp32 ? InvWidth<float>::v : InvWidth<double>::v;
+    const int cw = esf == sizeof(float) ? InvWidth<float>::v : InvWidth<double>::v;
     // shared-memory inversion where its column block fits, the global work
     // space elsewhere (sized for the largest such level)
     size_t inv = 0, inv_g = 0;
     for (int L = 0; L < P->nlevel; ++L) {
         const size_t sl = (size_t)P->lvl_maxS[L] * (cw + 33);
-        if (sl * es <= kInvSmemMax) {
-            inv = std::max(inv, sl * es);
+        if (sl * esf <= kInvSmemMax) {
+            inv = std::max(inv, sl * esf);
         } else {
             const size_t nbc = (P->lvl_maxS[L] + cw - 1) / cw;
             inv_g = std::max(inv_g, nbc * (size_t)(P->lvl_off[L + 1] - P->lvl_off[L]) * sl);
@@ -1963,9 +1973,9 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
         return V2D_EARG;
     }
     if (inv_g > 0) {
-        cudaError_t ge = cudaMalloc(&M->inv_g, inv_g * es);
+        cudaError_t ge = cudaMalloc(&M->inv_g, inv_g * esf);
         if (ge != cudaSuccess) {
-            set_error("mf_factor: inversion work space of %.1f MB: %s", inv_g * es / 1e6,
+            set_error("mf_factor: inversion work space of %.1f MB: %s", inv_g * esf / 1e6,
                       cudaGetErrorString(ge));
             mf_factor_destroy(M);
             return V2D_ENOMEM;
@@ -1986,14 +1996,14 @@ int mf_factor_create(const MfPlan *P, int fp32, MfFactor **out)
         attr((const void *)k_solve_flow<float>, solve);
         attr((const void *)k_tup_front<float>, tsolve);
         attr((const void *)k_tdown_front<float>, tsolve);
-        attr((const void *)k_trinv<float>, inv);
     } else {
         attr((const void *)k_solve_level<double>, solve);
         attr((const void *)k_solve_flow<double>, solve);
         attr((const void *)k_tup_front<double>, tsolve);
         attr((const void *)k_tdown_front<double>, tsolve);
-        attr((const void *)k_trinv<double>, inv);
     }
+    if (esf == sizeof(float)) attr((const void *)k_trinv<float>, inv);
+    else attr((const void *)k_trinv<double>, inv);
     if (e != cudaSuccess) {
         set_error("mf_factor: %s", cudaGetErrorString(e));
         mf_factor_destroy(M);
@@ -2025,8 +2035,8 @@ void mf_factor_destroy(MfFactor *M)
 {
     if (!M) return;
     if (M->graph) cudaGraphExecDestroy(M->graph);
-    void *ptrs[] = {M->F,    M->upd,  M->z,    M->tmp,  M->gh,    M->wb,  M->rs,
-                    M->ipiv, M->perm, M->flag, M->bar, M->inv_g, M->sctr};
+    void *ptrs[] = {M->F,    M->F32,  M->upd,  M->z,    M->tmp,  M->gh,    M->wb,
+                    M->rs,   M->ipiv, M->perm, M->flag, M->bar, M->inv_g, M->sctr};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     delete M;
@@ -2173,6 +2183,12 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
             launches += 2;
         }
     }
+    if (M->fact64) {   // FP64 factors rounded to FP32 for the solve
+        k_round_f32<<<grid_for(P->ftotal, 256), 256, 0, s>>>((const double *)M->F,
+                                                             (float *)M->F32, P->ftotal);
+        V2D_TRY(mark(11000));
+        ++launches;
+    }
     V2D_CUDA_TRY(cudaGetLastError());
     if (nev_out) *nev_out = nev;
     if (!ev) M->launches_per_factor = launches;
@@ -2186,8 +2202,8 @@ int mf_factor(const MfPlan *P, MfFactor *M, const int *rowptr, const double *val
         M->graph = nullptr;
         cudaGraph_t g = nullptr;
         V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        int st = M->fp32 ? factor_launches<float>(P, M, rowptr, val, s)
-                         : factor_launches<double>(P, M, rowptr, val, s);
+        int st = M->fp32 && !M->fact64 ? factor_launches<float>(P, M, rowptr, val, s)
+                                       : factor_launches<double>(P, M, rowptr, val, s);
         cudaError_t e = cudaStreamEndCapture(s, &g);
         if (st != V2D_OK) {
             if (g) cudaGraphDestroy(g);
@@ -2245,7 +2261,7 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
         return V2D_OK;
     };
     const MfDev D = mf_dev(P, M);
-    const T *F = (const T *)M->F;
+    const T *F = (const T *)(M->fact64 ? M->F32 : M->F);
     T *z = (T *)M->z, *upd = (T *)M->upd;
     const SolveItemDev *items = (const SolveItemDev *)P->d_items;
     const size_t smf = (size_t)(P->maxf + P->maxS) * sizeof(T);
@@ -2296,7 +2312,7 @@ static int apply_transpose_launches(const MfPlan *P, MfFactor *M, const T *g, T 
                                     cudaStream_t s)
 {
     const MfDev D = mf_dev(P, M);
-    const T *F = (const T *)M->F;
+    const T *F = (const T *)(M->fact64 ? M->F32 : M->F);
     const size_t smf = (size_t)2 * P->maxf * sizeof(T);
     for (int L = 0; L < P->nlevel; ++L) {
         const int q0 = P->lvl_off[L], nq = P->lvl_off[L + 1] - q0;
@@ -2416,9 +2432,9 @@ int mf_time_factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, con
     for (int r = 0; r < reps && st == V2D_OK; ++r) {
         k_delay<<<1, 32, 0, s>>>(2000);
         cudaEventRecord(ev[0], s);
-        st = M->fp32 ? factor_launches<float>(P, M, rowptr, val, s, ev.data() + 1, codes, cap, &nl)
-                     : factor_launches<double>(P, M, rowptr, val, s, ev.data() + 1, codes, cap,
-                                               &nl);
+        st = M->fp32 && !M->fact64
+                 ? factor_launches<float>(P, M, rowptr, val, s, ev.data() + 1, codes, cap, &nl)
+                 : factor_launches<double>(P, M, rowptr, val, s, ev.data() + 1, codes, cap, &nl);
         if (st == V2D_OK && cudaEventSynchronize(ev[nl]) != cudaSuccess) st = V2D_ECUDA;
         for (int k = 0; k < nl && st == V2D_OK; ++k) {
             float t = 0.f;

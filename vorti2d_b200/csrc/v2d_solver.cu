@@ -167,7 +167,13 @@ int ensure_lu(v2d_solver *S)
         S->plan_leaf = leaf;
     }
     const int q = k.precision == V2D_PREC_MIXED ? 1 : 0;
-    if (!S->lu[q]) V2D_TRY(mf_factor_create(S->plan, q, &S->lu[q]));
+    const int f64 = q && k.lu_factor64 ? 1 : 0;
+    if (S->lu[q] && S->lu[q]->fact64 != f64) {   // the factorization precision changed
+        mf_factor_destroy(S->lu[q]);
+        S->lu[q] = nullptr;
+        S->lu_valid = false;
+    }
+    if (!S->lu[q]) V2D_TRY(mf_factor_create(S->plan, q, f64, &S->lu[q]));
     S->lu[q]->flow = k.lu_solve == 0 ? 1 : 0;
     return V2D_OK;
 }
@@ -209,6 +215,7 @@ extern "C" void v2d_krylov_defaults(v2d_krylov_params *p)
     p->lu_reuse_its = 0;
     p->lu_reuse_steps = 0;
     p->lu_solve = 0;
+    p->lu_factor64 = 0;
 }
 
 extern "C" int v2d_solver_destroy(v2d_solver *S)
@@ -732,6 +739,36 @@ extern "C" int v2d_solver_shape_gradient(v2d_solver *S, const double *nx, const 
     return V2D_OK;
 }
 
+extern "C" int v2d_solver_shape_tangent(v2d_solver *S, const double *nx, const double *ny,
+                                        const double *phi, const double *lambda, double re,
+                                        double invdtau, double inv2dt, double urot, double ca,
+                                        double sa, double ref_length, double x0, double y0,
+                                        double *dots, double *dforces)
+{
+    V2D_ARG_CHECK(S && nx && ny && phi && lambda && dots && dforces,
+                  "solver_shape_tangent: null pointer");
+    V2D_ARG_CHECK(re > 0.0, "solver_shape_tangent: re must be positive");
+    const GridDev &g = S->g;
+    const int P = g.imax - 1;
+    const size_t N = (size_t)g.N, n = (size_t)g.n;
+    DevBuf<double> buf;
+    V2D_TRY(buf.alloc(N + n + 2 * (size_t)P + (size_t)P * 11, S->s));
+    double *dphi = buf.p, *dlam = dphi + N, *dnx = dlam + n, *dny = dnx + P, *ddot = dny + P;
+    double *dfor = ddot + P;
+    V2D_CUDA_TRY(cudaMemcpyAsync(dphi, phi, N * sizeof(double), cudaMemcpyHostToDevice, S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(dlam, lambda, n * sizeof(double), cudaMemcpyHostToDevice, S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(dnx, nx, P * sizeof(double), cudaMemcpyHostToDevice, S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(dny, ny, P * sizeof(double), cudaMemcpyHostToDevice, S->s));
+    AsmParams ap{re, invdtau, inv2dt, urot, ca, sa, S->prm.ff_bc};
+    V2D_TRY(launch_shape_tangent(g, ap, dphi, dnx, dny, dlam, ref_length, x0, y0, ddot, dfor,
+                                 S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(dots, ddot, P * sizeof(double), cudaMemcpyDeviceToHost, S->s));
+    V2D_CUDA_TRY(cudaMemcpyAsync(dforces, dfor, (size_t)P * 10 * sizeof(double),
+                                 cudaMemcpyDeviceToHost, S->s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    return V2D_OK;
+}
+
 extern "C" int v2d_solver_adjoint(v2d_solver *S, double urot, const double *g_host, double *lam_host,
                                   double rtol, int max_refine, int *refinements, double *rel_res)
 {
@@ -750,7 +787,7 @@ extern "C" int v2d_solver_adjoint(v2d_solver *S, double urot, const double *g_ho
         S->prm.krylov = keep;
         V2D_TRY(st);
     }
-    if (!S->lu[0]) V2D_TRY(mf_factor_create(S->plan, 0, &S->lu[0]));
+    if (!S->lu[0]) V2D_TRY(mf_factor_create(S->plan, 0, 0, &S->lu[0]));
     V2D_TRY(mf_factor(S->plan, S->lu[0], g.rowptr, g.val, S->s));
     S->lu_valid = false;   // lu[0] no longer holds the Newton solve's factors
     V2D_TRY(ensure_transpose(S));

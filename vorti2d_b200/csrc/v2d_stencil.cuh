@@ -10,6 +10,7 @@
 #pragma once
 
 #include "v2d_common.cuh"
+#include "v2d_dual.cuh"
 
 namespace v2d {
 
@@ -59,15 +60,16 @@ struct LocalTopo {
 };
 
 // ------------------------------------------------------------------ metrics
+// The metric expressions are templates on the scalar type T (double, or the
+// Dual numbers of the tangent derivatives) and on the coordinate accessor X
+// (x[k] yields a T): the FP64 path instantiates them with T = double and
+// plain pointers, which is the same arithmetic in the same order.
+//
 // d/deta and d2/deta2 of one coordinate along the column through node K (row
 // j of jmax, row stride st).  Interior: central (vorti2d_core.f90:109-114);
 // j=0: forward one-sided 3/4-point (:130-133); j=jmax-1: backward (:148-151).
-struct EtaDer {
-    double d1, d2;
-};
-
-__device__ __forceinline__ double eta_d1(const double *x, int K, int j, int jmax, int st,
-                                         double two_de)
+template <class T, class X>
+__device__ __forceinline__ T eta_d1_t(const X &x, int K, int j, int jmax, int st, double two_de)
 {
     if (j == 0) {
         int k1 = K, k2 = K + st, k3 = K + 2 * st;
@@ -79,8 +81,8 @@ __device__ __forceinline__ double eta_d1(const double *x, int K, int j, int jmax
     return (x[K + st] - x[K - st]) / two_de;
 }
 
-__device__ __forceinline__ double eta_d2(const double *x, int K, int j, int jmax, int st,
-                                         double de2)
+template <class T, class X>
+__device__ __forceinline__ T eta_d2_t(const X &x, int K, int j, int jmax, int st, double de2)
 {
     if (j == 0) {
         int k1 = K, k2 = K + st, k3 = K + 2 * st, k4 = K + 3 * st;
@@ -92,24 +94,38 @@ __device__ __forceinline__ double eta_d2(const double *x, int K, int j, int jmax
     return (x[K + st] - 2.0 * x[K] + x[K - st]) / de2;
 }
 
-struct MetricOut {
-    double jac, alfa, beta, gama, pmet, qmet, detadx, detady;
+__device__ __forceinline__ double eta_d1(const double *x, int K, int j, int jmax, int st,
+                                         double two_de)
+{
+    return eta_d1_t<double>(x, K, j, jmax, st, two_de);
+}
+
+__device__ __forceinline__ double eta_d2(const double *x, int K, int j, int jmax, int st,
+                                         double de2)
+{
+    return eta_d2_t<double>(x, K, j, jmax, st, de2);
+}
+
+template <class T>
+struct MetricOutT {
+    T jac, alfa, beta, gama, pmet, qmet, detadx, detady;
 };
+using MetricOut = MetricOutT<double>;
 
 // Jacobian + transformation metrics (vorti2d_core.f90:164-182).
-__device__ __forceinline__ MetricOut metric_point(double xi, double yi, double xh, double yh,
-                                                  double xii, double yii, double xhh,
-                                                  double yhh, double xih, double yih)
+template <class T>
+__device__ __forceinline__ MetricOutT<T> metric_point_t(T xi, T yi, T xh, T yh, T xii, T yii,
+                                                        T xhh, T yhh, T xih, T yih)
 {
-    MetricOut m;
-    double J = 1.0 / (xi * yh - xh * yi);
-    double dksidx = J * yh;
-    double dksidy = -J * xh;
-    double ex = -J * yi;
-    double ey = J * xi;
-    double a = dksidx * dksidx + dksidy * dksidy;
-    double b = ex * ex + ey * ey;
-    double g = dksidx * ex + dksidy * ey;
+    MetricOutT<T> m;
+    T J = 1.0 / (xi * yh - xh * yi);
+    T dksidx = J * yh;
+    T dksidy = -J * xh;
+    T ex = -J * yi;
+    T ey = J * xi;
+    T a = dksidx * dksidx + dksidy * dksidy;
+    T b = ex * ex + ey * ey;
+    T g = dksidx * ex + dksidy * ey;
     m.jac = J; m.detadx = ex; m.detady = ey; m.alfa = a; m.beta = b; m.gama = g;
     m.pmet = -(a * (xii * dksidx + yii * dksidy) + 2.0 * g * (xih * dksidx + yih * dksidy)
                + b * (xhh * dksidx + yhh * dksidy));
@@ -118,31 +134,109 @@ __device__ __forceinline__ MetricOut metric_point(double xi, double yi, double x
     return m;
 }
 
+__device__ __forceinline__ MetricOut metric_point(double xi, double yi, double xh, double yh,
+                                                  double xii, double yii, double xhh,
+                                                  double yhh, double xih, double yih)
+{
+    return metric_point_t<double>(xi, yi, xh, yh, xii, yii, xhh, yhh, xih, yih);
+}
+
 // Metrics at node K with east/west neighbours e, w on the same row j.
+template <class T, class X>
+__device__ __forceinline__ MetricOutT<T> metrics_at_t(const X &x, const X &y, int K, int e,
+                                                      int w, int j, int jmax, int st,
+                                                      double dksi, double deta)
+{
+    const double two_dk = 2.0 * dksi, two_de = 2.0 * deta;
+    const double dk2 = dksi * dksi, de2 = deta * deta;
+    T xi = (x[e] - x[w]) / two_dk;
+    T yi = (y[e] - y[w]) / two_dk;
+    T xii = (x[e] - 2.0 * x[K] + x[w]) / dk2;
+    T yii = (y[e] - 2.0 * y[K] + y[w]) / dk2;
+    T xh = eta_d1_t<T>(x, K, j, jmax, st, two_de);
+    T yh = eta_d1_t<T>(y, K, j, jmax, st, two_de);
+    T xhh = eta_d2_t<T>(x, K, j, jmax, st, de2);
+    T yhh = eta_d2_t<T>(y, K, j, jmax, st, de2);
+    // cross derivative = ksi-central of d/deta (vorti2d_core.f90:155-161):
+    // d/deta at the e and w columns is recomputed here with the same formula
+    T xih = (eta_d1_t<T>(x, e, j, jmax, st, two_de) - eta_d1_t<T>(x, w, j, jmax, st, two_de)) /
+            two_dk;
+    T yih = (eta_d1_t<T>(y, e, j, jmax, st, two_de) - eta_d1_t<T>(y, w, j, jmax, st, two_de)) /
+            two_dk;
+    return metric_point_t<T>(xi, yi, xh, yh, xii, yii, xhh, yhh, xih, yih);
+}
+
 __device__ __forceinline__ MetricOut metrics_at(const double *x, const double *y, int K, int e,
                                                 int w, int j, int jmax, int st, double dksi,
                                                 double deta)
 {
-    const double two_dk = 2.0 * dksi, two_de = 2.0 * deta;
-    const double dk2 = dksi * dksi, de2 = deta * deta;
-    double xi = (x[e] - x[w]) / two_dk;
-    double yi = (y[e] - y[w]) / two_dk;
-    double xii = (x[e] - 2.0 * x[K] + x[w]) / dk2;
-    double yii = (y[e] - 2.0 * y[K] + y[w]) / dk2;
-    double xh = eta_d1(x, K, j, jmax, st, two_de);
-    double yh = eta_d1(y, K, j, jmax, st, two_de);
-    double xhh = eta_d2(x, K, j, jmax, st, de2);
-    double yhh = eta_d2(y, K, j, jmax, st, de2);
-    // cross derivative = ksi-central of d/deta (vorti2d_core.f90:155-161):
-    // d/deta at the e and w columns is recomputed here with the same formula
-    double xih = (eta_d1(x, e, j, jmax, st, two_de) - eta_d1(x, w, j, jmax, st, two_de)) / two_dk;
-    double yih = (eta_d1(y, e, j, jmax, st, two_de) - eta_d1(y, w, j, jmax, st, two_de)) / two_dk;
-    return metric_point(xi, yi, xh, yh, xii, yii, xhh, yhh, xih, yih);
+    return metrics_at_t<double>(x, y, K, e, w, j, jmax, st, dksi, deta);
 }
 
 // ----------------------------------------------------------------- rows
 constexpr int kPsiMax = 10;  // interior psi row: 9 psi + 1 ome entries
 constexpr int kOmeMax = 13;  // interior ome row: 9 ome + 4 psi entries
+
+// Right-hand sides b = -R of the rows whose values depend on the metrics,
+// templates on the type T of the metric values (double, or Dual for the
+// tangent derivatives; the state is FP64 either way).
+// Interior psi row (vorti2d_core.f90:295-300).
+template <class T>
+__device__ __forceinline__ T psi_rhs_interior(double re, double dksi, double deta, T a, T bt,
+                                              T g, T pm, T qm, const double *psi,
+                                              const double *ome, int K, const Nbr &nb)
+{
+    T Pp = (a / re) * ((psi[nb.e] - 2.0 * psi[K] + psi[nb.w]) / (dksi * dksi));
+    T Qq = 2.0 * (g / re) *
+           ((psi[nb.ne] - psi[nb.nw] - psi[nb.se] + psi[nb.sw]) / (4.0 * deta * dksi));
+    T Rr = (bt / re) * ((psi[nb.n] - 2.0 * psi[K] + psi[nb.s]) / (deta * deta));
+    T Ss = (pm / re) * ((psi[nb.e] - psi[nb.w]) / (2.0 * dksi));
+    T Tt = (qm / re) * ((psi[nb.n] - psi[nb.s]) / (2.0 * deta));
+    return Pp + Qq + Rr + Ss + Tt + ome[K] / re;
+}
+
+// Far-field psi row, Dirichlet form (vorti2d_core.f90:266-269).
+template <class T>
+__device__ __forceinline__ T psi_rhs_far(double ca, double sa, T xk, T yk, double psik)
+{
+    return (ca * yk - sa * xk) - psik;
+}
+
+// Wall omega row, Thom type with the rotation term (vorti2d_core.f90:322-339).
+template <class T>
+__device__ __forceinline__ T ome_rhs_wall(double deta, double urot, T beta, T qmet, T detadx,
+                                          T detady, T xk, T yk, const double *psi,
+                                          const double *ome, int K, int n, int nn)
+{
+    T bw = beta / (deta * deta);
+    T rad = tsqrt(xk * xk + yk * yk);
+    T ct = xk / rad, sn = yk / rad;
+    return ome[K] - (7.0 / 2.0) * bw * psi[K] + (8.0 / 2.0) * bw * psi[n]
+           - (1.0 / 2.0) * bw * psi[nn]
+           - ((qmet - 3.0 * (beta / deta)) * (urot / (detadx * ct + detady * sn)));
+}
+
+// Interior omega row (vorti2d_core.f90:341-378).
+template <class T>
+__device__ __forceinline__ T ome_rhs_interior(double re, double dksi, double deta, double inv2dt,
+                                              T J, T a, T bt, T g, T pm, T qm,
+                                              const double *psi, const double *ome,
+                                              const double *omeold, const double *omeoldold,
+                                              int K, const Nbr &nb)
+{
+    double Aa = (psi[nb.n] - psi[nb.s]) / (2.0 * deta);
+    double Bb = (ome[nb.e] - ome[nb.w]) / (2.0 * dksi);
+    double Cc = (psi[nb.e] - psi[nb.w]) / (2.0 * dksi);
+    double Dd = (ome[nb.n] - ome[nb.s]) / (2.0 * deta);
+    T Ee = (a / re) * ((ome[nb.e] - 2.0 * ome[K] + ome[nb.w]) / (dksi * dksi));
+    T Ff = 2.0 * (g / re) *
+           ((ome[nb.ne] - ome[nb.nw] - ome[nb.se] + ome[nb.sw]) / (4.0 * deta * dksi));
+    T Gg = (bt / re) * ((ome[nb.n] - 2.0 * ome[K] + ome[nb.s]) / (deta * deta));
+    T Hh = (pm / re) * ((ome[nb.e] - ome[nb.w]) / (2.0 * dksi));
+    T Ii = (qm / re) * ((ome[nb.n] - ome[nb.s]) / (2.0 * deta));
+    return -(J * Aa * Bb) + (J * Cc * Dd) + Ee + Ff + Gg + Hh + Ii
+           - ((3.0 * ome[K] - 4.0 * omeold[K] + omeoldold[K]) * inv2dt);
+}
 
 __device__ __forceinline__ bool outflow_arc(const Coeffs &c, const Fields &f, int K)
 {
@@ -191,7 +285,7 @@ __device__ __forceinline__ int psi_row(const Topo &T, const Coeffs &c, const Fie
         col[0] = T.dof(K, 0);
         if (VAL) {
             val[0] = 1.0;
-            *b = (c.ca * f.yphys[K] - c.sa * f.xphys[K]) - f.psi[K];
+            *b = psi_rhs_far<double>(c.ca, c.sa, f.xphys[K], f.yphys[K], f.psi[K]);
         }
         return 1;
     }
@@ -222,13 +316,7 @@ __device__ __forceinline__ int psi_row(const Topo &T, const Coeffs &c, const Fie
         val[7] = cgam;
         val[8] = -cgam;
         val[9] = -1.0 / re;
-        double Pp = (a / re) * ((psi[nb.e] - 2.0 * psi[K] + psi[nb.w]) / (dksi * dksi));
-        double Qq = 2.0 * (g / re) *
-                    ((psi[nb.ne] - psi[nb.nw] - psi[nb.se] + psi[nb.sw]) / (4.0 * deta * dksi));
-        double Rr = (bt / re) * ((psi[nb.n] - 2.0 * psi[K] + psi[nb.s]) / (deta * deta));
-        double Ss = (pm / re) * ((psi[nb.e] - psi[nb.w]) / (2.0 * dksi));
-        double Tt = (qm / re) * ((psi[nb.n] - psi[nb.s]) / (2.0 * deta));
-        *b = Pp + Qq + Rr + Ss + Tt + f.ome[K] / re;
+        *b = psi_rhs_interior<double>(re, dksi, deta, a, bt, g, pm, qm, psi, f.ome, K, nb);
     }
     return kPsiMax;
 }
@@ -268,13 +356,9 @@ __device__ __forceinline__ int ome_row(const Topo &T, const Coeffs &c, const Fie
             val[1] = (7.0 / 2.0) * bw;
             val[2] = -(8.0 / 2.0) * bw;
             val[3] = (1.0 / 2.0) * bw;
-            double xk = f.xphys[K], yk = f.yphys[K];
-            double rad = sqrt(xk * xk + yk * yk);
-            double ct = xk / rad, sn = yk / rad;
-            *b = f.ome[K] - (7.0 / 2.0) * bw * psi[K] + (8.0 / 2.0) * bw * psi[n]
-                 - (1.0 / 2.0) * bw * psi[nn]
-                 - ((f.qmet[K] - 3.0 * (f.beta[K] / deta)) *
-                    (c.urot / (f.detadx[K] * ct + f.detady[K] * sn)));
+            *b = ome_rhs_wall<double>(deta, c.urot, f.beta[K], f.qmet[K], f.detadx[K],
+                                      f.detady[K], f.xphys[K], f.yphys[K], psi, f.ome, K, n,
+                                      nn);
         }
         return 4;
     }
@@ -292,12 +376,6 @@ __device__ __forceinline__ int ome_row(const Topo &T, const Coeffs &c, const Fie
         double Bb = (ome[nb.e] - ome[nb.w]) / (2.0 * dksi);
         double Cc = (psi[nb.e] - psi[nb.w]) / (2.0 * dksi);
         double Dd = (ome[nb.n] - ome[nb.s]) / (2.0 * deta);
-        double Ee = (a / re) * ((ome[nb.e] - 2.0 * ome[K] + ome[nb.w]) / (dksi * dksi));
-        double Ff = 2.0 * (g / re) *
-                    ((ome[nb.ne] - ome[nb.nw] - ome[nb.se] + ome[nb.sw]) / (4.0 * deta * dksi));
-        double Gg = (bt / re) * ((ome[nb.n] - 2.0 * ome[K] + ome[nb.s]) / (deta * deta));
-        double Hh = (pm / re) * ((ome[nb.e] - ome[nb.w]) / (2.0 * dksi));
-        double Ii = (qm / re) * ((ome[nb.n] - ome[nb.s]) / (2.0 * deta));
         double cab = a / (re * (dksi * dksi));
         double cbt = bt / (re * (deta * deta));
         double cgam = (2.0 * g) / (4.0 * re * dksi * deta);
@@ -315,8 +393,8 @@ __device__ __forceinline__ int ome_row(const Topo &T, const Coeffs &c, const Fie
         val[10] = -(J * Bb) / (2.0 * deta);
         val[11] = -(J * Dd) / (2.0 * dksi);
         val[12] = (J * Dd) / (2.0 * dksi);
-        *b = -(J * Aa * Bb) + (J * Cc * Dd) + Ee + Ff + Gg + Hh + Ii
-             - ((3.0 * ome[K] - 4.0 * f.omeold[K] + f.omeoldold[K]) * c.inv2dt);
+        *b = ome_rhs_interior<double>(re, dksi, deta, c.inv2dt, J, a, bt, g, pm, qm, psi, ome,
+                                      f.omeold, f.omeoldold, K, nb);
     }
     return kOmeMax;
 }

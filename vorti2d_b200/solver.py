@@ -45,6 +45,7 @@ def solver_params(cfg: Config) -> _lib.SolverParams:
     k.lu_reuse_its = int(cfg.lu_reuse_its)
     k.lu_reuse_steps = int(bool(cfg.lu_reuse_steps))
     k.lu_solve = {"flow": 0, "levels": 1}[cfg.lu_solve]
+    k.lu_factor64 = {"fp32": 0, "fp64": 1}[cfg.lu_factors]
     p.krylov = k
     return p
 
