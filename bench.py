@@ -281,11 +281,15 @@ def run_adjoint_workload(args):
     wall displaced by seeded Gaussian bumps of 1e-3 chord, alpha = 4 deg,
     Re = --adjoint-re.  The steady Newton solve (FP64 LU-preconditioned GMRES)
     is timed, then the gradients dCl/dalpha, dCd/dRe and dCd/d(256 wall-normal
-    displacements): one transposed solve per output weight plus central
-    differences of the residual and the wall forces on the displaced meshes.
+    displacements): one FP64 factorization of dR/dq shared by the three
+    transposed solves, residual parameter derivatives, and the exact tangent
+    derivatives of the residual and the wall forces along all 256 directions.
     value = gradient evaluations (all three) per second.  The steady solve is
     then repeated from the same start on the warm handle, and the line gives
-    the time of a gradient set over that of the solve."""
+    the time of a gradient set over that of the solve.  --adjoint-dtau > 0
+    solves the primal by pseudo-time continuation (dtau added to the Newton
+    diagonal as the reference's dual-time stepping does) where plain Newton
+    from the free stream fails; the adjoint uses dR/dq without it."""
     import torch
     import vorti2d_b200 as v
     from vorti2d_b200.adjoint import deform_ogrid, force_vjp, gaussian_bumps, shape_vjp
@@ -293,10 +297,11 @@ def run_adjoint_workload(args):
     base = v.generate_naca0012(257, 193)
     d0 = gaussian_bumps(256, n_bumps=8, amplitude=1e-3, seed=0)
     X, Y = deform_ogrid(*base, d0)
+    dtau = args.adjoint_dtau if args.adjoint_dtau > 0 else math.inf
     cfg = v.Config(verbose=False, write_csv=False, write_xdmf=False, compute_forces=False,
                    re=args.adjoint_re, alpha_deg=4.0, steady=True, pseudo_tol=1e-12,
-                   max_pseudo_iter=30, ksp_rtol=1e-12, ref_length=1.0, precision="fp64",
-                   raise_on_linear_failure=False)
+                   max_pseudo_iter=30 if math.isinf(dtau) else 600, ksp_rtol=1e-12,
+                   ref_length=1.0, precision="fp64", raise_on_linear_failure=False, dtau=dtau)
     s = v.Solver(cfg, mesh=(X, Y))
     q0 = s.get_state()
     t0 = time.perf_counter()
@@ -311,7 +316,9 @@ def run_adjoint_workload(args):
             "unit": "gradient sets/s", "n_gpus": 1, "higher_is_better": True,
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": "steady discrete adjoint, NACA-0012 257x193, alpha 4 deg, "
-                                   f"Re {args.adjoint_re:g}, 8 seeded 1e-3-chord wall bumps"},
+                                   f"Re {args.adjoint_re:g}, 8 seeded 1e-3-chord wall bumps",
+                       "primal": "plain Newton" if math.isinf(dtau)
+                                 else f"pseudo-time continuation, dtau {dtau:g}"},
             "steady_newton_its": its, "steady_res": res, "steady_converged": converged,
             "steady_solve_s": t_solve}
     if not converged:
@@ -768,6 +775,9 @@ def main():
                     help="BDF2 steps of the unsteady adjoint workload")
     ap.add_argument("--ua-checkpoint", type=int, default=5,
                     help="checkpoint spacing of the unsteady adjoint workload")
+    ap.add_argument("--adjoint-dtau", type=float, default=0.0,
+                    help="adjoint workload: pseudo-time step of the steady primal (0: plain "
+                         "Newton, dtau = inf)")
     ap.add_argument("--adjoint-re", type=float, default=500.0,
                     help="Reynolds number of the adjoint workload (--workload adjoint)")
     ap.add_argument("--kernels-only", action="store_true",

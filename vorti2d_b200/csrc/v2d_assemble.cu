@@ -107,18 +107,18 @@ int build_pattern(GridDev &g, const AsmParams &p, cudaStream_t s)
 // 32 rows).
 constexpr int kAsmNodes = 128;
 
+// One block of kAsmNodes nodes starting at node K0 (blockDim.x == kAsmNodes).
 template <bool W32>
-__global__ void __launch_bounds__(kAsmNodes) assemble_newton(GlobalTopo T, Coeffs c, Fields f,
-                                                             const int *__restrict__ rowptr,
-                                                             double *__restrict__ val,
-                                                             float *__restrict__ val32,
-                                                             double *__restrict__ b,
-                                                             double *__restrict__ dinv,
-                                                             float *__restrict__ dinv32, int *flag)
+__device__ __forceinline__ void assemble_block(const GlobalTopo &T, const Coeffs &c,
+                                               const Fields &f, const int *__restrict__ rowptr,
+                                               double *__restrict__ val,
+                                               float *__restrict__ val32,
+                                               double *__restrict__ b, double *__restrict__ dinv,
+                                               float *__restrict__ dinv32, int *flag, int K0,
+                                               double *stage)
 {
-    __shared__ double stage[kAsmNodes * kOmeMax];
     const int N = T.N;
-    for (int K0 = blockIdx.x * kAsmNodes; K0 < N; K0 += gridDim.x * kAsmNodes) {
+    {
         const int K = K0 + threadIdx.x;
         const bool live = K < N;
         const int K1 = min(K0 + kAsmNodes, N);
@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(kAsmNodes) assemble_newton(GlobalTopo T, Coeff
             if (W32) val32[obeg + e] = (float)x;
         }
         __syncthreads();
-        if (live) {
+        if (live && dinv) {
             // 2x2 block inverse for block Jacobi
             double det = a00 * a11 - a01 * a10;
             double i00, i01, i10, i11;
@@ -194,9 +194,23 @@ __global__ void __launch_bounds__(kAsmNodes) assemble_newton(GlobalTopo T, Coeff
                 dinv32[K] = (float)i00; dinv32[N + K] = (float)i01;
                 dinv32[2 * N + K] = (float)i10; dinv32[3 * N + K] = (float)i11;
             }
-            if (!isfinite(bk)) atomicOr(flag, 2);
         }
+        if (live && !isfinite(bk)) atomicOr(flag, 2);
     }
+}
+
+template <bool W32>
+__global__ void __launch_bounds__(kAsmNodes) assemble_newton(GlobalTopo T, Coeffs c, Fields f,
+                                                             const int *__restrict__ rowptr,
+                                                             double *__restrict__ val,
+                                                             float *__restrict__ val32,
+                                                             double *__restrict__ b,
+                                                             double *__restrict__ dinv,
+                                                             float *__restrict__ dinv32, int *flag)
+{
+    __shared__ double stage[kAsmNodes * kOmeMax];
+    for (int K0 = blockIdx.x * kAsmNodes; K0 < T.N; K0 += gridDim.x * kAsmNodes)
+        assemble_block<W32>(T, c, f, rowptr, val, val32, b, dinv, dinv32, flag, K0, stage);
 }
 
 // Right-hand side b = -R of the Newton system only (no Jacobian values), for

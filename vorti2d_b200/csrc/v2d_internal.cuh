@@ -209,3 +209,37 @@ int time_spmv(const CsrOp &A, bool fp32, int reps, size_t flush_bytes, cudaStrea
 int launch_block_inverse(CsrOp &A, double *dinv, float *dinv32, int *d_flag, cudaStream_t s);
 
 }  // namespace v2d
+
+// The device-resident solver handle behind the C ABI (v2d_solver.cu).
+struct v2d_solver {
+    v2d::GridDev g;
+    v2d_solver_params prm{};
+    v2d::AsmParams ap{};
+    cudaStream_t s = nullptr;
+    v2d::KrylovWork *kw = nullptr;
+    double *delta = nullptr;      // Newton update (2N)
+    double *partial = nullptr;    // reduction partials
+    double *scal = nullptr;       // device scalars: [0] res, [1..10] forces
+    int *flag = nullptr;
+    unsigned int *counter = nullptr;
+    double *host = nullptr;       // pinned mirror of scal
+    int pattern_ff_bc = -1;
+    double pattern_ca = 0, pattern_sa = 0;
+    bool assembled = false;
+    v2d::MfPlan *plan = nullptr;        // multifrontal plan of the current pattern
+    int plan_leaf = 0;
+    v2d::MfFactor *lu[2] = {nullptr, nullptr};  // [0] FP64 factors, [1] FP32 factors
+    bool lu_valid = false;           // factors of an earlier Jacobian kept for reuse
+    bool lu_ready = false;           // the factor storage holds some factorization
+    int lu_last_its = 0;             // Krylov iterations of the last solve with them
+    long long lu_factorizations = 0;
+    int *tptr = nullptr, *tind = nullptr, *tperm = nullptr;   // transposed CSR pattern (adjoint)
+    // versions for the adjoint's factor cache: the state (psi, ome) and the
+    // parameters, the assembled values, and the FP64 factors lu[0]
+    long long state_ver = 0, val_ver = 0, lu0_ver = 0;
+    long long adj_key[3] = {-1, -1, -1};   // the versions when lu[0] last held J (adjoint)
+    cudaEvent_t ev[5] = {};          // phase boundaries of the last Newton iteration
+    double phase_ms[4] = {0, 0, 0, 0};
+    long long phase_n = 0;
+};
+

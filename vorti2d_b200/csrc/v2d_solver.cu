@@ -16,33 +16,6 @@
 
 using namespace v2d;
 
-struct v2d_solver {
-    GridDev g;
-    v2d_solver_params prm{};
-    AsmParams ap{};
-    cudaStream_t s = nullptr;
-    KrylovWork *kw = nullptr;
-    double *delta = nullptr;      // Newton update (2N)
-    double *partial = nullptr;    // reduction partials
-    double *scal = nullptr;       // device scalars: [0] res, [1..10] forces
-    int *flag = nullptr;
-    unsigned int *counter = nullptr;
-    double *host = nullptr;       // pinned mirror of scal
-    int pattern_ff_bc = -1;
-    double pattern_ca = 0, pattern_sa = 0;
-    bool assembled = false;
-    MfPlan *plan = nullptr;        // multifrontal plan of the current pattern
-    int plan_leaf = 0;
-    MfFactor *lu[2] = {nullptr, nullptr};  // [0] FP64 factors, [1] FP32 factors
-    bool lu_valid = false;           // factors of an earlier Jacobian kept for reuse
-    bool lu_ready = false;           // the factor storage holds some factorization
-    int lu_last_its = 0;             // Krylov iterations of the last solve with them
-    long long lu_factorizations = 0;
-    int *tptr = nullptr, *tind = nullptr, *tperm = nullptr;   // transposed CSR pattern (adjoint)
-    cudaEvent_t ev[5] = {};          // phase boundaries of the last Newton iteration
-    double phase_ms[4] = {0, 0, 0, 0};
-    long long phase_n = 0;
-};
 
 namespace {
 
@@ -311,6 +284,7 @@ extern "C" int v2d_solver_set_params(v2d_solver *S, const v2d_solver_params *p)
     const int old_m = S->prm.krylov.restart;
     S->prm = *p;
     S->lu_valid = false;
+    ++S->state_ver;   // the Jacobian depends on the parameters
     V2D_TRY(ensure_pattern(S));
     V2D_TRY(ensure_lu(S));
     if (p->krylov.restart != old_m) {
@@ -333,6 +307,7 @@ extern "C" int v2d_solver_set_state(v2d_solver *S, const double *psi, const doub
         if (src[q]) V2D_CUDA_TRY(cudaMemcpyAsync(dst[q], src[q], bytes, cudaMemcpyHostToDevice, S->s));
     V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
     S->assembled = false;
+    ++S->state_ver;
     // a new state: old factors precondition it only when the caller keeps
     // factors across steps (a solve that needs more than lu_reuse_its + 5
     // iterations with them refactors and solves again)
@@ -365,11 +340,14 @@ extern "C" int v2d_solver_get_metrics(v2d_solver *S, double *const *out10)
     return V2D_OK;
 }
 
-static int assemble_now(v2d_solver *S, double urot)
+// Newton system of the current state; pseudo = false leaves out the
+// pseudo-time term invdtau (the adjoint needs dR/dq of the physical residual).
+static int assemble_now(v2d_solver *S, double urot, bool pseudo = true)
 {
     V2D_TRY(ensure_pattern(S));
     const v2d_solver_params &p = S->prm;
-    AsmParams ap{p.re, p.invdtau, p.inv2dt, urot, p.ca, p.sa, p.ff_bc};
+    AsmParams ap{p.re, pseudo ? p.invdtau : 0.0, p.inv2dt, urot, p.ca, p.sa, p.ff_bc};
+    ++S->val_ver;
     V2D_CUDA_TRY(cudaMemsetAsync(S->flag, 0, sizeof(int), S->s));
     V2D_TRY(launch_assemble(S->g, ap, p.krylov.precision == V2D_PREC_MIXED, S->flag, S->s));
     S->assembled = true;
@@ -403,6 +381,7 @@ extern "C" int v2d_solver_newton(v2d_solver *S, double urot, double *res, v2d_li
         const bool reuse = kp.lu_reuse_its > 0 && S->lu_valid && S->lu_last_its <= kp.lu_reuse_its;
         if (!reuse) {
             V2D_TRY(mf_factor(S->plan, S->lu[mixed], g.rowptr, g.val, S->s));
+            if (!mixed) ++S->lu0_ver;
             ++S->lu_factorizations;
             S->lu_ready = true;
             refactored = true;
@@ -421,6 +400,7 @@ extern "C" int v2d_solver_newton(v2d_solver *S, double urot, double *res, v2d_li
         if (!ls.converged) {
             const int its0 = ls.iterations;
             V2D_TRY(mf_factor(S->plan, S->lu[mixed], g.rowptr, g.val, S->s));
+            if (!mixed) ++S->lu0_ver;
             ++S->lu_factorizations;
             S->lu_ready = true;
             refactored = true;
@@ -440,6 +420,7 @@ extern "C" int v2d_solver_newton(v2d_solver *S, double urot, double *res, v2d_li
     const int grid = std::max(1, std::min(kUpdBlocks, (g.N + kUpdThreads * 8 - 1) / (kUpdThreads * 8)));
     k_newton_update<<<grid, kUpdThreads, 0, S->s>>>(g.N, S->delta, g.psi, g.ome, S->partial,
                                                      S->counter, S->scal);
+    ++S->state_ver;
     V2D_CUDA_TRY(cudaGetLastError());
     count_launches(1);
     V2D_CUDA_TRY(cudaEventRecord(S->ev[4], S->s));
@@ -777,19 +758,31 @@ extern "C" int v2d_solver_adjoint(v2d_solver *S, double urot, const double *g_ho
                   "solver_adjoint: needs the LU preconditioner");
     V2D_ARG_CHECK(max_refine >= 1, "solver_adjoint: max_refine must be >= 1");
     GridDev &g = S->g;
-    // FP64 factors of the Jacobian at the current state
-    V2D_TRY(assemble_now(S, urot));
-    V2D_TRY(sync_flag(S, "adjoint assembly"));
-    if (!S->plan) {
-        v2d_krylov_params keep = S->prm.krylov;
-        S->prm.krylov.precond = V2D_PC_LU;
-        const int st = ensure_lu(S);
-        S->prm.krylov = keep;
-        V2D_TRY(st);
+    // FP64 factors of the Jacobian dR/dq at the current state -- the
+    // physical residual's, without the pseudo-time term -- unless lu[0] and
+    // the assembled values still hold them from the last adjoint solve
+    // (J does not depend on urot: the rotation enters the wall rows' right-
+    // hand side only)
+    const bool cached = S->lu[0] && S->adj_key[0] == S->state_ver &&
+                        S->adj_key[1] == S->val_ver && S->adj_key[2] == S->lu0_ver;
+    if (!cached) {
+        V2D_TRY(assemble_now(S, urot, false));
+        V2D_TRY(sync_flag(S, "adjoint assembly"));
+        if (!S->plan) {
+            v2d_krylov_params keep = S->prm.krylov;
+            S->prm.krylov.precond = V2D_PC_LU;
+            const int st = ensure_lu(S);
+            S->prm.krylov = keep;
+            V2D_TRY(st);
+        }
+        if (!S->lu[0]) V2D_TRY(mf_factor_create(S->plan, 0, 0, &S->lu[0]));
+        V2D_TRY(mf_factor(S->plan, S->lu[0], g.rowptr, g.val, S->s));
+        ++S->lu0_ver;
+        S->lu_valid = false;   // lu[0] no longer holds the Newton solve's factors
+        S->adj_key[0] = S->state_ver;
+        S->adj_key[1] = S->val_ver;
+        S->adj_key[2] = S->lu0_ver;
     }
-    if (!S->lu[0]) V2D_TRY(mf_factor_create(S->plan, 0, 0, &S->lu[0]));
-    V2D_TRY(mf_factor(S->plan, S->lu[0], g.rowptr, g.val, S->s));
-    S->lu_valid = false;   // lu[0] no longer holds the Newton solve's factors
     V2D_TRY(ensure_transpose(S));
     const size_t n = g.n;
     DevBuf<double> buf;
@@ -930,6 +923,7 @@ extern "C" int v2d_solver_time_lu_factor(v2d_solver *S, int reps, double *ms, in
     const int q = S->prm.krylov.precision == V2D_PREC_MIXED ? 1 : 0;
     V2D_ARG_CHECK(S->lu[q] && S->lu_ready,
                   "time_lu_factor: no current factors (run a Newton iteration first)");
+    if (q == 0) ++S->lu0_ver;   // refactors lu[0]
     return mf_time_factor_launches(S->plan, S->lu[q], S->g.rowptr, S->g.val, reps, S->s, ms,
                                    codes, cap, n);
 }
@@ -950,6 +944,7 @@ extern "C" int v2d_solver_time_kernel(v2d_solver *S, int which, int reps, long l
     V2D_TRY(ensure_pattern(S));
     const v2d_solver_params &p = S->prm;
     AsmParams ap{p.re, p.invdtau, p.inv2dt, 0.0, p.ca, p.sa, p.ff_bc};
+    if (which == 1 || which == 2) ++S->val_ver;   // the timed assembly rewrites the values
     cudaEvent_t e0, e1;
     V2D_CUDA_TRY(cudaEventCreate(&e0));
     V2D_CUDA_TRY(cudaEventCreate(&e1));
