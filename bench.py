@@ -226,11 +226,14 @@ def run_sweep_workload(args):
     converged solves per second beside it."""
     import torch
     import vorti2d_b200 as v
-    from vorti2d_b200.batch import run_sweep, sweep_cases
+    from vorti2d_b200.batch import run_sweep, run_sweep_batched, sweep_cases
     torch.cuda.set_device(0)
     cases = sweep_cases(seed=0)
     cont = args.sweep_continuation if args.sweep_continuation > 1.0 else None
-    res = run_sweep(cases, workers=args.sweep_workers, precision="mixed", continuation=cont)
+    if args.sweep_mode == "batched" and cont is None:
+        res = run_sweep_batched(cases, precision="mixed", lu_factors=args.lu_factors)
+    else:
+        res = run_sweep(cases, workers=args.sweep_workers, precision="mixed", continuation=cont)
     kinds = {}
     for r in res.results:
         k = r.name.rsplit("_", 1)[0]
@@ -262,6 +265,9 @@ def run_sweep_workload(args):
             "converged_solves_per_s": res.solves_per_s, "newton_iters": res.newton_iters,
             "higher_is_better": True, "dtype": "f32-krylov/f64", "data": "synthetic",
             "config": {"workload": "batched steady sweep, seed 0", "workers": res.workers,
+                       "mode": ("one block-diagonal system, one launch per Newton phase"
+                                if args.sweep_mode == "batched" and cont is None
+                                else "one handle and stream per instance, thread pool"),
                        "precond": "multifrontal LU per Newton iteration",
                        "newton": "<=20 iterations, stop when ||dq|| > 1e3 x the first",
                        "krylov_max_it": 300,
@@ -760,6 +766,9 @@ def main():
                          "adjoint: steady adjoint gradients; large: the large unsteady grid; "
                          "unsteady_adjoint: the checkpointed unsteady adjoint")
     ap.add_argument("--sweep-workers", type=int, default=16)
+    ap.add_argument("--sweep-mode", default="batched", choices=["batched", "streams"],
+                    help="sweep: all instances as one block-diagonal system (batched) or one "
+                         "handle and stream per instance")
     ap.add_argument("--sweep-continuation", type=float, default=0.0,
                     help="sweep: Reynolds continuation factor per rung from Re 80 (0: none, "
                          "plain Newton from the free stream as the reference)")

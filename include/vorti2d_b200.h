@@ -422,6 +422,36 @@ int v2d_solver_time_kernel(v2d_solver *s, int which, int reps, long long flush_b
 /* The stream the handle's kernels run on (cudaStream_t as void*). */
 int v2d_solver_stream(v2d_solver *s, void **stream);
 
+/* ------------------------------------------------ 4. batched steady solves */
+/* Many steady Newton solves of uneven O-grids at once (no reference
+ * counterpart: the reference runs one solve per process,
+ * vorti2d/solver.py:136-145).  The instances' Newton systems are the diagonal
+ * blocks of one block-diagonal system: each Newton iteration is one
+ * assembly launch over all instances, one multifrontal factorization over
+ * the forest of their separator trees, GMRES on the combined system and one
+ * update launch.  params[i] holds instance i's Reynolds number, angle,
+ * far-field BC and pseudo-time term; the Krylov parameters are params[0]'s
+ * (precond must be V2D_PC_LU). */
+typedef struct v2d_batch v2d_batch;
+int v2d_batch_create(int ninst, const int *imax, const int *jmax, const double *const *xg,
+                     const double *const *yg, const v2d_solver_params *params,
+                     v2d_batch **out);
+int v2d_batch_destroy(v2d_batch *b);
+/* active[i] = 0 freezes instance i (its rows become identity rows with a zero
+ * right-hand side: its state stays as it is); 1 iterates it (all start
+ * active). */
+int v2d_batch_set_active(v2d_batch *b, const int *active);
+/* One Newton iteration of every active instance; res[i] = ||dq_i||_2 / (2 N_i)
+ * (0 for a frozen one), flags[i] (may be null) the instance's assembly flags
+ * (bit 1 non-finite right-hand side: no update is made then, V2D_ENONFINITE).
+ * V2D_ENOTCONVERGED after the update when GMRES missed its tolerance. */
+int v2d_batch_newton(v2d_batch *b, double *res, int *flags, v2d_lin_stats *st);
+/* The solver handle of instance i (state, forces, metrics); owned by the
+ * batch. */
+int v2d_batch_instance(v2d_batch *b, int i, v2d_solver **out);
+/* LU factorizations of the combined system so far. */
+int v2d_batch_factorizations(const v2d_batch *b, long long *n);
+
 #ifdef __cplusplus
 }
 #endif

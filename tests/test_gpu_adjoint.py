@@ -257,8 +257,8 @@ def test_shape_tangent_equals_extrapolated_differences(v2d, oracle_mod, kind, im
                                                        ref_length):
     """The exact tangent shape gradient (dual numbers through metrics,
     residual and wall integrals) against the displaced-mesh central
-    differences extrapolated in the step (Richardson, h and h/2: error
-    O(h^4)), for every wall node at once, within 1e-7 relative to the
+    differences extrapolated in the step (Richardson over h, h/2, h/4: error
+    O(h^6)), for every wall node at once, within 1e-8 relative to the
     gradient's largest component."""
     from vorti2d_b200.adjoint import deform_ogrid, gaussian_bumps, shape_vjp
     base = _base_mesh(v2d, oracle_mod, kind, im, jm)
@@ -271,10 +271,13 @@ def test_shape_tangent_equals_extrapolated_differences(v2d, oracle_mod, kind, im
     h = 1e-4 * max(np.ptp(base[0][:P, 0]), np.ptp(base[1][:P, 0]))
     f1, _ = shape_vjp(s, w, base, h=h, method="fd")
     f2, _ = shape_vjp(s, w, base, h=h / 2, method="fd")
-    rich = (4.0 * f2 - f1) / 3.0
+    f4, _ = shape_vjp(s, w, base, h=h / 4, method="fd")
+    r1, r2 = (4.0 * f2 - f1) / 3.0, (4.0 * f4 - f2) / 3.0
+    rich = (16.0 * r2 - r1) / 15.0
     scale = np.abs(tan).max()
     err = np.abs(tan - rich).max() / scale
     print(f"{kind}: tangent vs extrapolated differences, max rel {err:.2e} "
-          f"(plain h={h:.1e}: {np.abs(tan - f1).max() / scale:.2e})")
-    assert err <= 1e-7, err
+          f"(plain h={h:.1e}: {np.abs(tan - f1).max() / scale:.2e}, once extrapolated: "
+          f"{np.abs(tan - r2).max() / scale:.2e})")
+    assert err <= 1e-8, err
     s.close()

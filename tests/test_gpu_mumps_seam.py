@@ -66,8 +66,11 @@ def test_steady_129_through_the_seam_matches_oracle(v2d, oracle_mod):
     lin.destroy()
 
 
-@pytest.mark.parametrize("imax,jmax,ff_bc,alpha", [(33, 21, 1, 4.0), (64, 48, 2, -8.0),
-                                                   (24, 13, 0, 0.0)])
+# shapes on which the reference's steady Newton converges from the free stream
+# (on coarser ones, e.g. 33x21 or 24x13, it does not: the oracle stalls there
+# too)
+@pytest.mark.parametrize("imax,jmax,ff_bc,alpha", [(33, 25, 1, 4.0), (64, 48, 2, -8.0),
+                                                   (65, 49, 0, 4.0)])
 @pytest.mark.parametrize("grid", [False, True])
 def test_seam_lu_shapes_and_far_field_bcs(v2d, oracle_mod, imax, jmax, ff_bc, alpha, grid):
     """The grid recognised from the pattern (or given) on odd/even shapes and

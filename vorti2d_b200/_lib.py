@@ -111,6 +111,13 @@ _SIGS = {
     "v2d_solver_export_system": (_i, [_vp, _ip, _ip, _dp, _dp]),
     "v2d_solver_state_ptrs": (_i, [_vp] + [ctypes.POINTER(_vp)] * 4),
     "v2d_solver_stream": (_i, [_vp, ctypes.POINTER(_vp)]),
+    "v2d_batch_create": (_i, [_i, _ip, _ip, ctypes.POINTER(_dp), ctypes.POINTER(_dp),
+                              ctypes.POINTER(SolverParams), ctypes.POINTER(_vp)]),
+    "v2d_batch_destroy": (_i, [_vp]),
+    "v2d_batch_set_active": (_i, [_vp, _ip]),
+    "v2d_batch_newton": (_i, [_vp, _dp, _ip, ctypes.POINTER(LinStats)]),
+    "v2d_batch_instance": (_i, [_vp, _i, ctypes.POINTER(_vp)]),
+    "v2d_batch_factorizations": (_i, [_vp, ctypes.POINTER(_ll)]),
     "v2d_solver_time_spmv": (_i, [_vp, _i, _i, _ll, _dp]),
     "v2d_solver_phase_times": (_i, [_vp, _dp, _i]),
     "v2d_solver_time_kernel": (_i, [_vp, _i, _i, _ll, _dp]),

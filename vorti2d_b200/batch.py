@@ -1,12 +1,16 @@
 """Batched steady sweeps: many independent steady solves of uneven grid sizes
 (cylinders and NACA-0012 sections over a range of Reynolds numbers and
-angles of attack) run concurrently on one GPU.
+angles of attack) on one GPU.
 
-Every instance is its own device handle (state, CSR, multifrontal factors,
-Krylov workspace) with its own CUDA stream; a pool of host threads drives
-them (the C ABI releases the GIL).  One instance at these sizes occupies only
-a fraction of the B200's SMs -- its factor and solve kernels are
-latency-bound -- so the streams of the other instances fill the rest.
+``run_sweep_batched`` (the default) advances all instances by Newton
+together: their systems are the diagonal blocks of one block-diagonal system,
+so each Newton iteration is one assembly launch over all instances, one
+multifrontal factorization over the forest of their separator trees, GMRES
+on the combined system and one update launch (``v2d_batch_*``).  Converged
+and diverging instances are frozen and stop contributing work.
+
+``run_sweep`` is the earlier form: every instance its own device handle and
+CUDA stream, driven by a pool of host threads.
 
 Plain Newton from the free stream (the reference's steady method) does not
 reach a steady state at the higher Reynolds numbers of a sweep: each instance
@@ -226,5 +230,92 @@ def run_sweep(cases, workers: int = 16, precision: str = "mixed", max_newton: in
     out.solve_s = time.perf_counter() - t1
     for s in solvers:
         s.close()
+    out.results = results
+    return out
+
+
+def run_sweep_batched(cases, precision: str = "mixed", max_newton: int = 20,
+                      pseudo_tol: float = 1e-10, krylov_max_it: int = 300,
+                      diverge_factor: float = 1e3, **cfg_kw) -> SweepResult:
+    """Solve every case to a steady state in one batch (``v2d_batch_*``).
+
+    Each instance follows the reference's steady loop (vorti2d/solver.py:
+    136-145: iterate while ||dq||/(2N) > pseudo_tol, at most max_newton
+    times); an instance whose update norm exceeds ``diverge_factor`` times its
+    first one, or is not finite, is frozen as diverged.  Every Newton
+    iteration of the batch is one iteration of all instances still active.
+    ``setup_s`` covers the batch's creation (meshes, metrics, patterns, the
+    forest plan, factor storage); ``solve_s`` the Newton iterations."""
+    from ctypes import byref, c_void_p
+    from .solver import solver_params
+    n = len(cases)
+    cfgs = [_config(c, precision, max_newton, pseudo_tol, krylov_max_it, **cfg_kw) for c in cases]
+    params = (_lib.SolverParams * n)(*[solver_params(c) for c in cfgs])
+    xs = [np.asfortranarray(c.xg, dtype=np.float64) for c in cases]
+    ys = [np.asfortranarray(c.yg, dtype=np.float64) for c in cases]
+    imax = np.array([x.shape[0] for x in xs], dtype=np.intc)
+    jmax = np.array([x.shape[1] for x in xs], dtype=np.intc)
+    xp = (_lib._dp * n)(*[_lib.dptr(x) for x in xs])
+    yp = (_lib._dp * n)(*[_lib.dptr(y) for y in ys])
+    out = SweepResult(workers=1)
+    t0 = time.perf_counter()
+    h = c_void_p()
+    _lib.check(_lib.lib().v2d_batch_create(n, _lib.iptr(imax), _lib.iptr(jmax), xp, yp, params,
+                                            byref(h)), "batch_create")
+    out.setup_s = time.perf_counter() - t0
+    results = [CaseResult(c.name, c.re, c.alpha_deg, int(imax[i] * jmax[i]), False, 0, math.inf)
+               for i, c in enumerate(cases)]
+    active = np.ones(n, dtype=np.intc)
+    first = np.full(n, np.nan)
+    res = np.zeros(n)
+    flags = np.zeros(n, dtype=np.intc)
+    try:
+        t1 = time.perf_counter()
+        for it in range(max_newton):
+            st = _lib.LinStats()
+            code = _lib.lib().v2d_batch_newton(h, _lib.dptr(res), _lib.iptr(flags), byref(st))
+            if code == _lib.V2D_ENONFINITE:
+                # instances with a non-finite residual: diverged, frozen; the
+                # others are advanced by the next call
+                for i in np.nonzero(flags & 6)[0]:
+                    results[i].diverged = True
+                    results[i].error = "non-finite residual"
+                    active[i] = 0
+                _lib.check(_lib.lib().v2d_batch_set_active(h, _lib.iptr(active)))
+                if not active.any():
+                    break
+                continue
+            if code not in (_lib.V2D_OK, _lib.V2D_ENOTCONVERGED):
+                _lib.check(code, "batch_newton")
+            for i in np.nonzero(active)[0]:
+                r = results[i]
+                r.newton_iters += 1
+                r.krylov_iters += st.iterations
+                r.res = float(res[i])
+                if np.isnan(first[i]):
+                    first[i] = res[i]
+                if not np.isfinite(res[i]) or res[i] > diverge_factor * first[i]:
+                    r.diverged = True
+                    active[i] = 0
+                elif res[i] <= pseudo_tol:
+                    r.converged = True
+                    active[i] = 0
+            _lib.check(_lib.lib().v2d_batch_set_active(h, _lib.iptr(active)))
+            if not active.any():
+                break
+        out.solve_s = time.perf_counter() - t1
+        for i, (c, r) in enumerate(zip(cases, results)):
+            r.re_reached = c.re if r.converged else math.nan
+            r.rungs = 1
+            if r.converged:
+                s = c_void_p()
+                _lib.check(_lib.lib().v2d_batch_instance(h, i, byref(s)))
+                f10 = np.zeros(10)
+                rl = -1.0 if c.ref_length is None else float(c.ref_length)
+                _lib.check(_lib.lib().v2d_solver_forces(s, float(c.re), rl, 0.0, 0.0,
+                                                        _lib.dptr(f10)))
+                r.cd, r.cl, r.cm = float(f10[0]), float(f10[1]), float(f10[2])
+    finally:
+        _lib.lib().v2d_batch_destroy(h)
     out.results = results
     return out

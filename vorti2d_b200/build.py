@@ -32,6 +32,7 @@ SOURCES = [
     ("v2d_velocity.cu", ["-fmad=false"]),
     ("v2d_linsys.cu", []),
     ("v2d_shape.cu", ["-fmad=false"]),
+    ("v2d_batch.cu", []),
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -105,7 +105,7 @@ int build_pattern(GridDev &g, const AsmParams &p, cudaStream_t s)
 // a shared-memory copy of the range, and the block then writes the range with
 // coalesced stores (one row per thread would scatter every warp store over
 // 32 rows).
-constexpr int kAsmNodes = 128;
+constexpr int kAsmNodes = kAsmNodesHost;
 
 // One block of kAsmNodes nodes starting at node K0 (blockDim.x == kAsmNodes).
 template <bool W32>
@@ -211,6 +211,65 @@ __global__ void __launch_bounds__(kAsmNodes) assemble_newton(GlobalTopo T, Coeff
     __shared__ double stage[kAsmNodes * kOmeMax];
     for (int K0 = blockIdx.x * kAsmNodes; K0 < T.N; K0 += gridDim.x * kAsmNodes)
         assemble_block<W32>(T, c, f, rowptr, val, val32, b, dinv, dinv32, flag, K0, stage);
+}
+
+// Many instances' Newton systems in one launch (the batched sweep): block
+// kb belongs to the instance i with blk0[i] <= kb < blk0[i + 1] and covers its
+// nodes from (kb - blk0[i]) * kAsmNodes.  An active instance assembles into
+// its slices of the combined value and right-hand side arrays; a frozen one
+// (converged or given up) writes identity rows with a zero right-hand side,
+// so its update is zero and the combined pattern stays fixed.  flags[i] gets
+// the instance's assembly flags (bit 1: non-finite right-hand side).
+template <bool W32>
+__global__ void __launch_bounds__(kAsmNodes) assemble_batch(const BatchInst *__restrict__ inst,
+                                                            int ninst, const int *__restrict__ blk0,
+                                                            const int *__restrict__ active,
+                                                            double *val, float *val32, double *b,
+                                                            int *flags)
+{
+    __shared__ double stage[kAsmNodes * kOmeMax];
+    const int kb = blockIdx.x;
+    int lo = 0, hi = ninst;   // largest i with blk0[i] <= kb
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        if (blk0[mid] <= kb) lo = mid;
+        else hi = mid;
+    }
+    const BatchInst I = inst[lo];
+    const int K0 = (kb - blk0[lo]) * kAsmNodes;
+    double *v = val + I.nnz_off;
+    float *v32 = W32 ? val32 + I.nnz_off : nullptr;
+    double *bb = b + I.row_off;
+    if (active[lo]) {
+        assemble_block<W32>(I.T, I.c, I.f, I.rowptr, v, v32, bb, nullptr, nullptr, flags + lo,
+                            K0, stage);
+        return;
+    }
+    const int N = I.T.N, K = K0 + threadIdx.x;
+    if (K >= N) return;
+    for (int r : {K, N + K}) {
+        for (int p = I.rowptr[r]; p < I.rowptr[r + 1]; ++p) {
+            const double x = I.colind[p] == r ? 1.0 : 0.0;
+            v[p] = x;
+            if (W32) v32[p] = (float)x;
+        }
+        bb[r] = 0.0;
+    }
+}
+
+int launch_assemble_batch(const BatchInst *d_inst, int ninst, const int *d_blk0, int nblocks,
+                          const int *d_active, bool want32, double *val, float *val32, double *b,
+                          int *d_flags, cudaStream_t s)
+{
+    if (want32)
+        assemble_batch<true><<<nblocks, kAsmNodes, 0, s>>>(d_inst, ninst, d_blk0, d_active, val,
+                                                           val32, b, d_flags);
+    else
+        assemble_batch<false><<<nblocks, kAsmNodes, 0, s>>>(d_inst, ninst, d_blk0, d_active, val,
+                                                            val32, b, d_flags);
+    V2D_CUDA_TRY(cudaGetLastError());
+    count_launches(1);
+    return V2D_OK;
 }
 
 // Right-hand side b = -R of the Newton system only (no Jacobian values), for

@@ -3,6 +3,7 @@
 
 #include <vector>
 
+#include "v2d_stencil.cuh"
 #include "v2d_util.cuh"
 
 namespace v2d {
@@ -36,6 +37,25 @@ int launch_metrics(GridDev &g, cudaStream_t s);
 int launch_assemble(GridDev &g, const AsmParams &p, bool want32, int *d_flag, cudaStream_t s);
 // b = -R at the handle's state for the given scalar parameters (no CSR writes).
 int launch_residual(const GridDev &g, const AsmParams &p, double *d_b, cudaStream_t s);
+
+// One instance of a batched assembly (v2d_batch.cu): its grid, scalars and
+// fields, its own CSR pattern, and where its rows and entries sit in the
+// combined block-diagonal system.
+struct BatchInst {
+    GlobalTopo T;
+    Coeffs c;
+    Fields f;
+    const int *rowptr, *colind;
+    long long nnz_off;
+    int row_off;
+};
+// nodes per assembly block (one thread per node)
+constexpr int kAsmNodesHost = 128;
+// All instances' Newton systems in one launch of nblocks = sum ceil(N_i /
+// kAsmNodesHost) blocks; d_blk0 (ninst + 1) holds each instance's first block.
+int launch_assemble_batch(const BatchInst *d_inst, int ninst, const int *d_blk0, int nblocks,
+                          const int *d_active, bool want32, double *val, float *val32, double *b,
+                          int *d_flags, cudaStream_t s);
 
 // v2d_velocity.cu (vorti2d/velocity.py:76-93); vmag may be null
 int launch_velocity(int imax, int jmax, double dksi, double deta, const double *jac,
@@ -141,6 +161,11 @@ int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_c
 int mf_plan_create(int imax, int jmax, int n, const int *h_rowptr, const int *h_colind, int leaf,
                    MfPlan **out);
 void mf_plan_destroy(MfPlan *p);
+// One plan over several host plans (mf_plan_build) of the diagonal blocks of a
+// block-diagonal system: row_off / nnz_off place each block's rows and CSR
+// entries in the combined system of n rows (v2d_mf.cu).
+int mf_plan_forest(const std::vector<MfPlan *> &parts, const std::vector<int> &row_off,
+                   const std::vector<long long> &nnz_off, int n, MfPlan **out);
 // fp32: FP32 solve; fact64 (with fp32): FP64 factorization rounded to FP32.
 int mf_factor_create(const MfPlan *P, int fp32, int fact64, MfFactor **out);
 void mf_factor_destroy(MfFactor *M);

@@ -621,12 +621,10 @@ int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_c
     return V2D_OK;
 }
 
-int mf_plan_create(int imax, int jmax, int n, const int *h_rowptr, const int *h_colind,
-                   int leaf, MfPlan **out)
+// Device copies of a host plan's arrays; the host copies of the large index
+// arrays are released.  On failure the plan is destroyed.
+static int mf_plan_upload(MfPlan *P)
 {
-    *out = nullptr;
-    MfPlan *P = nullptr;
-    V2D_TRY(mf_plan_build(imax, jmax, n, h_rowptr, h_colind, leaf, &P));
     int st_up = V2D_OK;
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_S, P->S);
     if (st_up == V2D_OK) st_up = upload_vec(&P->d_f, P->f);
@@ -654,6 +652,169 @@ int mf_plan_create(int imax, int jmax, int n, const int *h_rowptr, const int *h_
     std::vector<int>().swap(P->h_asm_csr);
     std::vector<int>().swap(P->h_asm_row);
     std::vector<long long>().swap(P->h_asm_pos);
+    return V2D_OK;
+}
+
+int mf_plan_create(int imax, int jmax, int n, const int *h_rowptr, const int *h_colind,
+                   int leaf, MfPlan **out)
+{
+    *out = nullptr;
+    MfPlan *P = nullptr;
+    V2D_TRY(mf_plan_build(imax, jmax, n, h_rowptr, h_colind, leaf, &P));
+    V2D_TRY(mf_plan_upload(P));
+    *out = P;
+    return V2D_OK;
+}
+
+// One plan for a block-diagonal system of several O-grid systems: the union
+// of their front trees (a forest), fronts renumbered level by level across
+// the parts, each part's variables, CSR entries and factor positions shifted
+// by its offsets.  The factorization and the solve then treat every part in
+// the same launches.  parts are host plans (mf_plan_build); row_off[k] and
+// nnz_off[k] place part k's rows and CSR entries in the combined system of
+// n rows.
+int mf_plan_forest(const std::vector<MfPlan *> &parts, const std::vector<int> &row_off,
+                   const std::vector<long long> &nnz_off, int n, MfPlan **out)
+{
+    *out = nullptr;
+    const int np = (int)parts.size();
+    V2D_ARG_CHECK(np > 0 && (int)row_off.size() == np && (int)nnz_off.size() == np,
+                  "mf_plan_forest: %d parts, %zu row offsets, %zu entry offsets", np,
+                  row_off.size(), nnz_off.size());
+    int nl = 0;
+    for (const MfPlan *Q : parts) {
+        V2D_ARG_CHECK(Q && !Q->h_vars.empty(), "mf_plan_forest: a part without host arrays");
+        nl = std::max(nl, Q->nlevel);
+    }
+    MfPlan *P = new MfPlan();
+    P->n = n;
+    P->nlevel = nl;
+    // new front ids: level-major, parts in order within a level
+    std::vector<std::vector<int>> nid(np);
+    int nf = 0;
+    P->lvl_off.assign(nl + 1, 0);
+    for (int L = 0; L < nl; ++L) {
+        P->lvl_off[L] = nf;
+        for (int k = 0; k < np; ++k) {
+            const MfPlan *Q = parts[k];
+            if (nid[k].empty()) nid[k].assign(Q->nfront, -1);
+            if (L >= Q->nlevel) continue;
+            for (int q = Q->lvl_off[L]; q < Q->lvl_off[L + 1]; ++q) nid[k][q] = nf++;
+        }
+    }
+    P->lvl_off[nl] = nf;
+    P->nfront = nf;
+    P->S.assign(nf, 0); P->f.assign(nf, 0); P->voff.assign(nf, 0); P->uoff.assign(nf, 0);
+    P->child0.assign(nf, -1); P->child1.assign(nf, -1); P->parent.assign(nf, -1);
+    P->foff.assign(nf, 0);
+    std::vector<int> part_of(nf), old_of(nf);
+    for (int k = 0; k < np; ++k)
+        for (int q = 0; q < parts[k]->nfront; ++q) {
+            part_of[nid[k][q]] = k;
+            old_of[nid[k][q]] = q;
+        }
+    long long ftot = 0;
+    int vtot = 0, utot = 0;
+    for (int id = 0; id < nf; ++id) {
+        const MfPlan *Q = parts[part_of[id]];
+        const int q = old_of[id], k = part_of[id];
+        P->S[id] = Q->S[q];
+        P->f[id] = Q->f[q];
+        P->voff[id] = vtot; vtot += Q->f[q];
+        P->uoff[id] = utot; utot += Q->f[q] - Q->S[q];
+        P->foff[id] = ftot; ftot += (long long)Q->f[q] * Q->f[q];
+        if (Q->child0[q] >= 0) P->child0[id] = nid[k][Q->child0[q]];
+        if (Q->child1[q] >= 0) P->child1[id] = nid[k][Q->child1[q]];
+        if (Q->parent[q] >= 0) P->parent[id] = nid[k][Q->parent[q]];
+        P->maxS = std::max(P->maxS, Q->S[q]);
+        P->maxf = std::max(P->maxf, Q->f[q]);
+        P->flops += 2.0 * Q->S[q] * (double)Q->f[q] * Q->f[q];
+        P->apply_entries += (long long)Q->S[q] * (2LL * Q->f[q] - Q->S[q]);
+    }
+    P->ftotal = ftot; P->vtotal = vtot; P->utotal = utot;
+    P->lvl_maxS.assign(nl, 0); P->lvl_maxf.assign(nl, 0); P->lvl_maxm.assign(nl, 0);
+    P->lvl_maxm_child.assign(nl, 0);
+    P->lvl_fbeg.assign(nl, 0); P->lvl_fend.assign(nl, 0);
+    P->lvl_abeg.assign(nl, 0); P->lvl_aend.assign(nl, 0);
+    P->toff.assign(nf, 0);
+    P->goff.assign(nf, 0);
+    for (int L = 0; L < nl; ++L) {
+        const int a = P->lvl_off[L], b = P->lvl_off[L + 1];
+        long long t = 0, g = 0;
+        for (int id = a; id < b; ++id) {
+            P->lvl_maxS[L] = std::max(P->lvl_maxS[L], P->S[id]);
+            P->lvl_maxf[L] = std::max(P->lvl_maxf[L], P->f[id]);
+            P->lvl_maxm[L] = std::max(P->lvl_maxm[L], P->f[id] - P->S[id]);
+            for (int c : {P->child0[id], P->child1[id]})
+                if (c >= 0) P->lvl_maxm_child[L] = std::max(P->lvl_maxm_child[L], P->f[c] - P->S[c]);
+            P->toff[id] = t;
+            t += (long long)P->S[id] * P->S[id];
+            P->goff[id] = g;
+            g += 2LL * P->S[id] * (P->f[id] - P->S[id]);
+        }
+        P->tmax = std::max(P->tmax, t);
+        P->gmax = std::max(P->gmax, g);
+        if (b > a) {
+            P->lvl_fbeg[L] = P->foff[a];
+            P->lvl_fend[L] = P->foff[b - 1] + (long long)P->f[b - 1] * P->f[b - 1];
+        }
+    }
+    // front variables (shifted rows) and contribution maps (front-local)
+    P->h_vars.resize(vtot);
+    P->h_cbmap.resize(utot);
+    for (int id = 0; id < nf; ++id) {
+        const MfPlan *Q = parts[part_of[id]];
+        const int q = old_of[id], ro = row_off[part_of[id]];
+        for (int t = 0; t < Q->f[q]; ++t) P->h_vars[P->voff[id] + t] = Q->h_vars[Q->voff[q] + t] + ro;
+        for (int t = 0; t < Q->f[q] - Q->S[q]; ++t)
+            P->h_cbmap[P->uoff[id] + t] = Q->h_cbmap[Q->uoff[q] + t];
+    }
+    // assembly entries, level by level: each part's entries of the level with
+    // shifted CSR entry, row and factor position (the front of an entry is
+    // the one whose storage holds its position)
+    long long nasm = 0;
+    for (const MfPlan *Q : parts) nasm += Q->nasm;
+    P->nasm = nasm;
+    P->h_asm_csr.resize(nasm);
+    P->h_asm_row.resize(nasm);
+    P->h_asm_pos.resize(nasm);
+    long long o = 0;
+    for (int L = 0; L < nl; ++L) {
+        P->lvl_abeg[L] = o;
+        for (int k = 0; k < np; ++k) {
+            const MfPlan *Q = parts[k];
+            if (L >= Q->nlevel) continue;
+            int q = Q->lvl_off[L];
+            for (long long e = Q->lvl_abeg[L]; e < Q->lvl_aend[L]; ++e, ++o) {
+                const long long pos = Q->h_asm_pos[e];
+                while (q + 1 < Q->lvl_off[L + 1] && pos >= Q->foff[q + 1]) ++q;
+                if (pos < Q->foff[q] || pos >= Q->foff[q] + (long long)Q->f[q] * Q->f[q]) {
+                    set_error("mf_plan_forest: assembly entry outside its level's fronts");
+                    mf_plan_destroy(P);
+                    return V2D_EARG;
+                }
+                P->h_asm_csr[o] = (int)(Q->h_asm_csr[e] + nnz_off[k]);
+                P->h_asm_row[o] = Q->h_asm_row[e] + row_off[k];
+                P->h_asm_pos[o] = P->foff[nid[k][q]] + (pos - Q->foff[q]);
+            }
+        }
+        P->lvl_aend[L] = o;
+    }
+    bool ok = o == nasm;
+    for (int v : P->h_vars) ok = ok && v >= 0 && v < n;
+    for (long long e = 0; e < nasm && ok; ++e)
+        ok = P->h_asm_pos[e] >= 0 && P->h_asm_pos[e] < ftot && P->h_asm_row[e] >= 0 &&
+             P->h_asm_row[e] < n && P->h_asm_csr[e] >= 0;
+    if (!ok) {
+        set_error("mf_plan_forest: index check failed");
+        mf_plan_destroy(P);
+        return V2D_EARG;
+    }
+    if (items_build(P) != V2D_OK) {
+        mf_plan_destroy(P);
+        return V2D_EARG;
+    }
+    V2D_TRY(mf_plan_upload(P));
     *out = P;
     return V2D_OK;
 }
