@@ -136,10 +136,10 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------- our arm
-def make_solver(v, xg, yg, precision, lu_reuse=0, lu_steps=0):
+def make_solver(v, xg, yg, precision, lu_reuse=0, lu_steps=0, item_rows=None):
     cfg = v.Config(verbose=False, write_csv=False, write_xdmf=False, compute_forces=False,
                    raise_on_linear_failure=False, precision=precision, lu_reuse_its=lu_reuse,
-                   lu_reuse_steps=bool(lu_steps), **WORKLOAD, **SOLVER)
+                   lu_reuse_steps=bool(lu_steps), lu_item_rows=item_rows, **WORKLOAD, **SOLVER)
     return v.Solver(cfg, mesh=(xg, yg))
 
 
@@ -530,8 +530,10 @@ def profile_lu_launches(args):
         out[label] = {"total_ms": sum(t for _, _, t in rows), "launches": len(rows),
                       "by_kind_ms": by_kind,
                       "per_launch_us": [[kind, lvl, round(1e3 * t, 2)] for kind, lvl, t in rows]}
+    if SOLVER.get("lu_solve", "flow") == "flow":
+        out["dataflow_trace"] = lu_trace_summary(s)
     fkinds = ["rowscale", "scatter", "extend_add", "panel", "l21_swap_trsm", "-", "gemm", "trinv",
-              "trcopy", "gh", "ghcopy"]
+              "trcopy", "gh", "ghcopy", "round_f32"]
     cap = 1024
     ms = (ctypes.c_double * cap)()
     codes = (ctypes.c_int * cap)()
@@ -546,6 +548,37 @@ def profile_lu_launches(args):
                      "by_kind_ms": by_kind, "by_level_ms": by_level}
     print(json.dumps(out), flush=True)
     s.close()
+
+
+def lu_trace_summary(s):
+    """Per level and sweep of one dataflow LU solve (v2d_solver_trace_lu_apply):
+    items, the time from the solve's start to the level's first item start
+    and last item end, the mean time an item runs and the mean time it
+    waited for its dependencies (us)."""
+    import ctypes
+    from vorti2d_b200 import _lib
+    cap = 1 << 20
+    ticks = np.zeros(3 * cap, dtype=np.uint64)
+    items = np.zeros(12 * cap, dtype=np.intc)
+    n = ctypes.c_int()
+    _lib.check(_lib.lib().v2d_solver_trace_lu_apply(
+        s.dev.h, ticks.ctypes.data_as(ctypes.POINTER(ctypes.c_ulonglong)), _lib.iptr(items), cap,
+        ctypes.byref(n)))
+    n = n.value
+    t = ticks[:3 * n].reshape(n, 3).astype(np.float64) * 1e-3
+    it = items[:12 * n].reshape(n, 12)
+    t -= t[:, 0].min()
+    levels = []
+    for sweep in (0, 1):
+        for L in sorted(set(it[it[:, 0] == sweep, 10].tolist()), reverse=bool(sweep)):
+            sel = (it[:, 0] == sweep) & (it[:, 10] == L)
+            levels.append({"sweep": ["fwd", "bwd"][sweep], "level": int(L),
+                           "items": int(sel.sum()),
+                           "first_start_us": round(float(t[sel, 0].min()), 2),
+                           "last_end_us": round(float(t[sel, 2].max()), 2),
+                           "mean_run_us": round(float(np.mean(t[sel, 2] - t[sel, 1])), 2),
+                           "mean_wait_us": round(float(np.mean(t[sel, 1] - t[sel, 0])), 2)})
+    return {"total_us": round(float(t[:, 2].max()), 2), "items": n, "levels": levels}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -564,6 +597,12 @@ def run_ours(args, rank, world, local_rank):
         times = s.times()
         for m in range(W):
             s.advance(times[m])
+            if m == 0 and args.lu_tune:
+                # work-item split of the LU solve, tuned on this solver's
+                # factors after the first warm-up step (the remaining ones
+                # capture the GMRES graphs with the chosen split)
+                from vorti2d_b200.tune import tune_lu_solve
+                results.setdefault("lu_tuning", {})[prec] = tune_lu_solve(s)
         barrier(world)
         torch.cuda.synchronize()
         clocks = ClockSampler(local_rank).start() if prec == legs[0] else None
@@ -603,7 +642,8 @@ def run_ours(args, rank, world, local_rank):
             results["nnz"] = nnz.value
             # e2e: the same steps again through the public API, with the
             # state copied host->device and back every step
-            s2 = make_solver(v, xg, yg, prec, args.lu_reuse, args.lu_reuse_steps)
+            rows = results.get("lu_tuning", {}).get(prec, {}).get("rows")
+            s2 = make_solver(v, xg, yg, prec, args.lu_reuse, args.lu_reuse_steps, rows)
             for m in range(W):
                 s2.advance(times[m])
             results["e2e"] = _e2e(torch, v, s2, times, W, K, flush_buf)
@@ -752,6 +792,9 @@ def main():
     ap.add_argument("--lu-factors", default="fp32", choices=["fp32", "fp64"],
                     help="mixed leg: LU factorization in FP32, or in FP64 rounded to FP32 "
                          "for the FP32 solve")
+    ap.add_argument("--lu-tune", type=int, default=1, choices=[0, 1],
+                    help="tune the LU solve's work-item split on the warmed-up solver before "
+                         "timing (vorti2d_b200.tune)")
     ap.add_argument("--lu-solve", default="flow", choices=["flow", "levels"],
                     help="LU preconditioner solve: one dataflow launch over the front tree "
                          "(flow) or one launch per level and sweep (levels)")
@@ -925,6 +968,7 @@ def main():
         "gpu_launches": int(launches.get(head, 0)),
         "clocks": res.get("clocks"),
         "legs": {p: res[p] for p in ("mixed", "fp64") if p in res},
+        "lu_tuning": res.get("lu_tuning"),
     }
     if "mixed" in res and "fp64" in res:
         line["mixed_vs_fp64_speedup"] = res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"]

@@ -374,8 +374,8 @@ int v2d_lu_plan_info(int imax, int jmax, const int *indptr, const int *indices, 
  * reference counterpart): info4 = {work items, dependency counters, fronts,
  * levels}; when cap_items >= items, items gets 12 ints per item (kind 0
  * forward / 1 backward, front, first row, end row, wait counter and target,
- * second wait counter and target, two done counters, 0, 0; -1 for none);
- * when cap_fronts >= fronts, fronts3 gets each front's pivots S, size f and
+ * second wait counter and target, two done counters, tree level, 0; -1 for
+ * none); when cap_fronts >= fronts, fronts3 gets each front's pivots S, size f and
  * parent (-1 at the root).  Items run in this order in the one-launch
  * dataflow solve; the plan checks that every wait is met by earlier items. */
 int v2d_lu_solve_plan(int imax, int jmax, const int *indptr, const int *indices, int leaf,
@@ -396,6 +396,23 @@ int v2d_solver_phase_times(v2d_solver *s, double *out6, int reset);
  * H = U11^-1 U12, which hold as many entries as L21 and U12). */
 int v2d_solver_time_lu_apply(v2d_solver *s, int reps, long long flush_bytes, double *ms_avg,
                              long long *factor_bytes);
+
+/* Measurement aid (no reference counterpart): one dataflow LU solve of the
+ * current factors with a trace of every work item -- global-timer ns at its
+ * ticket, at the end of its dependency wait and after its done counters
+ * (ticks[3 i + k]) -- and the item table (items: 12 ints per item as in
+ * v2d_lu_solve_plan, may be null); cap >= items, *n = items. */
+int v2d_solver_trace_lu_apply(v2d_solver *s, unsigned long long *ticks, int *items, int cap,
+                              int *n);
+
+/* Tuning aid (no reference counterpart): the work-item granularity of the
+ * LU preconditioner solve, rows[L] rows of a front per work item on tree
+ * level L (0: whole fronts); rows may be null to only read the current
+ * setting into out_rows (cap >= levels) and *nlevels_out.  Every setting
+ * forms the same products; only how the rows are split over CTAs (and the
+ * order of a row's partial sums) changes. */
+int v2d_solver_lu_item_rows(v2d_solver *s, const int *rows, int nlevels, int *out_rows, int cap,
+                            int *nlevels_out);
 
 /* Measurement aid (no reference counterpart): the device time of each
  * launch of one LU preconditioner solve, averaged over `reps` solves (each

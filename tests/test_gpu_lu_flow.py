@@ -70,3 +70,32 @@ def test_launch_lists_181(v2d, oracle_mod):
         s.close()
     print(f"LU solve 181x181 mixed, warm: levels {totals['levels']:.3f} ms, "
           f"dataflow {totals['flow']:.3f} ms")
+
+
+def test_tuned_item_split_gives_the_same_newton_update(v2d, oracle_mod, tmp_path):
+    """The autotuner's split (vorti2d_b200.tune) is recorded to a file, read
+    back into a fresh solver, and the Newton update with it equals the
+    default split's to 1e-10 relative (the same products, partial sums in a
+    split-dependent order, each solve to its tolerance)."""
+    from vorti2d_b200 import tune
+    xg, yg = oracle_mod.generate_cylinder(65, 49)
+    M = oracle_mod.core().compute_metrics(1 / 64, 1 / 48, xg, yg)
+    st = smooth_state(M[8], M[9])
+    path = str(tmp_path / "lu_tuning.json")
+
+    def update(s):
+        s.set_state(*st)
+        code, _, _ = s.dev.newton(0.3)
+        assert code == 0, v2d._lib.last_error()
+        return np.concatenate(s.dev.get_state()[:2]) - np.concatenate(st[:2])
+
+    s = _solver(v2d, xg, yg, "outflow", "mixed", "flow")
+    default = update(s)
+    rec = tune.tune_lu_solve(s, sweeps=1, reps=5, path=path)
+    assert len(rec["rows"]) == len(tune.item_rows(s)) and rec["ms"] <= rec["default_ms"]
+    s.close()
+    s = _solver(v2d, xg, yg, "outflow", "mixed", "flow")
+    assert tune.load_tuning(s, path) and tune.item_rows(s) == rec["rows"]
+    tuned = update(s)
+    s.close()
+    assert np.max(np.abs(default - tuned)) <= 1e-10 * np.abs(default).max()

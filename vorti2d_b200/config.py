@@ -86,6 +86,10 @@ class Config:
     ``"fp64"`` factors in FP64 and rounds the factors to FP32 for the FP32
     solve (more accurate pivots and updates, the same bytes per solve).  The
     FP64 form always factors in FP64."""
+    lu_item_rows: list | None = None
+    """LU preconditioner solve: rows per work item on each tree level (0:
+    whole fronts), e.g. from ``vorti2d_b200.tune``; None keeps the default
+    split."""
     lu_solve: str = "flow"
     """LU preconditioner solve: ``"flow"`` runs each application as one
     dataflow launch over the whole front tree; ``"levels"`` as one launch per

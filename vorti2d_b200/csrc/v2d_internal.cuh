@@ -107,7 +107,9 @@ struct MfPlan {
     // checked when the plan is built (see items_build).
     int nitems = 0, nctr = 0;
     std::vector<int> h_items, lvl_fwd, lvl_bwd;
+    std::vector<int> item_rows;    // rows per item of each level (0: whole fronts)
     int *d_items = nullptr;
+    long long items_ver = 0;       // bumped whenever d_items is replaced
     // host copies, kept only between the build and the upload
     std::vector<int> h_vars, h_cbmap, h_asm_csr, h_asm_row;
     std::vector<long long> h_asm_pos;
@@ -137,7 +139,7 @@ struct MfFactor {
     int *ipiv = nullptr, *perm = nullptr, *flag = nullptr;
     MfBarrier *bar = nullptr;
     int *sctr = nullptr;        // dataflow solve: 3 counters per front + the work ticket
-    int flow_grid = 0;          // CTAs of the dataflow solve
+    int flow_grid = 0;          // most CTAs of the dataflow solve resident at once
     int flow = 1;               // 1: the solve is one dataflow launch; 0: one launch per level
                                 // and sweep
     cudaGraphExec_t graph = nullptr;
@@ -166,6 +168,9 @@ void mf_plan_destroy(MfPlan *p);
 // entries in the combined system of n rows (v2d_mf.cu).
 int mf_plan_forest(const std::vector<MfPlan *> &parts, const std::vector<int> &row_off,
                    const std::vector<long long> &nnz_off, int n, MfPlan **out);
+// Work-item granularity of the solve per level (rows per item, 0: whole
+// fronts); replaces the device item table.
+int mf_plan_set_item_rows(MfPlan *P, const int *rows, int nlevels);
 // fp32: FP32 solve; fact64 (with fp32): FP64 factorization rounded to FP32.
 int mf_factor_create(const MfPlan *P, int fp32, int fact64, MfFactor **out);
 void mf_factor_destroy(MfFactor *M);
@@ -189,6 +194,10 @@ int mf_check_barrier(MfFactor *M, cudaStream_t s);
 // write of flush_bytes (evicts L2); CUDA events on stream s.
 int mf_time_apply(const MfPlan *P, const MfFactor *M, int reps, size_t flush_bytes, cudaStream_t s,
                   double *ms_avg);
+// One dataflow solve with per-item global-timer ticks (3 per item: ticket,
+// end of wait, done); *n = items.
+int mf_trace_apply(const MfPlan *P, const MfFactor *M, cudaStream_t s, unsigned long long *ticks,
+                   int cap, int *n);
 // Per-launch device time of one solve (average of reps), with the launch
 // codes (kind * 1000 + level; kinds: 0 forward level, 1 backward level,
 // 2 the dataflow launch); *n receives the number of launches.

@@ -94,6 +94,7 @@ struct KrylovWork {
     int graph_pc[2] = {-1, -1};
     const void *graph_lu[2] = {nullptr, nullptr};
     int graph_lu_flow[2] = {-1, -1};   // the LU solve form the graph was captured with
+    long long graph_lu_items[2] = {-1, -1};   // and the plan's work-item table
 };
 
 // ---------------------------------------------------------------- helpers
@@ -667,6 +668,7 @@ static int capture_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, doub
     w->graph_pc[which] = precond;
     w->graph_lu[which] = lu ? (const void *)A.lu : nullptr;
     w->graph_lu_flow[which] = lu ? A.lu->flow : -1;
+    w->graph_lu_items[which] = lu ? A.lu_plan->items_ver : -1;
     return V2D_OK;
 }
 
@@ -679,7 +681,8 @@ static int run_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, double *
     if (w->seg[which].empty() || !w->fin[which] || w->graph_m[which] != w->m ||
         w->graph_pc[which] != precond ||
         w->graph_lu[which] != (lu ? (const void *)A.lu : nullptr) ||
-        w->graph_lu_flow[which] != (lu ? A.lu->flow : -1))
+        w->graph_lu_flow[which] != (lu ? A.lu->flow : -1) ||
+        w->graph_lu_items[which] != (lu ? A.lu_plan->items_ver : -1))
         V2D_TRY(capture_cycle<T>(w, which, V, wv, z, Z, x, A, precond, s));
     for (size_t q = 0; q < w->seg[which].size(); ++q) {
         V2D_CUDA_TRY(cudaGraphLaunch(w->seg[which][q], s));

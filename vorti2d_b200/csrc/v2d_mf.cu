@@ -230,15 +230,23 @@ static int items_build(MfPlan *P)
     it.clear();
     P->lvl_fwd.assign(nl + 1, 0);
     P->lvl_bwd.assign(nl + 1, 0);
-    auto per = [&](int L) {
-        return P->lvl_off[L + 1] - P->lvl_off[L] >= kFrontPerCtaHost ? INT_MAX : kSolveRowsHost;
-    };
+    // rows per item of each level (0: whole fronts); the default: whole fronts
+    // where a level has at least kFrontPerCtaHost fronts, kSolveRowsHost rows
+    // above
+    if ((int)P->item_rows.size() != nl) {
+        P->item_rows.assign(nl, kSolveRowsHost);
+        for (int L = 0; L < nl; ++L)
+            if (P->lvl_off[L + 1] - P->lvl_off[L] >= kFrontPerCtaHost) P->item_rows[L] = 0;
+    }
+    auto per = [&](int L) { return P->item_rows[L] > 0 ? P->item_rows[L] : INT_MAX; };
+    int cur_level = 0;
     auto push = [&](int kind, int q, int rb, int re) {
-        const int v[12] = {kind, q, rb, re, -1, 0, -1, 0, -1, -1, 0, 0};
+        const int v[12] = {kind, q, rb, re, -1, 0, -1, 0, -1, -1, cur_level, 0};
         it.insert(it.end(), v, v + 12);
     };
     for (int L = 0; L < nl; ++L) {
         P->lvl_fwd[L] = (int)it.size() / 12;
+        cur_level = L;
         const int R = per(L);
         for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q)
             for (int rb = 0; rb < P->f[q]; rb += std::min(R, P->f[q]))
@@ -247,6 +255,7 @@ static int items_build(MfPlan *P)
     P->lvl_fwd[nl] = (int)it.size() / 12;
     for (int L = nl - 1; L >= 0; --L) {
         P->lvl_bwd[L + 1] = (int)it.size() / 12;
+        cur_level = L;
         const int R = per(L);
         for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q)
             for (int rb = 0; rb < P->S[q]; rb += std::min(R, P->S[q]))
@@ -663,6 +672,32 @@ int mf_plan_create(int imax, int jmax, int n, const int *h_rowptr, const int *h_
     V2D_TRY(mf_plan_build(imax, jmax, n, h_rowptr, h_colind, leaf, &P));
     V2D_TRY(mf_plan_upload(P));
     *out = P;
+    return V2D_OK;
+}
+
+// New work-item granularity for the solve: rows[L] rows per item on level L
+// (0: whole fronts; otherwise a positive multiple of 1).  Rebuilds and
+// re-uploads the item table (its order is checked again); the device pointer
+// changes, so solves captured in graphs before must be captured again
+// (items_ver counts the tables).
+int mf_plan_set_item_rows(MfPlan *P, const int *rows, int nlevels)
+{
+    V2D_ARG_CHECK(rows && nlevels == P->nlevel, "lu item rows: %d levels given, the plan has %d",
+                  nlevels, P->nlevel);
+    for (int L = 0; L < nlevels; ++L)
+        V2D_ARG_CHECK(rows[L] >= 0, "lu item rows: level %d: %d", L, rows[L]);
+    std::vector<int> keep = P->item_rows;
+    P->item_rows.assign(rows, rows + nlevels);
+    if (items_build(P) != V2D_OK) {
+        P->item_rows = keep;
+        items_build(P);
+        return V2D_EARG;
+    }
+    int *d = nullptr;
+    V2D_TRY(upload_vec(&d, P->h_items));
+    if (P->d_items) cudaFree(P->d_items);
+    P->d_items = d;
+    ++P->items_ver;
     return V2D_OK;
 }
 
@@ -1900,6 +1935,14 @@ __device__ __forceinline__ int ld_acquire_gpu(const int *p)
     return v;
 }
 
+// Global nanosecond timer (per-item traces of the dataflow solve).
+__device__ __forceinline__ unsigned long long globaltimer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
 // Bounded wait until *ctr >= target; false if it ran out or another CTA
 // reported an error meanwhile.
 __device__ __forceinline__ bool wait_count(const int *ctr, int target, volatile int *err)
@@ -1927,7 +1970,7 @@ template <class T>
 __global__ void __launch_bounds__(kSolveThreads, 2) k_solve_flow(
     const MfDev D, const T *F, const T *b, const double *__restrict__ rs, T *zbuf, T *upd, T *x,
     const SolveItemDev *__restrict__ items, int nitems, int *ctr, int nctr, MfBarrier *bar,
-    const int *stop_a, const int *stop_b)
+    const int *stop_a, const int *stop_b, unsigned long long *trace)
 {
     if (stopped(stop_a, stop_b)) return;   // the flags are the same for every CTA
     extern __shared__ unsigned char smem_raw[];
@@ -1941,6 +1984,7 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_solve_flow(
         const int i = item_s;
         if (i >= nitems) return;
         const SolveItemDev it = items[i];
+        if (trace && threadIdx.x == 0) trace[3 * i] = globaltimer_ns();
         SolveItemCtx<T> c;
         c.pre(D, F, b, rs, it.x.x == 0, it.x.y, it.x.z, it.x.w);
         if (threadIdx.x == 0) {
@@ -1956,6 +2000,7 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_solve_flow(
         }
         __syncthreads();
         if (!ok_s) return;
+        if (trace && threadIdx.x == 0) trace[3 * i + 1] = globaltimer_ns();
         run_item<T>(c, D, b, rs, zbuf, upd, x, smem);
         __threadfence();
         __syncthreads();
@@ -1963,6 +2008,7 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_solve_flow(
             __threadfence();
             if (it.z.x >= 0) atomicAdd(ctr + it.z.x, 1);
             if (it.z.y >= 0) atomicAdd(ctr + it.z.y, 1);
+            if (trace) trace[3 * i + 2] = globaltimer_ns();
         }
     }
 }
@@ -2186,7 +2232,7 @@ int mf_factor_create(const MfPlan *P, int fp32, int fact64, MfFactor **out)
         mf_factor_destroy(M);
         return V2D_ECUDA;
     }
-    M->flow_grid = std::max(1, std::min(P->nitems, nsm * std::min(per_sm, 2)));
+    M->flow_grid = std::max(1, nsm * std::min(per_sm, 2));
     cudaGetLastError();
     *out = M;
     return V2D_OK;
@@ -2406,7 +2452,8 @@ enum { kCodeFwdLevel = 0, kCodeBwdLevel = 1, kCodeFlow = 2 };
 template <class T>
 static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, const int *stop_a,
                           const int *stop_b, cudaStream_t s, long long *n_launches,
-                          cudaEvent_t *ev = nullptr, int *codes = nullptr, int cap = 0)
+                          cudaEvent_t *ev = nullptr, int *codes = nullptr, int cap = 0,
+                          unsigned long long *trace = nullptr)
 {
     // with ev: an event is recorded after each launch (at most cap launches)
     int nev = 0;
@@ -2429,9 +2476,9 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
     long long launches = 0;
     if (M->flow) {
         V2D_CUDA_TRY(cudaMemsetAsync(M->sctr, 0, (size_t)(P->nctr + 1) * sizeof(int), s));
-        k_solve_flow<T><<<M->flow_grid, kSolveThreads, smf, s>>>(
+        k_solve_flow<T><<<std::max(1, std::min(P->nitems, M->flow_grid)), kSolveThreads, smf, s>>>(
             D, F, b, M->rs, z, upd, x, items, P->nitems, M->sctr, P->nctr, M->bar, stop_a,
-            stop_b);
+            stop_b, trace);
         V2D_TRY(solve_launch("k_solve_flow", 0));
         V2D_TRY(mark(kCodeFlow * 1000));
         launches = 1;
@@ -2530,6 +2577,35 @@ int mf_time_apply(const MfPlan *P, const MfFactor *M, int reps, size_t flush_byt
     if (st != V2D_OK) return st;
     V2D_TRY(mf_check_barrier(const_cast<MfFactor *>(M), s));   // a solve that gave up is no time
     *ms_avg = total / reps;
+    return V2D_OK;
+}
+
+// Measurement aid: one dataflow solve of a zero vector with a per-item
+// trace (ns of the global timer at the ticket, at the end of the item's
+// wait, after its done counters): ticks[3 i + k] for the n items (n <= cap).
+int mf_trace_apply(const MfPlan *P, const MfFactor *M, cudaStream_t s, unsigned long long *ticks,
+                   int cap, int *n)
+{
+    V2D_ARG_CHECK(M->flow, "LU solve trace: needs the dataflow solve");
+    V2D_ARG_CHECK(cap >= P->nitems, "LU solve trace: %d items, room for %d", P->nitems, cap);
+    const size_t es = M->fp32 ? sizeof(float) : sizeof(double);
+    DevBuf<char> buf;
+    V2D_TRY(buf.alloc(2 * P->n * es + 3 * (size_t)P->nitems * sizeof(unsigned long long) + 256, s));
+    V2D_CUDA_TRY(cudaMemsetAsync(buf.p, 0, 2 * P->n * es, s));
+    unsigned long long *tr = (unsigned long long *)(buf.p + ((2 * P->n * es + 15) / 16) * 16);
+    V2D_CUDA_TRY(cudaMemsetAsync(tr, 0, 3 * (size_t)P->nitems * sizeof(unsigned long long), s));
+    int st = M->fp32 ? apply_launches<float>(P, M, (const float *)buf.p,
+                                             (float *)(buf.p + P->n * es), nullptr, nullptr, s,
+                                             nullptr, nullptr, nullptr, 0, tr)
+                     : apply_launches<double>(P, M, (const double *)buf.p,
+                                              (double *)(buf.p + P->n * es), nullptr, nullptr, s,
+                                              nullptr, nullptr, nullptr, 0, tr);
+    V2D_TRY(st);
+    V2D_CUDA_TRY(cudaMemcpyAsync(ticks, tr, 3 * (size_t)P->nitems * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, s));
+    V2D_CUDA_TRY(cudaStreamSynchronize(s));
+    V2D_TRY(mf_check_barrier(const_cast<MfFactor *>(M), s));
+    *n = P->nitems;
     return V2D_OK;
 }
 

@@ -8,6 +8,7 @@
 // new Jacobian (one CUDA graph), GMRES(m) on the device, and a fused update
 // kernel (q += dq and ||dq||_2 in one pass).  The host reads one scalar per Newton
 // iteration to decide whether to continue, as the reference's loop does.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -747,6 +748,32 @@ extern "C" int v2d_solver_shape_tangent(v2d_solver *S, const double *nx, const d
     V2D_CUDA_TRY(cudaMemcpyAsync(dforces, dfor, (size_t)P * 10 * sizeof(double),
                                  cudaMemcpyDeviceToHost, S->s));
     V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    return V2D_OK;
+}
+
+extern "C" int v2d_solver_trace_lu_apply(v2d_solver *S, unsigned long long *ticks, int *items,
+                                         int cap, int *n)
+{
+    V2D_ARG_CHECK(S && ticks && n, "trace_lu_apply: null pointer");
+    const int q = S->prm.krylov.precision == V2D_PREC_MIXED ? 1 : 0;
+    V2D_ARG_CHECK(S->plan && S->lu[q] && S->lu_ready,
+                  "trace_lu_apply: no factors yet (run a Newton iteration)");
+    V2D_TRY(mf_trace_apply(S->plan, S->lu[q], S->s, ticks, cap, n));
+    if (items)
+        std::copy(S->plan->h_items.begin(), S->plan->h_items.end(), items);
+    return V2D_OK;
+}
+
+extern "C" int v2d_solver_lu_item_rows(v2d_solver *S, const int *rows, int nlevels, int *out_rows,
+                                       int cap, int *nlevels_out)
+{
+    V2D_ARG_CHECK(S, "null solver");
+    V2D_ARG_CHECK(S->plan, "lu_item_rows: no LU plan (precond must be V2D_PC_LU)");
+    V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+    if (rows) V2D_TRY(mf_plan_set_item_rows(S->plan, rows, nlevels));
+    if (nlevels_out) *nlevels_out = S->plan->nlevel;
+    if (out_rows && cap >= S->plan->nlevel)
+        for (int L = 0; L < S->plan->nlevel; ++L) out_rows[L] = S->plan->item_rows[L];
     return V2D_OK;
 }
 

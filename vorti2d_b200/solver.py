@@ -192,6 +192,9 @@ class Solver:
         self._ca = cfg.cos_alpha()
         self._sa = cfg.sin_alpha()
         self.dev = DeviceState(xg, yg, cfg)
+        if cfg.lu_item_rows is not None and cfg.precond.lower() == "lu":
+            from .tune import set_item_rows
+            set_item_rows(self, cfg.lu_item_rows)
         (self.jac, self.alfa, self.beta, self.gama, self.pmet, self.qmet, self.detadx,
          self.detady, self.xphys, self.yphys) = self.dev.metrics()
         self.r0, self.r1 = 0, 2 * self.ndof

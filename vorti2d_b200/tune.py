@@ -1,0 +1,120 @@
+"""In-house autotuner of the LU preconditioner solve's work-item granularity.
+
+The solve (one dataflow launch over the front tree) splits each front's rows
+into work items; on tree level L an item is ``rows[L]`` rows of one front, or
+the whole front (0).  Small items spread a level's rows over more CTAs and
+shorten the chain of dependent steps; large ones gather each front's
+right-hand side once and keep a CTA's rows together.  Which wins depends on
+the grid, the precision and the GPU, so it is measured: a coordinate search
+over the levels (each level's candidates tried with the others fixed, two
+sweeps), every trial timed as the average of warm applications of the
+current factors (``v2d_solver_time_lu_apply``, factors in L2 as inside
+GMRES).  Every setting forms the same products; a row's partial sums are
+added in an order that depends on the split, so results agree to rounding
+and each Krylov solve still meets its tolerance.
+
+The result can be written to a JSON file keyed by grid shape, precision and
+leaf size, and read back (``Config.lu_item_rows``, ``load_tuning``).
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+
+CANDIDATES = (0, 8, 16, 32, 64, 128)
+
+
+def item_rows(solver) -> list:
+    """The solve's current rows per item, one entry per tree level."""
+    n = ctypes.c_int()
+    check(lib().v2d_solver_lu_item_rows(solver.dev.h, None, 0, None, 0, ctypes.byref(n)),
+          "lu_item_rows")
+    out = np.zeros(n.value, dtype=np.intc)
+    check(lib().v2d_solver_lu_item_rows(solver.dev.h, None, 0, _lib.iptr(out), n.value, None),
+          "lu_item_rows")
+    return [int(v) for v in out]
+
+
+def set_item_rows(solver, rows) -> None:
+    r = np.ascontiguousarray(rows, dtype=np.intc)
+    check(lib().v2d_solver_lu_item_rows(solver.dev.h, _lib.iptr(r), r.size, None, 0, None),
+          "lu_item_rows")
+
+
+def time_apply(solver, reps: int = 30, repeats: int = 3) -> float:
+    """ms of one warm LU application: the smallest of `repeats` averages of
+    `reps` applications."""
+    best = float("inf")
+    for _ in range(repeats):
+        ms, fb = ctypes.c_double(), ctypes.c_longlong()
+        check(lib().v2d_solver_time_lu_apply(solver.dev.h, int(reps), 0, ctypes.byref(ms),
+                                             ctypes.byref(fb)), "time_lu_apply")
+        best = min(best, ms.value)
+    return best
+
+
+def _key(solver) -> str:
+    cfg = solver.cfg
+    return f"{solver.imax}x{solver.jmax}/{cfg.precision}/{cfg.lu_factors}"
+
+
+def tune_lu_solve(solver, candidates=CANDIDATES, sweeps: int = 2, reps: int = 30,
+                  path: str | None = None, gain: float = 0.01) -> dict:
+    """Tune the solver's rows per item in place (its factors must exist: run a
+    Newton iteration first).  A trial replaces the current choice when it is
+    faster by more than `gain` (relative).  Returns the record (and merges it
+    into the JSON file at `path` when given)."""
+    rows = item_rows(solver)
+    t0 = time_apply(solver, reps)
+    best = t0
+    trials = 0
+    for _ in range(sweeps):
+        changed = False
+        for L in range(len(rows)):
+            for c in candidates:
+                if c == rows[L]:
+                    continue
+                trial = list(rows)
+                trial[L] = int(c)
+                set_item_rows(solver, trial)
+                t = time_apply(solver, reps)
+                trials += 1
+                if t < best * (1.0 - gain):
+                    best, rows, changed = t, trial, True
+            set_item_rows(solver, rows)
+        if not changed:
+            break
+    set_item_rows(solver, rows)
+    rec = {"key": _key(solver), "rows": rows, "ms": best, "default_ms": t0, "trials": trials,
+           "candidates": list(candidates)}
+    if path:
+        table = {}
+        if os.path.exists(path):
+            with open(path) as fh:
+                table = json.load(fh)
+        table[rec["key"]] = rec
+        tmp = path + ".tmp"
+        with open(tmp, "w") as fh:
+            json.dump(table, fh, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    return rec
+
+
+def load_tuning(solver, path: str) -> bool:
+    """Apply the rows recorded for this solver's grid and precision in the
+    JSON file at `path`; False when the file has none (the default split
+    stays)."""
+    if not os.path.exists(path):
+        return False
+    with open(path) as fh:
+        rec = json.load(fh).get(_key(solver))
+    if not rec or len(rec.get("rows", [])) != len(item_rows(solver)):
+        return False
+    set_item_rows(solver, rec["rows"])
+    return True
