@@ -411,6 +411,7 @@ def run_large_workload(args):
             "data": "synthetic",
             "config": {"workload": f"large unsteady BDF2 cylinder {n}x{n} Re=200 dt=0.05 outflow",
                        "unknowns": 2 * n * n, "lu_reuse_its": args.lu_reuse,
+                       "lu_factors": SOLVER.get("lu_factors"),
                        "lu_reuse_steps": args.lu_reuse_steps,
                        "l2": "flushed (256 MiB write) before every timed step"},
             "setup_s": setup_s, "first_step_s": first_s, "newton_per_step": newton / K,

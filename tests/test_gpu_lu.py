@@ -34,15 +34,17 @@ SHAPES = [(5, 4, 0), (9, 7, 1), (24, 13, 2), (33, 21, 1), (57, 33, 0), (64, 48, 
 
 
 @pytest.mark.parametrize("imax,jmax,ff_bc", SHAPES)
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed-f64"])
 def test_one_newton_update_matches_direct_solve(v2d, oracle_mod, imax, jmax, ff_bc, precision):
     """Newton update dq of the smooth analytic state (the reference's
     tests/test_assemble_local.py:23-30 state) equals scipy's direct solve of
     the oracle's system to 1e-9 relative, in a few Krylov iterations."""
     bc = {0: "dirichlet", 1: "outflow", 2: "outflow_psi"}[ff_bc]
     xg, yg = oracle_mod.generate_cylinder(imax, jmax)
+    # "mixed-f64": the mixed form with FP64 factors rounded to FP32
+    prec, factors = (("mixed", "fp64") if precision == "mixed-f64" else (precision, "fp32"))
     s = v2d.Solver(cfg(v2d, re=80.0, steady=False, dt_phys=0.2, farfield_bc=bc,
-                       alpha_deg=4.0, precision=precision), mesh=(xg, yg))
+                       alpha_deg=4.0, precision=prec, lu_factors=factors), mesh=(xg, yg))
     M = oracle_mod.core().compute_metrics(1 / (imax - 1), 1 / (jmax - 1), xg, yg)
     st = smooth_state(M[8], M[9])
     s.set_state(*st)
@@ -57,7 +59,7 @@ def test_one_newton_update_matches_direct_solve(v2d, oracle_mod, imax, jmax, ff_
     got = np.concatenate(s.dev.get_state()[:2]) - np.concatenate(st[:2])
     assert _close(got, dq, 1e-9), np.max(np.abs(got - dq))
     assert lin.converged and lin.res <= 1e-12 * lin.res0 * 1.0001
-    assert lin.iterations <= (12 if precision == "mixed" else 6), lin.iterations
+    assert lin.iterations <= (6 if precision == "fp64" else 12), lin.iterations
     s.close()
 
 
@@ -106,7 +108,7 @@ def test_steady_cylinder_129_matches_oracle(v2d, oracle_mod):
 
 @pytest.mark.parametrize("precision,reuse,steps", [("fp64", 0, False), ("mixed", 0, False),
                                                     ("mixed", 20, False), ("fp64", 20, False),
-                                                    ("mixed", 12, True)])
+                                                    ("mixed", 12, True), ("mixed-f64", 12, True)])
 def test_unsteady_cylinder_181_matches_oracle(v2d, oracle_mod, precision, reuse, steps):
     """The benchmark case (181x181, Re=100, dt=0.2, rotational kick 0.5 until
     t=2, outflow far field, at most 5 Newton iterations per step): the first
@@ -119,8 +121,10 @@ def test_unsteady_cylinder_181_matches_oracle(v2d, oracle_mod, precision, reuse,
     kw = dict(re=100.0, steady=False, dt_phys=0.2, rot_speed=0.5, rot_until=2.0,
               farfield_bc="outflow")
     ref = oracle_mod.OracleSolver(xg, yg, pseudo_tol=1e-10, max_pseudo_iter=5, **kw)
+    prec, factors = (("mixed", "fp64") if precision == "mixed-f64" else (precision, "fp32"))
     s = v2d.Solver(cfg(v2d, ksp_rtol=1e-10, pseudo_tol=1e-10, max_pseudo_iter=5,
-                       precision=precision, lu_reuse_its=reuse, lu_reuse_steps=steps, **kw),
+                       precision=prec, lu_factors=factors, lu_reuse_its=reuse,
+                       lu_reuse_steps=steps, **kw),
                      mesh=(xg, yg))
     for t in ref.times()[:3]:
         _, it_ref = ref.advance(t)

@@ -915,7 +915,7 @@ constexpr int kGemmTile = 64;
 
 template <class T> struct PanelWidth;
 template <> struct PanelWidth<float> { static constexpr int v = 32; };
-template <> struct PanelWidth<double> { static constexpr int v = 16; };
+template <> struct PanelWidth<double> { static constexpr int v = 32; };
 
 // rs[r] = 1 / max_c |a_rc| (1 for an empty row).
 __global__ void k_rowscale(int n, const int *__restrict__ rowptr, const double *__restrict__ val,
