@@ -231,7 +231,9 @@ def run_sweep_workload(args):
     cases = sweep_cases(seed=0)
     cont = args.sweep_continuation if args.sweep_continuation > 1.0 else None
     if args.sweep_mode == "batched" and cont is None:
-        res = run_sweep_batched(cases, precision="mixed", lu_factors=args.lu_factors)
+        res = run_sweep_batched(cases, precision=args.sweep_precision,
+                                krylov_max_it=args.sweep_krylov_max,
+                                diverge_factor=args.sweep_diverge, lu_factors=args.lu_factors)
     else:
         res = run_sweep(cases, workers=args.sweep_workers, precision="mixed", continuation=cont)
     kinds = {}
@@ -269,8 +271,9 @@ def run_sweep_workload(args):
                                 if args.sweep_mode == "batched" and cont is None
                                 else "one handle and stream per instance, thread pool"),
                        "precond": "multifrontal LU per Newton iteration",
-                       "newton": "<=20 iterations, stop when ||dq|| > 1e3 x the first",
-                       "krylov_max_it": 300,
+                       "newton": "<=20 iterations, frozen when ||dq|| > diverge_factor x the first",
+                       "krylov_max_it": args.sweep_krylov_max,
+                       "precision": args.sweep_precision, "diverge_factor": args.sweep_diverge,
                        "continuation": (f"Re from 80 x{cont} per rung, rungs to ||dq||/(2N) <= 1e-7"
                                         if cont else "none (free stream at the case's Re)")},
             "max_re_converged": max([r.re for r in res.results if r.converged], default=None),
@@ -810,6 +813,12 @@ def main():
                          "adjoint: steady adjoint gradients; large: the large unsteady grid; "
                          "unsteady_adjoint: the checkpointed unsteady adjoint")
     ap.add_argument("--sweep-workers", type=int, default=16)
+    ap.add_argument("--sweep-precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--sweep-krylov-max", type=int, default=300,
+                    help="sweep: GMRES iterations per Newton step at most")
+    ap.add_argument("--sweep-diverge", type=float, default=1e3,
+                    help="sweep: an instance whose update norm exceeds this factor times its "
+                         "first is frozen as diverged")
     ap.add_argument("--sweep-mode", default="batched", choices=["batched", "streams"],
                     help="sweep: all instances as one block-diagonal system (batched) or one "
                          "handle and stream per instance")

@@ -18,7 +18,7 @@ def _cases(v2d, oracle_mod):
     cyl65 = oracle_mod.generate_cylinder(65, 49)
     naca = v2d.generate_naca0012(65, 33)
     return [Case("cyl33_a", *cyl33, 20.0, 0.0), Case("cyl65_a", *cyl65, 40.0, 4.0),
-            Case("naca65_a", *naca, 5.0, 3.0, 1.0), Case("cyl33_b", *cyl33, 35.0, -6.0),
+            Case("naca65_a", *naca, 5.0, 3.0, 1.0), Case("cyl33_b", *cyl33, 30.0, -6.0),
             Case("cyl65_b", *cyl65, 25.0, 8.0)]
 
 

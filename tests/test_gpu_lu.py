@@ -30,7 +30,7 @@ def cfg(v2d, **kw):
 # the 48 KB default only without the kernel's static shared memory; 265x33:
 # the FP64 inversion of the 530-wide root separator runs from global memory
 SHAPES = [(5, 4, 0), (9, 7, 1), (24, 13, 2), (33, 21, 1), (57, 33, 0), (64, 48, 0),
-          (129, 65, 2), (265, 33, 0)]
+          (129, 65, 2), (265, 33, 0), (513, 33, 1)]
 
 
 @pytest.mark.parametrize("imax,jmax,ff_bc", SHAPES)

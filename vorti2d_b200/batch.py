@@ -96,6 +96,7 @@ class SweepResult:
     setup_s: float = 0.0
     solve_s: float = 0.0
     workers: int = 0
+    shared_krylov: int | None = None   # batched: GMRES iterations of the combined system
 
     @property
     def converged(self) -> int:
@@ -107,6 +108,8 @@ class SweepResult:
 
     @property
     def krylov_iters(self) -> int:
+        if self.shared_krylov is not None:
+            return self.shared_krylov
         return sum(r.krylov_iters for r in self.results)
 
     @property
@@ -257,7 +260,7 @@ def run_sweep_batched(cases, precision: str = "mixed", max_newton: int = 20,
     jmax = np.array([x.shape[1] for x in xs], dtype=np.intc)
     xp = (_lib._dp * n)(*[_lib.dptr(x) for x in xs])
     yp = (_lib._dp * n)(*[_lib.dptr(y) for y in ys])
-    out = SweepResult(workers=1)
+    out = SweepResult(workers=1, shared_krylov=0)
     t0 = time.perf_counter()
     h = c_void_p()
     _lib.check(_lib.lib().v2d_batch_create(n, _lib.iptr(imax), _lib.iptr(jmax), xp, yp, params,
@@ -287,6 +290,7 @@ def run_sweep_batched(cases, precision: str = "mixed", max_newton: int = 20,
                 continue
             if code not in (_lib.V2D_OK, _lib.V2D_ENOTCONVERGED):
                 _lib.check(code, "batch_newton")
+            out.shared_krylov += st.iterations
             for i in np.nonzero(active)[0]:
                 r = results[i]
                 r.newton_iters += 1

@@ -140,6 +140,8 @@ struct MfFactor {
     MfBarrier *bar = nullptr;
     int *sctr = nullptr;        // dataflow solve: 3 counters per front + the work ticket
     int flow_grid = 0;          // most CTAs of the dataflow solve resident at once
+    int flow_grid1 = 0;         // the same for its high-occupancy form (FP32 only; 0: none)
+    int flow_form = 0;          // 0: 2 CTAs per SM, 32 row registers; 1: 3 CTAs, 16
     int flow = 1;               // 1: the solve is one dataflow launch; 0: one launch per level
                                 // and sweep
     cudaGraphExec_t graph = nullptr;

@@ -667,7 +667,7 @@ static int capture_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, doub
     w->graph_m[which] = w->m;
     w->graph_pc[which] = precond;
     w->graph_lu[which] = lu ? (const void *)A.lu : nullptr;
-    w->graph_lu_flow[which] = lu ? A.lu->flow : -1;
+    w->graph_lu_flow[which] = lu ? 10 * A.lu->flow + A.lu->flow_form : -1;
     w->graph_lu_items[which] = lu ? A.lu_plan->items_ver : -1;
     return V2D_OK;
 }
@@ -681,7 +681,7 @@ static int run_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, double *
     if (w->seg[which].empty() || !w->fin[which] || w->graph_m[which] != w->m ||
         w->graph_pc[which] != precond ||
         w->graph_lu[which] != (lu ? (const void *)A.lu : nullptr) ||
-        w->graph_lu_flow[which] != (lu ? A.lu->flow : -1) ||
+        w->graph_lu_flow[which] != (lu ? 10 * A.lu->flow + A.lu->flow_form : -1) ||
         w->graph_lu_items[which] != (lu ? A.lu_plan->items_ver : -1))
         V2D_TRY(capture_cycle<T>(w, which, V, wv, z, Z, x, A, precond, s));
     for (size_t q = 0; q < w->seg[which].size(); ++q) {

@@ -53,6 +53,7 @@
 #include <functional>
 #include <map>
 #include <mutex>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -912,6 +913,10 @@ namespace {
 
 constexpr int kMfThreads = 256;
 constexpr int kGemmTile = 64;
+// levels whose largest front has at least kDelayFront variables update the
+// trailing block once per kDelayPanels panels (k_gemm)
+constexpr int kDelayFront = 1024;
+constexpr int kDelayPanels = 8;
 
 template <class T> struct PanelWidth;
 template <> struct PanelWidth<float> { static constexpr int v = 32; };
@@ -1183,87 +1188,119 @@ __global__ void __launch_bounds__(kL21Rows) k_l21_trsm(int q0, int k, int nl,
         swap_trsm_cols<T>(A, f, S, k, voff[q], blockIdx.x - nl, ipiv, D, src);
 }
 
-// Tile (tr, tc) of the trailing update A22 -= L21 U12 (rows/cols from
-// base = k + w, 64 x 64, 256 threads with 4 x 4 outputs each).
+// One 64 x 64 tile of a trailing update: A[r][c] -= sum_{t in [ka, kb)}
+// A[r][t] A[t][c] for rows [r0, min(r0 + 64, r1)) and columns
+// [c0, min(c0 + 64, c1)), the inner range in slices of NB staged in shared
+// memory (256 threads with 4 x 4 outputs each).  With one slice (kb - ka <=
+// NB) the sums are formed in the same order as a rank-NB update.
 template <class T>
-__device__ __forceinline__ void gemm_tile(T *A, int f, int k, int w, int tr, int tc,
-                                          T (*As)[kGemmTile + 1], T (*Bs)[kGemmTile])
+__device__ __forceinline__ void gemm_tile_range(T *A, int f, int r0, int r1, int c0, int c1,
+                                                int ka, int kb, T (*As)[kGemmTile + 1],
+                                                T (*Bs)[kGemmTile])
 {
     constexpr int NB = PanelWidth<T>::v;
-    const int base = k + w;
-    const int r0 = base + tr * kGemmTile, c0 = base + tc * kGemmTile;
     const int tid = threadIdx.x;
-    for (int e = tid; e < kGemmTile * NB; e += blockDim.x) {
-        const int rr = e / NB, t = e - rr * NB;   // A tile: rows r0+rr, cols k+t
-        const int r = r0 + rr;
-        As[t][rr] = (r < f && t < w) ? A[(long long)r * f + k + t] : T(0);
-    }
-    for (int e = tid; e < NB * kGemmTile; e += blockDim.x) {
-        const int t = e / kGemmTile, cc = e - t * kGemmTile;
-        const int c = c0 + cc;
-        Bs[t][cc] = (c < f && t < w) ? A[(long long)(k + t) * f + c] : T(0);
-    }
-    __syncthreads();
     const int ty = tid / 16, tx = tid % 16;  // 16x16 threads, 4x4 outputs each
     T acc[4][4];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
+    for (int k = ka; k < kb; k += NB) {
+        const int kw = min(NB, kb - k);
+        for (int e = tid; e < kGemmTile * NB; e += blockDim.x) {
+            const int rr = e / NB, t = e - rr * NB;   // A tile: rows r0+rr, cols k+t
+            const int r = r0 + rr;
+            As[t][rr] = (r < r1 && t < kw) ? A[(long long)r * f + k + t] : T(0);
+        }
+        for (int e = tid; e < NB * kGemmTile; e += blockDim.x) {
+            const int t = e / kGemmTile, cc = e - t * kGemmTile;
+            const int c = c0 + cc;
+            Bs[t][cc] = (c < c1 && t < kw) ? A[(long long)(k + t) * f + c] : T(0);
+        }
+        __syncthreads();
 #pragma unroll 4
-    for (int t = 0; t < NB; ++t) {
-        T av[4], bv[4];
+        for (int t = 0; t < NB; ++t) {
+            T av[4], bv[4];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) av[a] = As[t][ty + 16 * a];
+            for (int a = 0; a < 4; ++a) av[a] = As[t][ty + 16 * a];
 #pragma unroll
-        for (int b = 0; b < 4; ++b) bv[b] = Bs[t][tx + 16 * b];
+            for (int b = 0; b < 4; ++b) bv[b] = Bs[t][tx + 16 * b];
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+            for (int a = 0; a < 4; ++a)
 #pragma unroll
-            for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
+                for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
+        }
+        __syncthreads();
     }
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
         const int r = r0 + ty + 16 * a;
-        if (r >= f) continue;
+        if (r >= r1) continue;
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             const int c = c0 + tx + 16 * b;
-            if (c < f) A[(long long)r * f + c] -= acc[a][b];
+            if (c < c1) A[(long long)r * f + c] -= acc[a][b];
         }
     }
 }
 
-// Trailing update A22 -= L21 U12 over rows/cols [k+w, f), 64x64 tiles.
-// The next panel's diagonal block, rows and columns [k+w, k+w+w'), lies in
-// tile (0, 0), and no other tile reads or writes it: so the CTA of that tile
-// factors the next panel right after its own update (panel_factor), which
-// saves the next step's panel launch.
+// Trailing updates after panel [k, k + w), with delayed updates in
+// super-panels of W columns (a multiple of NB; W = NB is the plain
+// right-looking scheme).  Within the super-panel [k0, E), E = min(k0 + W, S),
+// the panel's rank-w update goes only to the super-panel's remaining columns
+// [kn, E) (all rows below, kn = k + w), and the next panel's rows [kn,
+// kn + w') of the columns beyond it get the delayed contributions of the
+// super-panel's panels so far (rank kn - k0), so that the next panel's swaps
+// and U12 see updated rows; after the super-panel's last panel, one rank-W
+// update covers rows and columns [E, f).  A big trailing block is then read
+// and written once per W columns instead of once per panel.  Tiles are
+// numbered per front for whichever case applies to it; the tile holding the
+// next panel's diagonal block (the first one) factors that panel after its
+// update (panel_factor), which saves the next step's panel launch.
 template <class T>
-__global__ void __launch_bounds__(256) k_gemm(int q0, int k, const int *__restrict__ S_,
+__global__ void __launch_bounds__(256) k_gemm(int q0, int k, int W, const int *__restrict__ S_,
                                               const int *__restrict__ f_,
                                               const long long *__restrict__ foff,
                                               const int *__restrict__ voff, T *F, int *ipiv,
                                               int *perm, int *flag)
 {
     constexpr int NB = PanelWidth<T>::v;
-    __shared__ T As[NB][kGemmTile + 1];
-    __shared__ T Bs[NB][kGemmTile];
+    constexpr int TL = kGemmTile;
+    __shared__ T As[NB][TL + 1];
+    __shared__ T Bs[NB][TL];
     __shared__ T U[NB][NB + 1];
     __shared__ int pv[NB];
     const int q = q0 + blockIdx.y;
     const int S = S_[q], f = f_[q];
     if (S <= k) return;
-    const int w = min(NB, S - k);
-    const int base = k + w, rem = f - base;
-    if (rem <= 0) return;
-    const int nt = (rem + kGemmTile - 1) / kGemmTile;
-    if ((int)blockIdx.x >= nt * nt) return;
+    const int w = min(NB, S - k), kn = k + w;
+    const int k0 = (k / W) * W, E = min(k0 + W, S);
     T *A = F + foff[q];
-    gemm_tile<T>(A, f, k, w, blockIdx.x / nt, blockIdx.x % nt, As, Bs);
-    if (blockIdx.x == 0 && S > base) {
+    int t = blockIdx.x;
+    bool first = false;
+    if (kn < E) {
+        const int nr = (f - kn + TL - 1) / TL, nc = (E - kn + TL - 1) / TL;
+        if (t < nr * nc) {
+            gemm_tile_range<T>(A, f, kn + (t / nc) * TL, f, kn + (t % nc) * TL, E, k, kn, As, Bs);
+            first = t == 0;
+        } else {
+            t -= nr * nc;
+            const int wn = min(NB, S - kn), nf = (f - E + TL - 1) / TL;
+            if (t >= nf) return;
+            gemm_tile_range<T>(A, f, kn, kn + wn, E + t * TL, f, k0, kn, As, Bs);
+        }
+    } else {
+        const int rem = f - E;
+        if (rem <= 0) return;
+        const int nt = (rem + TL - 1) / TL;
+        if (t >= nt * nt) return;
+        gemm_tile_range<T>(A, f, E + (t / nt) * TL, f, E + (t % nt) * TL, f, k0, E, As, Bs);
+        first = t == 0;
+    }
+    if (first && kn < S) {
         __syncthreads();   // the tile's updated entries are visible to the block
-        panel_factor<T>(A, f, S, base, voff[q], ipiv, perm, flag, U, pv);
+        panel_factor<T>(A, f, S, kn, voff[q], ipiv, perm, flag, U, pv);
     }
 }
 
@@ -1693,9 +1730,8 @@ __device__ __forceinline__ void row_range(bool fwd, int r, int S, int f, int &lo
 // depend on no other item (indices, scaled right-hand side, the single row a
 // warp owns) are loaded by pre(); run() then gathers the vector the rows
 // multiply (after the item's dependencies are met) and computes the rows.
-template <class T>
+template <class T, int R = RowRegs<T>::v>
 struct SolveItemCtx {
-    static constexpr int R = RowRegs<T>::v;
     bool fwd;
     int q, S, f, vo, rbeg, rend;
     const T *A;
@@ -1899,8 +1935,8 @@ struct SolveItemDev {
     int4 x, y, z;
 };
 
-template <class T>
-__device__ __forceinline__ void run_item(SolveItemCtx<T> &c, const MfDev &D, const T *b,
+template <class T, int R>
+__device__ __forceinline__ void run_item(SolveItemCtx<T, R> &c, const MfDev &D, const T *b,
                                          const double *__restrict__ rs, T *zbuf, T *upd, T *x,
                                          T *smem)
 {
@@ -1921,7 +1957,7 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_solve_level(
     const int4 it = items[i0 + blockIdx.x].x;
     SolveItemCtx<T> c;
     c.pre(D, F, b, rs, it.x == 0, it.y, it.z, it.w);
-    run_item<T>(c, D, b, rs, zbuf, upd, x, smem);
+    run_item(c, D, b, rs, zbuf, upd, x, smem);
 }
 
 // Polls of one dependency counter before a CTA of the dataflow solve gives
@@ -1966,8 +2002,13 @@ __device__ __forceinline__ bool wait_count(const int *ctr, int target, volatile 
 // bar->err (bit 2) and *stop_a (so GMRES stops instead of using an
 // unfinished preconditioner) and ends the CTA.  ctr is zeroed before each
 // launch.
-template <class T>
-__global__ void __launch_bounds__(kSolveThreads, 2) k_solve_flow(
+// Two forms (the autotuner picks one): MINB resident CTAs per SM at least,
+// R row registers per lane (rows up to 32 R entries prefetched before the
+// wait).  Form 0: 2 CTAs and RowRegs<T> registers; form 1 (FP32): 3 CTAs
+// per SM with 16 row registers, more warps in flight for the levels whose
+// items are whole fronts.
+template <class T, int R, int MINB>
+__global__ void __launch_bounds__(kSolveThreads, MINB) k_solve_flow(
     const MfDev D, const T *F, const T *b, const double *__restrict__ rs, T *zbuf, T *upd, T *x,
     const SolveItemDev *__restrict__ items, int nitems, int *ctr, int nctr, MfBarrier *bar,
     const int *stop_a, const int *stop_b, unsigned long long *trace)
@@ -1985,7 +2026,7 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_solve_flow(
         if (i >= nitems) return;
         const SolveItemDev it = items[i];
         if (trace && threadIdx.x == 0) trace[3 * i] = globaltimer_ns();
-        SolveItemCtx<T> c;
+        SolveItemCtx<T, R> c;
         c.pre(D, F, b, rs, it.x.x == 0, it.x.y, it.x.z, it.x.w);
         if (threadIdx.x == 0) {
             next = atomicAdd(ctr + nctr, 1);   // in flight during the wait
@@ -2001,7 +2042,7 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_solve_flow(
         __syncthreads();
         if (!ok_s) return;
         if (trace && threadIdx.x == 0) trace[3 * i + 1] = globaltimer_ns();
-        run_item<T>(c, D, b, rs, zbuf, upd, x, smem);
+        run_item(c, D, b, rs, zbuf, upd, x, smem);
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -2200,12 +2241,13 @@ int mf_factor_create(const MfPlan *P, int fp32, int fact64, MfFactor **out)
     }
     if (fp32) {
         attr((const void *)k_solve_level<float>, solve);
-        attr((const void *)k_solve_flow<float>, solve);
+        attr((const void *)k_solve_flow<float, 32, 2>, solve);
+        attr((const void *)k_solve_flow<float, 16, 3>, solve);
         attr((const void *)k_tup_front<float>, tsolve);
         attr((const void *)k_tdown_front<float>, tsolve);
     } else {
         attr((const void *)k_solve_level<double>, solve);
-        attr((const void *)k_solve_flow<double>, solve);
+        attr((const void *)k_solve_flow<double, 16, 2>, solve);
         attr((const void *)k_tup_front<double>, tsolve);
         attr((const void *)k_tdown_front<double>, tsolve);
     }
@@ -2222,10 +2264,14 @@ int mf_factor_create(const MfPlan *P, int fp32, int fact64, MfFactor **out)
     cudaError_t oe = cudaGetDevice(&dev);
     if (oe == cudaSuccess) oe = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (oe == cudaSuccess)
-        oe = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_flow<float>,
-                                                                  kSolveThreads, solve)
-                  : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_flow<double>,
-                                                                  kSolveThreads, solve);
+        oe = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                        &per_sm, k_solve_flow<float, 32, 2>, kSolveThreads, solve)
+                  : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                        &per_sm, k_solve_flow<double, 16, 2>, kSolveThreads, solve);
+    int per_sm1 = 0;
+    if (oe == cudaSuccess && fp32)
+        oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k_solve_flow<float, 16, 3>,
+                                                           kSolveThreads, solve);
     if (oe != cudaSuccess || per_sm <= 0) {
         set_error("mf_factor: occupancy of the dataflow solve: %s",
                   oe != cudaSuccess ? cudaGetErrorString(oe) : "no CTA fits on an SM");
@@ -2233,6 +2279,7 @@ int mf_factor_create(const MfPlan *P, int fp32, int fact64, MfFactor **out)
         return V2D_ECUDA;
     }
     M->flow_grid = std::max(1, nsm * std::min(per_sm, 2));
+    M->flow_grid1 = fp32 && per_sm1 > 0 ? nsm * std::min(per_sm1, 3) : 0;
     cudaGetLastError();
     *out = M;
     return V2D_OK;
@@ -2318,6 +2365,8 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
             }
         }
         const int maxf = P->lvl_maxf[L];
+        // delayed trailing updates on levels with large fronts
+        const int W = maxf >= kDelayFront ? kDelayPanels * NB : NB;
         for (int k = 0; k < P->lvl_maxS[L]; k += NB) {
             if (k == 0) {   // later panels are factored by the previous trailing update
                 k_panel<T><<<nq, kMfThreads, 0, s>>>(q0, k, P->d_S, P->d_f, P->d_foff, P->d_voff,
@@ -2337,9 +2386,12 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
             V2D_TRY(mark(4000 + L));
             const int rem = std::max(1, maxf - k - 1);
             const int nt = (rem + kGemmTile - 1) / kGemmTile;
+            // tiles of the larger of the two cases (narrow + row block, or
+            // the super-panel's full update)
+            const int ntile = nt * nt + nt;
             for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
-                k_gemm<T><<<dim3(nt * nt, std::min(nq - qb, kMaxFrontsY)), 256, 0, s>>>(
-                    q0 + qb, k, P->d_S, P->d_f, P->d_foff, P->d_voff, F, M->ipiv, M->perm,
+                k_gemm<T><<<dim3(ntile, std::min(nq - qb, kMaxFrontsY)), 256, 0, s>>>(
+                    q0 + qb, k, W, P->d_S, P->d_f, P->d_foff, P->d_voff, F, M->ipiv, M->perm,
                     M->flag);
                 if (qb > 0) ++launches;
             }
@@ -2476,9 +2528,21 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
     long long launches = 0;
     if (M->flow) {
         V2D_CUDA_TRY(cudaMemsetAsync(M->sctr, 0, (size_t)(P->nctr + 1) * sizeof(int), s));
-        k_solve_flow<T><<<std::max(1, std::min(P->nitems, M->flow_grid)), kSolveThreads, smf, s>>>(
-            D, F, b, M->rs, z, upd, x, items, P->nitems, M->sctr, P->nctr, M->bar, stop_a,
-            stop_b, trace);
+        bool launched = false;
+        if constexpr (std::is_same<T, float>::value) {
+            if (M->flow_form == 1 && M->flow_grid1 > 0) {
+                k_solve_flow<T, 16, 3><<<std::max(1, std::min(P->nitems, M->flow_grid1)),
+                                         kSolveThreads, smf, s>>>(
+                    D, F, b, M->rs, z, upd, x, items, P->nitems, M->sctr, P->nctr, M->bar,
+                    stop_a, stop_b, trace);
+                launched = true;
+            }
+        }
+        if (!launched)
+            k_solve_flow<T, RowRegs<T>::v, 2><<<std::max(1, std::min(P->nitems, M->flow_grid)),
+                                                kSolveThreads, smf, s>>>(
+                D, F, b, M->rs, z, upd, x, items, P->nitems, M->sctr, P->nctr, M->bar, stop_a,
+                stop_b, trace);
         V2D_TRY(solve_launch("k_solve_flow", 0));
         V2D_TRY(mark(kCodeFlow * 1000));
         launches = 1;

@@ -764,6 +764,23 @@ extern "C" int v2d_solver_trace_lu_apply(v2d_solver *S, unsigned long long *tick
     return V2D_OK;
 }
 
+extern "C" int v2d_solver_lu_flow_form(v2d_solver *S, int form, int *current)
+{
+    V2D_ARG_CHECK(S, "null solver");
+    const int q = S->prm.krylov.precision == V2D_PREC_MIXED ? 1 : 0;
+    V2D_ARG_CHECK(S->lu[q], "lu_flow_form: no LU factors (precond must be V2D_PC_LU)");
+    MfFactor *M = S->lu[q];
+    if (form >= 0) {
+        V2D_ARG_CHECK(form <= 1, "lu_flow_form: form %d (0 or 1)", form);
+        V2D_ARG_CHECK(form == 0 || M->flow_grid1 > 0,
+                      "lu_flow_form: form 1 exists for the FP32 solve only");
+        V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+        M->flow_form = form;
+    }
+    if (current) *current = M->flow_form;
+    return V2D_OK;
+}
+
 extern "C" int v2d_solver_lu_item_rows(v2d_solver *S, const int *rows, int nlevels, int *out_rows,
                                        int cap, int *nlevels_out)
 {

@@ -1,6 +1,8 @@
 """In-house autotuner of the LU preconditioner solve's work-item granularity.
 
-The solve (one dataflow launch over the front tree) splits each front's rows
+The solve (one dataflow launch over the front tree) runs in one of two
+kernel forms (more resident CTAs per SM, or more row registers per lane) and
+splits each front's rows
 into work items; on tree level L an item is ``rows[L]`` rows of one front, or
 the whole front (0).  Small items spread a level's rows over more CTAs and
 shorten the chain of dependent steps; large ones gather each front's
@@ -47,6 +49,18 @@ def set_item_rows(solver, rows) -> None:
           "lu_item_rows")
 
 
+def flow_form(solver) -> int:
+    cur = ctypes.c_int()
+    check(lib().v2d_solver_lu_flow_form(solver.dev.h, -1, ctypes.byref(cur)), "lu_flow_form")
+    return cur.value
+
+
+def set_flow_form(solver, form: int) -> bool:
+    """Select a form of the dataflow solve kernel; False when the solve has
+    no such form (form 1 exists for the FP32 solve only)."""
+    return lib().v2d_solver_lu_flow_form(solver.dev.h, int(form), None) == _lib.V2D_OK
+
+
 def time_apply(solver, reps: int = 30, repeats: int = 3) -> float:
     """ms of one warm LU application: the smallest of `repeats` averages of
     `reps` applications."""
@@ -74,6 +88,16 @@ def tune_lu_solve(solver, candidates=CANDIDATES, sweeps: int = 2, reps: int = 30
     t0 = time_apply(solver, reps)
     best = t0
     trials = 0
+    # kernel form first (resident CTAs per SM against row registers)
+    form = flow_form(solver)
+    for f in (0, 1):
+        if f == form or not set_flow_form(solver, f):
+            continue
+        t = time_apply(solver, reps)
+        trials += 1
+        if t < best * (1.0 - gain):
+            best, form = t, f
+    set_flow_form(solver, form)
     for _ in range(sweeps):
         changed = False
         for L in range(len(rows)):
@@ -91,8 +115,8 @@ def tune_lu_solve(solver, candidates=CANDIDATES, sweeps: int = 2, reps: int = 30
         if not changed:
             break
     set_item_rows(solver, rows)
-    rec = {"key": _key(solver), "rows": rows, "ms": best, "default_ms": t0, "trials": trials,
-           "candidates": list(candidates)}
+    rec = {"key": _key(solver), "rows": rows, "form": form, "ms": best, "default_ms": t0,
+           "trials": trials, "candidates": list(candidates)}
     if path:
         table = {}
         if os.path.exists(path):
@@ -117,4 +141,5 @@ def load_tuning(solver, path: str) -> bool:
     if not rec or len(rec.get("rows", [])) != len(item_rows(solver)):
         return False
     set_item_rows(solver, rec["rows"])
+    set_flow_form(solver, rec.get("form", 0))
     return True
