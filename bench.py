@@ -451,24 +451,42 @@ def run_unsteady_adjoint_workload(args):
         cfg = v.Config(verbose=False, write_csv=False, write_xdmf=False, compute_forces=False,
                        re=200.0, steady=False, dt_phys=0.05, farfield_bc="outflow",
                        pseudo_tol=1e-12, max_pseudo_iter=20, ksp_rtol=1e-12,
-                       precision="fp64", raise_on_linear_failure=False)
+                       precision="fp64", raise_on_linear_failure=False,
+                       lu_reuse_its=args.ua_reuse, lu_reuse_steps=args.ua_reuse > 0)
         return v.Solver(cfg, mesh=mesh)
 
     unsteady_mean_force_vjp(make, 2, (0.0, 1.0, 0.0), checkpoint_every=1)   # warm-up
     torch.cuda.synchronize()
+    # device memory in use, sampled once a second during the run (the
+    # library's own allocations are not torch's, so ask the driver)
+    peak = [0]
+    done = threading.Event()
+
+    def watch():
+        while not done.is_set():
+            free, total = torch.cuda.mem_get_info()
+            peak[0] = max(peak[0], total - free)
+            done.wait(1.0)
+
+    th = threading.Thread(target=watch, daemon=True)
+    th.start()
     t0 = time.perf_counter()
     J, d_alpha, d_re, info = unsteady_mean_force_vjp(make, args.ua_steps, (0.0, 1.0, 0.0),
                                                      checkpoint_every=args.ua_checkpoint)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
+    done.set()
+    th.join()
     line = {"metric": f"unsteady adjoint gradients/s (mean Cd over {args.ua_steps} BDF2 steps, "
                       f"d/dalpha and d/dRe), {n}x{n} cylinder Re=200 dt=0.05",
             "value": 1.0 / dt, "unit": "gradients/s", "n_gpus": 1, "higher_is_better": True,
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"unsteady discrete adjoint, cylinder {n}x{n}, "
                                    f"{args.ua_steps} steps, checkpoint every "
-                                   f"{args.ua_checkpoint}"},
-            "seconds": dt, "mean_cd": J, "dJ_dalpha": d_alpha, "dJ_dRe": d_re, **info}
+                                   f"{args.ua_checkpoint}",
+                       "lu_reuse_its": args.ua_reuse},
+            "seconds": dt, "mean_cd": J, "dJ_dalpha": d_alpha, "dJ_dRe": d_re,
+            "device_memory_peak_gb": peak[0] / 1e9, **info}
     print(json.dumps(line), flush=True)
 
 
@@ -835,6 +853,9 @@ def main():
                     help="grid side of the unsteady adjoint workload")
     ap.add_argument("--ua-steps", type=int, default=20,
                     help="BDF2 steps of the unsteady adjoint workload")
+    ap.add_argument("--ua-reuse", type=int, default=0,
+                    help="unsteady adjoint: keep the forward solve's LU factors across Newton "
+                         "iterations and steps while GMRES needs at most this many iterations")
     ap.add_argument("--ua-checkpoint", type=int, default=5,
                     help="checkpoint spacing of the unsteady adjoint workload")
     ap.add_argument("--adjoint-dtau", type=float, default=0.0,

@@ -1690,28 +1690,39 @@ __device__ __forceinline__ T row_dot_reg(const T (&reg)[R], const T *v, int base
     return warp_sum(a0 + a1);
 }
 
-// Four rows' dot products by one warp at once: row u's entries [b_u, e_u)
-// with v (an empty range for an absent row), all loads in flight together.
+// N rows' dot products by one warp at once: row u's entries [b_u, e_u) with
+// v (an empty range for an absent row), all loads in flight together.  Each
+// row has its own accumulator, so its sum does not depend on N.
+template <class T, int N>
+__device__ __forceinline__ void dotN(const T *const (&p)[N], const int (&b)[N], const int (&e)[N],
+                                     const T *v, T (&s)[N])
+{
+    const int lane = threadIdx.x & 31;
+    int lo = b[0], hi = e[0];
+#pragma unroll
+    for (int u = 1; u < N; ++u) {
+        lo = min(lo, b[u]);
+        hi = max(hi, e[u]);
+    }
+    T a[N];
+#pragma unroll
+    for (int u = 0; u < N; ++u) a[u] = T(0);
+#pragma unroll 4
+    for (int c = (lo & ~31) + lane; c < hi; c += 32) {
+        const T x = v[c];
+#pragma unroll
+        for (int u = 0; u < N; ++u)
+            if (c >= b[u] && c < e[u]) a[u] += p[u][c] * x;
+    }
+#pragma unroll
+    for (int u = 0; u < N; ++u) s[u] = warp_sum(a[u]);
+}
+
 template <class T>
 __device__ __forceinline__ void dot4(const T *const (&p)[4], const int (&b)[4], const int (&e)[4],
                                      const T *v, T (&s)[4])
 {
-    const int lane = threadIdx.x & 31;
-    const int lo = min(min(b[0], b[1]), min(b[2], b[3]));
-    const int hi = max(max(e[0], e[1]), max(e[2], e[3]));
-    T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
-#pragma unroll 4
-    for (int c = (lo & ~31) + lane; c < hi; c += 32) {
-        const T x = v[c];
-        if (c >= b[0] && c < e[0]) a0 += p[0][c] * x;
-        if (c >= b[1] && c < e[1]) a1 += p[1][c] * x;
-        if (c >= b[2] && c < e[2]) a2 += p[2][c] * x;
-        if (c >= b[3] && c < e[3]) a3 += p[3][c] * x;
-    }
-    s[0] = warp_sum(a0);
-    s[1] = warp_sum(a1);
-    s[2] = warp_sum(a2);
-    s[3] = warp_sum(a3);
+    dotN<T, 4>(p, b, e, v, s);
 }
 
 // Column range of row r of front (S, f) in the forward (fwd) or backward sweep.
@@ -1902,11 +1913,12 @@ struct SolveItemCtx {
             }
             return;
         }
-        for (int r = rbeg + wid; r < rend; r += 4 * nw) {
-            const T *p[4];
-            int bb[4], ee[4], rr[4];
+        constexpr int G = R >= 32 ? 8 : 4;   // rows per warp in flight (register budget)
+        for (int r = rbeg + wid; r < rend; r += G * nw) {
+            const T *p[G];
+            int bb[G], ee[G], rr[G];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < G; ++u) {
                 rr[u] = r + u * nw;
                 if (rr[u] < rend) {
                     row_range(fwd, rr[u], S, f, bb[u], ee[u]);
@@ -1916,12 +1928,12 @@ struct SolveItemCtx {
                     p[u] = A;
                 }
             }
-            T s4[4];
-            dot4<T>(p, bb, ee, vec, s4);
+            T sg[G];
+            dotN<T, G>(p, bb, ee, vec, sg);
             if (lane == 0) {
 #pragma unroll
-                for (int u = 0; u < 4; ++u)
-                    if (rr[u] < rend) out(rr[u], s4[u]);
+                for (int u = 0; u < G; ++u)
+                    if (rr[u] < rend) out(rr[u], sg[u]);
             }
         }
     }
