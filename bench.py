@@ -521,6 +521,35 @@ def profile_newton(args):
     s.close()
 
 
+def profile_lu_apply(args):
+    """Two steps of the workload (factors, graphs), the autotuned work-item
+    split, then two warm LU preconditioner solves inside the NVTX range
+    v2d_lu_apply (for a profiler capture of the dataflow solve kernel)."""
+    import ctypes
+    import torch
+    import vorti2d_b200 as v
+    from vorti2d_b200 import _lib
+    from vorti2d_b200.tune import tune_lu_solve
+    torch.cuda.set_device(0)
+    xg, yg = v.generate_cylinder(IMAX, JMAX)
+    prec = "mixed" if args.precision == "both" else args.precision
+    s = make_solver(v, xg, yg, prec, args.lu_reuse, args.lu_reuse_steps)
+    times = s.times()
+    for m in range(2):
+        s.advance(times[m])
+    rec = tune_lu_solve(s) if args.lu_tune else None
+    torch.cuda.synchronize()
+    ms, fb = ctypes.c_double(), ctypes.c_longlong()
+    torch.cuda.nvtx.range_push("v2d_lu_apply")
+    _lib.check(_lib.lib().v2d_solver_time_lu_apply(s.dev.h, 2, 0, ctypes.byref(ms),
+                                                   ctypes.byref(fb)))
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    print(json.dumps({"profile": "LU apply", "precision": prec, "ms": ms.value,
+                      "factor_bytes": fb.value, "tuning": rec}), flush=True)
+    s.close()
+
+
 def profile_lu_launches(args):
     """Per-launch device time of one LU preconditioner solve after two steps
     of the workload, with the factors warm in L2 (as inside GMRES) and after
@@ -865,6 +894,8 @@ def main():
                     help="Reynolds number of the adjoint workload (--workload adjoint)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="print only the HBM-bound kernel roofline table (--kernels-grid)")
+    ap.add_argument("--lu-apply-profile", action="store_true",
+                    help="two steps, then two warm LU solves in the NVTX range v2d_lu_apply")
     ap.add_argument("--lu-launches", action="store_true",
                     help="per-launch device time of one LU preconditioner solve, warm and cold")
     ap.add_argument("--profile-newton", action="store_true",
@@ -878,6 +909,9 @@ def main():
         return
     if args.lu_launches:
         profile_lu_launches(args)
+        return
+    if args.lu_apply_profile:
+        profile_lu_apply(args)
         return
     if args.workload == "sweep" and args.impl == "ours":
         run_sweep_workload(args)

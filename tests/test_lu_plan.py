@@ -212,19 +212,32 @@ def test_solve_plan_order_is_safe(v2d, oracle_mod, imax, jmax, leaf):
 
 
 def test_solve_plan_181_items(v2d, oracle_mod):
-    """181x181, 64-node leaves: levels 0-3 (512, 256, 128, 64 fronts) take
-    whole fronts as items; the 65 fronts above split into 8-row items; the
-    root (362 pivots, no contribution rows) is the last forward front and the
-    first backward one."""
+    """181x181, 64-node leaves: the default split aims at about 600 items per
+    level -- R rows per item, R the level's rows over 600 rounded down to a
+    power of two in [8, 256], whole fronts where no front of the level has
+    more than R rows; the root (362 pivots, no contribution rows) is the last
+    forward front and the first backward one."""
     ip, ix = pattern(oracle_mod, 181, 181, 1)
     (ni, nc, nf, nl), items, fronts = solve_plan(v2d, 181, 181, ip, ix)
     assert (nf, nl) == (1025, 11)
-    whole = items[items[:, 1] < 960]
-    assert (whole[:, 2] == 0).all()
-    assert (whole[:, 3] == np.where(whole[:, 0] == FWD, fronts[whole[:, 1], 1],
-                                    fronts[whole[:, 1], 0])).all()
-    upper = items[items[:, 1] >= 960]
-    assert (upper[:, 3] - upper[:, 2] <= 8).all()
+    for L in range(nl):
+        it = items[items[:, 10] == L]
+        qs = np.unique(it[:, 1])
+        rows = int(fronts[qs, 1].sum())
+        R = 8
+        while R < 256 and 2 * R * 600 <= rows:
+            R *= 2
+        span = it[:, 3] - it[:, 2]
+        if fronts[qs, 1].max() <= R:
+            assert (it[:, 2] == 0).all()
+            assert (it[:, 3] == np.where(it[:, 0] == FWD, fronts[it[:, 1], 1],
+                                         fronts[it[:, 1], 0])).all()
+        else:
+            assert span.max() == R and (span > 0).all()
+            # every chunk but a front's last is full
+            last = it[:, 3] == np.where(it[:, 0] == FWD, fronts[it[:, 1], 1],
+                                        fronts[it[:, 1], 0])
+            assert (span[~last] == R).all()
     fwd = items[items[:, 0] == FWD]
     bwd = items[items[:, 0] == BWD]
     assert fwd[-1, 1] == 1024 and bwd[0, 1] == 1024 and fronts[1024, 2] == -1

@@ -65,8 +65,8 @@ namespace v2d {
 constexpr int kSolveRowsHost = 8;
 // threads of a solve work item (8 warps)
 constexpr int kSolveThreadsHost = 256;
-// levels with at least this many fronts take whole fronts as work items
-constexpr int kFrontPerCtaHost = 64;
+// the default work-item split aims at about this many items per level
+constexpr int kItemsPerLevel = 600;
 
 // Counters of the dataflow solve, three per front q: forward items of q
 // that wrote z rows (fz), the children's forward items that wrote
@@ -210,8 +210,8 @@ void mf_plan_destroy(MfPlan *p)
 }
 
 // Work items of the solve.  Forward: per level bottom-up, per front, rows
-// [0, f) -- whole fronts on levels with at least kFrontPerCtaHost fronts,
-// chunks of kSolveRowsHost rows above.  Backward: per level top-down, rows
+// [0, f) -- whole fronts, or chunks of the level's rows-per-item count
+// (item_rows, set by default from the level's size).  Backward: per level top-down, rows
 // [0, S) in the same granularity.  Waits and done counters:
 //   forward item of q   waits fin[q] = all children's items with contribution
 //                       rows; done: fz[q] if it has z rows, fin[parent] if
@@ -231,13 +231,19 @@ static int items_build(MfPlan *P)
     it.clear();
     P->lvl_fwd.assign(nl + 1, 0);
     P->lvl_bwd.assign(nl + 1, 0);
-    // rows per item of each level (0: whole fronts); the default: whole fronts
-    // where a level has at least kFrontPerCtaHost fronts, kSolveRowsHost rows
-    // above
+    // rows per item of each level (0: whole fronts).  The default aims at
+    // about kItemsPerLevel items per level: the level's rows over that
+    // count, rounded down to a power of two in [kSolveRowsHost, 256]; whole
+    // fronts where no front of the level is longer than that
     if ((int)P->item_rows.size() != nl) {
         P->item_rows.assign(nl, kSolveRowsHost);
-        for (int L = 0; L < nl; ++L)
-            if (P->lvl_off[L + 1] - P->lvl_off[L] >= kFrontPerCtaHost) P->item_rows[L] = 0;
+        for (int L = 0; L < nl; ++L) {
+            long long rows = 0;
+            for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q) rows += P->f[q];
+            int R = kSolveRowsHost;
+            while (R < 256 && 2LL * R * kItemsPerLevel <= rows) R *= 2;
+            P->item_rows[L] = P->lvl_maxf[L] <= R ? 0 : R;
+        }
     }
     auto per = [&](int L) { return P->item_rows[L] > 0 ? P->item_rows[L] : INT_MAX; };
     int cur_level = 0;
@@ -1888,12 +1894,34 @@ struct SolveItemCtx {
         rows(v, [&](int r, T val) { x[vars[r]] = val; });
     }
 
-    // The item's rows: one per warp from registers, or four per warp at a
-    // time (dot4) when the item has more rows than warps.
+    // The item's rows: one per warp from registers (at most one row per
+    // warp); one per thread when the item has at least half as many rows as
+    // threads (each thread sums its row left to right, four partial sums;
+    // the row's entries come through L1 line by line and the vector entries
+    // from shared memory); otherwise G rows per warp at a time (dotN).
     template <class Out>
     __device__ __forceinline__ void rows(const T *vec, Out out)
     {
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        if (2 * (rend - rbeg) >= (int)blockDim.x) {
+            for (int r = rbeg + (int)threadIdx.x; r < rend; r += blockDim.x) {
+                int lo, hi;
+                row_range(fwd, r, S, f, lo, hi);
+                const T *row = A + (long long)r * f;
+                T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+                int c = lo;
+#pragma unroll 4
+                for (; c + 3 < hi; c += 4) {
+                    a0 += row[c] * vec[c];
+                    a1 += row[c + 1] * vec[c + 1];
+                    a2 += row[c + 2] * vec[c + 2];
+                    a3 += row[c + 3] * vec[c + 3];
+                }
+                for (; c < hi; ++c) a0 += row[c] * vec[c];
+                out(r, (a0 + a1) + (a2 + a3));
+            }
+            return;
+        }
         if (rend - rbeg <= nw) {
             const int r = rbeg + wid;
             if (r < rend) {
