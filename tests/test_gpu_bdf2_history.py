@@ -14,9 +14,12 @@ kept across Newton iterations and time steps while GMRES(30) needs at most
 Checked: Cl, Cd, Cm within 1e-8 at every step, the Newton iteration count
 per step within one of the oracle's, psi and omega within 1e-9 (relative to
 the field's maximum) at steps 24, 100 and 399, and the Strouhal number of the
-lift over the second half of the run against the oracle's and against the
-reference's documented value at Re 100 (docs/verification.rst:181-204:
-0.1535 on its own grid, within 3 %).
+lift over the second half of the run against the oracle's (1e-6), and the
+shedding Strouhal number and mean drag against the reference's figures for
+this Re 100 cylinder case (README.md:12: St ~ 0.16, mean Cd ~ 1.31, two
+digits each).  The 0.1535 of docs/verification.rst:181-204 is measured on
+another grid over a longer saturated window; the oracle's 400-step run gives
+St 0.1602 and mean Cd 1.313 here.
 """
 import os
 
@@ -27,7 +30,8 @@ pytestmark = pytest.mark.gpu
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 FIXTURE = os.path.join(HERE, "golden", "bdf2_history_181.npz")
-ST_REFERENCE_RE100 = 0.1535
+ST_REFERENCE_RE100 = 0.16
+CD_MEAN_REFERENCE_RE100 = 1.31
 
 
 def _strouhal(t, cl, t_from):
@@ -54,6 +58,7 @@ def test_400_steps_match_oracle(v2d, precision):
     assert len(times) == nsteps and np.allclose(times, ref["t"], rtol=0, atol=1e-12)
     ckpt = {int(k): i for i, k in enumerate(ref["ckpt_steps"])}
     cl = np.zeros(nsteps)
+    cd = np.zeros(nsteps)
     worst = {"force": 0.0, "field": 0.0}
     for m, t in enumerate(times):
         _, its, _ = s.advance(t)
@@ -63,7 +68,7 @@ def test_400_steps_match_oracle(v2d, precision):
             d = abs(getattr(fc, k) - float(ref[k][m]))
             worst["force"] = max(worst["force"], d)
             assert d <= 1e-8, (m, k, getattr(fc, k), float(ref[k][m]))
-        cl[m] = fc.cl
+        cl[m], cd[m] = fc.cl, fc.cd
         if m in ckpt:
             for name, field in (("psi", s.psi), ("ome", s.ome)):
                 want = ref[name + "_ckpt"][ckpt[m]]
@@ -76,6 +81,8 @@ def test_400_steps_match_oracle(v2d, precision):
     st_ref = float(ref["st"])
     assert periods >= 3 and np.isfinite(st)
     assert abs(st - st_ref) <= 1e-6, (st, st_ref)
-    assert abs(st - ST_REFERENCE_RE100) <= 0.03 * ST_REFERENCE_RE100, st
+    assert abs(st - ST_REFERENCE_RE100) <= 0.005, st
+    cd_mean = float(np.mean(cd[ref["t"] >= t_from]))
+    assert abs(cd_mean - CD_MEAN_REFERENCE_RE100) <= 0.005, cd_mean
     print(f"{precision}: 400 steps, worst |dC| {worst['force']:.2e}, worst field "
           f"{worst['field']:.2e}, St {st:.5f} (oracle {st_ref:.5f}, {periods} periods)")
