@@ -360,6 +360,53 @@ def run_adjoint_workload(args):
     s.close()
 
 
+def fp64_gemm_tflops(torch, n=8192, reps=5):
+    """Dense FP64 GEMM rate of this GPU (torch.matmul, i.e. the vendor BLAS,
+    n x n x n), CUDA events: the reference rate for the factorization's
+    FP64 contractions."""
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    c = torch.matmul(a, b)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        torch.matmul(a, b, out=c)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    del a, b, c
+    return 2.0 * n ** 3 / (ms * 1e-3) / 1e12
+
+
+def factor_rate(torch, _lib, s):
+    """One LU factorization of the handle's current matrix, timed per launch
+    (v2d_solver_time_lu_factor), its flops (v2d_solver_lu_stats) and the
+    rate against the FP64 GEMM rate of the same GPU, with the time per
+    kernel kind."""
+    import ctypes
+    st = (ctypes.c_double * 6)()
+    _lib.check(_lib.lib().v2d_solver_lu_stats(s.dev.h, st))
+    cap = 16384
+    ms = (ctypes.c_double * cap)()
+    codes = (ctypes.c_int * cap)()
+    n = ctypes.c_int()
+    _lib.check(_lib.lib().v2d_solver_time_lu_factor(s.dev.h, 1, ms, codes, cap, ctypes.byref(n)))
+    fkinds = ["rowscale", "scatter", "extend_add", "panel", "l21_swap_trsm", "-", "gemm", "trinv",
+              "trcopy", "gh", "ghcopy", "round_f32"]
+    by_kind = {}
+    for k in range(n.value):
+        kind = fkinds[codes[k] // 1000]
+        by_kind[kind] = by_kind.get(kind, 0.0) + ms[k]
+    total = sum(ms[k] for k in range(n.value))
+    tf = st[3] / (total * 1e-3) / 1e12
+    peak = fp64_gemm_tflops(torch)
+    return {"ms": total, "launches": n.value, "flops": st[3], "tflops": tf,
+            "fp64_gemm_tflops": peak, "frac_of_fp64_gemm": tf / peak,
+            "fronts": int(st[0]), "levels": int(st[1]), "factor_entries": st[2],
+            "by_kind_ms": {k: round(v, 3) for k, v in by_kind.items()}}
+
+
 def run_large_workload(args):
     """Large unsteady run: cylinder O-grid N x N (default 2049, 8.4M
     unknowns), Re 200, dt 0.05, outflow far field, BDF2 with at most 5 Newton
@@ -389,6 +436,12 @@ def run_large_workload(args):
     s.advance(times[0])
     torch.cuda.synchronize()
     first_s = time.perf_counter() - t0
+    tuning = None
+    if args.lu_tune and SOLVER.get("lu_solve", "flow") == "flow":
+        from vorti2d_b200.tune import tune_lu_solve
+        t0 = time.perf_counter()
+        tuning = tune_lu_solve(s, sweeps=1)
+        tuning["seconds"] = time.perf_counter() - t0
     phase_times(_lib, s, reset=True)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     K = args.large_steps
@@ -398,6 +451,7 @@ def run_large_workload(args):
     fb = ctypes.c_longlong()
     _lib.check(_lib.lib().v2d_solver_time_lu_apply(s.dev.h, 3, L2_FLUSH_BYTES,
                                                   ctypes.byref(lu_ms), ctypes.byref(fb)))
+    factor = factor_rate(torch, _lib, s)
     hbm = 6650.0
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -427,6 +481,7 @@ def run_large_workload(args):
                          "achieved": gbs,
                          "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
                          "bytes_per_launch": fb.value, "ms_per_launch": lu_ms.value},
+            "factorization": factor, "lu_tuning": tuning,
             "cd": s.force_coeffs().cd}
     print(json.dumps(line), flush=True)
     s.close()
@@ -559,20 +614,26 @@ def profile_lu_launches(args):
     import vorti2d_b200 as v
     from vorti2d_b200 import _lib
     torch.cuda.set_device(0)
-    xg, yg = v.generate_cylinder(IMAX, JMAX)
+    grid = args.profile_grid
+    xg, yg = v.generate_cylinder(grid, grid)
     prec = "mixed" if args.precision == "both" else args.precision
     s = make_solver(v, xg, yg, prec, args.lu_reuse, args.lu_reuse_steps)
     times = s.times()
     for m in range(2):
         s.advance(times[m])
     kinds = ["forward_level", "backward_level", "dataflow"]
-    out = {"profile": "LU solve launches", "precision": prec}
+    out = {"profile": "LU solve launches", "precision": prec, "grid": f"{grid}x{grid}",
+           "lu_factors": SOLVER.get("lu_factors", "fp32")}
+    if args.lu_tune and SOLVER.get("lu_solve", "flow") == "flow":
+        from vorti2d_b200.tune import tune_lu_solve
+        out["lu_tuning"] = tune_lu_solve(s, sweeps=1 if grid > 513 else 2)
     for label, flush in (("warm", 0), ("cold", L2_FLUSH_BYTES)):
         cap = 256
         ms = (ctypes.c_double * cap)()
         codes = (ctypes.c_int * cap)()
         n = ctypes.c_int()
-        _lib.check(_lib.lib().v2d_solver_time_lu_launches(s.dev.h, 20, flush, ms, codes, cap,
+        _lib.check(_lib.lib().v2d_solver_time_lu_launches(s.dev.h, 20 if grid <= 513 else 3,
+                                                         flush, ms, codes, cap,
                                                          ctypes.byref(n)))
         rows = [(kinds[codes[k] // 1000], codes[k] % 1000, ms[k]) for k in range(n.value)]
         by_kind = {}
@@ -585,17 +646,22 @@ def profile_lu_launches(args):
         out["dataflow_trace"] = lu_trace_summary(s)
     fkinds = ["rowscale", "scatter", "extend_add", "panel", "l21_swap_trsm", "-", "gemm", "trinv",
               "trcopy", "gh", "ghcopy", "round_f32"]
-    cap = 1024
+    cap = 16384
     ms = (ctypes.c_double * cap)()
     codes = (ctypes.c_int * cap)()
     n = ctypes.c_int()
-    _lib.check(_lib.lib().v2d_solver_time_lu_factor(s.dev.h, 5, ms, codes, cap, ctypes.byref(n)))
+    _lib.check(_lib.lib().v2d_solver_time_lu_factor(s.dev.h, 5 if grid <= 513 else 2, ms, codes,
+                                                    cap, ctypes.byref(n)))
     by_kind, by_level = {}, {}
     for k in range(n.value):
         kind, lvl = fkinds[codes[k] // 1000], codes[k] % 1000
         by_kind[kind] = by_kind.get(kind, 0.0) + ms[k]
         by_level[lvl] = by_level.get(lvl, 0.0) + ms[k]
-    out["factor"] = {"total_ms": sum(ms[k] for k in range(n.value)), "launches": n.value,
+    st = (ctypes.c_double * 6)()
+    _lib.check(_lib.lib().v2d_solver_lu_stats(s.dev.h, st))
+    total = sum(ms[k] for k in range(n.value))
+    out["factor"] = {"total_ms": total, "launches": n.value, "flops": st[3],
+                     "tflops": st[3] / (total * 1e-3) / 1e12,
                      "by_kind_ms": by_kind, "by_level_ms": by_level}
     print(json.dumps(out), flush=True)
     s.close()
@@ -896,6 +962,8 @@ def main():
                     help="print only the HBM-bound kernel roofline table (--kernels-grid)")
     ap.add_argument("--lu-apply-profile", action="store_true",
                     help="two steps, then two warm LU solves in the NVTX range v2d_lu_apply")
+    ap.add_argument("--profile-grid", type=int, default=IMAX,
+                    help="grid of the --lu-launches profile (the cylinder O-grid N x N)")
     ap.add_argument("--lu-launches", action="store_true",
                     help="per-launch device time of one LU preconditioner solve, warm and cold")
     ap.add_argument("--profile-newton", action="store_true",

@@ -295,10 +295,12 @@ int v2d_solver_velocity(v2d_solver *s, double *u, double *v, double *vmag);
 /* Discrete adjoint (no reference counterpart; the reference has no adjoint):
  * J^T lambda = g for the Jacobian J = dR/dq of the current state (rotation
  * urot), R = -b the residual of the field-blocked 2N system.  FP64 multifrontal
- * factors of J are computed, the transposed solve is refined against J^T
- * products until ||g - J^T lambda|| <= rtol ||g||, max_refine passes, or a
- * pass no longer halves the residual (the attainable accuracy; accepted when
- * below 1e-8).
+ * factors of J are computed (kept while the state and J are unchanged), and
+ * GMRES(30) in FP64 on J^T, preconditioned by the transposed multifrontal
+ * solve, runs until ||g - J^T lambda|| <= rtol ||g|| or 30 * max_refine
+ * iterations (a residual that stagnates below 1e-8 is accepted as the
+ * attainable accuracy).  *refinements receives the GMRES iterations and
+ * *rel_res the final relative residual.
  * g and lambda: host arrays of 2N doubles. */
 int v2d_solver_adjoint(v2d_solver *s, double urot, const double *g, double *lambda, double rtol,
                        int max_refine, int *refinements, double *rel_res);
@@ -396,6 +398,14 @@ int v2d_solver_phase_times(v2d_solver *s, double *out6, int reset);
  * H = U11^-1 U12, which hold as many entries as L21 and U12). */
 int v2d_solver_time_lu_apply(v2d_solver *s, int reps, long long flush_bytes, double *ms_avg,
                              long long *factor_bytes);
+
+/* Measurement aid (no reference counterpart): sizes of the handle's LU
+ * preconditioner -- out6 = fronts, tree levels, factor entries (sum f^2),
+ * flops of one factorization (per front: the partial LU
+ * 2 sum_{k<S} (f-k-1)^2, the pivot-block inverses 2 S^3 / 3, and
+ * G = L21 L11^-1, H = U11^-1 U12 2 (f-S) S^2), factor entries one solve reads
+ * (sum S (2f - S)), work items of the dataflow solve. */
+int v2d_solver_lu_stats(v2d_solver *s, double *out6);
 
 /* Measurement aid (no reference counterpart): one dataflow LU solve of the
  * current factors with a trace of every work item -- global-timer ns at its

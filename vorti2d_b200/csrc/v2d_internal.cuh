@@ -85,6 +85,7 @@ struct MfPlan {
     long long ftotal = 0, nasm = 0;
     int vtotal = 0, utotal = 0;
     double flops = 0.0;   // 2 * sum S f^2 (upper bound of the factorization flops)
+    double factor_flops = 0.0;     // the factorization's flops, front_flops summed
     long long apply_entries = 0;   // factor entries one solve reads: sum S (2f - S)
     std::vector<int> S, f, voff, uoff, child0, child1, parent;
     std::vector<long long> foff;
@@ -114,6 +115,17 @@ struct MfPlan {
     std::vector<int> h_vars, h_cbmap, h_asm_csr, h_asm_row;
     std::vector<long long> h_asm_pos;
 };
+
+// Flops of one front's factorization into the solve's form (S pivots of f
+// variables, m = f - S): the partial LU, 2 sum_{k<S} (f - k - 1)^2; the two
+// inverses of the pivot block, 2 S^3 / 3; G = L21 L11^-1 and H = U11^-1 U12,
+// 2 m S^2 (multiply and add each counted).
+inline double front_flops(int S, int f)
+{
+    auto sq = [](double n) { return n * (n + 1.0) * (2.0 * n + 1.0) / 6.0; };   // sum_{j<=n} j^2
+    const double m = f - S;
+    return 2.0 * (sq(f - 1.0) - sq(m - 1.0)) + 2.0 * S * (double)S * S / 3.0 + 2.0 * m * S * S;
+}
 
 // Error state of the dataflow solve: err is set when a dependency wait ran
 // out (read and reset by mf_check_barrier).
@@ -187,7 +199,8 @@ int mf_apply(const MfPlan *P, const MfFactor *M, const void *b, void *x, const i
              const int *stop_b, cudaStream_t s, long long *n_launches);
 // lambda = A^-T g with the factors (the transposed solve: a bottom-up sweep
 // with U11^-T / H^T, then a top-down sweep with L11^-T / G^T).
-int mf_apply_transpose(const MfPlan *P, MfFactor *M, const void *g, void *lambda, cudaStream_t s);
+int mf_apply_transpose(const MfPlan *P, MfFactor *M, const void *g, void *lambda, cudaStream_t s,
+                       long long *launches = nullptr);
 int mf_flag(const MfFactor *M, int *flag, cudaStream_t s);
 // V2D_ETIMEOUT (and a reset error state) if a dependency wait of the
 // dataflow solve timed out since the last check.
@@ -228,6 +241,8 @@ struct CsrOp {
     int nblk = 0;  // number of 2x2 blocks (or n for point layout)
     const MfPlan *lu_plan = nullptr;   // V2D_PC_LU: factors of this operator
     const MfFactor *lu = nullptr;
+    bool lu_transpose = false;         // the operator is J^T and lu factors J: the
+                                       // preconditioner is the transposed solve
 };
 
 struct KrylovWork;  // defined in v2d_krylov.cu
@@ -270,6 +285,8 @@ struct v2d_solver {
     int lu_last_its = 0;             // Krylov iterations of the last solve with them
     long long lu_factorizations = 0;
     int *tptr = nullptr, *tind = nullptr, *tperm = nullptr;   // transposed CSR pattern (adjoint)
+    double *valT = nullptr;           // J^T values on that pattern (adjoint GMRES)
+    v2d::KrylovWork *kw_adj = nullptr;   // GMRES work space of the adjoint solves
     // versions for the adjoint's factor cache: the state (psi, ome) and the
     // parameters, the assembled values, and the FP64 factors lu[0]
     long long state_ver = 0, val_ver = 0, lu0_ver = 0;

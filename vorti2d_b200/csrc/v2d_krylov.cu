@@ -606,6 +606,14 @@ static void drop_graphs(KrylovWork *w, int which)
     w->fin[which] = nullptr;
 }
 
+// The LU solve a captured cycle launches: -1 none, -2 the transposed solve,
+// else 10 * (dataflow) + kernel form.
+static int lu_form(const CsrOp &A)
+{
+    if (!A.lu) return -1;
+    return A.lu_transpose ? -2 : 10 * A.lu->flow + A.lu->flow_form;
+}
+
 template <class T>
 static int capture_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, double *x,
                          const CsrOp &A, int precond, cudaStream_t s)
@@ -631,8 +639,11 @@ static int capture_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, doub
             if (lu) {
                 zj = Z + (size_t)j * n;
                 long long na = 0;
-                int st = mf_apply(A.lu_plan, A.lu, V + (size_t)j * n, zj, &w->ctl->conv,
-                                  &w->ctl->cyc_stop, s, &na);
+                int st = A.lu_transpose
+                             ? mf_apply_transpose(A.lu_plan, const_cast<MfFactor *>(A.lu),
+                                                  V + (size_t)j * n, zj, s, &na)
+                             : mf_apply(A.lu_plan, A.lu, V + (size_t)j * n, zj, &w->ctl->conv,
+                                        &w->ctl->cyc_stop, s, &na);
                 nl += na;
                 if (st != V2D_OK) {
                     cudaGraph_t junk = nullptr;
@@ -667,7 +678,7 @@ static int capture_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, doub
     w->graph_m[which] = w->m;
     w->graph_pc[which] = precond;
     w->graph_lu[which] = lu ? (const void *)A.lu : nullptr;
-    w->graph_lu_flow[which] = lu ? 10 * A.lu->flow + A.lu->flow_form : -1;
+    w->graph_lu_flow[which] = lu_form(A);
     w->graph_lu_items[which] = lu ? A.lu_plan->items_ver : -1;
     return V2D_OK;
 }
@@ -681,7 +692,7 @@ static int run_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, double *
     if (w->seg[which].empty() || !w->fin[which] || w->graph_m[which] != w->m ||
         w->graph_pc[which] != precond ||
         w->graph_lu[which] != (lu ? (const void *)A.lu : nullptr) ||
-        w->graph_lu_flow[which] != (lu ? 10 * A.lu->flow + A.lu->flow_form : -1) ||
+        w->graph_lu_flow[which] != lu_form(A) ||
         w->graph_lu_items[which] != (lu ? A.lu_plan->items_ver : -1))
         V2D_TRY(capture_cycle<T>(w, which, V, wv, z, Z, x, A, precond, s));
     for (size_t q = 0; q < w->seg[which].size(); ++q) {

@@ -598,6 +598,7 @@ int mf_plan_build(int imax, int jmax, int n, const int *h_rowptr, const int *h_c
     double fl = 0.0;
     for (int id = 0; id < nf; ++id) {
         fl += 2.0 * P->S[id] * (double)P->f[id] * P->f[id];
+        P->factor_flops += front_flops(P->S[id], P->f[id]);
         P->apply_entries += (long long)P->S[id] * (2LL * P->f[id] - P->S[id]);
     }
     P->flops = fl;
@@ -771,6 +772,7 @@ int mf_plan_forest(const std::vector<MfPlan *> &parts, const std::vector<int> &r
         P->maxS = std::max(P->maxS, Q->S[q]);
         P->maxf = std::max(P->maxf, Q->f[q]);
         P->flops += 2.0 * Q->S[q] * (double)Q->f[q] * Q->f[q];
+        P->factor_flops += front_flops(Q->S[q], Q->f[q]);
         P->apply_entries += (long long)Q->S[q] * (2LL * Q->f[q] - Q->S[q]);
     }
     P->ftotal = ftot; P->vtotal = vtot; P->utotal = utot;
@@ -1194,62 +1196,217 @@ __global__ void __launch_bounds__(kL21Rows) k_l21_trsm(int q0, int k, int nl,
         swap_trsm_cols<T>(A, f, S, k, voff[q], blockIdx.x - nl, ipiv, D, src);
 }
 
-// One 64 x 64 tile of a trailing update: A[r][c] -= sum_{t in [ka, kb)}
-// A[r][t] A[t][c] for rows [r0, min(r0 + 64, r1)) and columns
-// [c0, min(c0 + 64, c1)), the inner range in slices of NB staged in shared
-// memory (256 threads with 4 x 4 outputs each).  With one slice (kb - ka <=
-// NB) the sums are formed in the same order as a rank-NB update.
-template <class T>
-__device__ __forceinline__ void gemm_tile_range(T *A, int f, int r0, int r1, int c0, int c1,
-                                                int ka, int kb, T (*As)[kGemmTile + 1],
-                                                T (*Bs)[kGemmTile])
-{
-    constexpr int NB = PanelWidth<T>::v;
-    const int tid = threadIdx.x;
-    const int ty = tid / 16, tx = tid % 16;  // 16x16 threads, 4x4 outputs each
-    T acc[4][4];
+// Accumulator of one 64 x 64 output tile of a CTA of 256 threads, fed NB-wide
+// slices of its two operands through shared memory (Smem: a(rr, t) at
+// refA, b(t, cc) at refB; staged by tile_mac, t fastest for A and cc fastest
+// for B, then mac).
+//   float:  CUDA cores, each thread 4 x 4 outputs (rows ty + 16 a, columns
+//           tx + 16 b).
+//   double: FP64 tensor cores, mma.sync m8n8k4 (the one FP64 tensor-core
+//           instruction on sm_100a: tcgen05 has no FP64 kind).  Warp w owns
+//           rows 32 (w / 4) .. + 32 and columns 16 (w % 4) .. + 16, i.e. 4 x 2
+//           8x8 blocks; per k step of 4 a lane holds A[8 mi + g][t], the B
+//           element [t][8 ni + g] and the outputs [8 mi + g][8 ni + 2 t + j]
+//           (g = lane / 4, t = lane % 4).  Row strides of 36 and 72 doubles
+//           spread a warp's 32 fragment reads evenly over the shared-memory
+//           banks (two wavefronts, the minimum for 256 bytes).
+template <class T> struct TileAcc;
+
+template <> struct TileAcc<float> {
+    static constexpr int NB = PanelWidth<float>::v, TL = kGemmTile;
+    struct Smem {
+        float A[NB][TL + 1];
+        float B[NB][TL];
+    };
+    float acc[4][4];
+    __device__ __forceinline__ static float &refA(Smem &s, int rr, int t) { return s.A[t][rr]; }
+    __device__ __forceinline__ static float &refB(Smem &s, int t, int cc) { return s.B[t][cc]; }
+    __device__ __forceinline__ void zero()
+    {
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
-    for (int k = ka; k < kb; k += NB) {
-        const int kw = min(NB, kb - k);
-        for (int e = tid; e < kGemmTile * NB; e += blockDim.x) {
-            const int rr = e / NB, t = e - rr * NB;   // A tile: rows r0+rr, cols k+t
-            const int r = r0 + rr;
-            As[t][rr] = (r < r1 && t < kw) ? A[(long long)r * f + k + t] : T(0);
-        }
-        for (int e = tid; e < NB * kGemmTile; e += blockDim.x) {
-            const int t = e / kGemmTile, cc = e - t * kGemmTile;
-            const int c = c0 + cc;
-            Bs[t][cc] = (c < c1 && t < kw) ? A[(long long)(k + t) * f + c] : T(0);
-        }
-        __syncthreads();
+            for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
+    }
+    __device__ __forceinline__ void mac(const Smem &s)
+    {
+        const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
 #pragma unroll 4
         for (int t = 0; t < NB; ++t) {
-            T av[4], bv[4];
+            float av[4], bv[4];
 #pragma unroll
-            for (int a = 0; a < 4; ++a) av[a] = As[t][ty + 16 * a];
+            for (int a = 0; a < 4; ++a) av[a] = s.A[t][ty + 16 * a];
 #pragma unroll
-            for (int b = 0; b < 4; ++b) bv[b] = Bs[t][tx + 16 * b];
+            for (int b = 0; b < 4; ++b) bv[b] = s.B[t][tx + 16 * b];
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
                 for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
         }
-        __syncthreads();
     }
+    // fn(rr, cc, value) for every output of the thread
+    template <class Fn> __device__ __forceinline__ void each(Fn fn) const
+    {
+        const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        const int r = r0 + ty + 16 * a;
-        if (r >= r1) continue;
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int c = c0 + tx + 16 * b;
-            if (c < c1) A[(long long)r * f + c] -= acc[a][b];
+            for (int b = 0; b < 4; ++b) fn(ty + 16 * a, tx + 16 * b, acc[a][b]);
+    }
+};
+
+__device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+template <> struct TileAcc<double> {
+    static constexpr int NB = PanelWidth<double>::v, TL = kGemmTile;
+    struct Smem {
+        double A[TL][NB + 4];
+        double B[NB][TL + 8];
+    };
+    double acc[4][2][2];
+    __device__ __forceinline__ static double &refA(Smem &s, int rr, int t) { return s.A[rr][t]; }
+    __device__ __forceinline__ static double &refB(Smem &s, int t, int cc) { return s.B[t][cc]; }
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    }
+    __device__ __forceinline__ void mac(const Smem &s)
+    {
+        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+        const int wr = (w >> 2) * 32, wc = (w & 3) * 16;
+#pragma unroll
+        for (int k = 0; k < NB; k += 4) {
+            double a[4], b[2];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi) a[mi] = s.A[wr + 8 * mi + g][k + t];
+#pragma unroll
+            for (int ni = 0; ni < 2; ++ni) b[ni] = s.B[k + t][wc + 8 * ni + g];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 2; ++ni)
+                    dmma_8x8x4(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
         }
     }
+    template <class Fn> __device__ __forceinline__ void each(Fn fn) const
+    {
+        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+        const int wr = (w >> 2) * 32, wc = (w & 3) * 16;
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+                for (int j = 0; j < 2; ++j)
+                    fn(wr + 8 * mi + g, wc + 8 * ni + 2 * t + j, acc[mi][ni][j]);
+    }
+};
+
+// Asynchronous global -> shared copy of one element (cp.async, L1-allocating
+// form: 4- and 8-byte copies need no 16-byte alignment, so any row stride
+// works); ok == false writes zero and reads nothing.
+template <class T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src, bool ok)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src),
+                 "n"((int)sizeof(T)), "r"(ok ? (int)sizeof(T) : 0));
 }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// acc += sum over k in [ka, kb) of a(rr, k) b(k, cc), in NB-wide slices
+// through two shared buffers (sm[0], sm[1]): the copies of slice s + 1 are in
+// flight while the tensor cores (or CUDA cores) work on slice s.  srcA(rr, k)
+// and srcB(k, cc) give the element's address or nullptr (zero); oneB(k, cc)
+// marks B entries that are 1 instead (a unit diagonal), written after the
+// slice's copies have landed.  base: any valid address (the source of
+// zero-filled copies, never read).
+template <class T, class SA, class SB, class OB>
+__device__ __forceinline__ void tile_mac(TileAcc<T> &acc, typename TileAcc<T>::Smem *sm, int ka,
+                                         int kb, const T *base, SA srcA, SB srcB, OB oneB)
+{
+    constexpr int NB = PanelWidth<T>::v;
+    constexpr int TL = kGemmTile;
+    const int tid = threadIdx.x;
+    const int ns = (kb - ka + NB - 1) / NB;
+    auto stage = [&](int sl) {
+        const int k = ka + sl * NB;
+        typename TileAcc<T>::Smem &b = sm[sl & 1];
+        for (int e = tid; e < TL * NB; e += blockDim.x) {
+            const int rr = e / NB, t = e - rr * NB;
+            const T *p = k + t < kb ? srcA(rr, k + t) : nullptr;
+            cp_async_elem(&TileAcc<T>::refA(b, rr, t), p ? p : base, p != nullptr);
+        }
+        for (int e = tid; e < NB * TL; e += blockDim.x) {
+            const int t = e / TL, cc = e - t * TL;
+            const T *p = k + t < kb ? srcB(k + t, cc) : nullptr;
+            cp_async_elem(&TileAcc<T>::refB(b, t, cc), p ? p : base, p != nullptr);
+        }
+        cp_async_commit();
+    };
+    auto ones = [&](int sl) {
+        const int k = ka + sl * NB;
+        typename TileAcc<T>::Smem &b = sm[sl & 1];
+        for (int e = tid; e < NB * TL; e += blockDim.x) {
+            const int t = e / TL, cc = e - t * TL;
+            if (k + t < kb && oneB(k + t, cc)) TileAcc<T>::refB(b, t, cc) = T(1);
+        }
+    };
+    if (ns > 0) stage(0);
+    for (int sl = 0; sl < ns; ++sl) {
+        if (sl + 1 < ns) {
+            stage(sl + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        ones(sl);
+        __syncthreads();
+        acc.mac(sm[sl & 1]);
+        __syncthreads();
+    }
+}
+
+// One 64 x 64 tile of a trailing update: A[r][c] -= sum_{t in [ka, kb)}
+// A[r][t] A[t][c] for rows [r0, min(r0 + 64, r1)) and columns
+// [c0, min(c0 + 64, c1)).
+template <class T>
+__device__ __forceinline__ void gemm_tile_range(T *A, int f, int r0, int r1, int c0, int c1,
+                                                int ka, int kb, typename TileAcc<T>::Smem *sm)
+{
+    TileAcc<T> acc;
+    acc.zero();
+    tile_mac<T>(
+        acc, sm, ka, kb, A,
+        [&](int rr, int k) -> const T * {
+            const int r = r0 + rr;
+            return r < r1 ? A + (long long)r * f + k : nullptr;
+        },
+        [&](int k, int cc) -> const T * {
+            const int c = c0 + cc;
+            return c < c1 ? A + (long long)k * f + c : nullptr;
+        },
+        [](int, int) { return false; });
+    acc.each([&](int rr, int cc, T v) {
+        const int r = r0 + rr, c = c0 + cc;
+        if (r < r1 && c < c1) A[(long long)r * f + c] -= v;
+    });
+}
+
+// dynamic shared memory of k_gemm and k_gh: the two operand buffers
+template <class T> constexpr size_t tile_smem_bytes() { return 2 * sizeof(typename TileAcc<T>::Smem); }
 
 // Trailing updates after panel [k, k + w), with delayed updates in
 // super-panels of W columns (a multiple of NB; W = NB is the plain
@@ -1273,8 +1430,8 @@ __global__ void __launch_bounds__(256) k_gemm(int q0, int k, int W, const int *_
 {
     constexpr int NB = PanelWidth<T>::v;
     constexpr int TL = kGemmTile;
-    __shared__ T As[NB][TL + 1];
-    __shared__ T Bs[NB][TL];
+    extern __shared__ __align__(16) unsigned char tile_raw[];
+    typename TileAcc<T>::Smem *sm = reinterpret_cast<typename TileAcc<T>::Smem *>(tile_raw);
     __shared__ T U[NB][NB + 1];
     __shared__ int pv[NB];
     const int q = q0 + blockIdx.y;
@@ -1288,20 +1445,20 @@ __global__ void __launch_bounds__(256) k_gemm(int q0, int k, int W, const int *_
     if (kn < E) {
         const int nr = (f - kn + TL - 1) / TL, nc = (E - kn + TL - 1) / TL;
         if (t < nr * nc) {
-            gemm_tile_range<T>(A, f, kn + (t / nc) * TL, f, kn + (t % nc) * TL, E, k, kn, As, Bs);
+            gemm_tile_range<T>(A, f, kn + (t / nc) * TL, f, kn + (t % nc) * TL, E, k, kn, sm);
             first = t == 0;
         } else {
             t -= nr * nc;
             const int wn = min(NB, S - kn), nf = (f - E + TL - 1) / TL;
             if (t >= nf) return;
-            gemm_tile_range<T>(A, f, kn, kn + wn, E + t * TL, f, k0, kn, As, Bs);
+            gemm_tile_range<T>(A, f, kn, kn + wn, E + t * TL, f, k0, kn, sm);
         }
     } else {
         const int rem = f - E;
         if (rem <= 0) return;
         const int nt = (rem + TL - 1) / TL;
         if (t >= nt * nt) return;
-        gemm_tile_range<T>(A, f, E + (t / nt) * TL, f, E + (t % nt) * TL, f, k0, E, As, Bs);
+        gemm_tile_range<T>(A, f, E + (t / nt) * TL, f, E + (t % nt) * TL, f, k0, E, sm);
         first = t == 0;
     }
     if (first && kn < S) {
@@ -1524,8 +1681,8 @@ __global__ void k_round_f32(const double *__restrict__ a, float *__restrict__ b,
 // [0, S) x columns [S, f)) of every front of a level, from the inverted pivot
 // block, into the level's scratch (G row-major m x S, then H S x m; copied over
 // L21 and U12 by k_ghcopy: each tile of G reads L21 entries that other tiles
-// overwrite).  One CTA per 64 x 64 output tile, 256 threads with 4 x 4
-// outputs each; the triangular factor bounds the inner range (G: k >= c0,
+// overwrite).  One CTA per 64 x 64 output tile (TileAcc: CUDA cores in FP32,
+// FP64 tensor cores in FP64); the triangular factor bounds the inner range (G: k >= c0,
 // with L11^-1's unit diagonal; H: k >= r0).  Grid: (tiles of G then of H for
 // the level's largest front, fronts).
 template <class T>
@@ -1534,10 +1691,9 @@ __global__ void __launch_bounds__(256) k_gh(int q0, const int *__restrict__ S_,
                                             const long long *__restrict__ foff,
                                             const long long *__restrict__ goff, const T *F, T *gh)
 {
-    constexpr int NB = PanelWidth<T>::v;
     constexpr int TL = kGemmTile;
-    __shared__ T As[NB][TL + 1];
-    __shared__ T Bs[NB][TL];
+    extern __shared__ __align__(16) unsigned char tile_raw[];
+    typename TileAcc<T>::Smem *sm = reinterpret_cast<typename TileAcc<T>::Smem *>(tile_raw);
     const int q = q0 + blockIdx.y;
     const int S = S_[q], f = f_[q], m = f - S;
     if (m <= 0) return;
@@ -1558,61 +1714,29 @@ __global__ void __launch_bounds__(256) k_gh(int q0, const int *__restrict__ S_,
         c0 = S + (t % tm) * TL;
         kb = r0;
     }
-    const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
-    T acc[4][4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) acc[a][c] = T(0);
-    for (int k = kb; k < S; k += NB) {
-        for (int e = tid; e < TL * NB; e += blockDim.x) {
-            const int rr = e / NB, tt = e - rr * NB;
-            const int r = r0 + rr, kk = k + tt;
-            T a = T(0);
-            if (kk < S && (isG ? r < f : (r < S && kk >= r))) a = A[(long long)r * f + kk];
-            As[tt][rr] = a;
+    TileAcc<T> acc;
+    acc.zero();
+    // G: L21 rows times L11^-1 (strictly lower part stored, unit diagonal);
+    // H: U11^-1 (upper part with the diagonal) times U12
+    tile_mac<T>(
+        acc, sm, kb, S, A,
+        [&](int rr, int kk) -> const T * {
+            const int r = r0 + rr;
+            return (isG ? r < f : (r < S && kk >= r)) ? A + (long long)r * f + kk : nullptr;
+        },
+        [&](int kk, int cc) -> const T * {
+            const int c = c0 + cc;
+            return (isG ? (c < S && kk > c) : c < f) ? A + (long long)kk * f + c : nullptr;
+        },
+        [&](int kk, int cc) { return isG && kk == c0 + cc; });
+    acc.each([&](int rr, int cc, T v) {
+        const int r = r0 + rr, col = c0 + cc;
+        if (isG) {
+            if (r < f && col < S) out[(long long)(r - S) * S + col] = v;
+        } else if (r < S && col < f) {
+            out[(long long)m * S + (long long)r * m + (col - S)] = v;
         }
-        for (int e = tid; e < NB * TL; e += blockDim.x) {
-            const int tt = e / TL, cc = e - tt * TL;
-            const int c = c0 + cc, kk = k + tt;
-            T bv = T(0);
-            if (kk < S) {
-                if (isG) {
-                    if (c < S) bv = kk > c ? A[(long long)kk * f + c] : (kk == c ? T(1) : T(0));
-                } else if (c < f) {
-                    bv = A[(long long)kk * f + c];
-                }
-            }
-            Bs[tt][cc] = bv;
-        }
-        __syncthreads();
-#pragma unroll 4
-        for (int tt = 0; tt < NB; ++tt) {
-            T av[4], bv[4];
-#pragma unroll
-            for (int a = 0; a < 4; ++a) av[a] = As[tt][ty + 16 * a];
-#pragma unroll
-            for (int c = 0; c < 4; ++c) bv[c] = Bs[tt][tx + 16 * c];
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int c = 0; c < 4; ++c) acc[a][c] += av[a] * bv[c];
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        const int r = r0 + ty + 16 * a;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int col = c0 + tx + 16 * c;
-            if (isG) {
-                if (r < f && col < S) out[(long long)(r - S) * S + col] = acc[a][c];
-            } else if (r < S && col < f) {
-                out[(long long)m * S + (long long)r * m + (col - S)] = acc[a][c];
-            }
-        }
-    }
+    });
 }
 
 // G and H of the level's fronts: scratch -> factor storage.
@@ -2354,6 +2478,9 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
     constexpr int NB = PanelWidth<T>::v;
     T *F = (T *)M->F;
     long long launches = 0;
+    const size_t tile_smem = tile_smem_bytes<T>();
+    V2D_CUDA_TRY(raise_dyn_smem((const void *)k_gemm<T>, tile_smem));
+    V2D_CUDA_TRY(raise_dyn_smem((const void *)k_gh<T>, tile_smem));
     // with ev: an event is recorded after each kernel (kind * 1000 + level;
     // kinds 0 rowscale, 1 scatter, 2 extend_add, 3 first panel, 4 L21 + row
     // swaps + U12, 6 trailing update + next panel, 7 trinv, 8 trcopy, 9 G/H
@@ -2430,7 +2557,7 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
             // the super-panel's full update)
             const int ntile = nt * nt + nt;
             for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
-                k_gemm<T><<<dim3(ntile, std::min(nq - qb, kMaxFrontsY)), 256, 0, s>>>(
+                k_gemm<T><<<dim3(ntile, std::min(nq - qb, kMaxFrontsY)), 256, tile_smem, s>>>(
                     q0 + qb, k, W, P->d_S, P->d_f, P->d_foff, P->d_voff, F, M->ipiv, M->perm,
                     M->flag);
                 if (qb > 0) ++launches;
@@ -2468,7 +2595,7 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
             const long long sm = 2LL * P->lvl_maxS[L] * P->lvl_maxm[L];
             const int gcg = (int)std::max(1LL, std::min<long long>((sm + 255) / 256, 256));
             for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
-                k_gh<T><<<dim3(2 * ts * tm, std::min(nq - qb, kMaxFrontsY)), 256, 0, s>>>(
+                k_gh<T><<<dim3(2 * ts * tm, std::min(nq - qb, kMaxFrontsY)), 256, tile_smem, s>>>(
                     q0 + qb, P->d_S, P->d_f, P->d_foff, P->d_goff, F, (T *)M->gh);
                 if (qb > 0) ++launches;
             }
@@ -2621,7 +2748,7 @@ int mf_apply(const MfPlan *P, const MfFactor *M, const void *b, void *x, const i
 
 template <class T>
 static int apply_transpose_launches(const MfPlan *P, MfFactor *M, const T *g, T *lam,
-                                    cudaStream_t s)
+                                    cudaStream_t s, long long *launches)
 {
     const MfDev D = mf_dev(P, M);
     const T *F = (const T *)(M->fact64 ? M->F32 : M->F);
@@ -2637,14 +2764,18 @@ static int apply_transpose_launches(const MfPlan *P, MfFactor *M, const T *g, T 
     }
     V2D_CUDA_TRY(cudaGetLastError());
     count_launches(2LL * P->nlevel);
+    if (launches) *launches = 2LL * P->nlevel;
     return V2D_OK;
 }
 
-int mf_apply_transpose(const MfPlan *P, MfFactor *M, const void *g, void *lambda, cudaStream_t s)
+int mf_apply_transpose(const MfPlan *P, MfFactor *M, const void *g, void *lambda, cudaStream_t s,
+                       long long *launches)
 {
     if (M->fp32)
-        return apply_transpose_launches<float>(P, M, (const float *)g, (float *)lambda, s);
-    return apply_transpose_launches<double>(P, M, (const double *)g, (double *)lambda, s);
+        return apply_transpose_launches<float>(P, M, (const float *)g, (float *)lambda, s,
+                                               launches);
+    return apply_transpose_launches<double>(P, M, (const double *)g, (double *)lambda, s,
+                                            launches);
 }
 
 int mf_flag(const MfFactor *M, int *flag, cudaStream_t s)

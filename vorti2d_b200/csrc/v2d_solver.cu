@@ -95,6 +95,10 @@ void drop_transpose(v2d_solver *S)
     for (int *p : {S->tptr, S->tind, S->tperm})
         if (p) cudaFree(p);
     S->tptr = S->tind = S->tperm = nullptr;
+    if (S->valT) cudaFree(S->valT);
+    S->valT = nullptr;
+    krylov_destroy(S->kw_adj);
+    S->kw_adj = nullptr;
 }
 
 void drop_lu(v2d_solver *S)
@@ -525,6 +529,18 @@ extern "C" int v2d_solver_velocity(v2d_solver *S, double *u, double *v, double *
 // ------------------------------------------------------------------ adjoint
 namespace {
 
+// GMRES restart length of the adjoint solves
+constexpr int kAdjRestart = 30;
+
+// valT[e] = val[tperm[e]]: J's values in the order of the transposed pattern.
+__global__ void k_gather_vals(long long nnz, const int *__restrict__ tperm,
+                              const double *__restrict__ val, double *valT)
+{
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nnz;
+         e += (long long)gridDim.x * blockDim.x)
+        valT[e] = val[tperm[e]];
+}
+
 // y = J^T x over the transposed pattern (values gathered through tperm).
 __global__ void k_spmv_t(int n, const int *__restrict__ tptr, const int *__restrict__ tind,
                          const int *__restrict__ tperm, const double *__restrict__ val,
@@ -535,16 +551,6 @@ __global__ void k_spmv_t(int n, const int *__restrict__ tptr, const int *__restr
         double s = 0.0;
         for (int e = tptr[r]; e < tptr[r + 1]; ++e) s += val[tperm[e]] * x[tind[e]];
         y[r] = s;
-    }
-}
-
-__global__ void k_axpy_res(int n, const double *__restrict__ g, const double *__restrict__ jtl,
-                           const double *__restrict__ d, double *lam, double *r, int mode)
-{
-    V2D_GRID_STRIDE(i, n)
-    {
-        if (mode == 0) lam[i] += d[i];          // lambda += delta
-        else r[i] = g[i] - jtl[i];               // r = g - J^T lambda
     }
 }
 
@@ -829,42 +835,60 @@ extern "C" int v2d_solver_adjoint(v2d_solver *S, double urot, const double *g_ho
     }
     V2D_TRY(ensure_transpose(S));
     const size_t n = g.n;
+    // J^T on the transposed pattern, solved by GMRES(30) in FP64 with the
+    // transposed LU solve as the preconditioner: with factors whose pivoting
+    // stays inside 32-row blocks, the plain iterative refinement x += (LU)^-T r
+    // stalls on wide fronts; GMRES converges in a few iterations instead
+    if (!S->valT) V2D_CUDA_TRY(cudaMalloc(&S->valT, (size_t)g.nnz * sizeof(double)));
+    if (!S->kw_adj) V2D_TRY(krylov_create(&S->kw_adj, g.n, kAdjRestart, S->s));
+    k_gather_vals<<<grid_for(g.nnz, 256), 256, 0, S->s>>>(g.nnz, S->tperm, g.val, S->valT);
+    V2D_CUDA_TRY(cudaGetLastError());
+    count_launches(1);
     DevBuf<double> buf;
-    V2D_TRY(buf.alloc(5 * n, S->s));
-    double *dg = buf.p, *lam = dg + n, *r = lam + n, *del = r + n, *jtl = del + n;
+    V2D_TRY(buf.alloc(3 * n, S->s));
+    double *dg = buf.p, *lam = dg + n, *jtl = lam + n;
     V2D_CUDA_TRY(cudaMemcpyAsync(dg, g_host, n * sizeof(double), cudaMemcpyHostToDevice, S->s));
-    V2D_CUDA_TRY(cudaMemsetAsync(lam, 0, n * sizeof(double), S->s));
-    V2D_CUDA_TRY(cudaMemcpyAsync(r, dg, n * sizeof(double), cudaMemcpyDeviceToDevice, S->s));
-    std::vector<double> hr(n), hg(g_host, g_host + n);
-    const double gn = host_norm(hg);
-    double rel = gn > 0.0 ? 1.0 : 0.0, prev = HUGE_VAL;
-    int it = 0;
+    CsrOp AT;
+    AT.n = g.n;
+    AT.nnz = g.nnz;
+    AT.rowptr = S->tptr;
+    AT.colind = S->tind;
+    AT.val = S->valT;
+    AT.layout = 0;
+    AT.nblk = g.n;
+    AT.lu_plan = S->plan;
+    AT.lu = S->lu[0];
+    AT.lu_transpose = true;
+    v2d_krylov_params kp;
+    v2d_krylov_defaults(&kp);
+    kp.restart = kAdjRestart;
+    kp.max_it = kAdjRestart * max_refine;
+    kp.rtol = rtol;
+    kp.atol = 0.0;
+    kp.precond = V2D_PC_LU;
+    kp.precision = V2D_PREC_FP64;
+    v2d_lin_stats ls{};
+    V2D_TRY(krylov_solve(S->kw_adj, AT, dg, lam, kp, &ls, S->s));
+    // the true residual g - J^T lambda, on the original pattern
     const int grid = grid_for(n, 256);
-    // refine until rtol, or until a pass no longer halves the residual (the
-    // attainable accuracy of the FP64 factors)
-    while (rel > rtol && it < max_refine && rel < 0.5 * prev) {
-        prev = rel;
-        V2D_TRY(mf_apply_transpose(S->plan, S->lu[0], r, del, S->s));
-        k_axpy_res<<<grid, 256, 0, S->s>>>(g.n, dg, jtl, del, lam, r, 0);
-        k_spmv_t<<<grid, 256, 0, S->s>>>(g.n, S->tptr, S->tind, S->tperm, g.val, lam, jtl);
-        k_axpy_res<<<grid, 256, 0, S->s>>>(g.n, dg, jtl, del, lam, r, 1);
-        V2D_CUDA_TRY(cudaGetLastError());
-        count_launches(3);
-        V2D_CUDA_TRY(cudaMemcpyAsync(hr.data(), r, n * sizeof(double), cudaMemcpyDeviceToHost, S->s));
-        V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
-        rel = gn > 0.0 ? host_norm(hr) / gn : 0.0;
-        ++it;
-        if (!std::isfinite(rel)) {
-            set_error("solver_adjoint: non-finite residual");
-            return V2D_ENONFINITE;
-        }
-    }
+    k_spmv_t<<<grid, 256, 0, S->s>>>(g.n, S->tptr, S->tind, S->tperm, g.val, lam, jtl);
+    V2D_CUDA_TRY(cudaGetLastError());
+    count_launches(1);
+    std::vector<double> hr(n), hg(g_host, g_host + n);
+    V2D_CUDA_TRY(cudaMemcpyAsync(hr.data(), jtl, n * sizeof(double), cudaMemcpyDeviceToHost, S->s));
     V2D_CUDA_TRY(cudaMemcpyAsync(lam_host, lam, n * sizeof(double), cudaMemcpyDeviceToHost, S->s));
     V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
-    if (refinements) *refinements = it;
+    for (size_t i = 0; i < n; ++i) hr[i] = hg[i] - hr[i];
+    const double gn = host_norm(hg);
+    const double rel = gn > 0.0 ? host_norm(hr) / gn : 0.0;
+    if (!std::isfinite(rel)) {
+        set_error("solver_adjoint: non-finite residual");
+        return V2D_ENONFINITE;
+    }
+    if (refinements) *refinements = ls.iterations;
     if (rel_res) *rel_res = rel;
     if (rel > rtol && rel > 1e-8) {
-        set_error("solver_adjoint: residual %.3e after %d refinements", rel, it);
+        set_error("solver_adjoint: residual %.3e after %d GMRES iterations", rel, ls.iterations);
         return V2D_ENOTCONVERGED;
     }
     return V2D_OK;
@@ -941,6 +965,21 @@ extern "C" int v2d_solver_time_lu_apply(v2d_solver *S, int reps, long long flush
     V2D_ARG_CHECK(S->lu[q] && S->lu_ready, "time_lu_apply: no factors yet (run a Newton iteration)");
     *factor_bytes = S->plan->apply_entries * (long long)(q ? sizeof(float) : sizeof(double));
     return mf_time_apply(S->plan, S->lu[q], reps, (size_t)flush_bytes, S->s, ms_avg);
+}
+
+extern "C" int v2d_solver_lu_stats(v2d_solver *S, double *out6)
+{
+    V2D_ARG_CHECK(S && out6, "lu_stats: bad arguments");
+    V2D_ARG_CHECK(S->prm.krylov.precond == V2D_PC_LU && S->plan,
+                  "lu_stats: the handle does not use the LU preconditioner");
+    const MfPlan *P = S->plan;
+    out6[0] = P->nfront;
+    out6[1] = P->nlevel;
+    out6[2] = (double)P->ftotal;
+    out6[3] = P->factor_flops;
+    out6[4] = (double)P->apply_entries;
+    out6[5] = P->nitems;
+    return V2D_OK;
 }
 
 extern "C" int v2d_solver_time_lu_launches(v2d_solver *S, int reps, long long flush_bytes,

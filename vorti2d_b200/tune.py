@@ -29,7 +29,7 @@ import numpy as np
 from . import _lib
 from ._lib import check, lib
 
-CANDIDATES = (0, 8, 16, 32, 64, 128)
+CANDIDATES = (0, 8, 16, 32, 64, 128, 256)
 
 
 def item_rows(solver) -> list:
@@ -78,13 +78,16 @@ def _key(solver) -> str:
     return f"{solver.imax}x{solver.jmax}/{cfg.precision}/{cfg.lu_factors}"
 
 
-def tune_lu_solve(solver, candidates=CANDIDATES, sweeps: int = 2, reps: int = 30,
+def tune_lu_solve(solver, candidates=CANDIDATES, sweeps: int = 2, reps: int | None = None,
                   path: str | None = None, gain: float = 0.01) -> dict:
     """Tune the solver's rows per item in place (its factors must exist: run a
     Newton iteration first).  A trial replaces the current choice when it is
-    faster by more than `gain` (relative).  Returns the record (and merges it
-    into the JSON file at `path` when given)."""
+    faster by more than `gain` (relative).  `reps` applications per timing
+    (default: about 10 ms of them, 3 to 30).  Returns the record (and merges
+    it into the JSON file at `path` when given)."""
     rows = item_rows(solver)
+    if reps is None:
+        reps = int(min(30, max(3, round(10.0 / max(time_apply(solver, 3, 1), 1e-3)))))
     t0 = time_apply(solver, reps)
     best = t0
     trials = 0
@@ -116,7 +119,7 @@ def tune_lu_solve(solver, candidates=CANDIDATES, sweeps: int = 2, reps: int = 30
             break
     set_item_rows(solver, rows)
     rec = {"key": _key(solver), "rows": rows, "form": form, "ms": best, "default_ms": t0,
-           "trials": trials, "candidates": list(candidates)}
+           "trials": trials, "reps": reps, "candidates": list(candidates)}
     if path:
         table = {}
         if os.path.exists(path):
