@@ -37,9 +37,46 @@ def test_transposed_solve(v2d, oracle_mod):
     lam, its, rel = adjoint_solve(s, g, rtol=1e-12)
     ip, ix, dv, _ = s.dev.system(urot=0.0)
     J = sp.csr_matrix((dv, ix, ip), shape=(2 * s.ndof, 2 * s.ndof))
-    # refinement stops at the attainable accuracy of the FP64 factors
+    # GMRES on J^T, preconditioned by the transposed solve of FP64 factors
     assert np.linalg.norm(J.T @ lam - g) <= 1e-10 * np.linalg.norm(g), (its, rel)
     assert its <= 6
+    s.close()
+
+
+def test_transposed_solve_wide_fronts(v2d, oracle_mod):
+    """257x257 unsteady cylinder after one BDF2 step (separators of up to 514
+    unknowns): J^T lambda = g to 1e-10 through GMRES on J^T with the
+    transposed multifrontal solve as its preconditioner."""
+    from vorti2d_b200.adjoint import adjoint_solve
+    xg, yg = oracle_mod.generate_cylinder(257, 257)
+    cfg = v2d.Config(verbose=False, write_csv=False, write_xdmf=False, compute_forces=False,
+                     re=200.0, steady=False, dt_phys=0.05, farfield_bc="outflow",
+                     pseudo_tol=1e-12, max_pseudo_iter=8, ksp_rtol=1e-12, precision="fp64")
+    s = v2d.Solver(cfg, mesh=(xg, yg))
+    s.advance(s.times()[0])
+    g = np.random.default_rng(1).standard_normal(2 * s.ndof)
+    lam, its, rel = adjoint_solve(s, g, rtol=1e-10)
+    ip, ix, dv, _ = s.dev.system(urot=cfg.u_rot(0.0))
+    J = sp.csr_matrix((dv, ix, ip), shape=(2 * s.ndof, 2 * s.ndof))
+    assert np.linalg.norm(J.T @ lam - g) <= 2e-10 * np.linalg.norm(g), (its, rel)
+    s.close()
+
+
+def test_ser_continuation_reaches_the_newton_state(v2d, oracle_mod):
+    """steady_solve_ser (pseudo-time steps whose dtau grows as the update
+    norm falls) ends on the state plain Newton reaches: the fixed point
+    carries no pseudo-time term."""
+    from vorti2d_b200.adjoint import steady_solve_ser
+    xg, yg = oracle_mod.generate_cylinder(IMAX, JMAX)
+    ref = solve(v2d, xg, yg, RE, ADEG)
+    s = v2d.Solver(steady_cfg(v2d, RE, ADEG), mesh=(xg, yg))
+    res, its = steady_solve_ser(s, dtau0=0.5, max_iter=200)
+    assert res <= 1e-13 and its > 0, (res, its)
+    for a, b in ((s.psi, ref.psi), (s.ome, ref.ome)):
+        assert np.max(np.abs(a - b)) <= 1e-9 * max(1.0, np.max(np.abs(b)))
+    assert abs(s.force_coeffs().cd - ref.force_coeffs().cd) <= 1e-10
+    assert s.dev.params.invdtau == 0.0
+    ref.close()
     s.close()
 
 

@@ -134,6 +134,38 @@ def force_vjp(solver, weights, alpha_h=1e-3):
 
 
 # ------------------------------------------------------------------ shape
+def steady_solve_ser(solver, dtau0=1.0, tol=None, max_iter=300, dtau_max=1e12):
+    """Steady state by pseudo-time continuation with switched evolution
+    relaxation (Mulder and van Leer, 1985): iteration k adds 1/dtau_k to the
+    Newton Jacobian's diagonal, dtau_k = dtau0 * res_0 / res_{k-1} (capped at
+    dtau_max), so the first iterations are damped pseudo-time steps and the
+    last ones Newton steps as the update norm res = ||dq||/(2N) falls.  The
+    residual itself carries no pseudo-time term, so the fixed point is the
+    steady solution of the reference's equations.  For cases where Newton
+    from the free stream diverges.  Returns (res, iterations); the handle's
+    own 1/dtau is restored."""
+    dev, cfg = solver.dev, solver.cfg
+    tol = cfg.pseudo_tol if tol is None else float(tol)
+    urot = cfg.u_rot(0.0)
+    keep = dev.params.invdtau
+    res0, res, it, dtau = None, math.inf, 0, float(dtau0)
+    try:
+        while res > tol and it < max_iter:
+            dev.set_invdtau(1.0 / dtau)
+            code, res, _ = dev.newton(urot)
+            solver._host_state = None
+            if code not in (_lib.V2D_OK, _lib.V2D_ENOTCONVERGED):
+                check(code, "steady_solve_ser")
+            if not math.isfinite(res):
+                break
+            it += 1
+            res0 = res if res0 is None else res0
+            dtau = min(dtau_max, dtau0 * res0 / max(res, 1e-300))
+    finally:
+        dev.set_invdtau(keep)
+    return res, it
+
+
 def wall_normals(xg, yg):
     """Outward unit normals (nx, ny) of the P = imax-1 distinct wall nodes
     (j = 0) of an O-grid (xg, yg of shape (imax, jmax)), from the periodic

@@ -96,6 +96,14 @@ class DeviceState:
         self.params.re = float(re)
         check(lib().v2d_solver_set_params(self.h, ctypes.byref(self.params)), "set_params")
 
+    def set_invdtau(self, invdtau: float):
+        """Change the pseudo-time term 1/dtau that the Newton Jacobian's
+        diagonal carries (0: plain Newton)."""
+        if not (np.isfinite(invdtau) and invdtau >= 0):
+            raise ValueError(f"set_invdtau: 1/dtau must be finite and >= 0, got {invdtau}")
+        self.params.invdtau = float(invdtau)
+        check(lib().v2d_solver_set_params(self.h, ctypes.byref(self.params)), "set_params")
+
     def set_state(self, psi, ome, omeold, omeoldold):
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (psi, ome, omeold, omeoldold)]
         for a in arrs:
