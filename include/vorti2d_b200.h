@@ -375,13 +375,23 @@ int v2d_lu_plan_info(int imax, int jmax, const int *indptr, const int *indices, 
 /* Planning aid for the preconditioner solve's work items (host only; no
  * reference counterpart): info4 = {work items, dependency counters, fronts,
  * levels}; when cap_items >= items, items gets 12 ints per item (kind 0
- * forward / 1 backward, front, first row, end row, wait counter and target,
- * second wait counter and target, two done counters, tree level, 0; -1 for
- * none); when cap_fronts >= fronts, fronts3 gets each front's pivots S, size f and
+ * forward rows / 1 backward rows / 2 forward gather / 3 backward gather,
+ * front, first row, end row, wait counter and target, second wait counter and
+ * target, two done counters, tree level, 1 for the items of a front with
+ * gather items else 0; -1 for none); when cap_fronts >= fronts, fronts3 gets each front's pivots S, size f and
  * parent (-1 at the root).  Items run in this order in the one-launch
  * dataflow solve; the plan checks that every wait is met by earlier items. */
 int v2d_lu_solve_plan(int imax, int jmax, const int *indptr, const int *indices, int leaf,
                       int *info4, int *items, int cap_items, int *fronts3, int cap_fronts);
+
+/* Planning aid (no reference counterpart): v2d_lu_solve_plan with an explicit
+ * work-item split, rows[L] per tree level L (nrows = levels): 0 whole fronts,
+ * R > 0 items of R rows, R < 0 items of -R rows after one gather item per
+ * front split into several (kinds 2 forward and 3 backward in the table).
+ * rows null: the default split. */
+int v2d_lu_solve_plan_split(int imax, int jmax, const int *indptr, const int *indices, int leaf,
+                            const int *rows, int nrows, int *info4, int *items, int cap_items,
+                            int *fronts3, int cap_fronts);
 
 /* Measurement aid (no reference counterpart): device time in ms, summed over
  * the Newton iterations since the last reset, of the four phases of a Newton

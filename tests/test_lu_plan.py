@@ -95,20 +95,24 @@ def solve_plan(v2d, imax, jmax, ip, ix, leaf=64):
     return (ni, nc, nf, nl), items[:12 * ni].reshape(-1, 12), fronts[:3 * nf].reshape(-1, 3)
 
 
-FWD, BWD = 0, 1
+FWD, BWD, FWD_GATHER, BWD_GATHER = 0, 1, 2, 3
 
 
 def _producers(items, fronts):
-    """What each item reads, from the algorithm alone (not from the
-    counters): a forward item gathers its children's contribution rows; a
-    backward item multiplies its front's z rows and the x of every ancestor
-    (the front's contribution variables are pivots of ancestors)."""
+    """What each item reads (or overwrites), from the algorithm alone (not
+    from the counters): a forward item gathers its children's contribution
+    rows, or reads what its front's forward gather item gathered; a backward
+    item multiplies its front's z rows and the x of every ancestor (the
+    front's contribution variables are pivots of ancestors), or the x its
+    front's backward gather item collected; a backward gather item reads the
+    ancestors' x and overwrites the w part that the front's forward
+    contribution rows read."""
     S, f, parent = fronts[:, 0], fronts[:, 1], fronts[:, 2]
     kids = {}
     for q, pa in enumerate(parent):
         if pa >= 0:
             kids.setdefault(int(pa), []).append(q)
-    fwd_cb, fwd_z, bwd = {}, {}, {}
+    fwd_cb, fwd_z, bwd, fg, bg = {}, {}, {}, {}, {}
     for k, it in enumerate(items):
         kind, q, rb, re = (int(v) for v in it[:4])
         if kind == FWD:
@@ -116,20 +120,32 @@ def _producers(items, fronts):
                 fwd_cb.setdefault(q, []).append(k)
             if rb < S[q]:
                 fwd_z.setdefault(q, []).append(k)
-        else:
+        elif kind == BWD:
             bwd.setdefault(q, []).append(k)
+        elif kind == FWD_GATHER:
+            fg.setdefault(q, []).append(k)
+        else:
+            bg.setdefault(q, []).append(k)
+
+    def ancestors_x(q):
+        p, a = [], parent[q]
+        while a >= 0:
+            p += bwd.get(int(a), [])
+            a = parent[a]
+        return p
+
     prod = []
     for it in items:
-        kind, q = int(it[0]), int(it[1])
+        kind, q, gathered = int(it[0]), int(it[1]), int(it[11])
         if kind == FWD:
+            prod.append(list(fg[q]) if gathered
+                        else [k for c in kids.get(q, ()) for k in fwd_cb.get(c, [])])
+        elif kind == FWD_GATHER:
             prod.append([k for c in kids.get(q, ()) for k in fwd_cb.get(c, [])])
+        elif kind == BWD:
+            prod.append(list(fwd_z.get(q, [])) + (list(bg[q]) if gathered else ancestors_x(q)))
         else:
-            p = list(fwd_z.get(q, []))
-            a = parent[q]
-            while a >= 0:
-                p += bwd.get(int(a), [])
-                a = parent[a]
-            prod.append(p)
+            prod.append(ancestors_x(q) + list(fwd_cb.get(q, [])))
     return prod
 
 
@@ -193,7 +209,8 @@ def test_solve_plan_order_is_safe(v2d, oracle_mod, imax, jmax, leaf):
     reads."""
     ip, ix = pattern(oracle_mod, imax, jmax, 1)
     (ni, nc, nf, nl), items, fronts = solve_plan(v2d, imax, jmax, ip, ix, leaf)
-    assert ni == len(items) > 0 and nc == 3 * nf
+    assert ni == len(items) > 0 and nc == 5 * nf
+    assert (items[:, 0] <= BWD).all()   # the default split has no gather items
     S, f = fronts[:, 0], fronts[:, 1]
     cover = {}
     for it in items:
@@ -209,6 +226,66 @@ def test_solve_plan_order_is_safe(v2d, oracle_mod, imax, jmax, leaf):
     for ctas in (1, 2, 5, 37, 300):
         order = _simulate(items, fronts, nc, ctas, rng)
         assert len(order) == ni
+
+
+def solve_plan_split(v2d, imax, jmax, ip, ix, rows, leaf=64):
+    """solve_plan with an explicit rows-per-item entry per level."""
+    from vorti2d_b200 import _lib
+    r = np.ascontiguousarray(rows, dtype=np.intc)
+    info = np.zeros(4, dtype=np.intc)
+    code = _lib.lib().v2d_lu_solve_plan_split(imax, jmax, _lib.iptr(ip), _lib.iptr(ix), leaf,
+                                              _lib.iptr(r), r.size, _lib.iptr(info), None, 0,
+                                              None, 0)
+    assert code == 0, v2d._lib.last_error()
+    ni, nc, nf, nl = (int(v) for v in info)
+    items = np.zeros(12 * ni, dtype=np.intc)
+    fronts = np.zeros(3 * nf, dtype=np.intc)
+    code = _lib.lib().v2d_lu_solve_plan_split(imax, jmax, _lib.iptr(ip), _lib.iptr(ix), leaf,
+                                              _lib.iptr(r), r.size, _lib.iptr(info),
+                                              _lib.iptr(items), ni, _lib.iptr(fronts), nf)
+    assert code == 0, v2d._lib.last_error()
+    return (ni, nc, nf, nl), items.reshape(-1, 12), fronts.reshape(-1, 3)
+
+
+@pytest.mark.parametrize("imax,jmax,leaf,split", [
+    (33, 21, 16, "neg8"), (65, 49, 64, "neg8"), (181, 181, 64, "mixed"),
+    (257, 129, 64, "neg32")])
+def test_gathered_split_order_is_safe(v2d, oracle_mod, imax, jmax, leaf, split):
+    """Negative rows-per-item entries: a front split into several items gets
+    one forward gather item (before its level's row items) and, if it has
+    struct variables, one backward gather item; every front's rows are still
+    covered exactly once, the items of split fronts carry the gathered flag,
+    and the simulated dataflow schedule never deadlocks nor starts an item
+    before what it reads or overwrites."""
+    ip, ix = pattern(oracle_mod, imax, jmax, 1)
+    (_, _, _, nl), _, _ = solve_plan(v2d, imax, jmax, ip, ix, leaf)
+    rows = {"neg8": [-8] * nl, "neg32": [-32] * nl,
+            "mixed": [0 if L < 3 else (-16 if L % 2 else 8) for L in range(nl)]}[split]
+    (ni, nc, nf, nl2), items, fronts = solve_plan_split(v2d, imax, jmax, ip, ix, rows, leaf)
+    assert nl2 == nl and ni == len(items) and nc == 5 * nf
+    S, f = fronts[:, 0], fronts[:, 1]
+    lvl = {}
+    for it in items:
+        lvl[int(it[1])] = int(it[10])
+    n_fg = n_bg = 0
+    for q in range(nf):
+        R = rows[lvl[q]]
+        split_f = R < 0 and f[q] > -R
+        split_b = R < 0 and S[q] > -R and f[q] > S[q]
+        mine = items[items[:, 1] == q]
+        assert (mine[:, 0] == FWD_GATHER).sum() == int(split_f)
+        assert (mine[:, 0] == BWD_GATHER).sum() == int(split_b)
+        n_fg += int(split_f)
+        n_bg += int(split_b)
+        for kind, end, flag in ((FWD, f[q], split_f), (BWD, S[q], split_b)):
+            rr = sorted((int(a), int(b)) for a, b in mine[mine[:, 0] == kind][:, 2:4])
+            assert rr[0][0] == 0 and rr[-1][1] == end
+            assert all(a[1] == b[0] for a, b in zip(rr, rr[1:]))
+            assert (mine[mine[:, 0] == kind][:, 11] == int(flag)).all()
+    assert n_fg > 0
+    rng = np.random.default_rng(imax + jmax)
+    for ctas in (1, 3, 37, 300):
+        assert len(_simulate(items, fronts, nc, ctas, rng)) == ni
 
 
 def test_solve_plan_181_items(v2d, oracle_mod):

@@ -135,6 +135,7 @@ _SIGS = {
     "v2d_solver_time_lu_apply": (_i, [_vp, _i, _ll, _dp, ctypes.POINTER(_ll)]),
     "v2d_lu_plan_info": (_i, [_i, _i, _ip, _ip, _i, ctypes.POINTER(_ll)]),
     "v2d_lu_solve_plan": (_i, [_i, _i, _ip, _ip, _i, _ip, _ip, _i, _ip, _i]),
+    "v2d_lu_solve_plan_split": (_i, [_i, _i, _ip, _ip, _i, _ip, _i, _ip, _ip, _i, _ip, _i]),
 }
 
 _LIB = None

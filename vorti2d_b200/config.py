@@ -88,8 +88,8 @@ class Config:
     FP64 form always factors in FP64."""
     lu_item_rows: list | None = None
     """LU preconditioner solve: rows per work item on each tree level (0:
-    whole fronts), e.g. from ``vorti2d_b200.tune``; None keeps the default
-    split."""
+    whole fronts; R > 0: R rows; R < 0: -R rows after one gather item per
+    front), e.g. from ``vorti2d_b200.tune``; None keeps the default split."""
     lu_solve: str = "flow"
     """LU preconditioner solve: ``"flow"`` runs each application as one
     dataflow launch over the whole front tree; ``"levels"`` as one launch per

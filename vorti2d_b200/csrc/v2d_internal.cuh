@@ -108,7 +108,10 @@ struct MfPlan {
     // checked when the plan is built (see items_build).
     int nitems = 0, nctr = 0;
     std::vector<int> h_items, lvl_fwd, lvl_bwd;
-    std::vector<int> item_rows;    // rows per item of each level (0: whole fronts)
+    std::vector<int> item_rows;    // rows per item of each level (0: whole fronts; R < 0:
+                                   // -R rows per item after one gather item per front)
+    std::vector<int> lvl_fwd_g, lvl_bwd_g;   // gather items at the start of each level's
+                                             // forward / backward range
     int *d_items = nullptr;
     long long items_ver = 0;       // bumped whenever d_items is replaced
     // host copies, kept only between the build and the upload
@@ -147,6 +150,7 @@ struct MfFactor {
     void *inv_g = nullptr;      // inversion work space in global memory for separators too
                                 // wide for shared memory (per CTA: S x (CW + 33))
     void *wb = nullptr;         // transposed solve: per-front adjoint right-hand sides (vtotal)
+    void *tw = nullptr;         // solve: gathered fronts' t, w and struct x (vtotal)
     double *rs = nullptr;       // row scaling 1 / max |a_r.|
     int *ipiv = nullptr, *perm = nullptr, *flag = nullptr;
     MfBarrier *bar = nullptr;
@@ -168,6 +172,7 @@ struct MfDev {
     const long long *foff;
     const int *vars, *cbmap, *perm;
     int maxS, maxf;
+    void *tw;   // gathered fronts: t and w (forward), -x on the struct variables (backward)
 };
 
 // Host-only symbolic phase (validates every index it produces).

@@ -75,6 +75,9 @@ constexpr int kItemsPerLevel = 600;
 __host__ __device__ inline int ctr_fz(int q, int nf) { return q; }
 __host__ __device__ inline int ctr_fin(int q, int nf) { return nf + q; }
 __host__ __device__ inline int ctr_bx(int q, int nf) { return 2 * nf + q; }
+__host__ __device__ inline int ctr_fg(int q, int nf) { return 3 * nf + q; }
+__host__ __device__ inline int ctr_bg(int q, int nf) { return 4 * nf + q; }
+constexpr int kCtrPerFront = 5;
 
 // ================================================================ symbolic
 namespace {
@@ -220,6 +223,15 @@ void mf_plan_destroy(MfPlan *p)
 //                       and bx[parent] = all of the parent's backward items
 //                       (which waited for theirs: all ancestors' x);
 //                       done: bx[q]
+// On levels whose rows-per-item entry is negative, a front split into
+// several items gets a gather item first in each sweep:
+//   forward gather of q   waits fin[q]; writes t and the contribution rows'
+//                         w to tw; done: fg[q]; q's forward items wait fg[q]
+//   backward gather of q  waits bx[parent] (which implies that q's own
+//                         contribution rows, the last readers of tw's w part,
+//                         are done); writes -x of q's struct variables to
+//                         tw; done: bg[q]; q's backward items wait fz[q] and
+//                         bg[q]
 // The check: every wait's counter reaches exactly its target in all, and
 // only through items earlier in the order; so the items an item reads have
 // all finished before it starts, and a CTA that takes items in order only
@@ -245,19 +257,39 @@ static int items_build(MfPlan *P)
             P->item_rows[L] = P->lvl_maxf[L] <= R ? 0 : R;
         }
     }
-    auto per = [&](int L) { return P->item_rows[L] > 0 ? P->item_rows[L] : INT_MAX; };
+    // rows per item; a negative entry -R splits fronts of more than R rows
+    // into R-row items after one gather item per front (kind 2 forward: w and
+    // t = P w_FS into tw; kind 3 backward: -x of the struct variables into
+    // tw), so the front's items read one contiguous vector instead of each
+    // repeating the gather
+    auto per = [&](int L) {
+        const int r = P->item_rows[L];
+        return r > 0 ? r : (r < 0 ? -r : INT_MAX);
+    };
+    auto gath_f = [&](int L, int q) { return P->item_rows[L] < 0 && P->f[q] > per(L); };
+    auto gath_b = [&](int L, int q) {
+        return P->item_rows[L] < 0 && P->S[q] > per(L) && P->f[q] > P->S[q];
+    };
     int cur_level = 0;
-    auto push = [&](int kind, int q, int rb, int re) {
-        const int v[12] = {kind, q, rb, re, -1, 0, -1, 0, -1, -1, cur_level, 0};
+    auto push = [&](int kind, int q, int rb, int re, int flag) {
+        const int v[12] = {kind, q, rb, re, -1, 0, -1, 0, -1, -1, cur_level, flag};
         it.insert(it.end(), v, v + 12);
     };
+    P->lvl_fwd_g.assign(nl, 0);
+    P->lvl_bwd_g.assign(nl, 0);
     for (int L = 0; L < nl; ++L) {
         P->lvl_fwd[L] = (int)it.size() / 12;
         cur_level = L;
         const int R = per(L);
         for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q)
+            if (gath_f(L, q)) {
+                push(2, q, 0, P->f[q], 1);
+                ++P->lvl_fwd_g[L];
+            }
+        for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q)
             for (int rb = 0; rb < P->f[q]; rb += std::min(R, P->f[q]))
-                push(0, q, rb, (int)std::min<long long>((long long)rb + R, P->f[q]));
+                push(0, q, rb, (int)std::min<long long>((long long)rb + R, P->f[q]),
+                     gath_f(L, q) ? 1 : 0);
     }
     P->lvl_fwd[nl] = (int)it.size() / 12;
     for (int L = nl - 1; L >= 0; --L) {
@@ -265,12 +297,19 @@ static int items_build(MfPlan *P)
         cur_level = L;
         const int R = per(L);
         for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q)
+            if (gath_b(L, q)) {
+                push(3, q, 0, P->S[q], 1);
+                ++P->lvl_bwd_g[L];
+            }
+        for (int q = P->lvl_off[L]; q < P->lvl_off[L + 1]; ++q)
             for (int rb = 0; rb < P->S[q]; rb += std::min(R, P->S[q]))
-                push(1, q, rb, (int)std::min<long long>((long long)rb + R, P->S[q]));
+                push(1, q, rb, (int)std::min<long long>((long long)rb + R, P->S[q]),
+                     gath_b(L, q) ? 1 : 0);
     }
     P->lvl_bwd[0] = (int)it.size() / 12;
     const int ni = (int)it.size() / 12;
-    // totals per front
+    // totals per front (row items only; a gather item counts once into its
+    // own counter)
     std::vector<int> nfz(nf, 0), nfin(nf, 0), nbx(nf, 0);
     for (int k = 0; k < ni; ++k) {
         const int *v = &it[12 * k];
@@ -278,35 +317,51 @@ static int items_build(MfPlan *P)
         if (v[0] == 0) {
             if (v[2] < P->S[q]) ++nfz[q];
             if (v[3] > P->S[q] && P->parent[q] >= 0) ++nfin[P->parent[q]];
-        } else {
+        } else if (v[0] == 1) {
             ++nbx[q];
         }
     }
     for (int k = 0; k < ni; ++k) {
         int *v = &it[12 * k];
         const int q = v[1], pa = P->parent[q];
-        if (v[0] == 0) {
-            if (nfin[q] > 0) { v[4] = ctr_fin(q, nf); v[5] = nfin[q]; }
+        switch (v[0]) {
+        case 0:   // forward rows: the front's gather item, or the children's rows
+            if (v[11]) { v[4] = ctr_fg(q, nf); v[5] = 1; }
+            else if (nfin[q] > 0) { v[4] = ctr_fin(q, nf); v[5] = nfin[q]; }
             if (v[2] < P->S[q]) v[8] = ctr_fz(q, nf);
             if (v[3] > P->S[q] && pa >= 0) v[9] = ctr_fin(pa, nf);
-        } else {
+            break;
+        case 2:   // forward gather: the children's rows
+            if (nfin[q] > 0) { v[4] = ctr_fin(q, nf); v[5] = nfin[q]; }
+            v[8] = ctr_fg(q, nf);
+            break;
+        case 1:   // backward rows: the front's z, and the gather item or the parent's x
             v[4] = ctr_fz(q, nf);
             v[5] = nfz[q];
-            if (pa >= 0) { v[6] = ctr_bx(pa, nf); v[7] = nbx[pa]; }
+            if (v[11]) { v[6] = ctr_bg(q, nf); v[7] = 1; }
+            else if (pa >= 0) { v[6] = ctr_bx(pa, nf); v[7] = nbx[pa]; }
             v[8] = ctr_bx(q, nf);
+            break;
+        case 3:   // backward gather: the parent's x (hence every ancestor's)
+            if (pa >= 0) { v[4] = ctr_bx(pa, nf); v[5] = nbx[pa]; }
+            v[8] = ctr_bg(q, nf);
+            break;
         }
     }
     // the check
-    const int nc = 3 * nf;
+    const int nc = kCtrPerFront * nf;
     std::vector<int> total(nc, 0), seen(nc, 0);
     bool ok = true;
     for (int q = 0; q < nf; ++q)
         ok = ok && P->S[q] > 0 && (P->f[q] == P->S[q] || P->parent[q] >= 0);
     for (int k = 0; k < ni && ok; ++k) {
         const int *v = &it[12 * k];
-        const int q = v[1];
-        ok = ok && (v[0] == 0 || v[0] == 1) && q >= 0 && q < nf && v[2] >= 0 && v[3] > v[2] &&
-             v[3] <= (v[0] == 0 ? P->f[q] : P->S[q]);
+        const int q = v[1], kind = v[0];
+        ok = ok && kind >= 0 && kind <= 3 && q >= 0 && q < nf && v[2] >= 0 && v[3] > v[2] &&
+             v[3] <= ((kind == 0 || kind == 2) ? P->f[q] : P->S[q]) && (v[11] == 0 || v[11] == 1);
+        if (ok && kind >= 2)   // a gather item covers its whole front, once
+            ok = v[11] == 1 && v[2] == 0 && v[3] == (kind == 2 ? P->f[q] : P->S[q]) &&
+                 (kind == 2 || P->parent[q] >= 0);
         for (int d : {v[8], v[9]}) {
             ok = ok && d >= -1 && d < nc;
             if (ok && d >= 0) ++total[d];
@@ -314,15 +369,24 @@ static int items_build(MfPlan *P)
     }
     for (int k = 0; k < ni && ok; ++k) {
         const int *v = &it[12 * k];
+        const int q = v[1], pa = P->parent[q];
         for (int w : {0, 1}) {
             const int c = v[4 + 2 * w], t = v[5 + 2 * w];
             if (c < 0) continue;
             ok = ok && c < nc && t > 0 && total[c] == t && seen[c] == t;
         }
-        // a backward item needs its own z and, below the root, its parent's x
-        if (v[0] == 1)
-            ok = ok && v[4] == ctr_fz(v[1], nf) && v[5] == nfz[v[1]] &&
-                 (P->parent[v[1]] < 0 || v[6] == ctr_bx(P->parent[v[1]], nf));
+        // what each kind must have waited for, from the algorithm
+        if (v[0] == 0)
+            ok = ok && (v[11] ? v[4] == ctr_fg(q, nf) && v[5] == 1
+                              : (nfin[q] == 0 || (v[4] == ctr_fin(q, nf) && v[5] == nfin[q])));
+        else if (v[0] == 2)
+            ok = ok && (nfin[q] == 0 || (v[4] == ctr_fin(q, nf) && v[5] == nfin[q]));
+        else if (v[0] == 1)
+            ok = ok && v[4] == ctr_fz(q, nf) && v[5] == nfz[q] &&
+                 (v[11] ? v[6] == ctr_bg(q, nf) && v[7] == 1
+                        : (pa < 0 || (v[6] == ctr_bx(pa, nf) && v[7] == nbx[pa])));
+        else
+            ok = ok && v[4] == ctr_bx(pa, nf) && v[5] == nbx[pa];
         for (int d : {v[8], v[9]})
             if (d >= 0) ++seen[d];
     }
@@ -684,7 +748,8 @@ int mf_plan_create(int imax, int jmax, int n, const int *h_rowptr, const int *h_
 }
 
 // New work-item granularity for the solve: rows[L] rows per item on level L
-// (0: whole fronts; otherwise a positive multiple of 1).  Rebuilds and
+// (0: whole fronts; R > 0: R rows; R < 0: -R rows after one gather item per
+// front).  Rebuilds and
 // re-uploads the item table (its order is checked again); the device pointer
 // changes, so solves captured in graphs before must be captured again
 // (items_ver counts the tables).
@@ -693,7 +758,8 @@ int mf_plan_set_item_rows(MfPlan *P, const int *rows, int nlevels)
     V2D_ARG_CHECK(rows && nlevels == P->nlevel, "lu item rows: %d levels given, the plan has %d",
                   nlevels, P->nlevel);
     for (int L = 0; L < nlevels; ++L)
-        V2D_ARG_CHECK(rows[L] >= 0, "lu item rows: level %d: %d", L, rows[L]);
+        V2D_ARG_CHECK(rows[L] >= -4096 && rows[L] <= 4096, "lu item rows: level %d: %d", L,
+                      rows[L]);
     std::vector<int> keep = P->item_rows;
     P->item_rows.assign(rows, rows + nlevels);
     if (items_build(P) != V2D_OK) {
@@ -895,10 +961,32 @@ extern "C" int v2d_lu_solve_plan(int imax, int jmax, const int *indptr, const in
                                  int leaf, int *info4, int *items, int cap_items, int *fronts3,
                                  int cap_fronts)
 {
+    return v2d_lu_solve_plan_split(imax, jmax, indptr, indices, leaf, nullptr, 0, info4, items,
+                                   cap_items, fronts3, cap_fronts);
+}
+
+extern "C" int v2d_lu_solve_plan_split(int imax, int jmax, const int *indptr, const int *indices,
+                                       int leaf, const int *rows, int nrows, int *info4,
+                                       int *items, int cap_items, int *fronts3, int cap_fronts)
+{
     using namespace v2d;
     V2D_ARG_CHECK(indptr && indices && info4, "lu_solve_plan: null pointer");
     MfPlan *P = nullptr;
     V2D_TRY(mf_plan_build(imax, jmax, 2 * imax * jmax, indptr, indices, leaf, &P));
+    if (rows) {
+        if (nrows != P->nlevel) {
+            set_error("lu_solve_plan: %d rows-per-item entries, the plan has %d levels", nrows,
+                      P->nlevel);
+            mf_plan_destroy(P);
+            return V2D_EARG;
+        }
+        P->item_rows.assign(rows, rows + nrows);
+        const int st = items_build(P);
+        if (st != V2D_OK) {
+            mf_plan_destroy(P);
+            return st;
+        }
+    }
     info4[0] = P->nitems;
     info4[1] = P->nctr;
     info4[2] = P->nfront;
@@ -1874,6 +1962,8 @@ __device__ __forceinline__ void row_range(bool fwd, int r, int S, int f, int &lo
 template <class T, int R = RowRegs<T>::v>
 struct SolveItemCtx {
     bool fwd;
+    int kind;    // 0 forward rows, 1 backward rows, 2 forward gather, 3 backward gather
+    bool gath;   // rows of a front whose gather item ran (its vectors are in tw)
     int q, S, f, vo, rbeg, rend;
     const T *A;
     // staged gather (forward: vars/perm/child maps; backward: struct vars)
@@ -1887,10 +1977,12 @@ struct SolveItemCtx {
     T reg[R];
 
     __device__ __forceinline__ void pre(const MfDev &D, const T *F, const T *b,
-                                        const double *__restrict__ rs, bool fwd_, int q_,
-                                        int rbeg_, int rend_)
+                                        const double *__restrict__ rs, int kind_, int gath_,
+                                        int q_, int rbeg_, int rend_)
     {
-        fwd = fwd_;
+        kind = kind_;
+        fwd = kind == 0 || kind == 2;
+        gath = gath_ != 0 && kind < 2;
         q = q_;
         rbeg = rbeg_;
         rend = rend_;
@@ -1900,7 +1992,7 @@ struct SolveItemCtx {
         A = F + D.foff[q];
         const int tid = threadIdx.x, nt = blockDim.x, wid = tid >> 5, nw = nt >> 5;
         const int *vars = D.vars + vo;
-        onerow = rend - rbeg <= nw;
+        onerow = kind < 2 && rend - rbeg <= nw;
         const int r = rbeg + wid;
         if (onerow && r < rend) {
             int lo, hi;
@@ -1911,7 +2003,9 @@ struct SolveItemCtx {
         } else {
             onerow = false;
         }
-        if (fwd) {
+        if (gath) {
+            staged = false;   // the rows read the gather item's vectors
+        } else if (fwd) {
             ch[0] = D.child0[q];
             ch[1] = D.child1[q];
             for (int sl = 0; sl < 2; ++sl) {
@@ -1946,11 +2040,11 @@ struct SolveItemCtx {
         }
     }
 
-    // Forward: w (f entries: scaled b on the fully summed rows plus the
-    // children's contributions), t = P w_FS; then the item's rows.
-    __device__ __forceinline__ void run_fwd(const MfDev &D, const T *b,
-                                            const double *__restrict__ rs, T *zbuf, T *upd, T *w,
-                                            T *t)
+    // Forward gather: w (f entries: scaled b on the fully summed rows plus
+    // the children's contributions), t = P w_FS, in shared memory.
+    __device__ __forceinline__ void gather_w(const MfDev &D, const T *b,
+                                             const double *__restrict__ rs, const T *upd, T *w,
+                                             T *t)
     {
         const int tid = threadIdx.x, nt = blockDim.x;
         if (staged) {
@@ -1992,11 +2086,59 @@ struct SolveItemCtx {
             for (int i = tid; i < S; i += nt) t[i] = w[D.perm[vo + i]];
         }
         __syncthreads();
+    }
+
+    // Forward rows: t from the gather item (gathered fronts) or gathered
+    // here; then z_r = t_r + F[r, 0:r] t on pivot rows and u_r = w_r -
+    // F[r, 0:S] t on contribution rows.
+    __device__ __forceinline__ void run_fwd(const MfDev &D, const T *b,
+                                            const double *__restrict__ rs, T *zbuf, T *upd, T *w,
+                                            T *t)
+    {
         T *uo = upd + D.uoff[q] - S;   // row r >= S -> uo[r]
+        if (gath) {
+            const T *tw = (const T *)D.tw + vo;
+            for (int i = threadIdx.x; i < S; i += blockDim.x) t[i] = __ldcg(tw + i);
+            __syncthreads();
+            rows(t, [&](int r, T v) {
+                if (r < S) zbuf[vo + r] = t[r] + v;
+                else uo[r] = __ldcg(tw + r) - v;
+            });
+            return;
+        }
+        gather_w(D, b, rs, upd, w, t);
         rows(t, [&](int r, T v) {
             if (r < S) zbuf[vo + r] = t[r] + v;
             else uo[r] = w[r] - v;
         });
+    }
+
+    // Forward gather item: t on the pivot positions and w on the
+    // contribution rows into tw, once for all of the front's row items.
+    __device__ __forceinline__ void run_gather_fwd(const MfDev &D, const T *b,
+                                                   const double *__restrict__ rs, const T *upd,
+                                                   T *w, T *t)
+    {
+        gather_w(D, b, rs, upd, w, t);
+        T *tw = (T *)D.tw + vo;
+        for (int i = threadIdx.x; i < f; i += blockDim.x) tw[i] = i < S ? t[i] : w[i];
+    }
+
+    // Backward gather item: -x on the front's struct variables into tw.
+    __device__ __forceinline__ void run_gather_bwd(const MfDev &D, const T *x)
+    {
+        const int tid = threadIdx.x, nt = blockDim.x, mm = f - S;
+        T *tw = (T *)D.tw + vo + S;
+        if (staged) {
+#pragma unroll
+            for (int k = 0; k < kGatherRegs; ++k) {
+                const int e = tid + k * nt;
+                if (e < mm) tw[e] = -__ldcg(x + xi[k]);
+            }
+        } else {
+            const int *vars = D.vars + vo;
+            for (int e = tid; e < mm; e += nt) tw[e] = -__ldcg(x + vars[S + e]);
+        }
     }
 
     // Backward: v = (z, -x on the front's struct variables); then the rows.
@@ -2005,7 +2147,10 @@ struct SolveItemCtx {
         const int tid = threadIdx.x, nt = blockDim.x, mm = f - S;
         const int *vars = D.vars + vo;
         for (int i = tid; i < S; i += nt) v[i] = __ldcg(zbuf + vo + i);
-        if (staged) {
+        if (gath) {
+            const T *tw = (const T *)D.tw + vo + S;
+            for (int e = tid; e < mm; e += nt) v[S + e] = __ldcg(tw + e);
+        } else if (staged) {
 #pragma unroll
             for (int k = 0; k < kGatherRegs; ++k) {
                 const int e = tid + k * nt;
@@ -2104,8 +2249,12 @@ __device__ __forceinline__ void run_item(SolveItemCtx<T, R> &c, const MfDev &D, 
                                          const double *__restrict__ rs, T *zbuf, T *upd, T *x,
                                          T *smem)
 {
-    if (c.fwd) c.run_fwd(D, b, rs, zbuf, upd, smem, smem + D.maxf);
-    else c.run_bwd(D, zbuf, x, smem);
+    switch (c.kind) {
+    case 0: c.run_fwd(D, b, rs, zbuf, upd, smem, smem + D.maxf); break;
+    case 1: c.run_bwd(D, zbuf, x, smem); break;
+    case 2: c.run_gather_fwd(D, b, rs, upd, smem, smem + D.maxf); break;
+    default: c.run_gather_bwd(D, x); break;
+    }
 }
 
 // One launch per level and sweep: block i runs item i0 + i (its
@@ -2118,9 +2267,9 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_solve_level(
     if (stopped(stop_a, stop_b)) return;
     extern __shared__ unsigned char smem_raw[];
     T *smem = reinterpret_cast<T *>(smem_raw);
-    const int4 it = items[i0 + blockIdx.x].x;
+    const SolveItemDev it = items[i0 + blockIdx.x];
     SolveItemCtx<T> c;
-    c.pre(D, F, b, rs, it.x == 0, it.y, it.z, it.w);
+    c.pre(D, F, b, rs, it.x.x, it.z.w, it.x.y, it.x.z, it.x.w);
     run_item(c, D, b, rs, zbuf, upd, x, smem);
 }
 
@@ -2191,7 +2340,7 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_solve_flow(
         const SolveItemDev it = items[i];
         if (trace && threadIdx.x == 0) trace[3 * i] = globaltimer_ns();
         SolveItemCtx<T, R> c;
-        c.pre(D, F, b, rs, it.x.x == 0, it.x.y, it.x.z, it.x.w);
+        c.pre(D, F, b, rs, it.x.x, it.z.w, it.x.y, it.x.z, it.x.w);
         if (threadIdx.x == 0) {
             next = atomicAdd(ctr + nctr, 1);   // in flight during the wait
             bool ok = true;
@@ -2350,6 +2499,7 @@ int mf_factor_create(const MfPlan *P, int fp32, int fact64, MfFactor **out)
     grab(&M->gh, (size_t)P->gmax * esf);
     grab((void **)&M->sctr, (size_t)(P->nctr + 1) * sizeof(int));
     grab(&M->wb, (size_t)P->vtotal * es);
+    grab(&M->tw, (size_t)P->vtotal * es);
     grab((void **)&M->rs, (size_t)P->n * sizeof(double));
     grab((void **)&M->ipiv, (size_t)P->vtotal * sizeof(int));
     grab((void **)&M->perm, (size_t)P->vtotal * sizeof(int));
@@ -2453,8 +2603,8 @@ void mf_factor_destroy(MfFactor *M)
 {
     if (!M) return;
     if (M->graph) cudaGraphExecDestroy(M->graph);
-    void *ptrs[] = {M->F,    M->F32,  M->upd,  M->z,    M->tmp,  M->gh,    M->wb,
-                    M->rs,   M->ipiv, M->perm, M->flag, M->bar, M->inv_g, M->sctr};
+    void *ptrs[] = {M->F,    M->F32,  M->upd,  M->z,    M->tmp,   M->gh,    M->wb,  M->tw,
+                    M->rs,   M->ipiv, M->perm, M->flag, M->bar,  M->inv_g, M->sctr};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     delete M;
@@ -2467,6 +2617,7 @@ MfDev mf_dev(const MfPlan *P, const MfFactor *M)
     D.child0 = P->d_child0; D.child1 = P->d_child1; D.parent = P->d_parent; D.foff = P->d_foff;
     D.vars = P->d_vars; D.cbmap = P->d_cbmap; D.perm = M->perm;
     D.maxS = P->maxS; D.maxf = P->maxf;
+    D.tw = M->tw;
     return D;
 }
 
@@ -2714,21 +2865,30 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
         V2D_TRY(mark(kCodeFlow * 1000));
         launches = 1;
     } else {
+        // a level's gather items (first in its range) are a launch of their own
         for (int L = 0; L < P->nlevel; ++L) {
-            const int i0 = P->lvl_fwd[L], ni = P->lvl_fwd[L + 1] - i0;
-            k_solve_level<T><<<ni, kSolveThreads, smf, s>>>(D, F, b, M->rs, z, upd, x, items, i0,
-                                                           stop_a, stop_b);
-            V2D_TRY(solve_launch("k_solve_level (forward)", L));
-            V2D_TRY(mark(kCodeFwdLevel * 1000 + L));
-            ++launches;
+            const int i0 = P->lvl_fwd[L], ni = P->lvl_fwd[L + 1] - i0, ng = P->lvl_fwd_g[L];
+            for (const int part : {0, 1}) {
+                const int a = part == 0 ? i0 : i0 + ng, n = part == 0 ? ng : ni - ng;
+                if (n == 0) continue;
+                k_solve_level<T><<<n, kSolveThreads, smf, s>>>(D, F, b, M->rs, z, upd, x, items,
+                                                              a, stop_a, stop_b);
+                V2D_TRY(solve_launch("k_solve_level (forward)", L));
+                V2D_TRY(mark(kCodeFwdLevel * 1000 + L));
+                ++launches;
+            }
         }
         for (int L = P->nlevel - 1; L >= 0; --L) {
-            const int i0 = P->lvl_bwd[L + 1], ni = P->lvl_bwd[L] - i0;
-            k_solve_level<T><<<ni, kSolveThreads, smf, s>>>(D, F, b, M->rs, z, upd, x, items, i0,
-                                                           stop_a, stop_b);
-            V2D_TRY(solve_launch("k_solve_level (backward)", L));
-            V2D_TRY(mark(kCodeBwdLevel * 1000 + L));
-            ++launches;
+            const int i0 = P->lvl_bwd[L + 1], ni = P->lvl_bwd[L] - i0, ng = P->lvl_bwd_g[L];
+            for (const int part : {0, 1}) {
+                const int a = part == 0 ? i0 : i0 + ng, n = part == 0 ? ng : ni - ng;
+                if (n == 0) continue;
+                k_solve_level<T><<<n, kSolveThreads, smf, s>>>(D, F, b, M->rs, z, upd, x, items,
+                                                              a, stop_a, stop_b);
+                V2D_TRY(solve_launch("k_solve_level (backward)", L));
+                V2D_TRY(mark(kCodeBwdLevel * 1000 + L));
+                ++launches;
+            }
         }
     }
     V2D_CUDA_TRY(cudaGetLastError());

@@ -4,9 +4,12 @@ The solve (one dataflow launch over the front tree) runs in one of two
 kernel forms (more resident CTAs per SM, or more row registers per lane) and
 splits each front's rows
 into work items; on tree level L an item is ``rows[L]`` rows of one front, or
-the whole front (0).  Small items spread a level's rows over more CTAs and
-shorten the chain of dependent steps; large ones gather each front's
-right-hand side once and keep a CTA's rows together.  Which wins depends on
+the whole front (0), or, for ``rows[L] = -R``, R rows after one gather item
+per front that collects the front's right-hand side once for all of its
+items.  Small items spread a level's rows over more CTAs and shorten the
+chain of dependent steps; large ones gather each front's right-hand side once
+and keep a CTA's rows together; gather items add one dependent step but
+spare every item the indexed gather.  Which wins depends on
 the grid, the precision and the GPU, so it is measured: a coordinate search
 over the levels (each level's candidates tried with the others fixed, two
 sweeps), every trial timed as the average of warm applications of the
@@ -29,7 +32,9 @@ import numpy as np
 from . import _lib
 from ._lib import check, lib
 
-CANDIDATES = (0, 8, 16, 32, 64, 128, 256)
+# rows per item: 0 whole fronts, R > 0 R-row items, R < 0 (-R)-row items
+# after one gather item per split front
+CANDIDATES = (0, 8, 16, 32, 64, 128, 256, -8, -16, -32, -64, -128, -256)
 
 
 def item_rows(solver) -> list:
