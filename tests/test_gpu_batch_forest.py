@@ -101,3 +101,25 @@ def test_batch_fields_and_frozen_instance(v2d, oracle_mod):
     a, b = state(2)
     assert np.array_equal(a, psi2) and np.array_equal(b, ome2)
     _lib.lib().v2d_batch_destroy(h)
+
+
+def test_sweep_96_converges_where_the_oracle_does(v2d):
+    """The 96-instance sweep (seed 0) batched on the device with the bench's
+    rules (FP64, at most 20 Newton iterations, GMRES capped at 30 per Newton
+    step, frozen past 1000x the first update norm) converges on exactly the
+    instances the oracle's pure-Newton solves converge on
+    (tests/golden/sweep_oracle_96.json, tests/golden/make_sweep_oracle.py),
+    with the same forces there (1e-8)."""
+    import json
+    import os
+    from vorti2d_b200.batch import run_sweep_batched, sweep_cases
+    with open(os.path.join(os.path.dirname(__file__), "golden", "sweep_oracle_96.json")) as fh:
+        ref = {r["name"]: r for r in json.load(fh)["cases"]}
+    res = run_sweep_batched(sweep_cases(seed=0), precision="fp64", krylov_max_it=30)
+    got = {r.name: r for r in res.results}
+    assert set(got) == set(ref)
+    conv = sorted(n for n, r in got.items() if r.converged)
+    assert conv == sorted(n for n, r in ref.items() if r["converged"]), conv
+    for n in conv:
+        for k in ("cd", "cl", "cm"):
+            assert abs(getattr(got[n], k) - ref[n][k]) <= 1e-8, (n, k, getattr(got[n], k), ref[n][k])

@@ -291,6 +291,8 @@ struct v2d_solver {
     long long lu_factorizations = 0;
     int *tptr = nullptr, *tind = nullptr, *tperm = nullptr;   // transposed CSR pattern (adjoint)
     double *valT = nullptr;           // J^T values on that pattern (adjoint GMRES)
+    double *adj_vec = nullptr;        // adjoint g, lambda and J^T lambda (3 x 2N; kept, since
+                                      // the GMRES graphs write lambda by address)
     v2d::KrylovWork *kw_adj = nullptr;   // GMRES work space of the adjoint solves
     // versions for the adjoint's factor cache: the state (psi, ome) and the
     // parameters, the assembled values, and the FP64 factors lu[0]

@@ -95,6 +95,7 @@ struct KrylovWork {
     const void *graph_lu[2] = {nullptr, nullptr};
     int graph_lu_flow[2] = {-1, -1};   // the LU solve form the graph was captured with
     long long graph_lu_items[2] = {-1, -1};   // and the plan's work-item table
+    const double *graph_x[2] = {nullptr, nullptr};   // the solution vector k_correct writes
 };
 
 // ---------------------------------------------------------------- helpers
@@ -680,6 +681,7 @@ static int capture_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, doub
     w->graph_lu[which] = lu ? (const void *)A.lu : nullptr;
     w->graph_lu_flow[which] = lu_form(A);
     w->graph_lu_items[which] = lu ? A.lu_plan->items_ver : -1;
+    w->graph_x[which] = x;
     return V2D_OK;
 }
 
@@ -693,7 +695,8 @@ static int run_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, double *
         w->graph_pc[which] != precond ||
         w->graph_lu[which] != (lu ? (const void *)A.lu : nullptr) ||
         w->graph_lu_flow[which] != lu_form(A) ||
-        w->graph_lu_items[which] != (lu ? A.lu_plan->items_ver : -1))
+        w->graph_lu_items[which] != (lu ? A.lu_plan->items_ver : -1) ||
+        w->graph_x[which] != x)
         V2D_TRY(capture_cycle<T>(w, which, V, wv, z, Z, x, A, precond, s));
     for (size_t q = 0; q < w->seg[which].size(); ++q) {
         V2D_CUDA_TRY(cudaGraphLaunch(w->seg[which][q], s));

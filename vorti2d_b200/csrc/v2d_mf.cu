@@ -1875,6 +1875,7 @@ __device__ __forceinline__ bool stopped(const int *a, const int *b)
 
 constexpr int kSolveThreads = kSolveThreadsHost;   // 8 warps per work item
 constexpr int kGatherRegs = 4;   // staged gather entries per thread (fronts up to 4 x 256)
+constexpr int kThreadRowMaxF = 256;   // fronts whose rows a thread sums alone (FP32)
 
 // Row registers: a warp that computes a single row of an item loads it into
 // registers before the item's dependency wait; rows up to kRowRegs<T> x 32
@@ -1911,7 +1912,7 @@ __device__ __forceinline__ T row_dot_reg(const T (&reg)[R], const T *v, int base
 // N rows' dot products by one warp at once: row u's entries [b_u, e_u) with
 // v (an empty range for an absent row), all loads in flight together.  Each
 // row has its own accumulator, so its sum does not depend on N.
-template <class T, int N>
+template <class T, int N, int K = (N >= 8 ? 2 : 4)>
 __device__ __forceinline__ void dotN(const T *const (&p)[N], const int (&b)[N], const int (&e)[N],
                                      const T *v, T (&s)[N])
 {
@@ -1922,11 +1923,29 @@ __device__ __forceinline__ void dotN(const T *const (&p)[N], const int (&b)[N], 
         lo = min(lo, b[u]);
         hi = max(hi, e[u]);
     }
+    // K column chunks of each of the N rows are loaded before any is used:
+    // N * K loads of the factor rows in flight per lane
     T a[N];
 #pragma unroll
     for (int u = 0; u < N; ++u) a[u] = T(0);
-#pragma unroll 4
-    for (int c = (lo & ~31) + lane; c < hi; c += 32) {
+    int c = (lo & ~31) + lane;
+    for (; c + 32 * (K - 1) < hi; c += 32 * K) {
+        T xv[K], rv[N][K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) xv[k] = v[c + 32 * k];
+#pragma unroll
+        for (int u = 0; u < N; ++u)
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const int cc = c + 32 * k;
+                rv[u][k] = (cc >= b[u] && cc < e[u]) ? p[u][cc] : T(0);
+            }
+#pragma unroll
+        for (int u = 0; u < N; ++u)
+#pragma unroll
+            for (int k = 0; k < K; ++k) a[u] += rv[u][k] * xv[k];
+    }
+    for (; c < hi; c += 32) {
         const T x = v[c];
 #pragma unroll
         for (int u = 0; u < N; ++u)
@@ -2073,19 +2092,81 @@ struct SolveItemCtx {
             for (int k = 0; k < kGatherRegs; ++k)
                 if (tid + k * nt < S) t[tid + k * nt] = w[pi[k]];
         } else {
+            // wide fronts: the same in batches of kGatherRegs entries per
+            // thread, each batch's index loads issued before its gathers
             const int *vars = D.vars + vo;
-            for (int p = tid; p < f; p += nt)
-                w[p] = p < S ? (T)(rs[vars[p]] * (double)b[vars[p]]) : T(0);
+            for (int p0 = tid; p0 < f; p0 += kGatherRegs * nt) {
+                int vi[kGatherRegs];
+#pragma unroll
+                for (int k = 0; k < kGatherRegs; ++k) {
+                    const int p = p0 + k * nt;
+                    vi[k] = p < S ? vars[p] : -1;
+                }
+                T val[kGatherRegs];
+#pragma unroll
+                for (int k = 0; k < kGatherRegs; ++k)
+                    val[k] = vi[k] >= 0 ? (T)(rs[vi[k]] * (double)b[vi[k]]) : T(0);
+#pragma unroll
+                for (int k = 0; k < kGatherRegs; ++k)
+                    if (p0 + k * nt < f) w[p0 + k * nt] = val[k];
+            }
             __syncthreads();
             for (int sl = 0; sl < 2; ++sl) {
                 const int *map = D.cbmap + uof[sl];
                 const T *u = upd + uof[sl];
-                for (int e = tid; e < m[sl]; e += nt) w[map[e]] += __ldcg(u + e);
+                for (int e0 = tid; e0 < m[sl]; e0 += kGatherRegs * nt) {
+                    int mi[kGatherRegs];
+                    T uv[kGatherRegs];
+#pragma unroll
+                    for (int k = 0; k < kGatherRegs; ++k) {
+                        const int e = e0 + k * nt;
+                        mi[k] = e < m[sl] ? map[e] : -1;
+                        uv[k] = e < m[sl] ? __ldcg(u + e) : T(0);
+                    }
+#pragma unroll
+                    for (int k = 0; k < kGatherRegs; ++k)
+                        if (mi[k] >= 0) w[mi[k]] += uv[k];
+                }
                 __syncthreads();
             }
-            for (int i = tid; i < S; i += nt) t[i] = w[D.perm[vo + i]];
+            for (int i0 = tid; i0 < S; i0 += kGatherRegs * nt) {
+                int pk[kGatherRegs];
+#pragma unroll
+                for (int k = 0; k < kGatherRegs; ++k)
+                    pk[k] = i0 + k * nt < S ? D.perm[vo + i0 + k * nt] : -1;
+#pragma unroll
+                for (int k = 0; k < kGatherRegs; ++k)
+                    if (pk[k] >= 0) t[i0 + k * nt] = w[pk[k]];
+            }
         }
         __syncthreads();
+    }
+
+    // -x on the struct variables [S, f) into dst[0, f - S), in batches of
+    // kGatherRegs entries per thread (index loads first)
+    __device__ __forceinline__ void gather_struct_x(const MfDev &D, const T *x, T *dst) const
+    {
+        const int tid = threadIdx.x, nt = blockDim.x, mm = f - S;
+        if (staged) {
+#pragma unroll
+            for (int k = 0; k < kGatherRegs; ++k) {
+                const int e = tid + k * nt;
+                if (e < mm) dst[e] = -__ldcg(x + xi[k]);
+            }
+            return;
+        }
+        const int *vars = D.vars + vo + S;
+        for (int e0 = tid; e0 < mm; e0 += kGatherRegs * nt) {
+            int vi[kGatherRegs];
+#pragma unroll
+            for (int k = 0; k < kGatherRegs; ++k) vi[k] = e0 + k * nt < mm ? vars[e0 + k * nt] : -1;
+            T xv[kGatherRegs];
+#pragma unroll
+            for (int k = 0; k < kGatherRegs; ++k) xv[k] = vi[k] >= 0 ? __ldcg(x + vi[k]) : T(0);
+#pragma unroll
+            for (int k = 0; k < kGatherRegs; ++k)
+                if (vi[k] >= 0) dst[e0 + k * nt] = -xv[k];
+        }
     }
 
     // Forward rows: t from the gather item (gathered fronts) or gathered
@@ -2127,18 +2208,7 @@ struct SolveItemCtx {
     // Backward gather item: -x on the front's struct variables into tw.
     __device__ __forceinline__ void run_gather_bwd(const MfDev &D, const T *x)
     {
-        const int tid = threadIdx.x, nt = blockDim.x, mm = f - S;
-        T *tw = (T *)D.tw + vo + S;
-        if (staged) {
-#pragma unroll
-            for (int k = 0; k < kGatherRegs; ++k) {
-                const int e = tid + k * nt;
-                if (e < mm) tw[e] = -__ldcg(x + xi[k]);
-            }
-        } else {
-            const int *vars = D.vars + vo;
-            for (int e = tid; e < mm; e += nt) tw[e] = -__ldcg(x + vars[S + e]);
-        }
+        gather_struct_x(D, x, (T *)D.tw + vo + S);
     }
 
     // Backward: v = (z, -x on the front's struct variables); then the rows.
@@ -2150,29 +2220,26 @@ struct SolveItemCtx {
         if (gath) {
             const T *tw = (const T *)D.tw + vo + S;
             for (int e = tid; e < mm; e += nt) v[S + e] = __ldcg(tw + e);
-        } else if (staged) {
-#pragma unroll
-            for (int k = 0; k < kGatherRegs; ++k) {
-                const int e = tid + k * nt;
-                if (e < mm) v[S + e] = -__ldcg(x + xi[k]);
-            }
         } else {
-            for (int e = tid; e < mm; e += nt) v[S + e] = -__ldcg(x + vars[S + e]);
+            gather_struct_x(D, x, v + S);
         }
         __syncthreads();
         rows(v, [&](int r, T val) { x[vars[r]] = val; });
     }
 
-    // The item's rows: one per warp from registers (at most one row per
-    // warp); one per thread when the item has at least half as many rows as
-    // threads (each thread sums its row left to right, four partial sums;
+    // The item's rows: one per thread when the item has at least half as
+    // many rows as threads, in FP32 fronts of at most kThreadRowMaxF
+    // variables (each thread sums its row left to right, four partial sums;
     // the row's entries come through L1 line by line and the vector entries
-    // from shared memory); otherwise G rows per warp at a time (dotN).
+    // from shared memory); one per warp from registers (at most one row per
+    // warp); otherwise G rows per warp at a time (dotN).
     template <class Out>
     __device__ __forceinline__ void rows(const T *vec, Out out)
     {
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-        if (2 * (rend - rbeg) >= (int)blockDim.x) {
+        // one row per thread: short FP32 rows only (a warp's loads touch 32
+        // rows at once, which pays only while the rows stay in L1)
+        if (sizeof(T) == 4 && f <= kThreadRowMaxF && 2 * (rend - rbeg) >= (int)blockDim.x) {
             for (int r = rbeg + (int)threadIdx.x; r < rend; r += blockDim.x) {
                 int lo, hi;
                 row_range(fwd, r, S, f, lo, hi);
@@ -2211,6 +2278,8 @@ struct SolveItemCtx {
             return;
         }
         constexpr int G = R >= 32 ? 8 : 4;   // rows per warp in flight (register budget)
+        // column chunks per row in flight: 2 in the small-register FP32 form
+        constexpr int KC = (sizeof(T) == 4 && R < 32) ? 2 : (G >= 8 ? 2 : 4);
         for (int r = rbeg + wid; r < rend; r += G * nw) {
             const T *p[G];
             int bb[G], ee[G], rr[G];
@@ -2226,7 +2295,7 @@ struct SolveItemCtx {
                 }
             }
             T sg[G];
-            dotN<T, G>(p, bb, ee, vec, sg);
+            dotN<T, G, KC>(p, bb, ee, vec, sg);
             if (lane == 0) {
 #pragma unroll
                 for (int u = 0; u < G; ++u)

@@ -97,6 +97,8 @@ void drop_transpose(v2d_solver *S)
     S->tptr = S->tind = S->tperm = nullptr;
     if (S->valT) cudaFree(S->valT);
     S->valT = nullptr;
+    if (S->adj_vec) cudaFree(S->adj_vec);
+    S->adj_vec = nullptr;
     krylov_destroy(S->kw_adj);
     S->kw_adj = nullptr;
 }
@@ -844,9 +846,8 @@ extern "C" int v2d_solver_adjoint(v2d_solver *S, double urot, const double *g_ho
     k_gather_vals<<<grid_for(g.nnz, 256), 256, 0, S->s>>>(g.nnz, S->tperm, g.val, S->valT);
     V2D_CUDA_TRY(cudaGetLastError());
     count_launches(1);
-    DevBuf<double> buf;
-    V2D_TRY(buf.alloc(3 * n, S->s));
-    double *dg = buf.p, *lam = dg + n, *jtl = lam + n;
+    if (!S->adj_vec) V2D_CUDA_TRY(cudaMalloc(&S->adj_vec, 3 * n * sizeof(double)));
+    double *dg = S->adj_vec, *lam = dg + n, *jtl = lam + n;
     V2D_CUDA_TRY(cudaMemcpyAsync(dg, g_host, n * sizeof(double), cudaMemcpyHostToDevice, S->s));
     CsrOp AT;
     AT.n = g.n;
