@@ -1417,13 +1417,18 @@ template <int N> __device__ __forceinline__ void cp_async_wait()
 // acc += sum over k in [ka, kb) of a(rr, k) b(k, cc), in NB-wide slices
 // through two shared buffers (sm[0], sm[1]): the copies of slice s + 1 are in
 // flight while the tensor cores (or CUDA cores) work on slice s.  srcA(rr, k)
-// and srcB(k, cc) give the element's address or nullptr (zero); oneB(k, cc)
-// marks B entries that are 1 instead (a unit diagonal), written after the
-// slice's copies have landed.  base: any valid address (the source of
-// zero-filled copies, never read).
-template <class T, class SA, class SB, class OB>
+// and srcB(k, cc) give the element's address or nullptr (zero); oneA(rr, k)
+// and oneB(k, cc) mark entries that are 1 instead (a unit diagonal), written
+// after the slice's copies have landed.  base: any valid address (the source
+// of zero-filled copies, never read).
+struct NoOnes {
+    __device__ __forceinline__ bool operator()(int, int) const { return false; }
+};
+
+template <class T, class SA, class SB, class OB, class OA = NoOnes>
 __device__ __forceinline__ void tile_mac(TileAcc<T> &acc, typename TileAcc<T>::Smem *sm, int ka,
-                                         int kb, const T *base, SA srcA, SB srcB, OB oneB)
+                                         int kb, const T *base, SA srcA, SB srcB, OB oneB,
+                                         OA oneA = OA())
 {
     constexpr int NB = PanelWidth<T>::v;
     constexpr int TL = kGemmTile;
@@ -1450,6 +1455,10 @@ __device__ __forceinline__ void tile_mac(TileAcc<T> &acc, typename TileAcc<T>::S
         for (int e = tid; e < NB * TL; e += blockDim.x) {
             const int t = e / TL, cc = e - t * TL;
             if (k + t < kb && oneB(k + t, cc)) TileAcc<T>::refB(b, t, cc) = T(1);
+        }
+        for (int e = tid; e < TL * NB; e += blockDim.x) {
+            const int rr = e / NB, t = e - rr * NB;
+            if (k + t < kb && oneA(rr, k + t)) TileAcc<T>::refA(b, rr, t) = T(1);
         }
     };
     if (ns > 0) stage(0);
@@ -1738,6 +1747,156 @@ __global__ void __launch_bounds__(kTrinvThreadsG) k_trinv_g(int q0, const int *_
     T *Xs = work + ((long long)blockIdx.y * gridDim.x + blockIdx.x) * sstride;
     T *Lp = Xs + (size_t)S * CW;
     trinv_colblock<T>(F + foff[q], S, f, tmp + toff[q], c0, Xs, Lp, Dg);
+}
+
+// Explicit inverses of separators too wide for the shared-memory column
+// blocks (FP64), by 64 x 64 blocks on the tile engine.  With X = L11^-1 and
+// Y = U11^-1 in blocks of 64 (nb blocks), X L11 = I and U11 Y = I give, for
+// s = nb-2 down to 0,
+//   X_is = -sum_{k=s+1..i} X_ik (L_ks X_ss)     (i > s, block column s)
+//   Y_sj = -sum_{k=s+1..j} (Y_ss U_sk) Y_kj     (j > s, block row s)
+// from blocks of later steps and the diagonal blocks' inverses X_kk (unit
+// diagonal, stored strictly below it) and Y_kk.  k_trinv_diag inverts every
+// diagonal block; each step is two launches of k_trinv_step: phase 0 forms
+// W_k = L_ks X_ss and V_sk = Y_ss U_sk in place of L_ks and U_sk (read by
+// this step only; the whole pivot block is replaced by k_trcopy afterwards),
+// phase 1 the products.  Results go to the level's scratch like k_trinv's.
+constexpr int kInvBlk = 64;   // the tile engine's tile
+constexpr int kTrinvDiagThreads = 128;
+
+template <class T> constexpr size_t trinv_diag_smem() { return 3 * kInvBlk * (kInvBlk + 1) * sizeof(T); }
+
+template <class T>
+__global__ void __launch_bounds__(kTrinvDiagThreads) k_trinv_diag(int q0, const int *__restrict__ S_,
+                                                                  const int *__restrict__ f_,
+                                                                  const long long *__restrict__ foff,
+                                                                  const long long *__restrict__ toff,
+                                                                  const T *__restrict__ F, T *tmp)
+{
+    constexpr int B = kInvBlk;
+    extern __shared__ __align__(16) unsigned char diag_raw[];
+    T (*Ab)[B + 1] = reinterpret_cast<T (*)[B + 1]>(diag_raw);
+    T (*Xs)[B + 1] = Ab + B;
+    T (*Ys)[B + 1] = Xs + B;
+    const int q = q0 + blockIdx.y;
+    const int S = S_[q], f = f_[q], s0 = blockIdx.x * B;
+    if (s0 >= S) return;
+    const int bs = min(B, S - s0), tid = threadIdx.x;
+    const T *A = F + foff[q] + (long long)s0 * f + s0;
+    for (int e = tid; e < B * B; e += blockDim.x) {
+        const int r = e / B, c = e - r * B;
+        Ab[r][c] = (r < bs && c < bs) ? A[(long long)r * f + c] : T(0);
+    }
+    __syncthreads();
+    const int c = tid & (B - 1);
+    if (c < bs) {
+        if (tid < B) {   // column c of L^-1 (unit lower): forward substitution
+            Xs[c][c] = T(1);
+            for (int r = c + 1; r < bs; ++r) {
+                T v = T(0);
+                for (int t = c; t < r; ++t) v -= Ab[r][t] * Xs[t][c];
+                Xs[r][c] = v;
+            }
+        } else {         // column c of U^-1: back substitution
+            const T dc = Ab[c][c];
+            Ys[c][c] = dc != T(0) ? T(1) / dc : T(0);
+            for (int r = c - 1; r >= 0; --r) {
+                T v = T(0);
+                for (int t = r + 1; t <= c; ++t) v -= Ab[r][t] * Ys[t][c];
+                const T d = Ab[r][r];
+                Ys[r][c] = d != T(0) ? v / d : T(0);
+            }
+        }
+    }
+    __syncthreads();
+    T *X = tmp + toff[q] + (long long)s0 * S + s0;
+    for (int e = tid; e < bs * bs; e += blockDim.x) {
+        const int r = e / bs, cc = e - r * bs;
+        X[(long long)r * S + cc] = r > cc ? Xs[r][cc] : Ys[r][cc];
+    }
+}
+
+// One step s of the blocked inversion (see k_trinv_diag); grid: (2 half,
+// fronts), tiles [0, half) the blocks k = s + 1 + t of L's block column s,
+// [half, 2 half) those of U's block row s.
+template <class T>
+__global__ void __launch_bounds__(256) k_trinv_step(int q0, int s, int phase, int half,
+                                                    const int *__restrict__ S_,
+                                                    const int *__restrict__ f_,
+                                                    const long long *__restrict__ foff,
+                                                    const long long *__restrict__ toff, T *F,
+                                                    T *tmp)
+{
+    constexpr int B = kInvBlk;
+    extern __shared__ __align__(16) unsigned char tile_raw[];
+    typename TileAcc<T>::Smem *sm = reinterpret_cast<typename TileAcc<T>::Smem *>(tile_raw);
+    const int q = q0 + blockIdx.y;
+    const int S = S_[q], f = f_[q], nb = (S + B - 1) / B;
+    int t = blockIdx.x;
+    const bool up = t >= half;
+    if (up) t -= half;
+    const int k = s + 1 + t;
+    if (k >= nb) return;
+    T *A = F + foff[q];
+    T *X = tmp + toff[q];
+    const int s0 = s * B, k0 = k * B, se = s0 + B, ke = min(k0 + B, S);
+    TileAcc<T> acc;
+    acc.zero();
+    if (phase == 0 && !up) {          // W_k = L_ks X_ss (in place of L_ks)
+        tile_mac<T>(
+            acc, sm, s0, se, A,
+            [&](int rr, int j) -> const T * {
+                const int r = k0 + rr;
+                return r < ke ? A + (long long)r * f + j : nullptr;
+            },
+            [&](int j, int cc) -> const T * {
+                return j > s0 + cc ? X + (long long)j * S + s0 + cc : nullptr;
+            },
+            [&](int j, int cc) { return j == s0 + cc; });
+        acc.each([&](int rr, int cc, T v) {
+            if (k0 + rr < ke) A[(long long)(k0 + rr) * f + s0 + cc] = v;
+        });
+    } else if (phase == 0) {          // V_sk = Y_ss U_sk (in place of U_sk)
+        tile_mac<T>(
+            acc, sm, s0, se, A,
+            [&](int rr, int j) -> const T * {
+                return j >= s0 + rr ? X + (long long)(s0 + rr) * S + j : nullptr;
+            },
+            [&](int j, int cc) -> const T * {
+                const int c = k0 + cc;
+                return c < ke ? A + (long long)j * f + c : nullptr;
+            },
+            NoOnes());
+        acc.each([&](int rr, int cc, T v) {
+            if (k0 + cc < ke) A[(long long)(s0 + rr) * f + k0 + cc] = v;
+        });
+    } else if (!up) {                 // X_ks = -sum_{m=s+1..k} X_km W_m
+        tile_mac<T>(
+            acc, sm, se, ke, A,
+            [&](int rr, int j) -> const T * {
+                const int r = k0 + rr;
+                if (r >= ke || (j >= k0 && j >= r)) return nullptr;   // X_kk: strictly lower
+                return X + (long long)r * S + j;
+            },
+            [&](int j, int cc) -> const T * { return A + (long long)j * f + s0 + cc; },
+            NoOnes(), [&](int rr, int j) { return k0 + rr == j; });
+        acc.each([&](int rr, int cc, T v) {
+            if (k0 + rr < ke) X[(long long)(k0 + rr) * S + s0 + cc] = -v;
+        });
+    } else {                          // Y_sk = -sum_{m=s+1..k} V_sm Y_mk
+        tile_mac<T>(
+            acc, sm, se, ke, A,
+            [&](int rr, int j) -> const T * { return A + (long long)(s0 + rr) * f + j; },
+            [&](int j, int cc) -> const T * {
+                const int c = k0 + cc;
+                if (c >= ke || (j >= k0 && j > c)) return nullptr;    // Y_kk: upper
+                return X + (long long)j * S + c;
+            },
+            NoOnes());
+        acc.each([&](int rr, int cc, T v) {
+            if (k0 + cc < ke) X[(long long)(s0 + rr) * S + k0 + cc] = -v;
+        });
+    }
 }
 
 // Inverted S x S blocks of the level's fronts: scratch -> factor storage.
@@ -2592,7 +2751,7 @@ int mf_factor_create(const MfPlan *P, int fp32, int fact64, MfFactor **out)
         const size_t sl = (size_t)P->lvl_maxS[L] * (cw + 33);
         if (sl * esf <= kInvSmemMax) {
             inv = std::max(inv, sl * esf);
-        } else {
+        } else if (esf == sizeof(float)) {   // FP64 inverts these by blocks in place
             const size_t nbc = (P->lvl_maxS[L] + cw - 1) / cw;
             inv_g = std::max(inv_g, nbc * (size_t)(P->lvl_off[L + 1] - P->lvl_off[L]) * sl);
         }
@@ -2701,6 +2860,8 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
     const size_t tile_smem = tile_smem_bytes<T>();
     V2D_CUDA_TRY(raise_dyn_smem((const void *)k_gemm<T>, tile_smem));
     V2D_CUDA_TRY(raise_dyn_smem((const void *)k_gh<T>, tile_smem));
+    V2D_CUDA_TRY(raise_dyn_smem((const void *)k_trinv_step<T>, tile_smem));
+    V2D_CUDA_TRY(raise_dyn_smem((const void *)k_trinv_diag<T>, trinv_diag_smem<T>()));
     // with ev: an event is recorded after each kernel (kind * 1000 + level;
     // kinds 0 rowscale, 1 scatter, 2 extend_add, 3 first panel, 4 L21 + row
     // swaps + U12, 6 trailing update + next panel, 7 trinv, 8 trcopy, 9 G/H
@@ -2789,13 +2950,27 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
         const size_t inv_bytes = (size_t)P->lvl_maxS[L] * (InvWidth<T>::v + 33) * sizeof(T);
         for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
             const int nb = std::min(nq - qb, kMaxFrontsY);
-            if (inv_bytes <= kInvSmemMax)
+            if (inv_bytes <= kInvSmemMax) {
                 k_trinv<T><<<dim3(nbc, nb), kTrinvThreads, inv_bytes, s>>>(
                     q0 + qb, P->d_S, P->d_foff, P->d_f, P->d_toff, F, (T *)M->tmp);
-            else
+            } else if (std::is_same<T, double>::value) {
+                // wide separators in FP64: blocked inversion on the tensor cores
+                const int nbk = (P->lvl_maxS[L] + kInvBlk - 1) / kInvBlk;
+                k_trinv_diag<T><<<dim3(nbk, nb), kTrinvDiagThreads, trinv_diag_smem<T>(), s>>>(
+                    q0 + qb, P->d_S, P->d_f, P->d_foff, P->d_toff, F, (T *)M->tmp);
+                for (int st = nbk - 2; st >= 0; --st)
+                    for (int phase = 0; phase < 2; ++phase) {
+                        const int half = nbk - st - 1;
+                        k_trinv_step<T><<<dim3(2 * half, nb), 256, tile_smem, s>>>(
+                            q0 + qb, st, phase, half, P->d_S, P->d_f, P->d_foff, P->d_toff, F,
+                            (T *)M->tmp);
+                        ++launches;
+                    }
+            } else {
                 k_trinv_g<T><<<dim3(nbc, nb), kTrinvThreadsG, 0, s>>>(
                     q0 + qb, P->d_S, P->d_foff, P->d_f, P->d_toff, F, (T *)M->tmp,
                     (T *)M->inv_g, (long long)P->lvl_maxS[L] * (InvWidth<T>::v + 33));
+            }
             if (qb > 0) ++launches;
         }
         V2D_TRY(mark(7000 + L));
