@@ -427,8 +427,8 @@ int v2d_solver_trace_lu_apply(v2d_solver *s, unsigned long long *ticks, int *ite
 
 /* Tuning aid (no reference counterpart): the form of the dataflow LU solve
  * kernel -- 0: two resident CTAs per SM with 32 row registers per lane (16 in
- * FP64); 1 (FP32 solve only): three CTAs per SM with 16.  form < 0 only
- * reads the current one into *current (may be null). */
+ * FP64); 1: three CTAs per SM with 16 (8 in FP64).  form < 0 only reads the
+ * current one into *current (may be null). */
 int v2d_solver_lu_flow_form(v2d_solver *s, int form, int *current);
 
 /* Tuning aid (no reference counterpart): the work-item granularity of the

@@ -137,18 +137,21 @@ def force_vjp(solver, weights, alpha_h=1e-3):
 def steady_solve_ser(solver, dtau0=1.0, tol=None, max_iter=300, dtau_max=1e12):
     """Steady state by pseudo-time continuation with switched evolution
     relaxation (Mulder and van Leer, 1985): iteration k adds 1/dtau_k to the
-    Newton Jacobian's diagonal, dtau_k = dtau0 * res_0 / res_{k-1} (capped at
-    dtau_max), so the first iterations are damped pseudo-time steps and the
-    last ones Newton steps as the update norm res = ||dq||/(2N) falls.  The
-    residual itself carries no pseudo-time term, so the fixed point is the
-    steady solution of the reference's equations.  For cases where Newton
-    from the free stream diverges.  Returns (res, iterations); the handle's
+    Newton Jacobian's diagonal, dtau_k = dtau0 * ||R_0|| / ||R_k|| (R the
+    residual at the iterate, capped at dtau_max), so the first iterations are
+    damped pseudo-time steps and the last ones Newton steps as the residual
+    falls.  The residual carries no pseudo-time term, so the fixed point is
+    the steady solution of the reference's equations; the stopping rule is
+    the reference's, ||dq||/(2N) <= tol.  For cases where Newton from the
+    free stream diverges.  Returns (||dq||/(2N), iterations); the handle's
     own 1/dtau is restored."""
     dev, cfg = solver.dev, solver.cfg
     tol = cfg.pseudo_tol if tol is None else float(tol)
     urot = cfg.u_rot(0.0)
+    re, adeg = float(cfg.re), float(cfg.alpha_deg)
     keep = dev.params.invdtau
-    res0, res, it, dtau = None, math.inf, 0, float(dtau0)
+    r0 = float(np.linalg.norm(_residual(solver, re, adeg, urot)))
+    res, it, dtau = math.inf, 0, float(dtau0)
     try:
         while res > tol and it < max_iter:
             dev.set_invdtau(1.0 / dtau)
@@ -159,8 +162,8 @@ def steady_solve_ser(solver, dtau0=1.0, tol=None, max_iter=300, dtau_max=1e12):
             if not math.isfinite(res):
                 break
             it += 1
-            res0 = res if res0 is None else res0
-            dtau = min(dtau_max, dtau0 * res0 / max(res, 1e-300))
+            rk = float(np.linalg.norm(_residual(solver, re, adeg, urot)))
+            dtau = min(dtau_max, dtau0 * r0 / max(rk, 1e-300))
     finally:
         dev.set_invdtau(keep)
     return res, it

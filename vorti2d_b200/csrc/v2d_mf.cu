@@ -2034,7 +2034,7 @@ __device__ __forceinline__ bool stopped(const int *a, const int *b)
 
 constexpr int kSolveThreads = kSolveThreadsHost;   // 8 warps per work item
 constexpr int kGatherRegs = 4;   // staged gather entries per thread (fronts up to 4 x 256)
-constexpr int kThreadRowMaxF = 256;   // fronts whose rows a thread sums alone (FP32)
+constexpr int kThreadRowMaxF = 256;   // fronts whose forward rows a thread sums alone
 
 // Row registers: a warp that computes a single row of an item loads it into
 // registers before the item's dependency wait; rows up to kRowRegs<T> x 32
@@ -2042,6 +2042,10 @@ constexpr int kThreadRowMaxF = 256;   // fronts whose rows a thread sums alone (
 template <class T> struct RowRegs;
 template <> struct RowRegs<float> { static constexpr int v = 32; };
 template <> struct RowRegs<double> { static constexpr int v = 16; };
+// the three-CTAs-per-SM form of the dataflow solve: fewer row registers
+template <class T> struct RowRegs3;
+template <> struct RowRegs3<float> { static constexpr int v = 16; };
+template <> struct RowRegs3<double> { static constexpr int v = 8; };
 
 template <class T, int R>
 __device__ __forceinline__ void row_load(T (&reg)[R], const T *row, int base, int lo, int hi)
@@ -2386,9 +2390,9 @@ struct SolveItemCtx {
         rows(v, [&](int r, T val) { x[vars[r]] = val; });
     }
 
-    // The item's rows: one per thread when the item has at least half as
-    // many rows as threads, in FP32 fronts of at most kThreadRowMaxF
-    // variables (each thread sums its row left to right, four partial sums;
+    // The item's rows: one per thread when a forward item has at least half
+    // as many rows as threads, in fronts of at most kThreadRowMaxF variables
+    // (each thread sums its row left to right, four partial sums;
     // the row's entries come through L1 line by line and the vector entries
     // from shared memory); one per warp from registers (at most one row per
     // warp); otherwise G rows per warp at a time (dotN).
@@ -2398,7 +2402,7 @@ struct SolveItemCtx {
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
         // one row per thread: short FP32 rows only (a warp's loads touch 32
         // rows at once, which pays only while the rows stay in L1)
-        if (sizeof(T) == 4 && f <= kThreadRowMaxF && 2 * (rend - rbeg) >= (int)blockDim.x) {
+        if (fwd && f <= kThreadRowMaxF && 2 * (rend - rbeg) >= (int)blockDim.x) {
             for (int r = rbeg + (int)threadIdx.x; r < rend; r += blockDim.x) {
                 int lo, hi;
                 row_range(fwd, r, S, f, lo, hi);
@@ -2437,8 +2441,8 @@ struct SolveItemCtx {
             return;
         }
         constexpr int G = R >= 32 ? 8 : 4;   // rows per warp in flight (register budget)
-        // column chunks per row in flight: 2 in the small-register FP32 form
-        constexpr int KC = (sizeof(T) == 4 && R < 32) ? 2 : (G >= 8 ? 2 : 4);
+        // column chunks per row in flight: 2 in the small-register forms
+        constexpr int KC = (R < RowRegs<T>::v || G >= 8) ? 2 : 4;
         for (int r = rbeg + wid; r < rend; r += G * nw) {
             const T *p[G];
             int bb[G], ee[G], rr[G];
@@ -2545,9 +2549,9 @@ __device__ __forceinline__ bool wait_count(const int *ctr, int target, volatile 
 // launch.
 // Two forms (the autotuner picks one): MINB resident CTAs per SM at least,
 // R row registers per lane (rows up to 32 R entries prefetched before the
-// wait).  Form 0: 2 CTAs and RowRegs<T> registers; form 1 (FP32): 3 CTAs
-// per SM with 16 row registers, more warps in flight for the levels whose
-// items are whole fronts.
+// wait).  Form 0: 2 CTAs and RowRegs<T> registers; form 1: 3 CTAs per SM
+// with RowRegs3<T>, more warps in flight for the levels whose items are
+// whole fronts.
 template <class T, int R, int MINB>
 __global__ void __launch_bounds__(kSolveThreads, MINB) k_solve_flow(
     const MfDev D, const T *F, const T *b, const double *__restrict__ rs, T *zbuf, T *upd, T *x,
@@ -2783,13 +2787,14 @@ int mf_factor_create(const MfPlan *P, int fp32, int fact64, MfFactor **out)
     }
     if (fp32) {
         attr((const void *)k_solve_level<float>, solve);
-        attr((const void *)k_solve_flow<float, 32, 2>, solve);
-        attr((const void *)k_solve_flow<float, 16, 3>, solve);
+        attr((const void *)k_solve_flow<float, RowRegs<float>::v, 2>, solve);
+        attr((const void *)k_solve_flow<float, RowRegs3<float>::v, 3>, solve);
         attr((const void *)k_tup_front<float>, tsolve);
         attr((const void *)k_tdown_front<float>, tsolve);
     } else {
         attr((const void *)k_solve_level<double>, solve);
-        attr((const void *)k_solve_flow<double, 16, 2>, solve);
+        attr((const void *)k_solve_flow<double, RowRegs<double>::v, 2>, solve);
+        attr((const void *)k_solve_flow<double, RowRegs3<double>::v, 3>, solve);
         attr((const void *)k_tup_front<double>, tsolve);
         attr((const void *)k_tdown_front<double>, tsolve);
     }
@@ -2807,13 +2812,18 @@ int mf_factor_create(const MfPlan *P, int fp32, int fact64, MfFactor **out)
     if (oe == cudaSuccess) oe = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (oe == cudaSuccess)
         oe = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                        &per_sm, k_solve_flow<float, 32, 2>, kSolveThreads, solve)
+                        &per_sm, k_solve_flow<float, RowRegs<float>::v, 2>, kSolveThreads, solve)
                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                        &per_sm, k_solve_flow<double, 16, 2>, kSolveThreads, solve);
+                        &per_sm, k_solve_flow<double, RowRegs<double>::v, 2>, kSolveThreads,
+                        solve);
     int per_sm1 = 0;
-    if (oe == cudaSuccess && fp32)
-        oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k_solve_flow<float, 16, 3>,
-                                                           kSolveThreads, solve);
+    if (oe == cudaSuccess)
+        oe = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                        &per_sm1, k_solve_flow<float, RowRegs3<float>::v, 3>, kSolveThreads,
+                        solve)
+                  : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                        &per_sm1, k_solve_flow<double, RowRegs3<double>::v, 3>, kSolveThreads,
+                        solve);
     if (oe != cudaSuccess || per_sm <= 0) {
         set_error("mf_factor: occupancy of the dataflow solve: %s",
                   oe != cudaSuccess ? cudaGetErrorString(oe) : "no CTA fits on an SM");
@@ -2821,7 +2831,7 @@ int mf_factor_create(const MfPlan *P, int fp32, int fact64, MfFactor **out)
         return V2D_ECUDA;
     }
     M->flow_grid = std::max(1, nsm * std::min(per_sm, 2));
-    M->flow_grid1 = fp32 && per_sm1 > 0 ? nsm * std::min(per_sm1, 3) : 0;
+    M->flow_grid1 = per_sm1 > 0 ? nsm * std::min(per_sm1, 3) : 0;
     cudaGetLastError();
     *out = M;
     return V2D_OK;
@@ -3091,14 +3101,12 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
     if (M->flow) {
         V2D_CUDA_TRY(cudaMemsetAsync(M->sctr, 0, (size_t)(P->nctr + 1) * sizeof(int), s));
         bool launched = false;
-        if constexpr (std::is_same<T, float>::value) {
-            if (M->flow_form == 1 && M->flow_grid1 > 0) {
-                k_solve_flow<T, 16, 3><<<std::max(1, std::min(P->nitems, M->flow_grid1)),
-                                         kSolveThreads, smf, s>>>(
-                    D, F, b, M->rs, z, upd, x, items, P->nitems, M->sctr, P->nctr, M->bar,
-                    stop_a, stop_b, trace);
-                launched = true;
-            }
+        if (M->flow_form == 1 && M->flow_grid1 > 0) {
+            k_solve_flow<T, RowRegs3<T>::v, 3><<<std::max(1, std::min(P->nitems, M->flow_grid1)),
+                                                 kSolveThreads, smf, s>>>(
+                D, F, b, M->rs, z, upd, x, items, P->nitems, M->sctr, P->nctr, M->bar, stop_a,
+                stop_b, trace);
+            launched = true;
         }
         if (!launched)
             k_solve_flow<T, RowRegs<T>::v, 2><<<std::max(1, std::min(P->nitems, M->flow_grid)),

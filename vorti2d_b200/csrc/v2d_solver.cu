@@ -781,7 +781,7 @@ extern "C" int v2d_solver_lu_flow_form(v2d_solver *S, int form, int *current)
     if (form >= 0) {
         V2D_ARG_CHECK(form <= 1, "lu_flow_form: form %d (0 or 1)", form);
         V2D_ARG_CHECK(form == 0 || M->flow_grid1 > 0,
-                      "lu_flow_form: form 1 exists for the FP32 solve only");
+                      "lu_flow_form: form 1 does not fit on this GPU");
         V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
         M->flow_form = form;
     }

@@ -62,7 +62,7 @@ def flow_form(solver) -> int:
 
 def set_flow_form(solver, form: int) -> bool:
     """Select a form of the dataflow solve kernel; False when the solve has
-    no such form (form 1 exists for the FP32 solve only)."""
+    no such form on this GPU."""
     return lib().v2d_solver_lu_flow_form(solver.dev.h, int(form), None) == _lib.V2D_OK
 
 
