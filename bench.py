@@ -149,13 +149,16 @@ def flush_l2(torch, buf):
 
 def timed_steps(torch, s, times, k0, K, flush_buf):
     """K BDF2 steps on the solver's stream, each preceded by an L2 flush
-    (outside the events); returns (per-step ms list, Newton its, Krylov its)."""
+    (outside the events), inside the NVTX range v2d_timed (for a profiler's
+    launch list of the timed region); returns (per-step ms list, Newton its,
+    Krylov its)."""
     import ctypes
     from vorti2d_b200 import _lib
     sp = ctypes.c_void_p()
     _lib.check(_lib.lib().v2d_solver_stream(s.dev.h, ctypes.byref(sp)))
     stream = torch.cuda.ExternalStream(sp.value)
     ms, newton, krylov = [], 0, 0
+    torch.cuda.nvtx.range_push("v2d_timed")
     for m in range(K):
         flush_l2(torch, flush_buf)
         torch.cuda.synchronize()
@@ -168,6 +171,7 @@ def timed_steps(torch, s, times, k0, K, flush_buf):
         ms.append(e0.elapsed_time(e1))
         newton += it
         krylov += s.newton_log[-1][2]
+    torch.cuda.nvtx.range_pop()
     return ms, newton, krylov
 
 

@@ -70,7 +70,7 @@ def test_ser_continuation_reaches_the_newton_state(v2d, oracle_mod):
     xg, yg = oracle_mod.generate_cylinder(IMAX, JMAX)
     ref = solve(v2d, xg, yg, RE, ADEG)
     s = v2d.Solver(steady_cfg(v2d, RE, ADEG), mesh=(xg, yg))
-    res, its = steady_solve_ser(s, dtau0=0.5, max_iter=200)
+    res, its = steady_solve_ser(s, dtau0=0.5, max_iter=120)
     assert res <= 1e-13 and its > 0, (res, its)
     for a, b in ((s.psi, ref.psi), (s.ome, ref.ome)):
         assert np.max(np.abs(a - b)) <= 1e-9 * max(1.0, np.max(np.abs(b)))

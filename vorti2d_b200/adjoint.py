@@ -134,23 +134,25 @@ def force_vjp(solver, weights, alpha_h=1e-3):
 
 
 # ------------------------------------------------------------------ shape
-def steady_solve_ser(solver, dtau0=1.0, tol=None, max_iter=300, dtau_max=1e12):
-    """Steady state by pseudo-time continuation with switched evolution
-    relaxation (Mulder and van Leer, 1985): iteration k adds 1/dtau_k to the
-    Newton Jacobian's diagonal, dtau_k = dtau0 * ||R_0|| / ||R_k|| (R the
-    residual at the iterate, capped at dtau_max), so the first iterations are
-    damped pseudo-time steps and the last ones Newton steps as the residual
-    falls.  The residual carries no pseudo-time term, so the fixed point is
-    the steady solution of the reference's equations; the stopping rule is
-    the reference's, ||dq||/(2N) <= tol.  For cases where Newton from the
-    free stream diverges.  Returns (||dq||/(2N), iterations); the handle's
-    own 1/dtau is restored."""
+def steady_solve_ser(solver, dtau0=1.0, tol=None, max_iter=300, dtau_max=1e12, growth=2.0):
+    """Steady state by pseudo-transient continuation: iteration k adds
+    1/dtau_k to the Newton Jacobian's diagonal.  While the residual norm
+    ||R|| falls, dtau grows by `growth` per iteration, and at least to the
+    switched-evolution-relaxation value dtau0 ||R_0|| / ||R_k|| (Mulder and
+    van Leer, 1985); when it rises, dtau halves (not below dtau0).  The
+    first iterations are damped pseudo-time steps, the last ones Newton
+    steps (dtau capped at dtau_max).  The residual carries no pseudo-time
+    term, so the fixed point is the steady solution of the reference's
+    equations; the stopping rule is the reference's, ||dq||/(2N) <= tol.
+    For cases where Newton from the free stream diverges.  Returns
+    (||dq||/(2N), iterations); the handle's own 1/dtau is restored."""
     dev, cfg = solver.dev, solver.cfg
     tol = cfg.pseudo_tol if tol is None else float(tol)
     urot = cfg.u_rot(0.0)
     re, adeg = float(cfg.re), float(cfg.alpha_deg)
     keep = dev.params.invdtau
     r0 = float(np.linalg.norm(_residual(solver, re, adeg, urot)))
+    r_prev = r0
     res, it, dtau = math.inf, 0, float(dtau0)
     try:
         while res > tol and it < max_iter:
@@ -163,7 +165,11 @@ def steady_solve_ser(solver, dtau0=1.0, tol=None, max_iter=300, dtau_max=1e12):
                 break
             it += 1
             rk = float(np.linalg.norm(_residual(solver, re, adeg, urot)))
-            dtau = min(dtau_max, dtau0 * r0 / max(rk, 1e-300))
+            if rk < r_prev:
+                dtau = min(dtau_max, max(dtau * growth, dtau0 * r0 / max(rk, 1e-300)))
+            else:
+                dtau = max(float(dtau0), 0.5 * dtau)
+            r_prev = rk
     finally:
         dev.set_invdtau(keep)
     return res, it
