@@ -618,6 +618,36 @@ def profile_lu_apply(args):
     s.close()
 
 
+def profile_lu_factor(args):
+    """Two steps of the workload on the cylinder --profile-grid, then one LU
+    factorization of the current Jacobian inside the NVTX range v2d_lu_factor
+    (for a profiler capture of one factorization kernel)."""
+    import ctypes
+    import torch
+    import vorti2d_b200 as v
+    from vorti2d_b200 import _lib
+    torch.cuda.set_device(0)
+    grid = args.profile_grid
+    xg, yg = v.generate_cylinder(grid, grid)
+    prec = "mixed" if args.precision == "both" else args.precision
+    s = make_solver(v, xg, yg, prec, args.lu_reuse, args.lu_reuse_steps)
+    times = s.times()
+    for m in range(2):
+        s.advance(times[m])
+    torch.cuda.synchronize()
+    cap = 16384
+    ms = (ctypes.c_double * cap)()
+    codes = (ctypes.c_int * cap)()
+    n = ctypes.c_int()
+    torch.cuda.nvtx.range_push("v2d_lu_factor")
+    _lib.check(_lib.lib().v2d_solver_time_lu_factor(s.dev.h, 1, ms, codes, cap, ctypes.byref(n)))
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    print(json.dumps({"profile": "LU factorization", "grid": f"{grid}x{grid}", "precision": prec,
+                      "ms": sum(ms[k] for k in range(n.value)), "launches": n.value}), flush=True)
+    s.close()
+
+
 def profile_lu_launches(args):
     """Per-launch device time of one LU preconditioner solve after two steps
     of the workload, with the factors warm in L2 (as inside GMRES) and after
@@ -977,6 +1007,8 @@ def main():
                     help="two steps, then two warm LU solves in the NVTX range v2d_lu_apply")
     ap.add_argument("--profile-grid", type=int, default=IMAX,
                     help="grid of the --lu-launches profile (the cylinder O-grid N x N)")
+    ap.add_argument("--lu-factor-profile", action="store_true",
+                    help="one LU factorization inside the NVTX range v2d_lu_factor (profiling)")
     ap.add_argument("--lu-launches", action="store_true",
                     help="per-launch device time of one LU preconditioner solve, warm and cold")
     ap.add_argument("--profile-newton", action="store_true",
@@ -993,6 +1025,9 @@ def main():
         return
     if args.lu_apply_profile:
         profile_lu_apply(args)
+        return
+    if args.lu_factor_profile:
+        profile_lu_factor(args)
         return
     if args.workload == "sweep" and args.impl == "ours":
         run_sweep_workload(args)
