@@ -1009,6 +1009,7 @@ namespace {
 
 constexpr int kMfThreads = 256;
 constexpr int kGemmTile = 64;
+constexpr int kTileStages = 3;   // operand slices in flight in the tile engine
 // levels whose largest front has at least kDelayFront variables update the
 // trailing block once per kDelayPanels panels (k_gemm)
 constexpr int kDelayFront = 1024;
@@ -1415,8 +1416,9 @@ template <int N> __device__ __forceinline__ void cp_async_wait()
 }
 
 // acc += sum over k in [ka, kb) of a(rr, k) b(k, cc), in NB-wide slices
-// through two shared buffers (sm[0], sm[1]): the copies of slice s + 1 are in
-// flight while the tensor cores (or CUDA cores) work on slice s.  srcA(rr, k)
+// through kTileStages shared buffers (sm[0 .. kTileStages)): the copies of
+// slices s + 1 and s + 2 are in flight while the tensor cores (or CUDA
+// cores) work on slice s.  srcA(rr, k)
 // and srcB(k, cc) give the element's address or nullptr (zero); oneA(rr, k)
 // and oneB(k, cc) mark entries that are 1 instead (a unit diagonal), written
 // after the slice's copies have landed.  base: any valid address (the source
@@ -1436,7 +1438,7 @@ __device__ __forceinline__ void tile_mac(TileAcc<T> &acc, typename TileAcc<T>::S
     const int ns = (kb - ka + NB - 1) / NB;
     auto stage = [&](int sl) {
         const int k = ka + sl * NB;
-        typename TileAcc<T>::Smem &b = sm[sl & 1];
+        typename TileAcc<T>::Smem &b = sm[sl % kTileStages];
         for (int e = tid; e < TL * NB; e += blockDim.x) {
             const int rr = e / NB, t = e - rr * NB;
             const T *p = k + t < kb ? srcA(rr, k + t) : nullptr;
@@ -1451,7 +1453,7 @@ __device__ __forceinline__ void tile_mac(TileAcc<T> &acc, typename TileAcc<T>::S
     };
     auto ones = [&](int sl) {
         const int k = ka + sl * NB;
-        typename TileAcc<T>::Smem &b = sm[sl & 1];
+        typename TileAcc<T>::Smem &b = sm[sl % kTileStages];
         for (int e = tid; e < NB * TL; e += blockDim.x) {
             const int t = e / TL, cc = e - t * TL;
             if (k + t < kb && oneB(k + t, cc)) TileAcc<T>::refB(b, t, cc) = T(1);
@@ -1461,19 +1463,21 @@ __device__ __forceinline__ void tile_mac(TileAcc<T> &acc, typename TileAcc<T>::S
             if (k + t < kb && oneA(rr, k + t)) TileAcc<T>::refA(b, rr, t) = T(1);
         }
     };
+    static_assert(kTileStages == 3, "the wait counts below assume three stages");
     if (ns > 0) stage(0);
+    if (ns > 1) stage(1);
     for (int sl = 0; sl < ns; ++sl) {
-        if (sl + 1 < ns) {
-            stage(sl + 1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
+        // slice sl has landed once at most the copies of slice sl + 1 pend
+        if (sl + 1 < ns) cp_async_wait<1>();
+        else cp_async_wait<0>();
         ones(sl);
         __syncthreads();
-        acc.mac(sm[sl & 1]);
-        __syncthreads();
+        // the buffer of slice sl + 2 held slice sl - 1, which every thread
+        // finished before the barrier above
+        if (sl + 2 < ns) stage(sl + 2);
+        acc.mac(sm[sl % kTileStages]);
     }
+    __syncthreads();   // the buffers may be reused after the last slice
 }
 
 // One 64 x 64 tile of a trailing update: A[r][c] -= sum_{t in [ka, kb)}
@@ -1502,8 +1506,11 @@ __device__ __forceinline__ void gemm_tile_range(T *A, int f, int r0, int r1, int
     });
 }
 
-// dynamic shared memory of k_gemm and k_gh: the two operand buffers
-template <class T> constexpr size_t tile_smem_bytes() { return 2 * sizeof(typename TileAcc<T>::Smem); }
+// dynamic shared memory of the tile engine's kernels: the operand buffers
+template <class T> constexpr size_t tile_smem_bytes()
+{
+    return kTileStages * sizeof(typename TileAcc<T>::Smem);
+}
 
 // Trailing updates after panel [k, k + w), with delayed updates in
 // super-panels of W columns (a multiple of NB; W = NB is the plain
@@ -1529,8 +1536,10 @@ __global__ void __launch_bounds__(256) k_gemm(int q0, int k, int W, const int *_
     constexpr int TL = kGemmTile;
     extern __shared__ __align__(16) unsigned char tile_raw[];
     typename TileAcc<T>::Smem *sm = reinterpret_cast<typename TileAcc<T>::Smem *>(tile_raw);
-    __shared__ T U[NB][NB + 1];
-    __shared__ int pv[NB];
+    // the next panel's block and pivots reuse the operand buffers once the
+    // tile is done
+    T(*U)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(tile_raw);
+    int *pv = reinterpret_cast<int *>(tile_raw + sizeof(T) * NB * (NB + 1));
     const int q = q0 + blockIdx.y;
     const int S = S_[q], f = f_[q];
     if (S <= k) return;
