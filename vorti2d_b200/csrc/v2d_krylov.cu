@@ -546,20 +546,20 @@ static int tile_grid(long long n)
     return (int)std::max(1LL, std::min<long long>(kTileBlocks, g));
 }
 
-// A restart cycle runs as a few captured segments of Arnoldi steps of
-// growing length ([0,2), [2,6), [6,14), ...), then a finishing graph
+// A restart cycle runs as a few captured segments of Arnoldi steps
+// ([0,2), [2,6), [6,10), [10,14), then 8 at a time), then a finishing graph
 // (back-substitution, correction, FP64 residual).  The host reads the control
 // block after each segment and skips the remaining segments once the cycle
 // has stopped, so a cycle that converges in a few steps (the usual case with
-// the LU preconditioner) does not pay for launching m steps.
+// the LU preconditioner: 6-12 with factors kept across Newton iterations)
+// launches few steps past its last one; each step after the stop is a chain
+// of launches that return at once.
 static std::vector<int> segment_bounds(int m)
 {
     std::vector<int> b{0};
-    int len = 2;
-    while (b.back() < m) {
-        b.push_back(std::min(m, b.back() + len));
-        len *= 2;
-    }
+    const int len[] = {2, 4, 4, 4};
+    for (int q = 0; b.back() < m; ++q)
+        b.push_back(std::min(m, b.back() + (q < 4 ? len[q] : 8)));
     return b;
 }
 
