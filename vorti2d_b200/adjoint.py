@@ -134,18 +134,23 @@ def force_vjp(solver, weights, alpha_h=1e-3):
 
 
 # ------------------------------------------------------------------ shape
-def steady_solve_ser(solver, dtau0=1.0, tol=None, max_iter=300, dtau_max=1e12, growth=2.0):
+def steady_solve_ser(solver, dtau0=1.0, tol=None, max_iter=300, dtau_max=1e12, growth=2.0,
+                     reject=1e3):
     """Steady state by pseudo-transient continuation: iteration k adds
     1/dtau_k to the Newton Jacobian's diagonal.  While the residual norm
     ||R|| falls, dtau grows by `growth` per iteration, and at least to the
     switched-evolution-relaxation value dtau0 ||R_0|| / ||R_k|| (Mulder and
-    van Leer, 1985); when it rises, dtau halves (not below dtau0).  The
-    first iterations are damped pseudo-time steps, the last ones Newton
-    steps (dtau capped at dtau_max).  The residual carries no pseudo-time
+    van Leer, 1985); a step that raises ||R|| more than `reject` times, or
+    fails, is undone (the previous state is restored) and dtau shrinks
+    fourfold; a step that raises it less halves dtau (the residual may rise
+    for a while on the way; only blow-ups are undone).  dtau stays within
+    [dtau0 / 64, dtau_max].  The first iterations are damped pseudo-time
+    steps, the last ones Newton steps.  The residual carries no pseudo-time
     term, so the fixed point is the steady solution of the reference's
     equations; the stopping rule is the reference's, ||dq||/(2N) <= tol.
     For cases where Newton from the free stream diverges.  Returns
-    (||dq||/(2N), iterations); the handle's own 1/dtau is restored."""
+    (||dq||/(2N), iterations, counting rejected ones); the handle's own
+    1/dtau is restored."""
     dev, cfg = solver.dev, solver.cfg
     tol = cfg.pseudo_tol if tol is None else float(tol)
     urot = cfg.u_rot(0.0)
@@ -154,21 +159,28 @@ def steady_solve_ser(solver, dtau0=1.0, tol=None, max_iter=300, dtau_max=1e12, g
     r0 = float(np.linalg.norm(_residual(solver, re, adeg, urot)))
     r_prev = r0
     res, it, dtau = math.inf, 0, float(dtau0)
+    dmin = float(dtau0) / 64.0
     try:
         while res > tol and it < max_iter:
+            saved = [a.copy() for a in dev.get_state()]
             dev.set_invdtau(1.0 / dtau)
             code, res, _ = dev.newton(urot)
             solver._host_state = None
-            if code not in (_lib.V2D_OK, _lib.V2D_ENOTCONVERGED):
-                check(code, "steady_solve_ser")
-            if not math.isfinite(res):
-                break
             it += 1
-            rk = float(np.linalg.norm(_residual(solver, re, adeg, urot)))
+            ok = code in (_lib.V2D_OK, _lib.V2D_ENOTCONVERGED) and math.isfinite(res)
+            rk = float(np.linalg.norm(_residual(solver, re, adeg, urot))) if ok else math.inf
+            if not (ok and math.isfinite(rk)) or rk > reject * r_prev:
+                dev.set_state(*saved)       # undo the step
+                solver._host_state = None
+                if dtau <= dmin:
+                    break
+                dtau = max(dmin, 0.25 * dtau)
+                res = math.inf
+                continue
             if rk < r_prev:
                 dtau = min(dtau_max, max(dtau * growth, dtau0 * r0 / max(rk, 1e-300)))
             else:
-                dtau = max(float(dtau0), 0.5 * dtau)
+                dtau = max(dmin, 0.5 * dtau)
             r_prev = rk
     finally:
         dev.set_invdtau(keep)
