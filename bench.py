@@ -324,7 +324,15 @@ def run_adjoint_workload(args):
     def primal():
         if math.isinf(dtau):
             return s.advance(0.0)[:2]
-        return steady_solve_ser(s, dtau0=dtau, max_iter=300)
+        # a second, gentler continuation from the same start if the first fails
+        total = 0
+        for growth in (2.0, 1.25):
+            s.set_state(*q0)
+            res, its = steady_solve_ser(s, dtau0=dtau, max_iter=300, growth=growth)
+            total += its
+            if math.isfinite(res) and res <= cfg.pseudo_tol:
+                break
+        return res, total
 
     t0 = time.perf_counter()
     try:
