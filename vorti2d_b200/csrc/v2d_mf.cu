@@ -2535,6 +2535,11 @@ __device__ __forceinline__ unsigned long long globaltimer_ns()
 
 // Bounded wait until *ctr >= target; false if it ran out or another CTA
 // reported an error meanwhile.
+__device__ __forceinline__ void red_release_gpu(int *p, int v)
+{
+    asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 __device__ __forceinline__ bool wait_count(const int *ctr, int target, volatile int *err)
 {
     long long spins = 0;
@@ -2549,7 +2554,8 @@ __device__ __forceinline__ bool wait_count(const int *ctr, int target, volatile 
 // bottom-up, then backward top-down).  A CTA takes items by ticket
 // (ctr[nctr]), loads what needs no other item, waits (thread 0, acquire
 // loads) until the item's counters reach their targets, runs the item and,
-// after a fence, adds one to the item's done counters.  The plan checks that
+// after a barrier, adds one to the item's done counters with release
+// semantics.  The plan checks that
 // every counter an item waits on is advanced only by items before it, so a
 // CTA only ever waits for items held by running CTAs: no co-resident grid is
 // needed.  A wait that runs out (or an error seen while waiting) sets
@@ -2597,12 +2603,13 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_solve_flow(
         if (!ok_s) return;
         if (trace && threadIdx.x == 0) trace[3 * i + 1] = globaltimer_ns();
         run_item(c, D, b, rs, zbuf, upd, x, smem);
-        __threadfence();
+        // the barrier orders every thread's writes before thread 0's release
+        // additions (cumulative at GPU scope), which the waiters' acquire
+        // loads pair with
         __syncthreads();
         if (threadIdx.x == 0) {
-            __threadfence();
-            if (it.z.x >= 0) atomicAdd(ctr + it.z.x, 1);
-            if (it.z.y >= 0) atomicAdd(ctr + it.z.y, 1);
+            if (it.z.x >= 0) red_release_gpu(ctr + it.z.x, 1);
+            if (it.z.y >= 0) red_release_gpu(ctr + it.z.y, 1);
             if (trace) trace[3 * i + 2] = globaltimer_ns();
         }
     }
