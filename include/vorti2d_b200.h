@@ -431,6 +431,16 @@ int v2d_solver_trace_lu_apply(v2d_solver *s, unsigned long long *ticks, int *ite
  * current one into *current (may be null). */
 int v2d_solver_lu_flow_form(v2d_solver *s, int form, int *current);
 
+/* Tuning aid (no reference counterpart): the split form of the dataflow LU
+ * solve -- level > 0 runs the tree levels [0, level) as launches of their own
+ * (their forward items before, their backward items after the upper levels'
+ * launch), with 128-thread CTAs and shared memory for their own largest
+ * front, so that more of their many small work items are in flight per SM;
+ * 0: one launch for the whole tree.  level < 0 only reads the current
+ * setting into *current (may be null).  Every setting forms the same
+ * products. */
+int v2d_solver_lu_split(v2d_solver *s, int level, int *current);
+
 /* Tuning aid (no reference counterpart): the work-item granularity of the
  * LU preconditioner solve, rows[L] rows of a front per work item on tree
  * level L (0: whole fronts); rows may be null to only read the current

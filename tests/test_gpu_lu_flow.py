@@ -133,3 +133,35 @@ def test_gathered_split(v2d, oracle_mod, imax, jmax, ff_bc, precision):
     assert np.array_equal(out["gathered"], out["gathered_levels"])
     scale = np.abs(out["plain"]).max()
     assert np.max(np.abs(out["plain"] - out["gathered"])) <= 1e-10 * scale
+
+
+@pytest.mark.parametrize("imax,jmax,ff_bc", [(33, 21, 1), (129, 65, 2), (181, 181, 1)])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_split_launches(v2d, oracle_mod, imax, jmax, ff_bc, precision):
+    """The split form (tree levels [0, L) as launches of their own, forward
+    before and backward after the upper levels' launch, in 128-thread CTAs)
+    gives the Newton update of the one-launch form to 1e-10 relative, for
+    every split level the tuner may pick."""
+    from vorti2d_b200 import tune
+    bc = {0: "dirichlet", 1: "outflow", 2: "outflow_psi"}[ff_bc]
+    xg, yg = oracle_mod.generate_cylinder(imax, jmax)
+    M = oracle_mod.core().compute_metrics(1 / (imax - 1), 1 / (jmax - 1), xg, yg)
+    st = smooth_state(M[8], M[9])
+
+    def update(split):
+        s = _solver(v2d, xg, yg, bc, precision, "flow")
+        if split:
+            assert tune.set_split_level(s, split) and tune.split_level(s) == split
+        s.set_state(*st)
+        code, _, _ = s.dev.newton(0.3)
+        assert code == 0, v2d._lib.last_error()
+        out = np.concatenate(s.dev.get_state()[:2]) - np.concatenate(st[:2])
+        nl = len(tune.item_rows(s))
+        s.close()
+        return out, nl
+
+    ref, nl = update(0)
+    scale = np.abs(ref).max()
+    for split in sorted({1, min(3, nl - 1), nl - 1}):
+        got, _ = update(split)
+        assert np.max(np.abs(got - ref)) <= 1e-10 * scale, split

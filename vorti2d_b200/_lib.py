@@ -124,6 +124,7 @@ _SIGS = {
     "v2d_solver_time_lu_launches": (_i, [_vp, _i, _ll, _dp, _ip, _i, _ip]),
     "v2d_solver_time_lu_factor": (_i, [_vp, _i, _dp, _ip, _i, _ip]),
     "v2d_solver_lu_stats": (_i, [_vp, _dp]),
+    "v2d_solver_lu_split": (_i, [_vp, _i, _ip]),
     "v2d_solver_residual_mesh": (_i, [_vp, _dp, _dp, _d, _d, _d, _d, _d, _d, _dp, _i, _dp]),
     "v2d_solver_trace_lu_apply": (_i, [_vp, ctypes.POINTER(ctypes.c_ulonglong), _ip, _i, _ip]),
     "v2d_solver_lu_flow_form": (_i, [_vp, _i, _ip]),

@@ -156,8 +156,13 @@ struct MfFactor {
     MfBarrier *bar = nullptr;
     int *sctr = nullptr;        // dataflow solve: 3 counters per front + the work ticket
     int flow_grid = 0;          // most CTAs of the dataflow solve resident at once
-    int flow_grid1 = 0;         // the same for its high-occupancy form (FP32 only; 0: none)
+    int flow_grid1 = 0;         // the same for its high-occupancy form (0: none)
     int flow_form = 0;          // 0: 2 CTAs per SM, 32 row registers; 1: 3 CTAs, 16
+    int split = 0;              // > 0: tree levels [0, split) in launches of their own
+                                // (forward before, backward after the upper levels)
+    int low_grid = 0;           // CTAs of those launches
+    size_t low_smem = 0;        // and their shared memory
+    int low_wcap = 0;           // their largest front
     int flow = 1;               // 1: the solve is one dataflow launch; 0: one launch per level
                                 // and sweep
     cudaGraphExec_t graph = nullptr;
@@ -190,6 +195,9 @@ int mf_plan_forest(const std::vector<MfPlan *> &parts, const std::vector<int> &r
 // Work-item granularity of the solve per level (rows per item, 0: whole
 // fronts); replaces the device item table.
 int mf_plan_set_item_rows(MfPlan *P, const int *rows, int nlevels);
+// Split form of the dataflow solve: levels [0, split) in launches of their
+// own (0: one launch); sizes their shared memory and grid.
+int mf_set_split(const MfPlan *P, MfFactor *M, int split);
 // fp32: FP32 solve; fact64 (with fp32): FP64 factorization rounded to FP32.
 int mf_factor_create(const MfPlan *P, int fp32, int fact64, MfFactor **out);
 void mf_factor_destroy(MfFactor *M);

@@ -608,11 +608,11 @@ static void drop_graphs(KrylovWork *w, int which)
 }
 
 // The LU solve a captured cycle launches: -1 none, -2 the transposed solve,
-// else 10 * (dataflow) + kernel form.
+// else 1000 * split level + 10 * (dataflow) + kernel form.
 static int lu_form(const CsrOp &A)
 {
     if (!A.lu) return -1;
-    return A.lu_transpose ? -2 : 10 * A.lu->flow + A.lu->flow_form;
+    return A.lu_transpose ? -2 : 1000 * A.lu->split + 10 * A.lu->flow + A.lu->flow_form;
 }
 
 template <class T>

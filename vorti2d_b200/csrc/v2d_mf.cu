@@ -2042,6 +2042,7 @@ __device__ __forceinline__ bool stopped(const int *a, const int *b)
 }
 
 constexpr int kSolveThreads = kSolveThreadsHost;   // 8 warps per work item
+constexpr int kFlowSlots = 3;   // ticket counters after the dependency counters
 constexpr int kGatherRegs = 4;   // staged gather entries per thread (fronts up to 4 x 256)
 constexpr int kThreadRowMaxF = 256;   // fronts whose forward rows a thread sums alone
 
@@ -2488,12 +2489,13 @@ struct SolveItemDev {
 template <class T, int R>
 __device__ __forceinline__ void run_item(SolveItemCtx<T, R> &c, const MfDev &D, const T *b,
                                          const double *__restrict__ rs, T *zbuf, T *upd, T *x,
-                                         T *smem)
+                                         T *smem, int wcap)
 {
+    // shared memory: w (wcap entries, the largest front of the launch), then t
     switch (c.kind) {
-    case 0: c.run_fwd(D, b, rs, zbuf, upd, smem, smem + D.maxf); break;
+    case 0: c.run_fwd(D, b, rs, zbuf, upd, smem, smem + wcap); break;
     case 1: c.run_bwd(D, zbuf, x, smem); break;
-    case 2: c.run_gather_fwd(D, b, rs, upd, smem, smem + D.maxf); break;
+    case 2: c.run_gather_fwd(D, b, rs, upd, smem, smem + wcap); break;
     default: c.run_gather_bwd(D, x); break;
     }
 }
@@ -2511,8 +2513,12 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_solve_level(
     const SolveItemDev it = items[i0 + blockIdx.x];
     SolveItemCtx<T> c;
     c.pre(D, F, b, rs, it.x.x, it.z.w, it.x.y, it.x.z, it.x.w);
-    run_item(c, D, b, rs, zbuf, upd, x, smem);
+    run_item(c, D, b, rs, zbuf, upd, x, smem, D.maxf);
 }
+
+// The split form's lower-level launches: CTA size and resident CTAs per SM.
+constexpr int kLowThreads = 128;
+constexpr int kLowMinBlocks = 4;
 
 // Polls of one dependency counter before a CTA of the dataflow solve gives
 // up (each poll sleeps ~40 ns: well under a second in all).
@@ -2566,30 +2572,37 @@ __device__ __forceinline__ bool wait_count(const int *ctr, int target, volatile 
 // R row registers per lane (rows up to 32 R entries prefetched before the
 // wait).  Form 0: 2 CTAs and RowRegs<T> registers; form 1: 3 CTAs per SM
 // with RowRegs3<T>, more warps in flight for the levels whose items are
-// whole fronts.
-template <class T, int R, int MINB>
-__global__ void __launch_bounds__(kSolveThreads, MINB) k_solve_flow(
+// whole fronts.  A launch runs the items [item0, item1) with ticket counter
+// ctr[nctr + slot]: the whole table, or (split form) the lower levels'
+// forward items, the upper levels, the lower levels' backward items as three
+// launches in stream order -- an item then only waits for items of its own
+// launch or of an earlier, finished one.  The lower launches use NT = 128
+// threads and shared memory for their own largest front (wcap), so more of
+// their many small items are in flight per SM.
+template <class T, int R, int MINB, int NT = kSolveThreads>
+__global__ void __launch_bounds__(NT, MINB) k_solve_flow(
     const MfDev D, const T *F, const T *b, const double *__restrict__ rs, T *zbuf, T *upd, T *x,
-    const SolveItemDev *__restrict__ items, int nitems, int *ctr, int nctr, MfBarrier *bar,
-    const int *stop_a, const int *stop_b, unsigned long long *trace)
+    const SolveItemDev *__restrict__ items, int item0, int item1, int wcap, int *ctr, int nctr,
+    int slot, MfBarrier *bar, const int *stop_a, const int *stop_b, unsigned long long *trace)
 {
     if (stopped(stop_a, stop_b)) return;   // the flags are the same for every CTA
     extern __shared__ unsigned char smem_raw[];
     T *smem = reinterpret_cast<T *>(smem_raw);
     __shared__ int item_s, ok_s;
     volatile int *err = &bar->err;
-    int next = threadIdx.x == 0 ? atomicAdd(ctr + nctr, 1) : 0;
+    int *ticket = ctr + nctr + slot;
+    int next = threadIdx.x == 0 ? item0 + atomicAdd(ticket, 1) : 0;
     for (;;) {
         if (threadIdx.x == 0) item_s = next;
         __syncthreads();
         const int i = item_s;
-        if (i >= nitems) return;
+        if (i >= item1) return;
         const SolveItemDev it = items[i];
         if (trace && threadIdx.x == 0) trace[3 * i] = globaltimer_ns();
         SolveItemCtx<T, R> c;
         c.pre(D, F, b, rs, it.x.x, it.z.w, it.x.y, it.x.z, it.x.w);
         if (threadIdx.x == 0) {
-            next = atomicAdd(ctr + nctr, 1);   // in flight during the wait
+            next = item0 + atomicAdd(ticket, 1);   // in flight during the wait
             bool ok = true;
             if (it.y.x >= 0 && it.y.y > 0) ok = wait_count(ctr + it.y.x, it.y.y, err);
             if (ok && it.y.z >= 0 && it.y.w > 0) ok = wait_count(ctr + it.y.z, it.y.w, err);
@@ -2602,7 +2615,7 @@ __global__ void __launch_bounds__(kSolveThreads, MINB) k_solve_flow(
         __syncthreads();
         if (!ok_s) return;
         if (trace && threadIdx.x == 0) trace[3 * i + 1] = globaltimer_ns();
-        run_item(c, D, b, rs, zbuf, upd, x, smem);
+        run_item(c, D, b, rs, zbuf, upd, x, smem, wcap);
         // the barrier orders every thread's writes before thread 0's release
         // additions (cumulative at GPU scope), which the waiters' acquire
         // loads pair with
@@ -2745,7 +2758,7 @@ int mf_factor_create(const MfPlan *P, int fp32, int fact64, MfFactor **out)
     grab(&M->z, (size_t)P->vtotal * es);
     grab(&M->tmp, (size_t)P->tmax * esf);
     grab(&M->gh, (size_t)P->gmax * esf);
-    grab((void **)&M->sctr, (size_t)(P->nctr + 1) * sizeof(int));
+    grab((void **)&M->sctr, (size_t)(P->nctr + kFlowSlots) * sizeof(int));
     grab(&M->wb, (size_t)P->vtotal * es);
     grab(&M->tw, (size_t)P->vtotal * es);
     grab((void **)&M->rs, (size_t)P->n * sizeof(double));
@@ -3115,23 +3128,44 @@ static int apply_launches(const MfPlan *P, const MfFactor *M, const T *b, T *x, 
     const size_t smf = (size_t)(P->maxf + P->maxS) * sizeof(T);
     long long launches = 0;
     if (M->flow) {
-        V2D_CUDA_TRY(cudaMemsetAsync(M->sctr, 0, (size_t)(P->nctr + 1) * sizeof(int), s));
-        bool launched = false;
-        if (M->flow_form == 1 && M->flow_grid1 > 0) {
-            k_solve_flow<T, RowRegs3<T>::v, 3><<<std::max(1, std::min(P->nitems, M->flow_grid1)),
-                                                 kSolveThreads, smf, s>>>(
-                D, F, b, M->rs, z, upd, x, items, P->nitems, M->sctr, P->nctr, M->bar, stop_a,
-                stop_b, trace);
-            launched = true;
+        V2D_CUDA_TRY(cudaMemsetAsync(M->sctr, 0, (size_t)(P->nctr + kFlowSlots) * sizeof(int), s));
+        auto upper = [&](int i0, int i1, int slot) {
+            const int n = std::max(1, i1 - i0);
+            if (M->flow_form == 1 && M->flow_grid1 > 0)
+                k_solve_flow<T, RowRegs3<T>::v, 3><<<std::min(n, M->flow_grid1), kSolveThreads, smf,
+                                                     s>>>(D, F, b, M->rs, z, upd, x, items, i0, i1,
+                                                          P->maxf, M->sctr, P->nctr, slot, M->bar,
+                                                          stop_a, stop_b, trace);
+            else
+                k_solve_flow<T, RowRegs<T>::v, 2><<<std::min(n, M->flow_grid), kSolveThreads, smf,
+                                                    s>>>(D, F, b, M->rs, z, upd, x, items, i0, i1,
+                                                         P->maxf, M->sctr, P->nctr, slot, M->bar,
+                                                         stop_a, stop_b, trace);
+        };
+        auto lower = [&](int i0, int i1, int slot) {
+            k_solve_flow<T, RowRegs<T>::v, kLowMinBlocks, kLowThreads>
+                <<<std::max(1, std::min(i1 - i0, M->low_grid)), kLowThreads, M->low_smem, s>>>(
+                    D, F, b, M->rs, z, upd, x, items, i0, i1, M->low_wcap, M->sctr, P->nctr, slot,
+                    M->bar, stop_a, stop_b, trace);
+        };
+        const int Ls = M->split;
+        if (Ls > 0 && Ls < P->nlevel && M->low_grid > 0) {
+            lower(P->lvl_fwd[0], P->lvl_fwd[Ls], 0);
+            V2D_TRY(solve_launch("k_solve_flow (lower levels, forward)", 0));
+            V2D_TRY(mark(kCodeFlow * 1000));
+            upper(P->lvl_fwd[Ls], P->lvl_bwd[Ls], 1);
+            V2D_TRY(solve_launch("k_solve_flow (upper levels)", 0));
+            V2D_TRY(mark(kCodeFlow * 1000 + 1));
+            lower(P->lvl_bwd[Ls], P->nitems, 2);
+            V2D_TRY(solve_launch("k_solve_flow (lower levels, backward)", 0));
+            V2D_TRY(mark(kCodeFlow * 1000 + 2));
+            launches = 3;
+        } else {
+            upper(0, P->nitems, 0);
+            V2D_TRY(solve_launch("k_solve_flow", 0));
+            V2D_TRY(mark(kCodeFlow * 1000));
+            launches = 1;
         }
-        if (!launched)
-            k_solve_flow<T, RowRegs<T>::v, 2><<<std::max(1, std::min(P->nitems, M->flow_grid)),
-                                                kSolveThreads, smf, s>>>(
-                D, F, b, M->rs, z, upd, x, items, P->nitems, M->sctr, P->nctr, M->bar, stop_a,
-                stop_b, trace);
-        V2D_TRY(solve_launch("k_solve_flow", 0));
-        V2D_TRY(mark(kCodeFlow * 1000));
-        launches = 1;
     } else {
         // a level's gather items (first in its range) are a launch of their own
         for (int L = 0; L < P->nlevel; ++L) {
@@ -3209,6 +3243,39 @@ int mf_apply_transpose(const MfPlan *P, MfFactor *M, const void *g, void *lambda
 int mf_flag(const MfFactor *M, int *flag, cudaStream_t s)
 {
     V2D_CUDA_TRY(cudaMemcpyAsync(flag, M->flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    return V2D_OK;
+}
+
+int mf_set_split(const MfPlan *P, MfFactor *M, int split)
+{
+    V2D_ARG_CHECK(split >= 0 && split < P->nlevel, "lu split: level %d (0 .. %d)", split,
+                  P->nlevel - 1);
+    if (split == 0) {
+        M->split = 0;
+        return V2D_OK;
+    }
+    int wcap = 0, smax = 0;
+    for (int L = 0; L < split; ++L) {
+        wcap = std::max(wcap, P->lvl_maxf[L]);
+        smax = std::max(smax, P->lvl_maxS[L]);
+    }
+    const size_t es = M->fp32 ? sizeof(float) : sizeof(double);
+    const size_t bytes = (size_t)(wcap + smax) * es;
+    const void *fn = M->fp32
+                         ? (const void *)k_solve_flow<float, RowRegs<float>::v, kLowMinBlocks,
+                                                      kLowThreads>
+                         : (const void *)k_solve_flow<double, RowRegs<double>::v, kLowMinBlocks,
+                                                      kLowThreads>;
+    V2D_CUDA_TRY(raise_dyn_smem(fn, bytes));
+    int dev = 0, nsm = 0, per_sm = 0;
+    V2D_CUDA_TRY(cudaGetDevice(&dev));
+    V2D_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    V2D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kLowThreads, bytes));
+    V2D_ARG_CHECK(per_sm > 0, "lu split: no CTA of the lower-level launch fits on an SM");
+    M->low_wcap = wcap;
+    M->low_smem = bytes;
+    M->low_grid = nsm * per_sm;
+    M->split = split;
     return V2D_OK;
 }
 

@@ -789,6 +789,19 @@ extern "C" int v2d_solver_lu_flow_form(v2d_solver *S, int form, int *current)
     return V2D_OK;
 }
 
+extern "C" int v2d_solver_lu_split(v2d_solver *S, int level, int *current)
+{
+    V2D_ARG_CHECK(S, "null solver");
+    const int q = S->prm.krylov.precision == V2D_PREC_MIXED ? 1 : 0;
+    V2D_ARG_CHECK(S->lu[q] && S->plan, "lu_split: no LU factors (precond must be V2D_PC_LU)");
+    if (level >= 0) {
+        V2D_CUDA_TRY(cudaStreamSynchronize(S->s));
+        V2D_TRY(mf_set_split(S->plan, S->lu[q], level));
+    }
+    if (current) *current = S->lu[q]->split;
+    return V2D_OK;
+}
+
 extern "C" int v2d_solver_lu_item_rows(v2d_solver *S, const int *rows, int nlevels, int *out_rows,
                                        int cap, int *nlevels_out)
 {

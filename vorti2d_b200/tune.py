@@ -12,7 +12,9 @@ and keep a CTA's rows together; gather items add one dependent step but
 spare every item the indexed gather.  Which wins depends on
 the grid, the precision and the GPU, so it is measured: a coordinate search
 over the levels (each level's candidates tried with the others fixed, two
-sweeps), every trial timed as the average of warm applications of the
+sweeps), then the split form (the lower levels as launches of their own with
+smaller CTAs, ``split`` levels, followed by one more sweep over those
+levels' rows), every trial timed as the average of warm applications of the
 current factors (``v2d_solver_time_lu_apply``, factors in L2 as inside
 GMRES).  Every setting forms the same products; a row's partial sums are
 added in an order that depends on the split, so results agree to rounding
@@ -66,6 +68,18 @@ def set_flow_form(solver, form: int) -> bool:
     return lib().v2d_solver_lu_flow_form(solver.dev.h, int(form), None) == _lib.V2D_OK
 
 
+def split_level(solver) -> int:
+    cur = ctypes.c_int()
+    check(lib().v2d_solver_lu_split(solver.dev.h, -1, ctypes.byref(cur)), "lu_split")
+    return cur.value
+
+
+def set_split_level(solver, level: int) -> bool:
+    """Run the tree levels [0, level) of the solve as launches of their own
+    (0: one launch); False when the setting does not fit."""
+    return lib().v2d_solver_lu_split(solver.dev.h, int(level), None) == _lib.V2D_OK
+
+
 def time_apply(solver, reps: int = 30, repeats: int = 3) -> float:
     """ms of one warm LU application: the smallest of `repeats` averages of
     `reps` applications."""
@@ -106,9 +120,10 @@ def tune_lu_solve(solver, candidates=CANDIDATES, sweeps: int = 2, reps: int | No
         if t < best * (1.0 - gain):
             best, form = t, f
     set_flow_form(solver, form)
-    for _ in range(sweeps):
+    def sweep(levels):
+        nonlocal best, rows, trials
         changed = False
-        for L in range(len(rows)):
+        for L in levels:
             for c in candidates:
                 if c == rows[L]:
                     continue
@@ -120,11 +135,28 @@ def tune_lu_solve(solver, candidates=CANDIDATES, sweeps: int = 2, reps: int | No
                 if t < best * (1.0 - gain):
                     best, rows, changed = t, trial, True
             set_item_rows(solver, rows)
-        if not changed:
+        return changed
+
+    for _ in range(sweeps):
+        if not sweep(range(len(rows))):
             break
     set_item_rows(solver, rows)
-    rec = {"key": _key(solver), "rows": rows, "form": form, "ms": best, "default_ms": t0,
-           "trials": trials, "reps": reps, "candidates": list(candidates)}
+    # split form: the lower levels as launches of their own, then their rows
+    # again under it
+    split = split_level(solver)
+    for lv in range(1, min(len(rows), 9)):
+        if lv == split or not set_split_level(solver, lv):
+            continue
+        t = time_apply(solver, reps)
+        trials += 1
+        if t < best * (1.0 - gain):
+            best, split = t, lv
+    set_split_level(solver, split)
+    if split > 0:
+        sweep(range(split))
+    set_item_rows(solver, rows)
+    rec = {"key": _key(solver), "rows": rows, "form": form, "split": split, "ms": best,
+           "default_ms": t0, "trials": trials, "reps": reps, "candidates": list(candidates)}
     if path:
         table = {}
         if os.path.exists(path):
@@ -150,4 +182,5 @@ def load_tuning(solver, path: str) -> bool:
         return False
     set_item_rows(solver, rec["rows"])
     set_flow_form(solver, rec.get("form", 0))
+    set_split_level(solver, rec.get("split", 0))
     return True
