@@ -324,14 +324,24 @@ def run_adjoint_workload(args):
     def primal():
         if math.isinf(dtau):
             return s.advance(0.0)[:2]
-        # a second, gentler continuation from the same start if the first fails
+        # a second, gentler continuation from the same start if the first
+        # fails, then a Reynolds ladder (each rung from the previous state)
         total = 0
         for growth in (2.0, 1.25):
             s.set_state(*q0)
             res, its = steady_solve_ser(s, dtau0=dtau, max_iter=300, growth=growth)
             total += its
             if math.isfinite(res) and res <= cfg.pseudo_tol:
+                return res, total
+        s.set_state(*q0)
+        target = float(cfg.re)
+        for re_k in [r for r in (50.0, 100.0, 200.0, 300.0, 400.0) if r < target] + [target]:
+            s.dev.set_re(re_k)
+            res, its = steady_solve_ser(s, dtau0=dtau, max_iter=300, growth=1.5, re=re_k)
+            total += its
+            if not (math.isfinite(res) and res <= cfg.pseudo_tol):
                 break
+        s.dev.set_re(target)
         return res, total
 
     t0 = time.perf_counter()
@@ -447,7 +457,7 @@ def run_large_workload(args):
     cfg = v.Config(verbose=False, write_csv=False, write_xdmf=False, compute_forces=False,
                    re=200.0, steady=False, dt_phys=0.05, farfield_bc="outflow",
                    raise_on_linear_failure=False, precision=args.large_precision,
-                   lu_reuse_its=args.lu_reuse, lu_reuse_steps=bool(args.lu_reuse_steps),
+                   lu_reuse_its=args.large_reuse, lu_reuse_steps=bool(args.lu_reuse_steps),
                    **SOLVER)
     t0 = time.perf_counter()
     s = v.Solver(cfg, mesh=(xg, yg))
@@ -488,7 +498,7 @@ def run_large_workload(args):
             "dtype": "f32-krylov/f64" if args.large_precision == "mixed" else "f64",
             "data": "synthetic",
             "config": {"workload": f"large unsteady BDF2 cylinder {n}x{n} Re=200 dt=0.05 outflow",
-                       "unknowns": 2 * n * n, "lu_reuse_its": args.lu_reuse,
+                       "unknowns": 2 * n * n, "lu_reuse_its": args.large_reuse,
                        "lu_factors": SOLVER.get("lu_factors"),
                        "lu_reuse_steps": args.lu_reuse_steps,
                        "l2": "flushed (256 MiB write) before every timed step"},
@@ -954,7 +964,7 @@ def main():
                     help="timed steps of the one-core CPU sample in the device arm's line")
     ap.add_argument("--cpu-procs", type=int, default=128,
                     help="--impl reference: at most this many CPU replicas (one per core)")
-    ap.add_argument("--lu-reuse", type=int, default=12,
+    ap.add_argument("--lu-reuse", type=int, default=8,
                     help="keep LU factors while GMRES needs at most this many iterations "
                          "(0: factor every Newton Jacobian)")
     ap.add_argument("--lu-factors", default="fp32", choices=["fp32", "fp64"],
@@ -991,6 +1001,9 @@ def main():
                          "plain Newton from the free stream as the reference)")
     ap.add_argument("--large-grid", type=int, default=2049,
                     help="grid side of the large unsteady workload (--workload large)")
+    ap.add_argument("--large-reuse", type=int, default=12,
+                    help="large: keep the (expensive) FP64 factors while GMRES needs at most "
+                         "this many iterations")
     ap.add_argument("--large-steps", type=int, default=3,
                     help="timed BDF2 steps of the large unsteady workload")
     ap.add_argument("--large-precision", default="fp64", choices=["mixed", "fp64"],

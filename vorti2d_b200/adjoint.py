@@ -135,7 +135,7 @@ def force_vjp(solver, weights, alpha_h=1e-3):
 
 # ------------------------------------------------------------------ shape
 def steady_solve_ser(solver, dtau0=1.0, tol=None, max_iter=300, dtau_max=1e12, growth=2.0,
-                     reject=1e3):
+                     reject=1e3, re=None):
     """Steady state by pseudo-transient continuation: iteration k adds
     1/dtau_k to the Newton Jacobian's diagonal.  While the residual norm
     ||R|| falls, dtau grows by `growth` per iteration, and at least to the
@@ -150,11 +150,14 @@ def steady_solve_ser(solver, dtau0=1.0, tol=None, max_iter=300, dtau_max=1e12, g
     equations; the stopping rule is the reference's, ||dq||/(2N) <= tol.
     For cases where Newton from the free stream diverges.  Returns
     (||dq||/(2N), iterations, counting rejected ones); the handle's own
-    1/dtau is restored."""
+    1/dtau is restored.  `re`: the Reynolds number the handle currently
+    solves for, when it was changed from the configuration's (continuation
+    in Re)."""
     dev, cfg = solver.dev, solver.cfg
     tol = cfg.pseudo_tol if tol is None else float(tol)
     urot = cfg.u_rot(0.0)
-    re, adeg = float(cfg.re), float(cfg.alpha_deg)
+    re = float(cfg.re) if re is None else float(re)
+    adeg = float(cfg.alpha_deg)
     keep = dev.params.invdtau
     r0 = float(np.linalg.norm(_residual(solver, re, adeg, urot)))
     r_prev = r0

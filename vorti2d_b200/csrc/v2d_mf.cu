@@ -1009,7 +1009,7 @@ namespace {
 
 constexpr int kMfThreads = 256;
 constexpr int kGemmTile = 64;
-constexpr int kTileStages = 3;   // operand slices in flight in the tile engine
+constexpr int kTileStages = 2;   // operand slices in flight in the tile engine
 // levels whose largest front has at least kDelayFront variables update the
 // trailing block once per kDelayPanels panels (k_gemm)
 constexpr int kDelayFront = 1024;
@@ -1417,8 +1417,9 @@ template <int N> __device__ __forceinline__ void cp_async_wait()
 
 // acc += sum over k in [ka, kb) of a(rr, k) b(k, cc), in NB-wide slices
 // through kTileStages shared buffers (sm[0 .. kTileStages)): the copies of
-// slices s + 1 and s + 2 are in flight while the tensor cores (or CUDA
-// cores) work on slice s.  srcA(rr, k)
+// the next kTileStages - 1 slices are in flight while the tensor cores (or
+// CUDA cores) work on slice s.  Two buffers leave room for three CTAs per SM
+// in FP64, which hide the copies' latency better than a third buffer.  srcA(rr, k)
 // and srcB(k, cc) give the element's address or nullptr (zero); oneA(rr, k)
 // and oneB(k, cc) mark entries that are 1 instead (a unit diagonal), written
 // after the slice's copies have landed.  base: any valid address (the source
@@ -1463,18 +1464,17 @@ __device__ __forceinline__ void tile_mac(TileAcc<T> &acc, typename TileAcc<T>::S
             if (k + t < kb && oneA(rr, k + t)) TileAcc<T>::refA(b, rr, t) = T(1);
         }
     };
-    static_assert(kTileStages == 3, "the wait counts below assume three stages");
-    if (ns > 0) stage(0);
-    if (ns > 1) stage(1);
+    static_assert(kTileStages == 2 || kTileStages == 3, "two or three stages");
+    for (int p = 0; p < kTileStages - 1 && p < ns; ++p) stage(p);
     for (int sl = 0; sl < ns; ++sl) {
-        // slice sl has landed once at most the copies of slice sl + 1 pend
-        if (sl + 1 < ns) cp_async_wait<1>();
+        // slice sl has landed once at most the later slices already issued pend
+        if (kTileStages == 3 && sl + 1 < ns) cp_async_wait<kTileStages - 2>();
         else cp_async_wait<0>();
         ones(sl);
         __syncthreads();
-        // the buffer of slice sl + 2 held slice sl - 1, which every thread
-        // finished before the barrier above
-        if (sl + 2 < ns) stage(sl + 2);
+        // the buffer of slice sl + kTileStages - 1 held slice sl - 1, which
+        // every thread finished before the barrier above
+        if (sl + kTileStages - 1 < ns) stage(sl + kTileStages - 1);
         acc.mac(sm[sl % kTileStages]);
     }
     __syncthreads();   // the buffers may be reused after the last slice
