@@ -335,7 +335,8 @@ def run_adjoint_workload(args):
                 return res, total
         s.set_state(*q0)
         target = float(cfg.re)
-        for re_k in [r for r in (50.0, 100.0, 200.0, 300.0, 400.0) if r < target] + [target]:
+        ladder = (5.0, 10.0, 20.0, 40.0, 70.0, 100.0, 150.0, 200.0, 300.0, 400.0)
+        for re_k in [r for r in ladder if r < target] + [target]:
             s.dev.set_re(re_k)
             res, its = steady_solve_ser(s, dtau0=dtau, max_iter=300, growth=1.5, re=re_k)
             total += its
