@@ -540,6 +540,15 @@ static int red_grid(long long n)
 // Gram-Schmidt grids: one element per thread up to kTileBlocks blocks
 // (latency hiding needs many loads in flight), grid-stride beyond.
 constexpr int kTileBlocks = 8 * kSMs;
+
+// FP64 residual grid: one CSR row per kTPR threads up to kTileBlocks blocks
+// (each row's index -> vector gather chain is latency bound; a small grid
+// would walk tens of rows per thread one after another).
+static int res_grid(long long n)
+{
+    const long long g = (n * kTPR + kSpmvThreads - 1) / kSpmvThreads;
+    return (int)std::max(1LL, std::min<long long>(kTileBlocks, g));
+}
 static int tile_grid(long long n)
 {
     long long g = (n + kRedThreads - 1) / kRedThreads;
@@ -673,7 +682,7 @@ static int capture_cycle(KrylovWork *w, int which, T *V, T *wv, T *z, T *Z, doub
     V2D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     k_backsolve<<<1, 32, 0, s>>>(w->desc, w->ctl, w->H, w->g, w->y);
     k_correct<T><<<gp, 256, 0, s>>>(w->desc, w->ctl, V, w->y, z, x, Z);
-    k_residual<<<gr, kSpmvThreads, 0, s>>>(w->desc, w->ctl, w->r, w->partial, w->g, 0);
+    k_residual<<<res_grid(n), kSpmvThreads, 0, s>>>(w->desc, w->ctl, w->r, w->partial, w->g, 0);
     V2D_TRY(end_capture(s, &w->fin[which]));
     w->seg_bounds[which] = bnd;
     w->graph_m[which] = w->m;
@@ -803,7 +812,7 @@ int krylov_solve(KrylovWork *w, const CsrOp &A, const double *d_b, double *d_x,
     V2D_CUDA_TRY(cudaMemcpyAsync(w->ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, s));
     V2D_CUDA_TRY(cudaMemsetAsync(d_x, 0, (size_t)A.n * sizeof(double), s));
     const int gr = red_grid(A.n);
-    k_residual<<<gr, kSpmvThreads, 0, s>>>(w->desc, w->ctl, w->r, w->partial, w->g, 1);
+    k_residual<<<res_grid(A.n), kSpmvThreads, 0, s>>>(w->desc, w->ctl, w->r, w->partial, w->g, 1);
     V2D_CUDA_TRY(cudaGetLastError());
     count_launches(1);
     // atol: tol_abs = max(rtol * ||b||, atol) -- applied on the host after the first pass
