@@ -722,9 +722,13 @@ def profile_lu_launches(args):
     st = (ctypes.c_double * 6)()
     _lib.check(_lib.lib().v2d_solver_lu_stats(s.dev.h, st))
     total = sum(ms[k] for k in range(n.value))
+    top = int(st[1]) - 2   # the two top levels launch by launch
     out["factor"] = {"total_ms": total, "launches": n.value, "flops": st[3],
                      "tflops": st[3] / (total * 1e-3) / 1e12,
-                     "by_kind_ms": by_kind, "by_level_ms": by_level}
+                     "by_kind_ms": by_kind, "by_level_ms": by_level,
+                     "top_levels_us": [[fkinds[codes[k] // 1000], codes[k] % 1000,
+                                        round(1e3 * ms[k], 1)]
+                                       for k in range(n.value) if codes[k] % 1000 >= top]}
     print(json.dumps(out), flush=True)
     s.close()
 
