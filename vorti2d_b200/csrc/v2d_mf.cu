@@ -1771,6 +1771,9 @@ __global__ void __launch_bounds__(kTrinvThreadsG) k_trinv_g(int q0, const int *_
 // this step only; the whole pivot block is replaced by k_trcopy afterwards),
 // phase 1 the products.  Results go to the level's scratch like k_trinv's.
 constexpr int kInvBlk = 64;   // the tile engine's tile
+// separators from this width on are inverted by blocks (fewer dependent
+// steps per CTA than the column-block solves; measured on 362-wide ones)
+constexpr int kBlockedInvMinS = 256;
 constexpr int kTrinvDiagThreads = 128;
 
 template <class T> constexpr size_t trinv_diag_smem() { return 3 * kInvBlk * (kInvBlk + 1) * sizeof(T); }
@@ -2989,11 +2992,14 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
         const size_t inv_bytes = (size_t)P->lvl_maxS[L] * (InvWidth<T>::v + 33) * sizeof(T);
         for (int qb = 0; qb < nq; qb += kMaxFrontsY) {
             const int nb = std::min(nq - qb, kMaxFrontsY);
-            if (inv_bytes <= kInvSmemMax) {
+            const bool blocked = P->lvl_maxS[L] >= kBlockedInvMinS &&
+                                 (std::is_same<T, double>::value || inv_bytes <= kInvSmemMax);
+            if (inv_bytes <= kInvSmemMax && !blocked) {
                 k_trinv<T><<<dim3(nbc, nb), kTrinvThreads, inv_bytes, s>>>(
                     q0 + qb, P->d_S, P->d_foff, P->d_f, P->d_toff, F, (T *)M->tmp);
-            } else if (std::is_same<T, double>::value) {
-                // wide separators in FP64: blocked inversion on the tensor cores
+            } else if (blocked) {
+                // wide separators: blocked inversion on the tile engine (the
+                // FP64 tensor cores; CUDA cores in FP32)
                 const int nbk = (P->lvl_maxS[L] + kInvBlk - 1) / kInvBlk;
                 k_trinv_diag<T><<<dim3(nbk, nb), kTrinvDiagThreads, trinv_diag_smem<T>(), s>>>(
                     q0 + qb, P->d_S, P->d_f, P->d_foff, P->d_toff, F, (T *)M->tmp);
