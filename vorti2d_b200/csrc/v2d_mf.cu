@@ -1124,7 +1124,22 @@ __device__ __forceinline__ void panel_factor(T *A, int f, int S, int k, int vo, 
             if (lane > c && lane < w) {
                 const T l = U[lane][c] * inv;
                 U[lane][c] = l;
-                for (int j = c + 1; j < w; ++j) U[lane][j] -= l * U[c][j];
+                // eight entries per batch: their loads issue together (a store
+                // to this lane's row may not be reordered with the next
+                // entry's loads, so one entry at a time is a chain of
+                // shared-memory round trips)
+                int j = c + 1;
+                for (; j + 7 < w; j += 8) {
+                    T a[8], bv[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        a[u] = U[lane][j + u];
+                        bv[u] = U[c][j + u];
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) U[lane][j + u] = a[u] - l * bv[u];
+                }
+                for (; j < w; ++j) U[lane][j] -= l * U[c][j];
             }
             __syncwarp();
         }
@@ -1243,11 +1258,15 @@ __device__ __forceinline__ void swap_trsm_cols(T *A, int f, int S, int k, int vo
         const int r = e / NB, c = e - r * NB;
         Ld[r][c] = (r < w && c < w) ? A[(long long)(k + r) * f + k + c] : T(0);
     }
+    // the panel's pivot rows, loaded by the first NB threads at once (thread 0
+    // loading them one after another would wait out NB dependent load
+    // latencies), then new row t of the block = old row src[t]
+    if (threadIdx.x < NB) src[NB + threadIdx.x] = threadIdx.x < w ? ipiv[vo + k + threadIdx.x] - k : 0;
+    __syncthreads();
     if (threadIdx.x == 0) {
-        // new row t of the block = old row src[t]
         for (int t = 0; t < NB; ++t) src[t] = t;
         for (int t = 0; t < w; ++t) {
-            const int p = ipiv[vo + k + t] - k;
+            const int p = src[NB + t];
             const int u = src[t];
             src[t] = src[p];
             src[p] = u;
@@ -1274,7 +1293,7 @@ __global__ void __launch_bounds__(kL21Rows) k_l21_trsm(int q0, int k, int nl,
 {
     constexpr int NB = PanelWidth<T>::v;
     __shared__ T D[NB][NB + 1];
-    __shared__ int src[NB];
+    __shared__ int src[2 * NB];
     const int q = q0 + blockIdx.y;
     const int S = S_[q], f = f_[q];
     if (S <= k) return;
