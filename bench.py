@@ -714,11 +714,13 @@ def profile_lu_launches(args):
     n = ctypes.c_int()
     _lib.check(_lib.lib().v2d_solver_time_lu_factor(s.dev.h, 5 if grid <= 513 else 2, ms, codes,
                                                     cap, ctypes.byref(n)))
-    by_kind, by_level = {}, {}
+    by_kind, by_level, by_level_kind = {}, {}, {}
     for k in range(n.value):
         kind, lvl = fkinds[codes[k] // 1000], codes[k] % 1000
         by_kind[kind] = by_kind.get(kind, 0.0) + ms[k]
         by_level[lvl] = by_level.get(lvl, 0.0) + ms[k]
+        row = by_level_kind.setdefault(lvl, {})
+        row[kind] = round(row.get(kind, 0.0) + 1e3 * ms[k], 1)
     st = (ctypes.c_double * 6)()
     _lib.check(_lib.lib().v2d_solver_lu_stats(s.dev.h, st))
     total = sum(ms[k] for k in range(n.value))
@@ -726,6 +728,7 @@ def profile_lu_launches(args):
     out["factor"] = {"total_ms": total, "launches": n.value, "flops": st[3],
                      "tflops": st[3] / (total * 1e-3) / 1e12,
                      "by_kind_ms": by_kind, "by_level_ms": by_level,
+                     "by_level_kind_us": by_level_kind,
                      "top_levels_us": [[fkinds[codes[k] // 1000], codes[k] % 1000,
                                         round(1e3 * ms[k], 1)]
                                        for k in range(n.value) if codes[k] % 1000 >= top]}

@@ -1602,6 +1602,12 @@ __global__ void __launch_bounds__(256) k_gemm(int q0, int k, int W, const int *_
 // product (all threads).  With the inverses the solve applies each front by
 // row-parallel products instead of a chain of dependent triangular blocks.
 constexpr int kTrinvThreads = 512;
+// levels with more column blocks than SMs launch k_trinv with this many
+// threads: at 95 (FP32) / 126 (FP64) registers a 512-thread CTA fills an SM's
+// register file alone, 128-thread CTAs fit four or five per SM, and on those
+// levels resident CTAs matter more than the row updates' thread count
+constexpr int kTrinvThreadsMany = 128;
+constexpr int kTrinvManyCtas = 148;
 template <class T> struct InvWidth;
 template <> struct InvWidth<float> { static constexpr int v = 32; };
 template <> struct InvWidth<double> { static constexpr int v = 16; };
@@ -3014,7 +3020,8 @@ static int factor_launches(const MfPlan *P, MfFactor *M, const int *rowptr, cons
             const bool blocked = P->lvl_maxS[L] >= kBlockedInvMinS &&
                                  (std::is_same<T, double>::value || inv_bytes <= kInvSmemMax);
             if (inv_bytes <= kInvSmemMax && !blocked) {
-                k_trinv<T><<<dim3(nbc, nb), kTrinvThreads, inv_bytes, s>>>(
+                const int nth = nbc * nb > kTrinvManyCtas ? kTrinvThreadsMany : kTrinvThreads;
+                k_trinv<T><<<dim3(nbc, nb), nth, inv_bytes, s>>>(
                     q0 + qb, P->d_S, P->d_foff, P->d_f, P->d_toff, F, (T *)M->tmp);
             } else if (blocked) {
                 // wide separators: blocked inversion on the tile engine (the
