@@ -1187,13 +1187,15 @@ __device__ __forceinline__ void l21_row(T *A, int f, int k, int w, int r,
     T *row = A + (long long)r * f + k;
 #pragma unroll
     for (int c = 0; c < NB; ++c) x[c] = c < w ? row[c] : T(0);
+    // by rows of U: each finished entry updates the entries after it, so the
+    // dependent chain is NB steps long, not NB^2 / 2 products
 #pragma unroll
     for (int c = 0; c < NB; ++c) {
-        T sacc = x[c];
-#pragma unroll
-        for (int t = 0; t < c; ++t) sacc -= x[t] * U[t][c];
         const T d = U[c][c];
-        x[c] = (c < w && d != T(0)) ? sacc / d : T(0);
+        const T xc = (c < w && d != T(0)) ? x[c] / d : T(0);
+        x[c] = xc;
+#pragma unroll
+        for (int j = c + 1; j < NB; ++j) x[j] -= xc * U[c][j];
     }
 #pragma unroll
     for (int c = 0; c < NB; ++c)
@@ -1235,11 +1237,10 @@ __device__ __forceinline__ void swap_trsm_col(T *A, int f, int k, int w, int col
     for (int t = 0; t < NB; ++t) x[t] = t < w ? A[(long long)(k + src[t]) * f + col] : T(0);
     if (col >= k + w) {
 #pragma unroll
-        for (int t = 1; t < NB; ++t) {
-            T s = x[t];
+        for (int u = 0; u < NB - 1; ++u) {   // by columns of L: an NB-step chain
+            const T xu = x[u];
 #pragma unroll
-            for (int u = 0; u < t; ++u) s -= Ld[t][u] * x[u];
-            x[t] = s;
+            for (int t = u + 1; t < NB; ++t) x[t] -= Ld[t][u] * xu;
         }
     }
 #pragma unroll
@@ -1647,11 +1648,10 @@ __device__ __forceinline__ void trinv_colblock(const T *A, int S, int f, T *X, i
 #pragma unroll
             for (int r = 0; r < 32; ++r) xr[r] = r < bh ? Xs[(r0 + r) * CW + tid] : T(0);
 #pragma unroll
-            for (int r = 1; r < 32; ++r) {
-                T v = xr[r];
+            for (int t = 0; t < 31; ++t) {   // by columns: a 31-step chain
+                const T xt = xr[t];
 #pragma unroll
-                for (int t = 0; t < r; ++t) v -= Dg[r][t] * xr[t];
-                xr[r] = v;
+                for (int r = t + 1; r < 32; ++r) xr[r] -= Dg[r][t] * xt;
             }
 #pragma unroll
             for (int r = 1; r < 32; ++r)
@@ -1701,14 +1701,13 @@ __device__ __forceinline__ void trinv_colblock(const T *A, int S, int f, T *X, i
 #pragma unroll
             for (int r = 0; r < 32; ++r) xr[r] = r < bh ? Xs[(r0 + r) * CW + tid] : T(0);
 #pragma unroll
-            for (int r = 31; r >= 0; --r) {
-                if (r < bh) {
-                    T v = xr[r];
+            for (int t = 31; t >= 0; --t) {   // by columns, from the bottom row up
+                if (t < bh) {
+                    const T d = Dg[t][t];
+                    const T xt = d != T(0) ? xr[t] / d : T(0);
+                    xr[t] = xt;
 #pragma unroll
-                    for (int t = r + 1; t < 32; ++t)
-                        if (t < bh) v -= Dg[r][t] * xr[t];
-                    const T d = Dg[r][r];
-                    xr[r] = d != T(0) ? v / d : T(0);
+                    for (int r = 0; r < t; ++r) xr[r] -= Dg[r][t] * xt;
                 }
             }
 #pragma unroll
@@ -1825,24 +1824,36 @@ __global__ void __launch_bounds__(kTrinvDiagThreads) k_trinv_diag(int q0, const 
         Ab[r][c] = (r < bs && c < bs) ? A[(long long)r * f + c] : T(0);
     }
     __syncthreads();
+    // One column of an inverse per thread, held in registers and solved by
+    // columns of the block (each finished entry updates all rows after it):
+    // the dependent chain is B steps long instead of B^2 / 2 dependent
+    // products through shared memory.  The padding beyond bs is zero and
+    // leaves the solution's zeros in place.
     const int c = tid & (B - 1);
     if (c < bs) {
-        if (tid < B) {   // column c of L^-1 (unit lower): forward substitution
-            Xs[c][c] = T(1);
-            for (int r = c + 1; r < bs; ++r) {
-                T v = T(0);
-                for (int t = c; t < r; ++t) v -= Ab[r][t] * Xs[t][c];
-                Xs[r][c] = v;
+        T x[B];
+#pragma unroll
+        for (int r = 0; r < B; ++r) x[r] = r == c ? T(1) : T(0);
+        if (tid < B) {   // column c of L^-1 (unit lower): L x = e_c
+#pragma unroll
+            for (int t = 0; t < B - 1; ++t) {
+                const T xt = x[t];
+#pragma unroll
+                for (int r = t + 1; r < B; ++r) x[r] -= Ab[r][t] * xt;
             }
-        } else {         // column c of U^-1: back substitution
-            const T dc = Ab[c][c];
-            Ys[c][c] = dc != T(0) ? T(1) / dc : T(0);
-            for (int r = c - 1; r >= 0; --r) {
-                T v = T(0);
-                for (int t = r + 1; t <= c; ++t) v -= Ab[r][t] * Ys[t][c];
-                const T d = Ab[r][r];
-                Ys[r][c] = d != T(0) ? v / d : T(0);
+#pragma unroll
+            for (int r = 0; r < B; ++r) Xs[r][c] = x[r];
+        } else {         // column c of U^-1: U x = e_c from the bottom row up
+#pragma unroll
+            for (int t = B - 1; t >= 0; --t) {
+                const T d = Ab[t][t];
+                const T xt = d != T(0) ? x[t] / d : T(0);
+                x[t] = xt;
+#pragma unroll
+                for (int r = 0; r < t; ++r) x[r] -= Ab[r][t] * xt;
             }
+#pragma unroll
+            for (int r = 0; r < B; ++r) Ys[r][c] = x[r];
         }
     }
     __syncthreads();
