@@ -175,10 +175,10 @@ def steady_solve_ser(solver, dtau0=1.0, tol=None, max_iter=300, dtau_max=1e12, g
             if not (ok and math.isfinite(rk)) or rk > reject * r_prev:
                 dev.set_state(*saved)       # undo the step
                 solver._host_state = None
+                res = math.inf              # the undone step's update norm is no result
                 if dtau <= dmin:
                     break
                 dtau = max(dmin, 0.25 * dtau)
-                res = math.inf
                 continue
             if rk < r_prev:
                 dtau = min(dtau_max, max(dtau * growth, dtau0 * r0 / max(rk, 1e-300)))
