@@ -1604,9 +1604,10 @@ __global__ void __launch_bounds__(256) k_gemm(int q0, int k, int W, const int *_
 // row-parallel products instead of a chain of dependent triangular blocks.
 constexpr int kTrinvThreads = 512;
 // levels with more column blocks than SMs launch k_trinv with this many
-// threads: at 95 (FP32) / 126 (FP64) registers a 512-thread CTA fills an SM's
-// register file alone, 128-thread CTAs fit four or five per SM, and on those
-// levels resident CTAs matter more than the row updates' thread count
+// threads: at about 100 (FP32) / 128 (FP64) registers a 512-thread CTA fills
+// an SM's register file alone, 128-thread CTAs fit four or five per SM, and
+// on those levels resident CTAs matter more than the row updates' thread
+// count
 constexpr int kTrinvThreadsMany = 128;
 constexpr int kTrinvManyCtas = 148;
 template <class T> struct InvWidth;
