@@ -315,13 +315,13 @@ class Solver:
         cfg = self.cfg
         if cfg.write_xdmf and cfg.verbose:
             self._log("  note: write_xdmf ignored (XDMF/HDF5 output is not part of vorti2d_b200)")
-        needs_dir = cfg.write_csv or cfg.compute_forces or True
-        if needs_dir:
-            fields_io.ensure_dirs(cfg.out_dir)
-            fields_io.write_grid(cfg.out_dir, self.xg, self.yg)
-            forces_path = os.path.join(cfg.out_dir, "forces.csv")
-            if cfg.compute_forces and (not self.restarted or not os.path.exists(forces_path)):
-                fields_io.init_force_history(cfg.out_dir, forcesmod.FORCE_COLUMNS)
+        # the output folder and the grid are written on every run, as the
+        # reference does (vorti2d/solver.py:150-160)
+        fields_io.ensure_dirs(cfg.out_dir)
+        fields_io.write_grid(cfg.out_dir, self.xg, self.yg)
+        forces_path = os.path.join(cfg.out_dir, "forces.csv")
+        if cfg.compute_forces and (not self.restarted or not os.path.exists(forces_path)):
+            fields_io.init_force_history(cfg.out_dir, forcesmod.FORCE_COLUMNS)
         t_wall0 = time.time()
         local_step = 0
         for t in self.times():
