@@ -104,6 +104,51 @@ def test_argument_errors_before_any_device_work(v2d):
     assert "null" in _lib.last_error()
 
 
+def handle_entry_points():
+    """(name, argument count) of every declared function whose first
+    parameter is a solver, linear-system or batch handle."""
+    out = []
+    for fn in os.listdir(HEADER_DIR):
+        if not fn.endswith(".h"):
+            continue
+        text = re.sub(r"/\*.*?\*/", "", open(os.path.join(HEADER_DIR, fn)).read(), flags=re.S)
+        for m in re.finditer(r"^int (v2d_\w+)\(([^;]*?)\);", text, re.M | re.S):
+            params = " ".join(m.group(2).split())
+            if re.match(r"(const )?v2d_(solver|linsys|batch) \*", params):
+                out.append((m.group(1), params.count(",") + 1))
+    return sorted(out)
+
+
+@pytest.mark.parametrize("name,nargs", handle_entry_points())
+def test_null_handle_is_an_argument_error(v2d, name, nargs):
+    """Every entry point taking a handle rejects a null one with V2D_EARG
+    before touching the device (the destroy calls accept null, as free
+    does)."""
+    from vorti2d_b200 import _lib
+    f = getattr(_lib.lib(), name)
+    types = f.argtypes or []
+    args = []
+    for k in range(nargs):
+        t = types[k] if k < len(types) else ctypes.c_void_p
+        if t in (ctypes.c_int, ctypes.c_uint, ctypes.c_long, ctypes.c_longlong, ctypes.c_size_t):
+            args.append(0)
+        elif t in (ctypes.c_double, ctypes.c_float):
+            args.append(0.0)
+        else:
+            args.append(None)
+    code = f(*args)
+    if name.endswith("_destroy"):
+        assert code == _lib.V2D_OK
+    else:
+        assert code == _lib.V2D_EARG, (name, code, _lib.last_error())
+
+
+def test_handle_entry_points_are_found():
+    names = [n for n, _ in handle_entry_points()]
+    assert len(names) >= 40
+    assert {"v2d_solver_newton", "v2d_linsys_solve", "v2d_batch_newton"} <= set(names)
+
+
 def test_no_cpu_fallback(v2d, monkeypatch, tmp_path):
     """A missing library raises instead of falling back to another path."""
     from vorti2d_b200 import _lib
