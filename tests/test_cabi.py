@@ -143,6 +143,43 @@ def test_null_handle_is_an_argument_error(v2d, name, nargs):
         assert code == _lib.V2D_EARG, (name, code, _lib.last_error())
 
 
+def value_entry_points():
+    """(name, argument count) of every declared function that takes no
+    handle and has arguments."""
+    out = []
+    for fn in os.listdir(HEADER_DIR):
+        if not fn.endswith(".h"):
+            continue
+        text = re.sub(r"/\*.*?\*/", "", open(os.path.join(HEADER_DIR, fn)).read(), flags=re.S)
+        for m in re.finditer(r"^int (v2d_\w+)\(([^;]*?)\);", text, re.M | re.S):
+            params = " ".join(m.group(2).split())
+            if params in ("", "void") or re.match(r"(const )?v2d_(solver|linsys|batch) \*", params):
+                continue
+            out.append((m.group(1), params.count(",") + 1))
+    return sorted(out)
+
+
+@pytest.mark.parametrize("sizes", [(0, 0), (9, 7)])
+@pytest.mark.parametrize("name,nargs", value_entry_points())
+def test_null_arrays_are_an_argument_error(v2d, name, nargs, sizes):
+    """Entry points without a handle reject zero sizes, and null arrays at
+    valid sizes, with V2D_EARG and a message, before any device work."""
+    from vorti2d_b200 import _lib
+    f = getattr(_lib.lib(), name)
+    types = f.argtypes or []
+    args = []
+    for k in range(nargs):
+        t = types[k] if k < len(types) else ctypes.c_void_p
+        if t in (ctypes.c_int, ctypes.c_uint, ctypes.c_long, ctypes.c_longlong, ctypes.c_size_t):
+            args.append(sizes[k] if k < 2 else 0)
+        elif t in (ctypes.c_double, ctypes.c_float):
+            args.append(0.0)
+        else:
+            args.append(None)
+    assert f(*args) == _lib.V2D_EARG, name
+    assert _lib.last_error()
+
+
 def test_handle_entry_points_are_found():
     names = [n for n, _ in handle_entry_points()]
     assert len(names) >= 40
