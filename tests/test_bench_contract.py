@@ -41,3 +41,21 @@ def test_reference_arm_prints_one_contract_line():
     assert e["value"] == d["value"] and e["unit"] == d["unit"]
     assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
     assert d["vs_baseline"] is None
+
+
+def test_reference_arm_under_torchrun_prints_once():
+    """Launched like the multi-GPU arm (torchrun, two ranks here on the CPU),
+    the reference arm runs on rank 0 alone: one JSON line, every rank exits
+    0."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    p = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+                        "--nproc-per-node", "2", "--master-addr", "127.0.0.1",
+                        "--master-port", str(port), "bench.py", "--impl", "reference",
+                        "--gpus", "2", "--steps", "1", "--warmup", "1", "--cpu-procs", "1"],
+                       cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    d = _last_json(p.stdout)
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
