@@ -125,13 +125,20 @@ class ClockSampler:
             except ValueError:
                 return float("nan")
         sm = np.array([num(r[1]) for r in self.rows])
-        smax = np.nanmax([num(r[2]) for r in self.rows])
+        mx = np.array([num(r[2]) for r in self.rows])
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in self.rows for k in range(4)
                           if r[5 + k].lower().startswith("active")})
-        load = sm[sm > 0.5 * smax] if np.isfinite(smax) else sm
-        med = float(np.median(load if load.size else sm))
-        return {"sm_mhz": med, "sm_max_mhz": float(smax), "reasons": reasons,
+        sm = sm[np.isfinite(sm)]
+        mx = mx[np.isfinite(mx)]
+        # fields the driver reports as not available give None, not NaN
+        # (NaN is not JSON)
+        smax = float(mx.max()) if mx.size else None
+        load = sm[sm > 0.5 * smax] if smax is not None else sm
+        if not load.size:
+            load = sm
+        med = float(np.median(load)) if load.size else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": reasons,
                 "samples": len(self.rows)}
 
 

@@ -59,3 +59,32 @@ def test_reference_arm_under_torchrun_prints_once():
     assert p.returncode == 0, p.stderr[-2000:]
     d = _last_json(p.stdout)
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+
+
+def _sampler(rows):
+    sys.path.insert(0, ROOT)
+    import bench
+    c = bench.ClockSampler()
+    c.rows = [[p.strip() for p in r.split(",")] for r in rows]
+    return c.summary()
+
+
+def test_clock_summary_median_under_load_and_reasons():
+    rows = ["0, 345, 1965, 150.0, 0x0, Not Active, Not Active, Not Active, Not Active",
+            "0, 1965, 1965, 700.1, 0x0, Not Active, Not Active, Not Active, Not Active",
+            "0, 1950, 1965, 990.3, 0x4, Not Active, Not Active, Not Active, Active",
+            "0, 1965, 1965, 800.0, 0x0, Not Active, Not Active, Not Active, Not Active"]
+    s = _sampler(rows)
+    # the idle sample (below half the maximum) is left out of the median
+    assert s["sm_mhz"] == 1965.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["sw_power_cap"] and s["samples"] == 4
+    json.dumps(s, allow_nan=False)
+
+
+def test_clock_summary_without_values_is_valid_json():
+    rows = ["0, [N/A], [N/A], [N/A], [N/A], Active, Not Active, Not Active, Not Active"]
+    s = _sampler(rows)
+    assert s["sm_mhz"] is None and s["sm_max_mhz"] is None
+    assert s["reasons"] == ["hw_slowdown"]
+    json.dumps(s, allow_nan=False)
+    assert _sampler([])["reasons"] == ["unsampled"]
