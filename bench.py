@@ -75,6 +75,22 @@ def max_over_ranks(x: float, world: int, device=None) -> float:
 
 
 # ----------------------------------------------------------------- clocks
+def _finite_or_none(o):
+    if isinstance(o, float):
+        return o if math.isfinite(o) else None
+    if isinstance(o, dict):
+        return {k: _finite_or_none(v) for k, v in o.items()}
+    if isinstance(o, (list, tuple)):
+        return [_finite_or_none(v) for v in o]
+    return o
+
+
+def jline(obj) -> str:
+    """One JSON line; a number that is not finite is written as null (NaN
+    and Infinity are not JSON)."""
+    return json.dumps(_finite_or_none(obj), allow_nan=False)
+
+
 class ClockSampler:
     """nvidia-smi samples of SM clock and throttle reasons during the timed
     region."""
@@ -293,7 +309,7 @@ def run_sweep_workload(args):
             "errors": sorted({r.error for r in res.results if r.error})[:4],
             "converged": res.converged, "instances": len(cases), "solve_s": res.solve_s,
             "setup_s": res.setup_s, "by_kind": kinds, "cpu_baseline": cpu}
-    print(json.dumps(line), flush=True)
+    print(jline(line), flush=True)
 
 
 def run_adjoint_workload(args):
@@ -372,7 +388,7 @@ def run_adjoint_workload(args):
     if not converged:
         line.update(value=None, note="the primal did not converge from the free stream at "
                                      "this Re; no gradient at an unconverged state")
-        print(json.dumps(line), flush=True)
+        print(jline(line), flush=True)
         s.close()
         return
     reps = max(1, args.steps // 5)
@@ -395,7 +411,7 @@ def run_adjoint_workload(args):
     line.update(value=1.0 / dt, ms_per_gradient_set=1e3 * dt, reps=reps,
                 dCl_dalpha=d_alpha, dCd_dRe=d_re, dCd_dd_norm=float(np.linalg.norm(gshape)),
                 adjoint_refinements=sinfo["refinements"], adjoint_rel_res=sinfo["rel_res"])
-    print(json.dumps(line), flush=True)
+    print(jline(line), flush=True)
     s.close()
 
 
@@ -522,7 +538,7 @@ def run_large_workload(args):
                          "bytes_per_launch": fb.value, "ms_per_launch": lu_ms.value},
             "factorization": factor, "lu_tuning": tuning,
             "cd": s.force_coeffs().cd}
-    print(json.dumps(line), flush=True)
+    print(jline(line), flush=True)
     s.close()
 
 
@@ -581,7 +597,7 @@ def run_unsteady_adjoint_workload(args):
                        "lu_reuse_its": args.ua_reuse},
             "seconds": dt, "mean_cd": J, "dJ_dalpha": d_alpha, "dJ_dRe": d_re,
             "device_memory_peak_gb": peak[0] / 1e9, **info}
-    print(json.dumps(line), flush=True)
+    print(jline(line), flush=True)
 
 
 def phase_times(_lib, s, reset=False):
@@ -610,7 +626,7 @@ def profile_newton(args):
     code, res, lin = s.dev.newton(s.cfg.u_rot(times[1]))
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
-    print(json.dumps({"profile": "one Newton iteration", "precision": prec, "code": code,
+    print(jline({"profile": "one Newton iteration", "precision": prec, "code": code,
                       "res": res, "krylov_its": lin.iterations}), flush=True)
     s.close()
 
@@ -639,7 +655,7 @@ def profile_lu_apply(args):
                                                    ctypes.byref(fb)))
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
-    print(json.dumps({"profile": "LU apply", "precision": prec, "ms": ms.value,
+    print(jline({"profile": "LU apply", "precision": prec, "ms": ms.value,
                       "factor_bytes": fb.value, "tuning": rec}), flush=True)
     s.close()
 
@@ -669,7 +685,7 @@ def profile_lu_factor(args):
     _lib.check(_lib.lib().v2d_solver_time_lu_factor(s.dev.h, 1, ms, codes, cap, ctypes.byref(n)))
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
-    print(json.dumps({"profile": "LU factorization", "grid": f"{grid}x{grid}", "precision": prec,
+    print(jline({"profile": "LU factorization", "grid": f"{grid}x{grid}", "precision": prec,
                       "ms": sum(ms[k] for k in range(n.value)), "launches": n.value}), flush=True)
     s.close()
 
@@ -739,7 +755,7 @@ def profile_lu_launches(args):
                      "top_levels_us": [[fkinds[codes[k] // 1000], codes[k] % 1000,
                                         round(1e3 * ms[k], 1)]
                                        for k in range(n.value) if codes[k] % 1000 >= top]}
-    print(json.dumps(out), flush=True)
+    print(jline(out), flush=True)
     s.close()
 
 
@@ -1086,7 +1102,7 @@ def main():
                 hbm = json.load(fh)["hbm_gbs"]
         except (OSError, ValueError, KeyError):
             pass
-        print(json.dumps(kernel_rooflines(args.kernels_grid, hbm, reps=3)), flush=True)
+        print(jline(kernel_rooflines(args.kernels_grid, hbm, reps=3)), flush=True)
         return
 
     if args.impl == "reference":
@@ -1120,7 +1136,7 @@ def main():
             "e2e": {"value": val, "unit": "steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
         }
-        print(json.dumps(line), flush=True)
+        print(jline(line), flush=True)
         return
 
     init_dist(world, "nccl")
@@ -1190,7 +1206,7 @@ def main():
     if "mixed" in res and "fp64" in res:
         line["mixed_vs_fp64_speedup"] = res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"]
         line["dCd_mixed_vs_fp64"] = abs(res["mixed"]["cd"] - res["fp64"]["cd"])
-    print(json.dumps(line), flush=True)
+    print(jline(line), flush=True)
 
 
 if __name__ == "__main__":

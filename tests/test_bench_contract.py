@@ -88,3 +88,12 @@ def test_clock_summary_without_values_is_valid_json():
     assert s["reasons"] == ["hw_slowdown"]
     json.dumps(s, allow_nan=False)
     assert _sampler([])["reasons"] == ["unsampled"]
+
+
+def test_json_lines_carry_no_nan():
+    sys.path.insert(0, ROOT)
+    import bench
+    import numpy as np
+    d = json.loads(bench.jline({"value": float("nan"), "e2e": {"value": float("inf")},
+                                "rows": [1.0, np.float64("nan"), 2], "name": "x"}))
+    assert d == {"value": None, "e2e": {"value": None}, "rows": [1.0, None, 2], "name": "x"}
